@@ -1,0 +1,201 @@
+/*
+ * vlsg.h -- C ABI of the B200 level-set advection library (libvlsgpu.so).
+ *
+ * This is the boundary a host front binds to in place of
+ * viennals::Advect<T,D>::apply (include/viennals/lsAdvect.hpp:1017-1043 of
+ * ViennaLS 5.8.3).  Every entry point takes plain pointers and sizes, returns
+ * an int status (VLSG_OK == 0, negative on error) and leaves a message for
+ * vlsg_last_error(), mirroring the error model of the reference (log + return,
+ * lsAdvect.hpp:1019-1027) and the handle/last-error style of the reference's
+ * own GPU interface (lsOxidationBiCGSTABInterface.hpp:27-73).
+ *
+ * Threading: one context == one CUDA stream; a context must be used by one
+ * host thread at a time (viennals::Advect is not re-entrant either).
+ *
+ * Level-set exchange format: a level set is the sequence that the reference's
+ * viennahrle::ConstSparseIterator yields -- defined points (index, value) and
+ * undefined runs (start index, sign) in HRLE lexicographic order (x fastest,
+ * highest dimension slowest).  Upload takes both lists; download returns the
+ * defined points in the same order.  Values are in grid units (signed
+ * distance / gridDelta), as lsDomain stores them.
+ */
+#ifndef VLSG_H
+#define VLSG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VLSG_OK 0
+#define VLSG_ERR_ARGUMENT -1     /* bad argument / unsupported option        */
+#define VLSG_ERR_CUDA -2         /* CUDA runtime error                       */
+#define VLSG_ERR_CAPACITY -3     /* pool / brick map capacity exceeded        */
+#define VLSG_ERR_STATE -4        /* call out of order (no grid, no level set) */
+#define VLSG_ERR_NUMERIC -5      /* time step <= 0, step limit reached        */
+#define VLSG_ERR_DEVICE_CHECK -6 /* a kernel's own bounds check fired         */
+#define VLSG_ERR_CALLBACK -7     /* the host velocity callback failed         */
+
+#define VLSG_MAX_LEVEL_SETS 8
+#define VLSG_MAX_MATERIALS 16
+
+/* SpatialSchemeEnum, lsAdvectIntegrationSchemes.hpp:10-23 (same values). */
+enum vlsg_spatial_scheme {
+  VLSG_ENGQUIST_OSHER_1ST_ORDER = 0,
+  VLSG_ENGQUIST_OSHER_2ND_ORDER = 1,
+  VLSG_LAX_FRIEDRICHS_1ST_ORDER = 2,
+  VLSG_LAX_FRIEDRICHS_2ND_ORDER = 3,
+  VLSG_LOCAL_LAX_FRIEDRICHS_ANALYTICAL_1ST_ORDER = 4,
+  VLSG_LOCAL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER = 5,
+  VLSG_LOCAL_LOCAL_LAX_FRIEDRICHS_2ND_ORDER = 6,
+  VLSG_LOCAL_LAX_FRIEDRICHS_1ST_ORDER = 7,
+  VLSG_LOCAL_LAX_FRIEDRICHS_2ND_ORDER = 8,
+  VLSG_STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER = 9,
+  VLSG_WENO_3RD_ORDER = 10,
+  VLSG_WENO_5TH_ORDER = 11
+};
+
+/* TemporalSchemeEnum, lsAdvectIntegrationSchemes.hpp:31-35. */
+enum vlsg_temporal_scheme {
+  VLSG_FORWARD_EULER = 0,
+  VLSG_RUNGE_KUTTA_2ND_ORDER = 1,
+  VLSG_RUNGE_KUTTA_3RD_ORDER = 2
+};
+
+/* viennahrle::BoundaryType (python/viennals/_core.pyi:25-30). */
+enum vlsg_boundary {
+  VLSG_REFLECTIVE_BOUNDARY = 0,
+  VLSG_INFINITE_BOUNDARY = 1,
+  VLSG_PERIODIC_BOUNDARY = 2,
+  VLSG_POS_INFINITE_BOUNDARY = 3,
+  VLSG_NEG_INFINITE_BOUNDARY = 4
+};
+
+/* Storage / stencil precision of a context.  FP64 reproduces the reference's
+ * Advect<double,3> rule for rule; FP32 stores phi and evaluates the stencils
+ * in float, keeping the CFL reduction, the advected time and the RK stage
+ * combination in double. */
+enum vlsg_precision { VLSG_FP64 = 0, VLSG_FP32 = 1 };
+
+/* All setters of viennals::Advect (lsAdvect.hpp:856-969) in one struct.
+ * vlsg_default_params() fills the reference defaults (lsAdvect.hpp:64-79). */
+typedef struct vlsg_advect_params {
+  int32_t spatial_scheme;          /* setSpatialScheme            :936 */
+  int32_t temporal_scheme;         /* setTemporalScheme           :949 */
+  double time_step_ratio;          /* setTimeStepRatio (0.4999)   :885 */
+  double dissipation_alpha;        /* setDissipationAlpha (1.0)   :955 */
+  double advection_time;           /* setAdvectionTime (0)        :873 */
+  int32_t single_step;             /* setSingleStep               :879 */
+  int32_t calculate_normal_vectors;/* setCalculateNormalVectors   :891 */
+  int32_t ignore_voids;            /* setIgnoreVoids (must be 0)  :899 */
+  int32_t adaptive_time_stepping;  /* setAdaptiveTimeStepping     :904 */
+  uint32_t adaptive_subdivisions;  /*   (20)                      :904 */
+  int32_t check_dissipation;       /* setCheckDissipation (1)     :958 */
+  int32_t save_advection_velocities; /* setSaveAdvectionVelocities :916 */
+  int32_t update_point_data;       /* setUpdatePointData (1)      :962 */
+  uint32_t max_steps;              /* guard against dt == 0 loops (0 = 1e7) */
+} vlsg_advect_params;
+
+/* Getters of viennals::Advect (lsAdvect.hpp:920-932) plus work counters. */
+typedef struct vlsg_advect_result {
+  double advected_time;        /* getAdvectedTime     */
+  double current_time_step;    /* getCurrentTimeStep  */
+  uint32_t number_of_time_steps; /* getNumberOfTimeSteps */
+  uint32_t number_of_stages;   /* forward-Euler stages executed */
+  uint64_t point_updates;      /* sum over stages of active points */
+  uint64_t kernel_launches;    /* kernels this library launched */
+} vlsg_advect_result;
+
+/* Device velocity functor: evaluates, for material m (clamped to
+ * n_materials-1) and unit normal n,
+ *   scalar = rate[m]
+ *          + sum_k (n_k > 0 ? lin_pos : lin_neg)[m][k] * n_k
+ *          + sum_k (n_k > 0 ? abs_pos : abs_neg)[m][k] * |n_k|
+ *          + sum_k (n_k > 0 ? sq_pos  : sq_neg )[m][k] * (n_k * n_k)
+ * in exactly that order, skipping terms whose coefficient is 0 (so a
+ * constant field never reads a normal), and vector = vec[m].
+ * This covers the fields of the reference's tests and examples
+ * (TimeIntegration.cpp:17-35, Advection.cpp:25-44,
+ * MultiMaterialEtch.cpp:30-49, SquareEtch.cpp:26-41).  Any other
+ * VelocityField goes through vlsg_set_velocity_callback. */
+typedef struct vlsg_velocity_desc {
+  int32_t n_materials;
+  double rate[VLSG_MAX_MATERIALS];
+  double lin_pos[VLSG_MAX_MATERIALS][3];
+  double lin_neg[VLSG_MAX_MATERIALS][3];
+  double abs_pos[VLSG_MAX_MATERIALS][3];
+  double abs_neg[VLSG_MAX_MATERIALS][3];
+  double sq_pos[VLSG_MAX_MATERIALS][3];
+  double sq_neg[VLSG_MAX_MATERIALS][3];
+  double vec[VLSG_MAX_MATERIALS][3];
+} vlsg_velocity_desc;
+
+/* Host velocity callback (viennals::VelocityField<T>::getScalarVelocity and
+ * getVectorVelocity, lsVelocityField.hpp:17-30, batched).  Called with n
+ * queries; coords = index * gridDelta, normals as the scheme computes them,
+ * point_ids = HRLE linear id of the centre point.  Must fill scalar_out[n]
+ * and vector_out[3n]; return 0 on success.  It may be called from several
+ * host threads at once for disjoint batches (as the reference calls the
+ * virtuals from OpenMP threads, lsAdvect.hpp:464). */
+typedef int (*vlsg_velocity_cb)(void *user, int64_t n, const double *coords,
+                                const int32_t *materials,
+                                const double *normals,
+                                const uint64_t *point_ids, double *scalar_out,
+                                double *vector_out);
+
+typedef struct vlsg_context vlsg_context;
+
+/* Library / context lifetime ---------------------------------------------- */
+int vlsg_version(void);
+const char *vlsg_last_error(const vlsg_context *ctx); /* ctx may be NULL */
+int vlsg_create(vlsg_context **out, int32_t device, int32_t precision);
+int vlsg_destroy(vlsg_context *ctx);
+void vlsg_default_params(vlsg_advect_params *p);
+
+/* Grid: Domain(bounds, boundaryConditions, gridDelta), lsDomain.hpp:68-78.
+ * grid_min/grid_max are INDEX bounds (floor(min/dx), ceil(max/dx)); for a
+ * periodic direction the points are grid_min..grid_max-1, for a reflective
+ * one grid_min..grid_max, an infinite direction is unbounded. */
+int vlsg_set_grid(vlsg_context *ctx, int32_t dim, const int64_t *grid_min,
+                  const int64_t *grid_max, const int32_t *boundary,
+                  double grid_delta);
+
+/* Level sets are numbered bottom (0) to top (n-1) like the vector passed to
+ * Advect (lsAdvect.hpp:46-53); the top one is advected and must wrap the
+ * others.  vlsg_set_level_set_count drops slots >= n. */
+int vlsg_set_level_set_count(vlsg_context *ctx, int32_t n);
+int vlsg_upload_levelset(vlsg_context *ctx, int32_t slot, int64_t n_points,
+                         const int32_t *indices, const double *values,
+                         int64_t n_runs, const int32_t *run_start,
+                         const int8_t *run_sign, int32_t width);
+int vlsg_count_points(vlsg_context *ctx, int32_t slot, int64_t *n_points);
+int vlsg_download_levelset(vlsg_context *ctx, int32_t slot, int64_t capacity,
+                           int32_t *indices, double *values, int32_t *width);
+
+/* Velocity plugin: either a device functor or a host callback. */
+int vlsg_set_velocity_functor(vlsg_context *ctx, const vlsg_velocity_desc *v);
+int vlsg_set_velocity_callback(vlsg_context *ctx, vlsg_velocity_cb cb,
+                               void *user);
+
+/* Advect::apply(), lsAdvect.hpp:1017-1043. */
+int vlsg_advect(vlsg_context *ctx, const vlsg_advect_params *params,
+                vlsg_advect_result *result);
+
+/* Timing of the last vlsg_advect: per kernel family, device milliseconds and
+ * algorithmic bytes, as measured with CUDA events on the context stream
+ * (filled only when profiling is switched on with vlsg_set_profiling). */
+typedef struct vlsg_kernel_stat {
+  char name[32];
+  uint64_t launches;
+  double device_ms;
+  double algorithmic_bytes;
+} vlsg_kernel_stat;
+int vlsg_set_profiling(vlsg_context *ctx, int32_t on);
+int vlsg_get_kernel_stats(vlsg_context *ctx, int32_t capacity,
+                          vlsg_kernel_stat *out, int32_t *count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VLSG_H */

@@ -1,0 +1,721 @@
+// vlso_advect.hpp -- TEST INFRASTRUCTURE ONLY (the oracle): FP64 restatement
+// of viennals::Advect<double,D> (lsAdvect.hpp), its spatial schemes
+// (lsEngquistOsher.hpp, lsLaxFriedrichs.hpp, lsLocalLaxFriedrichs.hpp,
+// lsLocalLocalLaxFriedrichs.hpp, lsWENO.hpp + lsFiniteDifferences.hpp) and
+// time integration (lsAdvectIntegrationSchemes.hpp).  Build with
+// -ffp-contract=off: every expression keeps the reference's evaluation order.
+//
+// One deliberate choice: the reference accumulates the Lax-Friedrichs
+// dissipation coefficients of LocalLaxFriedrichs / LocalLocalLaxFriedrichs per
+// OpenMP thread and bounds the time step per thread (lsAdvect.hpp:493,
+// :595-606), which makes dt depend on the thread count.  Here the maximum is
+// taken over all points, i.e. the reference run with one thread.
+#pragma once
+
+#include "vlso_core.hpp"
+
+namespace vlso {
+
+inline double pow2(double v) { return v * v; }
+inline double stdMax(double a, double b) { return (a < b) ? b : a; }
+inline double stdMin(double a, double b) { return (b < a) ? b : a; }
+
+// Velocity functor of vlsg.h (vlsg_velocity_desc), evaluated term by term.
+inline double scalarVelocity(const vlsg_velocity_desc &v, int material,
+                             const double n[3]) {
+  int m = material < v.n_materials ? material : v.n_materials - 1;
+  if (m < 0) m = 0;
+  double s = v.rate[m];
+  for (int k = 0; k < 3; ++k) {
+    const double c = n[k] > 0 ? v.lin_pos[m][k] : v.lin_neg[m][k];
+    if (c != 0) s = s + c * n[k];
+  }
+  for (int k = 0; k < 3; ++k) {
+    const double c = n[k] > 0 ? v.abs_pos[m][k] : v.abs_neg[m][k];
+    if (c != 0) s = s + c * std::fabs(n[k]);
+  }
+  for (int k = 0; k < 3; ++k) {
+    const double c = n[k] > 0 ? v.sq_pos[m][k] : v.sq_neg[m][k];
+    if (c != 0) s = s + c * (n[k] * n[k]);
+  }
+  return s;
+}
+inline void vectorVelocity(const vlsg_velocity_desc &v, int material,
+                           double out[3]) {
+  int m = material < v.n_materials ? material : v.n_materials - 1;
+  if (m < 0) m = 0;
+  for (int k = 0; k < 3; ++k) out[k] = v.vec[m][k];
+}
+
+struct Params {
+  int spatial = VLSG_ENGQUIST_OSHER_1ST_ORDER;
+  int temporal = VLSG_FORWARD_EULER;
+  double timeStepRatio = 0.4999;
+  double dissipationAlpha = 1.0;
+  double advectionTime = 0.;
+  bool singleStep = false;
+  bool calculateNormalVectors = true;
+  bool adaptiveTimeStepping = false;
+  unsigned adaptiveSubdivisions = 20;
+  bool checkDissipation = true;
+  uint32_t maxSteps = 10000000;
+  static constexpr double integrationCutoff = 0.5;    // lsAdvect.hpp:77
+  static constexpr double wrappingLayerEpsilon = 1e-4; // lsAdvect.hpp:80
+};
+
+// Expand width each scheme's prepareLS asks for.
+inline int schemeWidth(int s) {
+  switch (s) {
+  case VLSG_ENGQUIST_OSHER_1ST_ORDER: return 3;          // lsEngquistOsher.hpp:31
+  case VLSG_ENGQUIST_OSHER_2ND_ORDER: return 5;
+  case VLSG_LAX_FRIEDRICHS_1ST_ORDER: return 3;          // lsLaxFriedrichs.hpp:225
+  case VLSG_LAX_FRIEDRICHS_2ND_ORDER: return 5;
+  case VLSG_LOCAL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER: return 3; // lsLocalLocalLaxFriedrichs.hpp:288
+  case VLSG_LOCAL_LOCAL_LAX_FRIEDRICHS_2ND_ORDER: return 5;
+  case VLSG_LOCAL_LAX_FRIEDRICHS_1ST_ORDER: return 7;    // lsLocalLaxFriedrichs.hpp:55
+  case VLSG_LOCAL_LAX_FRIEDRICHS_2ND_ORDER: return 9;
+  case VLSG_WENO_3RD_ORDER: return 5;                    // lsWENO.hpp:44 (r=2)
+  case VLSG_WENO_5TH_ORDER: return 7;                    // (r=3)
+  default: return -1;
+  }
+}
+inline bool schemeSupported(int s) { return schemeWidth(s) > 0; }
+
+// Central/one-sided differences with the second-order correction of
+// lsEngquistOsher.hpp:59-111 (identical in lsLaxFriedrichs.hpp:256-309,
+// lsLocalLaxFriedrichs.hpp:85-143, lsLocalLocalLaxFriedrichs.hpp:318-371).
+template <int D, class F>
+inline void oneSided(F V, int i, double phi0, double gridDelta, int order,
+                     double &diffPos, double &diffNeg) {
+  const double deltaPos = gridDelta;
+  const double deltaNeg = -gridDelta;
+  const double phiPos = V(i, 1);
+  const double phiNeg = V(i, -1);
+  diffPos = (phiPos - phi0) / deltaPos;
+  diffNeg = (phiNeg - phi0) / deltaNeg;
+  if (order == 2) {
+    const double deltaPosPos = 2 * gridDelta;
+    const double deltaNegNeg = -2 * gridDelta;
+    const double phiPosPos = V(i, 2);
+    const double phiNegNeg = V(i, -2);
+    const double diff00 =
+        (((deltaNeg * phiPos - deltaPos * phiNeg) / (deltaPos - deltaNeg) +
+          phi0)) /
+        (deltaPos * deltaNeg);
+    const double diffNegNeg = (((deltaNeg * phiNegNeg - deltaNegNeg * phiNeg) /
+                                    (deltaNegNeg - deltaNeg) +
+                                phi0)) /
+                              (deltaNegNeg * deltaNeg);
+    const double diffPosPos = (((deltaPos * phiPosPos - deltaPosPos * phiPos) /
+                                    (deltaPosPos - deltaPos) +
+                                phi0)) /
+                              (deltaPosPos * deltaPos);
+    if (std::signbit(diff00) == std::signbit(diffPosPos)) {
+      if (std::abs(diffPosPos * deltaPos) < std::abs(diff00 * deltaNeg))
+        diffPos -= deltaPos * diffPosPos;
+      else
+        diffPos += deltaNeg * diff00;
+    }
+    if (std::signbit(diff00) == std::signbit(diffNegNeg)) {
+      if (std::abs(diffNegNeg * deltaNeg) < std::abs(diff00 * deltaPos))
+        diffNeg -= deltaNeg * diffNegNeg;
+      else
+        diffNeg += deltaPos * diff00;
+    }
+  }
+}
+
+// FiniteDifferences::weno3 / weno5, lsFiniteDifferences.hpp:58-123.
+inline double weno3(const double *x, double delta, bool plus,
+                    double eps = 1e-6) {
+  double d[3];
+  if (plus) {
+    d[0] = x[2] - x[1];
+    d[1] = x[3] - x[2];
+    d[2] = x[4] - x[3];
+    double N = eps + pow2(d[2] - d[1]);
+    double Dd = eps + pow2(d[1] - d[0]);
+    double D2 = Dd * Dd;
+    double wp = D2 / (D2 + 2 * N * N);
+    return (d[0] + d[1] - wp * (d[2] - 2 * d[1] + d[0])) / (2 * delta);
+  }
+  d[0] = x[1] - x[0];
+  d[1] = x[2] - x[1];
+  d[2] = x[3] - x[2];
+  double N = eps + pow2(d[1] - d[0]);
+  double Dd = eps + pow2(d[2] - d[1]);
+  double D2 = Dd * Dd;
+  double wp = D2 / (D2 + 2 * N * N);
+  return (d[1] + d[2] - wp * (d[0] - 2 * d[1] + d[2])) / (2 * delta);
+}
+inline double weno5(const double *x, double dx, bool plus, double eps = 1e-6) {
+  double d[5];
+  if (!plus) {
+    for (int i = 0; i < 5; ++i) d[i] = x[i + 1] - x[i];
+  } else {
+    for (int i = 0; i < 5; ++i) d[i] = x[6 - i] - x[5 - i];
+  }
+  double s1 = double(13.0 / 12.0) * pow2(d[0] - 2 * d[1] + d[2]) +
+              double(1.0 / 4.0) * pow2(d[0] - 4 * d[1] + 3 * d[2]);
+  double s2 = double(13.0 / 12.0) * pow2(d[1] - 2 * d[2] + d[3]) +
+              double(1.0 / 4.0) * pow2(d[1] - d[3]);
+  double s3 = double(13.0 / 12.0) * pow2(d[2] - 2 * d[3] + d[4]) +
+              double(1.0 / 4.0) * pow2(3 * d[2] - 4 * d[3] + d[4]);
+  double eps_scaled = eps * dx * dx;
+  double al1 = double(0.1) / (eps_scaled + s1);
+  double al2 = double(0.6) / (eps_scaled + s2);
+  double al3 = double(0.3) / (eps_scaled + s3);
+  double alsum = al1 + al2 + al3;
+  double p1 = double(1.0 / 6.0) * (2 * d[0] - 7 * d[1] + 11 * d[2]);
+  double p2 = double(1.0 / 6.0) * (-d[1] + 5 * d[2] + 2 * d[3]);
+  double p3 = double(1.0 / 6.0) * (2 * d[2] + 5 * d[3] - d[4]);
+  return (al1 * p1 + al2 * p2 + al3 * p3) / (alsum * dx);
+}
+
+template <int D> struct SchemeCtx {
+  const LS<D> &top;
+  const Params &P;
+  const vlsg_velocity_desc &vel;
+  const double *globalAlphas; // LF: findGlobalAlphas result
+};
+
+// One scheme evaluation at `key` for `material` (operator() of each scheme).
+// `alphas` accumulates finalAlphas of LLF / LLLF.
+template <int D>
+std::pair<double, double> evalScheme(const SchemeCtx<D> &S, uint64_t key,
+                                     int material, double *alphas) {
+  const LS<D> &ls = S.top;
+  const Grid<D> &g = ls.grid;
+  const double gridDelta = g.delta;
+  const int sch = S.P.spatial;
+  auto V = [&](int d, int off) { return ls.at(shiftKey<D>(g, key, d, off)); };
+  const double C = ls.at(key);
+
+  if (sch == VLSG_WENO_3RD_ORDER || sch == VLSG_WENO_5TH_ORDER) {
+    // lsWENO.hpp:53-160
+    const int r = sch == VLSG_WENO_3RD_ORDER ? 2 : 3;
+    double gradPosTotal = 0, gradNegTotal = 0;
+    double wMinus[D], wPlus[D], st[7];
+    for (int i = 0; i < D; i++) {
+      st[r] = C;
+      for (int k = 1; k <= r; ++k) {
+        st[r + k] = V(i, k);
+        st[r - k] = V(i, -k);
+      }
+      if (r == 2) {
+        wMinus[i] = weno3(st, gridDelta, false);
+        wPlus[i] = weno3(st, gridDelta, true);
+      } else {
+        wMinus[i] = weno5(st, gridDelta, false);
+        wPlus[i] = weno5(st, gridDelta, true);
+      }
+      gradPosTotal += pow2(stdMax(wMinus[i], 0.)) + pow2(stdMin(wPlus[i], 0.));
+      gradNegTotal += pow2(stdMin(wMinus[i], 0.)) + pow2(stdMax(wPlus[i], 0.));
+    }
+    double vel_grad = 0.;
+    double n[3] = {0, 0, 0};
+    // Advect passes dissipationAlpha as the calcNormal flag (lsAdvect.hpp:670-676)
+    if (S.P.dissipationAlpha != 0.0) {
+      double denominator = 0;
+      for (int i = 0; i < D; i++) {
+        const double pos = V(i, 1);
+        const double neg = V(i, -1);
+        n[i] = pos - neg;
+        denominator += n[i] * n[i];
+      }
+      if (denominator > 0) {
+        denominator = 1. / std::sqrt(denominator);
+        for (int i = 0; i < D; ++i) n[i] *= denominator;
+      }
+    }
+    const double scalarVel = scalarVelocity(S.vel, material, n);
+    double vv[3];
+    vectorVelocity(S.vel, material, vv);
+    if (scalarVel > 0)
+      vel_grad += std::sqrt(gradPosTotal) * scalarVel;
+    else
+      vel_grad += std::sqrt(gradNegTotal) * scalarVel;
+    for (int w = 0; w < D; w++) {
+      if (vv[w] > 0.)
+        vel_grad += vv[w] * wMinus[w];
+      else
+        vel_grad += vv[w] * wPlus[w];
+    }
+    return {vel_grad, 0.};
+  }
+
+  const int order = (sch == VLSG_ENGQUIST_OSHER_2ND_ORDER ||
+                     sch == VLSG_LAX_FRIEDRICHS_2ND_ORDER ||
+                     sch == VLSG_LOCAL_LOCAL_LAX_FRIEDRICHS_2ND_ORDER ||
+                     sch == VLSG_LOCAL_LAX_FRIEDRICHS_2ND_ORDER)
+                        ? 2
+                        : 1;
+  double gradPos[D], gradNeg[D];
+
+  if (sch == VLSG_ENGQUIST_OSHER_1ST_ORDER ||
+      sch == VLSG_ENGQUIST_OSHER_2ND_ORDER) {
+    // lsEngquistOsher.hpp:42-162
+    double gradPosTotal = 0, gradNegTotal = 0;
+    for (int i = 0; i < D; i++) {
+      double diffPos, diffNeg;
+      oneSided<D>(V, i, C, gridDelta, order, diffPos, diffNeg);
+      gradPos[i] = diffNeg;
+      gradNeg[i] = diffPos;
+      gradPosTotal += pow2(stdMax(diffNeg, 0.)) + pow2(stdMin(diffPos, 0.));
+      gradNegTotal += pow2(stdMin(diffNeg, 0.)) + pow2(stdMax(diffPos, 0.));
+    }
+    double vel_grad = 0.;
+    double n[3] = {0, 0, 0};
+    if (S.P.calculateNormalVectors) {
+      double denominator = 0;
+      for (int i = 0; i < D; i++) {
+        const double pos = V(i, 1) - C;
+        const double neg = C - V(i, -1);
+        n[i] = (pos + neg) * 0.5;
+        denominator += n[i] * n[i];
+      }
+      denominator = 1. / std::sqrt(denominator);
+      for (int i = 0; i < D; ++i) n[i] *= denominator;
+    }
+    const double sv = scalarVelocity(S.vel, material, n);
+    double vv[3];
+    vectorVelocity(S.vel, material, vv);
+    if (sv > 0)
+      vel_grad += std::sqrt(gradPosTotal) * sv;
+    else
+      vel_grad += std::sqrt(gradNegTotal) * sv;
+    for (int w = 0; w < D; w++) {
+      if (vv[w] > 0.)
+        vel_grad += vv[w] * gradPos[w];
+      else
+        vel_grad += vv[w] * gradNeg[w];
+    }
+    return {vel_grad, 0.};
+  }
+
+  // Lax-Friedrichs family: central gradient, dissipation from alphas.
+  const bool globalLF = (sch == VLSG_LAX_FRIEDRICHS_1ST_ORDER ||
+                         sch == VLSG_LAX_FRIEDRICHS_2ND_ORDER);
+  const bool calcNormal = globalLF ? S.P.calculateNormalVectors : true;
+  const double alphaFactor = S.P.dissipationAlpha;
+  double grad = 0., dissipation = 0.;
+  double n[3] = {0, 0, 0};
+  double normalModulus = 0;
+  for (int i = 0; i < D; i++) {
+    double diffPos, diffNeg;
+    oneSided<D>(V, i, C, gridDelta, order, diffPos, diffNeg);
+    gradPos[i] = diffNeg;
+    gradNeg[i] = diffPos;
+    if (calcNormal) {
+      n[i] = (diffNeg + diffPos) * 0.5;
+      normalModulus += n[i] * n[i];
+    }
+    grad += pow2((diffNeg + diffPos) * 0.5);
+    if (globalLF) // lsLaxFriedrichs.hpp:317
+      dissipation +=
+          alphaFactor * S.globalAlphas[i] * (diffPos - diffNeg) * 0.5;
+  }
+  if (calcNormal) {
+    normalModulus = 1. / std::sqrt(normalModulus);
+    for (int i = 0; i < D; ++i) n[i] *= normalModulus;
+  }
+  const double sv = scalarVelocity(S.vel, material, n);
+  double vv[3];
+  vectorVelocity(S.vel, material, vv);
+  double totalGrad = 0.;
+  if (sv != 0.) totalGrad = sv * std::sqrt(grad);
+  for (int w = 0; w < D; w++) {
+    if (vv[w] > 0.)
+      totalGrad += vv[w] * gradPos[w];
+    else
+      totalGrad += vv[w] * gradNeg[w];
+  }
+  if (globalLF) // lsLaxFriedrichs.hpp:347
+    return {totalGrad, ((totalGrad != 0.) ? dissipation : 0)};
+
+  if (totalGrad == 0.) return {0, 0}; // lsLocalLaxFriedrichs.hpp:179-181
+
+  if (sch == VLSG_LOCAL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER ||
+      sch == VLSG_LOCAL_LOCAL_LAX_FRIEDRICHS_2ND_ORDER) {
+    // lsLocalLocalLaxFriedrichs.hpp:413-420
+    for (int i = 0; i < D; ++i) {
+      const double alpha = std::abs((sv + vv[i]) * n[i]);
+      alphas[i] = stdMax(alphas[i], alpha);
+      dissipation += alphaFactor * alpha * (gradNeg[i] - gradPos[i]) * 0.5;
+    }
+    return {totalGrad, dissipation};
+  }
+
+  // LocalLaxFriedrichs: alphas over the 3^D box, lsLocalLaxFriedrichs.hpp:183-240
+  double alpha[D];
+  for (int i = 0; i < D; ++i) alpha[i] = 0;
+  int nIdx[D];
+  for (int d = 0; d < D; ++d) nIdx[d] = -1;
+  int numNeighbors = 1;
+  for (int d = 0; d < D; ++d) numNeighbors *= 3;
+  auto VB = [&](const int *off) { return ls.at(offsetKey<D>(g, key, off)); };
+  for (int q = 0; q < numNeighbors; ++q) {
+    double normal[3] = {0, 0, 0};
+    double nm = 0.;
+    const double center = VB(nIdx);
+    for (int dir = 0; dir < D; ++dir) {
+      int o[D];
+      for (int d = 0; d < D; ++d) o[d] = nIdx[d];
+      o[dir] = nIdx[dir] - 1;
+      const double neg = VB(o);
+      o[dir] = nIdx[dir] + 1;
+      const double pos = VB(o);
+      // calculateNormalComponent, :32-36
+      const double dPos = (pos - center) / gridDelta;
+      const double dNeg = (center - neg) / gridDelta;
+      normal[dir] = (dPos + dNeg) * 0.5;
+      nm += normal[dir] * normal[dir];
+    }
+    nm = 1. / std::sqrt(nm);
+    for (int dir = 0; dir < D; ++dir) normal[dir] *= nm;
+    const double scaVel = scalarVelocity(S.vel, material, normal);
+    double vecVel[3];
+    vectorVelocity(S.vel, material, vecVel);
+    for (int dir = 0; dir < D; ++dir) {
+      const double tempAlpha = std::abs((scaVel + vecVel[dir]) * normal[dir]);
+      alpha[dir] = stdMax(alpha[dir], tempAlpha);
+      alphas[dir] = stdMax(alphas[dir], tempAlpha);
+    }
+    // incrementIndices, :38-48 (x fastest)
+    int dim = 0;
+    for (; dim < D - 1; ++dim) {
+      if (nIdx[dim] < 1) break;
+      nIdx[dim] = -1;
+    }
+    ++nIdx[dim];
+  }
+  for (int i = 0; i < D; ++i)
+    dissipation += alphaFactor * alpha[i] * (gradNeg[i] - gradPos[i]) * 0.5;
+  return {totalGrad, dissipation};
+}
+
+// Per-point rate chain of integrateTime (lsAdvect.hpp:530-588).
+struct RateEntry {
+  double gradient, dissipation, stop;
+};
+
+template <int D> struct Advector {
+  std::vector<LS<D>> &lss; // bottom .. top
+  Params P;
+  vlsg_velocity_desc vel;
+  std::vector<LS<D>> initial;
+  double currentTimeStep = -1.;
+  uint64_t pointUpdates = 0;
+  uint32_t stages = 0;
+
+  // storedRates, in HRLE order of the active points
+  std::vector<uint64_t> activeKeys;
+  std::vector<int64_t> rateStart;
+  std::vector<RateEntry> rates;
+
+  Advector(std::vector<LS<D>> &l, const Params &p, const vlsg_velocity_desc &v)
+      : lss(l), P(p), vel(v) {}
+
+  LS<D> &top() { return lss.back(); }
+
+  // findGlobalAlphas, lsAdvect.hpp:90-195
+  void findGlobalAlphas(double *finalAlphas) {
+    const LS<D> &t = top();
+    for (int i = 0; i < D; ++i) finalAlphas[i] = 0;
+    const int nt = omp_get_max_threads();
+    std::vector<std::array<double, 3>> loc(nt, std::array<double, 3>{0, 0, 0});
+#pragma omp parallel for schedule(static)
+    for (int64_t p = 0; p < (int64_t)t.keys.size(); ++p) {
+      const double value = t.vals[p];
+      if (!isDefined(value) || std::abs(value) > Params::integrationCutoff) continue;
+      const uint64_t key = t.keys[p];
+      auto &la = loc[omp_get_thread_num()];
+      for (int lower = 0; lower < (int)lss.size(); ++lower) {
+        if (lss[lower].at(key) <= value + Params::wrappingLayerEpsilon) {
+          double normal[3] = {0, 0, 0};
+          double normalModulus = 0.;
+          for (int i = 0; i < D; ++i) {
+            const double phiPos = t.at(shiftKey<D>(t.grid, key, i, 1));
+            const double phiNeg = t.at(shiftKey<D>(t.grid, key, i, -1));
+            normal[i] = phiPos - phiNeg;
+            normalModulus += normal[i] * normal[i];
+          }
+          normalModulus = 1. / std::sqrt(normalModulus);
+          for (int i = 0; i < D; ++i) normal[i] *= normalModulus;
+          const double scaVel = scalarVelocity(vel, lower, normal);
+          double vecVel[3];
+          vectorVelocity(vel, lower, vecVel);
+          for (int i = 0; i < D; ++i) {
+            const double tempAlpha = std::abs((scaVel + vecVel[i]) * normal[i]);
+            la[i] = stdMax(la[i], tempAlpha);
+          }
+          break;
+        }
+      }
+    }
+    for (auto &la : loc)
+      for (int i = 0; i < D; ++i) finalAlphas[i] = stdMax(finalAlphas[i], la[i]);
+  }
+
+  // integrateTime, lsAdvect.hpp:435-612
+  double integrateTime(double maxTimeStep, const double *globalAlphas) {
+    LS<D> &t = top();
+    activeKeys.clear();
+    std::vector<int64_t> activePos;
+    for (int64_t p = 0; p < (int64_t)t.keys.size(); ++p) {
+      const double v = t.vals[p];
+      if (isDefined(v) && std::abs(v) <= Params::integrationCutoff) {
+        activeKeys.push_back(t.keys[p]);
+        activePos.push_back(p);
+      }
+    }
+    const int64_t n = activeKeys.size();
+    const int L = lss.size();
+    std::vector<RateEntry> chainStore(size_t(n) * L);
+    std::vector<int> chainLen(n);
+    const int nt = omp_get_max_threads();
+    std::vector<double> tmin(nt, maxTimeStep);
+    std::vector<std::array<double, 3>> alp(nt, std::array<double, 3>{0, 0, 0});
+    const SchemeCtx<D> S{t, P, vel, globalAlphas};
+    const double adaptiveFactor = 1.0 / P.adaptiveSubdivisions;
+#pragma omp parallel for schedule(static)
+    for (int64_t a = 0; a < n; ++a) {
+      const int th = omp_get_thread_num();
+      const uint64_t key = activeKeys[a];
+      double value = t.vals[activePos[a]];
+      double maxStepTime = 0;
+      double cfl = P.timeStepRatio;
+      int len = 0;
+      RateEntry *chain = &chainStore[size_t(a) * L];
+      for (int cur = L - 1; cur >= 0; --cur) {
+        std::pair<double, double> gd{0., 0.};
+        for (int lower = 0; lower < L; ++lower) {
+          if (lss[lower].at(key) <= value + Params::wrappingLayerEpsilon) {
+            gd = evalScheme<D>(S, key, lower, alp[th].data());
+            break;
+          }
+        }
+        const double velocity = gd.first - gd.second;
+        if (velocity > 0.) {
+          maxStepTime += cfl / velocity;
+          chain[len++] = {gd.first, gd.second, NEG};
+          break;
+        } else if (velocity == 0.) {
+          maxStepTime = POS;
+          chain[len++] = {gd.first, gd.second, POS};
+          break;
+        } else {
+          double valueBelow;
+          if (cur > 0)
+            valueBelow = lss[cur - 1].at(key);
+          else
+            valueBelow = POS;
+          const double difference = std::abs(valueBelow - value);
+          if (difference >= cfl) {
+            maxStepTime -= cfl / velocity;
+            chain[len++] = {gd.first, gd.second, POS};
+            break;
+          } else {
+            if (P.adaptiveTimeStepping && difference > adaptiveFactor * cfl) {
+              maxStepTime -= adaptiveFactor * cfl / velocity;
+              chain[len++] = {gd.first, gd.second, POS};
+              break;
+            } else {
+              cfl -= difference;
+              value = valueBelow;
+              maxStepTime -= difference / velocity;
+              chain[len++] = {gd.first, gd.second, valueBelow};
+            }
+          }
+        }
+      }
+      chainLen[a] = len;
+      if (maxStepTime < tmin[th]) tmin[th] = maxStepTime;
+    }
+    double tempMax = maxTimeStep;
+    for (int i = 0; i < nt; ++i)
+      if (tmin[i] < tempMax) tempMax = tmin[i];
+    // reduceTimeStepHamiltonJacobi of the LF family (e.g. lsLaxFriedrichs.hpp:350-362)
+    const int s = P.spatial;
+    const bool lfFamily = !(s == VLSG_ENGQUIST_OSHER_1ST_ORDER ||
+                            s == VLSG_ENGQUIST_OSHER_2ND_ORDER ||
+                            s == VLSG_WENO_3RD_ORDER || s == VLSG_WENO_5TH_ORDER);
+    if (lfFamily) {
+      double fa[3] = {0, 0, 0};
+      if (s == VLSG_LAX_FRIEDRICHS_1ST_ORDER || s == VLSG_LAX_FRIEDRICHS_2ND_ORDER) {
+        for (int i = 0; i < D; ++i) fa[i] = globalAlphas[i];
+      } else {
+        for (int th = 0; th < nt; ++th)
+          for (int i = 0; i < D; ++i) fa[i] = stdMax(fa[i], alp[th][i]);
+      }
+      double timeStep = 0;
+      for (int i = 0; i < D; ++i) timeStep += fa[i] / t.grid.delta;
+      timeStep = 1.0 / timeStep;
+      tempMax = stdMin(timeStep, tempMax);
+    }
+    if (tempMax < maxTimeStep) maxTimeStep = tempMax;
+    rateStart.assign(n + 1, 0);
+    for (int64_t a = 0; a < n; ++a) rateStart[a + 1] = rateStart[a] + chainLen[a];
+    rates.resize(rateStart[n]);
+    for (int64_t a = 0; a < n; ++a)
+      for (int j = 0; j < chainLen[a]; ++j)
+        rates[rateStart[a] + j] = chainStore[size_t(a) * L + j];
+    return maxTimeStep;
+  }
+
+  // computeRates, lsAdvect.hpp:616-682
+  bool computeRates(double maxTimeStep) {
+    if (!schemeSupported(P.spatial)) return false;
+    expand<D>(top(), schemeWidth(P.spatial)); // prepareLS, :973-1015
+    double globalAlphas[3] = {0, 0, 0};
+    if (P.spatial == VLSG_LAX_FRIEDRICHS_1ST_ORDER ||
+        P.spatial == VLSG_LAX_FRIEDRICHS_2ND_ORDER)
+      findGlobalAlphas(globalAlphas);
+    currentTimeStep = integrateTime(maxTimeStep, globalAlphas);
+    return true;
+  }
+
+  // updateLevelSet, lsAdvect.hpp:686-800
+  void updateLevelSet(double dt) {
+    LS<D> &t = top();
+    reduce<D>(t, 1); // :700
+    const bool checkDiss = P.checkDissipation;
+    // after Reduce(1) the defined points are exactly the active points
+    int64_t a = 0;
+    for (int64_t p = 0; p < (int64_t)t.keys.size(); ++p) {
+      double &value = t.vals[p];
+      if (!isDefined(value)) continue;
+      if (std::abs(value) > Params::integrationCutoff) continue;
+      if (a >= (int64_t)activeKeys.size() || activeKeys[a] != t.keys[p])
+        throw std::runtime_error("updateLevelSet: rate/point mismatch");
+      const RateEntry *it = &rates[rateStart[a]];
+      double time = dt;
+      double velocity = it->gradient - it->dissipation;
+      if ((checkDiss && (it->gradient < 0 && velocity > 0)) ||
+          (it->gradient > 0 && velocity < 0))
+        velocity = 0;
+      double rate = time * velocity;
+      while (std::abs(it->stop - value) < std::abs(rate)) {
+        time -= std::abs((it->stop - value) / velocity);
+        value = it->stop;
+        ++it;
+        velocity = it->gradient - it->dissipation;
+        if ((checkDiss && (it->gradient < 0 && velocity > 0)) ||
+            (it->gradient > 0 && velocity < 0))
+          velocity = 0;
+        rate = time * velocity;
+      }
+      value -= rate;
+      ++a;
+    }
+    pointUpdates += a;
+    ++stages;
+    t.finalizeMap();
+  }
+
+  void rebuildLS() { rebuild<D>(top(), 1.0, 2); } // :250-256 (SLLF: 1.5, 3)
+
+  void adjustLowerLayers() { // :802-813
+    for (size_t i = 0; i + 1 < lss.size(); ++i)
+      booleanOp<D>(lss[i], top(), maxComp);
+  }
+
+  // combineLevelSets, lsAdvect.hpp:199-236
+  bool combineLevelSets(double wTarget, double wSource) {
+    int steps = 1;
+    if (P.temporal == VLSG_RUNGE_KUTTA_2ND_ORDER) steps = 2;
+    else if (P.temporal == VLSG_RUNGE_KUTTA_3RD_ORDER) steps = 3;
+    const int expansionWidth = std::ceil(2.0 * steps * P.timeStepRatio + 1);
+    expand<D>(top(), expansionWidth);
+    expand<D>(initial.back(), expansionWidth);
+    bool movedDown = false;
+    std::atomic<bool> md{false};
+    booleanOp<D>(top(), initial.back(), [&](double a, double b) {
+      if (a != POS && a != NEG && b != POS && b != NEG) {
+        const double res = wSource * a + wTarget * b;
+        if (res > b) md.store(true, std::memory_order_relaxed);
+        return res;
+      }
+      if (a == POS || a == NEG) return a;
+      return b;
+    });
+    movedDown = md.load();
+    rebuildLS();
+    return movedDown;
+  }
+
+  // AdvectTimeIntegration, lsAdvectIntegrationSchemes.hpp:46-168
+  double evolveForwardEuler(double maxTimeStep, bool updateLowerLayers = true) {
+    if (!computeRates(maxTimeStep)) throw std::runtime_error("scheme not supported");
+    updateLevelSet(currentTimeStep);
+    rebuildLS();
+    if (updateLowerLayers) adjustLowerLayers();
+    return currentTimeStep;
+  }
+  void saveInitial(bool all) {
+    if (initial.size() != lss.size()) initial.resize(lss.size());
+    if (all) {
+      for (size_t i = 0; i < lss.size(); ++i) initial[i] = lss[i];
+    } else {
+      initial.back() = lss.back();
+    }
+  }
+  void restoreLower() {
+    for (size_t i = 0; i + 1 < lss.size(); ++i) lss[i] = initial[i];
+  }
+  double evolveRungeKutta2(double maxTimeStep) {
+    saveInitial(false); // no velocity-update callback in the oracle
+    const double dt1 = evolveForwardEuler(maxTimeStep, false);
+    if (dt1 <= 0.) return 0.;
+    const double dt2 = evolveForwardEuler(dt1, false);
+    combineLevelSets(0.5, 0.5);
+    adjustLowerLayers();
+    return 0.5 * dt1 + 0.5 * dt2;
+  }
+  double evolveRungeKutta3(double maxTimeStep) {
+    saveInitial(true);
+    const double dt1 = evolveForwardEuler(maxTimeStep, false);
+    if (dt1 <= 0.) return 0.;
+    const double dt2 = evolveForwardEuler(dt1, false);
+    combineLevelSets(0.75, 0.25);
+    adjustLowerLayers();
+    const double dt3 = evolveForwardEuler(dt1, false);
+    const bool etched2 = combineLevelSets(1.0 / 3.0, 2.0 / 3.0);
+    if (etched2) restoreLower();
+    adjustLowerLayers();
+    return (dt1 + dt2 + 4.0 * dt3) / 6.0;
+  }
+  double advect(double maxTimeStep) { // :817-830
+    switch (P.temporal) {
+    case VLSG_RUNGE_KUTTA_2ND_ORDER: return evolveRungeKutta2(maxTimeStep);
+    case VLSG_RUNGE_KUTTA_3RD_ORDER: return evolveRungeKutta3(maxTimeStep);
+    default: return evolveForwardEuler(maxTimeStep);
+    }
+  }
+  // apply, lsAdvect.hpp:1017-1043
+  void apply(vlsg_advect_result &res) {
+    double advectedTime = 0.;
+    unsigned steps = 0;
+    if (P.advectionTime == 0.) {
+      advectedTime = advect(std::numeric_limits<double>::max());
+      steps = 1;
+    } else {
+      double currentTime = 0.0;
+      while (currentTime < P.advectionTime) {
+        currentTime += advect(P.advectionTime - currentTime);
+        ++steps;
+        if (P.singleStep) break;
+        if (steps >= P.maxSteps) throw std::runtime_error("step limit reached");
+      }
+      advectedTime = currentTime;
+    }
+    res.advected_time = advectedTime;
+    res.current_time_step = currentTimeStep;
+    res.number_of_time_steps = steps;
+    res.number_of_stages = stages;
+    res.point_updates = pointUpdates;
+    res.kernel_launches = 0;
+  }
+};
+
+} // namespace vlso

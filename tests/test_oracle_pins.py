@@ -1,0 +1,88 @@
+"""The oracle against the reference's own pins (no GPU).
+
+- TimeIntegration.cpp:177-313: Chamfer distance of an advected sphere to the
+  analytic result, for EO1 / WENO3 / WENO5 x FE / RK2 / RK3.
+- BooleanOperationExactZero (result.hpp): the golden run list of Box u Plane
+  after the boolean operation's Prune passes (2D, reflective x).
+- LSTEST_ASSERT_VALID_LS (lsTestAsserts.hpp:11-23) after every advection.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from viennals_b200 import AdvectParams, BoundaryConditionEnum as BC, Domain, Grid
+from viennals_b200.domain import make_runs
+from viennals_b200.geometry import make_sphere
+from viennals_b200.velocity import constant_vector
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+# (spatial, temporal, threshold) -- TimeIntegration.cpp:177-313
+TIME_INTEGRATION_PINS = [
+    (0, 0, 0.08), (0, 1, 0.14), (0, 2, 0.14),
+    (10, 0, 0.06), (10, 1, 0.016), (10, 2, 0.016),
+    (11, 0, 0.04), (11, 1, 0.008), (11, 2, 0.008),
+]
+
+
+@pytest.fixture(scope="module")
+def ti_setup():
+    g = Grid([-5, 5, -5, 5, -5, 5], [BC.INFINITE_BOUNDARY] * 3, 0.15)
+    start = O.OracleLS(g, make_sphere(g, [0, 0, 0], 1.5))
+    ref = O.OracleLS(g, make_sphere(g, [0.5, 0, 0], 1.5))
+    return start, ref
+
+
+@pytest.mark.parametrize("spatial,temporal,threshold", TIME_INTEGRATION_PINS)
+def test_time_integration_chamfer(ti_setup, spatial, temporal, threshold):
+    start, ref = ti_setup
+    ls = start.copy()
+    p = AdvectParams.defaults()
+    p.spatial_scheme = spatial
+    p.temporal_scheme = temporal
+    p.advection_time = 0.5
+    res = O.advect([ls], p, constant_vector([1.0, 0.0, 0.0]))
+    assert res.advected_time == pytest.approx(0.5)
+    assert ls.check() == 0
+    c = O.chamfer(ref, ls)
+    assert c["chamfer"] < threshold
+
+
+def test_boolean_exact_zero_golden():
+    from fromsurface2d import box_mesh, from_segments, plane_mesh
+
+    g = Grid([-10, 10, -10, 10], [BC.REFLECTIVE_BOUNDARY, BC.INFINITE_BOUNDARY], 1.0, dim=2)
+
+    def dom(pts, sign_fn):
+        keys = sorted(pts, key=lambda k: (k[1], k[0]))
+        idx = np.array(keys, np.int32)
+        vals = np.array([pts[k] for k in keys])
+        idx3 = np.concatenate([idx, np.zeros((len(idx), 1), np.int32)], 1)
+        rs, sg = make_runs(idx3, lambda x, y, z: sign_fn(x, y), [-10, -12, 0], [10, 12, 0])
+        return Domain(g, idx, vals, rs[:, :2], sg, width=2)
+
+    bn, bl = box_mesh([-5, 1], [5, 10])
+    box = from_segments(g, bn, bl, remove_boundary_triangles=False)
+    pn, pl = plane_mesh(g, [0, 1], [0, 1])
+    plane = from_segments(g, pn, pl)
+    mask = O.OracleLS(g, dom(box, lambda x, y: np.where((x > -5) & (x < 5) & (y > 1) & (y < 10), -1, 1)))
+    substrate = O.OracleLS(g, dom(plane, lambda x, y: np.where(y < 1, -1, 1)))
+    substrate.boolean(mask, 1)  # UNION, then Prune(removeStrayZeros) + Prune
+
+    gold = json.load(open(os.path.join(HERE, "golden", "boolean_exact_zero.json")))["runs"]
+    di, dv = substrate.points(0)
+    mine = {tuple(k): v for k, v in zip(di.tolist(), dv)}
+    gdef = {tuple(r["index"]): r["value"] for r in gold if abs(r["value"]) < 1e300}
+    assert set(mine) == set(gdef)
+    for k, v in gdef.items():
+        assert abs(mine[k] - v) < 1e-4, k
+    und = [r for r in gold if abs(r["value"]) > 1e300]
+    st = np.array([r["index"] for r in und], np.int32)
+    st[:, 1] = np.clip(st[:, 1], -1000, 1000)
+    got = substrate.values_at(st)
+    for r, v in zip(und, got):
+        assert abs(v) > 1e300
+        assert (v < 0) == (r["value"] < 0), r

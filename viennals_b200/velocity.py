@@ -1,0 +1,123 @@
+"""Velocity fields for the device functor of vlsg.h.
+
+`VelocityField` mirrors viennals::VelocityField<T> (lsVelocityField.hpp:11-41).
+A subclass that only sets coefficients runs entirely on the GPU
+(vlsg_set_velocity_functor); a subclass that overrides getScalarVelocity /
+getVectorVelocity is called back from the host once per stage with a batch of
+points (vlsg_set_velocity_callback).
+"""
+from ._abi import MAX_MATERIALS, VelocityDesc
+
+
+class VelocityField:
+    """Base class with the reference's defaults (zero velocity)."""
+
+    def getScalarVelocity(self, coordinate, material, normalVector, pointId):
+        return 0.0
+
+    def getVectorVelocity(self, coordinate, material, normalVector, pointId):
+        return (0.0, 0.0, 0.0)
+
+    def getDissipationAlpha(self, direction, material, centralDifferences):
+        return 0.0
+
+    def descriptor(self):
+        """Return a VelocityDesc when the field is a device functor, else None."""
+        return None
+
+
+class FunctorVelocity(VelocityField):
+    """Per-material polynomial in the unit normal, evaluated on the device.
+
+    For material m (clamped to the last entry) and normal n:
+        scalar = rate[m] + sum_k c_lin[m][k](n_k) * n_k
+                         + sum_k c_abs[m][k](n_k) * |n_k|
+                         + sum_k c_sq [m][k](n_k) * n_k^2
+    where each c(n_k) takes its `pos` coefficient for n_k > 0 and its `neg`
+    one otherwise; zero coefficients are skipped.  vector = vec[m].
+    """
+
+    def __init__(self, n_materials=1):
+        if not 1 <= n_materials <= MAX_MATERIALS:
+            raise ValueError("n_materials out of range")
+        self.n = n_materials
+        z3 = lambda: [[0.0, 0.0, 0.0] for _ in range(n_materials)]
+        self.rate = [0.0] * n_materials
+        self.lin_pos, self.lin_neg = z3(), z3()
+        self.abs_pos, self.abs_neg = z3(), z3()
+        self.sq_pos, self.sq_neg = z3(), z3()
+        self.vec = z3()
+
+    # convenience builders -------------------------------------------------
+    def set_rate(self, material, rate):
+        self.rate[material] = float(rate)
+        return self
+
+    def set_linear(self, material, axis, coeff, coeff_neg=None):
+        self.lin_pos[material][axis] = float(coeff)
+        self.lin_neg[material][axis] = float(coeff if coeff_neg is None else coeff_neg)
+        return self
+
+    def set_abs(self, material, axis, coeff_pos, coeff_neg=None):
+        self.abs_pos[material][axis] = float(coeff_pos)
+        self.abs_neg[material][axis] = float(coeff_pos if coeff_neg is None else coeff_neg)
+        return self
+
+    def set_square(self, material, axis, coeff_pos, coeff_neg=None):
+        self.sq_pos[material][axis] = float(coeff_pos)
+        self.sq_neg[material][axis] = float(coeff_pos if coeff_neg is None else coeff_neg)
+        return self
+
+    def set_vector(self, material, v):
+        self.vec[material] = [float(v[0]), float(v[1]), float(v[2])]
+        return self
+
+    def _m(self, material):
+        return min(max(material, 0), self.n - 1)
+
+    def getScalarVelocity(self, coordinate, material, normalVector, pointId):
+        m = self._m(material)
+        s = self.rate[m]
+        n = normalVector
+        for tab_pos, tab_neg, f in (
+            (self.lin_pos, self.lin_neg, lambda x: x),
+            (self.abs_pos, self.abs_neg, abs),
+            (self.sq_pos, self.sq_neg, lambda x: x * x),
+        ):
+            for k in range(3):
+                c = tab_pos[m][k] if n[k] > 0 else tab_neg[m][k]
+                if c != 0:
+                    s = s + c * f(n[k])
+        return s
+
+    def getVectorVelocity(self, coordinate, material, normalVector, pointId):
+        return tuple(self.vec[self._m(material)])
+
+    def descriptor(self):
+        d = VelocityDesc()
+        d.n_materials = self.n
+        for m in range(self.n):
+            d.rate[m] = self.rate[m]
+            for k in range(3):
+                d.lin_pos[m][k] = self.lin_pos[m][k]
+                d.lin_neg[m][k] = self.lin_neg[m][k]
+                d.abs_pos[m][k] = self.abs_pos[m][k]
+                d.abs_neg[m][k] = self.abs_neg[m][k]
+                d.sq_pos[m][k] = self.sq_pos[m][k]
+                d.sq_neg[m][k] = self.sq_neg[m][k]
+                d.vec[m][k] = self.vec[m][k]
+        return d
+
+
+def constant_scalar(v, n_materials=1):
+    f = FunctorVelocity(n_materials)
+    for m in range(n_materials):
+        f.set_rate(m, v)
+    return f
+
+
+def constant_vector(vec, n_materials=1):
+    f = FunctorVelocity(n_materials)
+    for m in range(n_materials):
+        f.set_vector(m, vec)
+    return f
