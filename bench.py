@@ -1,0 +1,332 @@
+"""Benchmark: narrow-band point-updates/s of the level-set advection step.
+
+Workload (one "step" = one RK3 time step, Advect::apply with
+advectionTime = 0, over the whole band): the precision form -- a sphere of
+radius 40 at gridDelta 0.05 whose radius is modulated by seeded real
+spherical harmonics (l <= 8, coefficients ~ N(0, 0.02 R)), velocity
+1 + 0.3 n_z, WENO5 + RK3, CFL 0.4, phi stored in FP32 with FP64 time step,
+advected time and stage combination.  Inputs are synthetic (seeded), built
+on the GPU before the timed region.
+
+value : point-updates/s with the level set resident in HBM (K steps of the
+        C ABI's vlsg_advect, timed with CUDA events on the library stream).
+e2e   : the same metric through the C ABI with host buffers: every step
+        uploads the level set from host memory, advects one step and
+        downloads the result.
+Multi-GPU (torchrun): replicas -- every rank advects its own copy of the
+domain; value = all ranks' point updates / max-over-ranks time.
+
+--impl reference times the CPU restatement of the reference's algorithm
+(oracle/, FP64, OpenMP on all host cores) on a bounded sample of the same
+workload, since the reference itself cannot be built on this image.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "band point-updates/s WENO5-RK3 FP32 vs FP64 on 1 B200 at stated err; % HBM peak"
+UNIT = "point-updates/s"
+HBM_PEAK_FALLBACK = 6650.0
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([s.strip() for s in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = sorted(float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit())
+        mx = max((float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()), default=None)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for k, nm in enumerate(names):
+                if len(s) > 5 + k and s[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def build_workload(args, device):
+    from viennals_b200.synth import perturbed_sphere, precision_velocity
+
+    grid, dom = perturbed_sphere(radius=args.radius, grid_delta=args.grid_delta,
+                                 seed=args.seed, device=device)
+    return grid, dom, precision_velocity()
+
+
+def params_for(args):
+    from viennals_b200 import AdvectParams
+
+    p = AdvectParams.defaults()
+    p.spatial_scheme = 11  # WENO_5TH_ORDER
+    p.temporal_scheme = 2  # RUNGE_KUTTA_3RD_ORDER
+    p.time_step_ratio = 0.4
+    p.advection_time = 0.0  # one step per call
+    return p
+
+
+def run_ours(args, rank, world):
+    import numpy as np
+    import torch
+
+    from viennals_b200.advect import Context
+    from viennals_b200._abi import Precision
+
+    dev = torch.device("cuda", args.local_rank)
+    torch.cuda.set_device(dev)
+    t0 = time.time()
+    grid, dom, vel = build_workload(args, f"cuda:{args.local_rank}")
+    gen_s = time.time() - t0
+    prec = Precision.FP32 if args.precision == "fp32" else Precision.FP64
+    stream = torch.cuda.Stream(device=dev)
+    ctx = Context(args.local_rank, prec)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.set_grid(grid)
+    ctx.set_level_set_count(1)
+    ctx.upload(0, dom)
+    ctx.set_velocity(vel.descriptor())
+    p = params_for(args)
+    for _ in range(args.warmup):
+        ctx.advect(p)
+    dist = world > 1
+    if dist:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    updates = 0
+    launches = 0
+    with ClockSampler(args.local_rank) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            r = ctx.advect(p)
+            updates += r.point_updates
+            launches += r.kernel_launches
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        torch.distributed.barrier()
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+        u = torch.tensor([float(updates)], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(u)
+        total_updates = float(u.item())
+    else:
+        total_updates = float(updates)
+    value = total_updates / (ms / 1e3)
+    out = {"ms": ms, "updates": updates, "value": value, "launches": launches,
+           "clocks": clk.summary(), "gen_s": gen_s, "n_points": int(dom.n_points)}
+
+    if rank == 0:
+        # per-kernel device times of one more step (events around every
+        # launch) -> dominant kernel and its roofline
+        ctx.set_profiling(True)
+        r = ctx.advect(p)
+        stats = ctx.kernel_stats()
+        ctx.set_profiling(False)
+        out["kernels"] = stats
+        out["profile_updates"] = r.point_updates
+        # e2e through the C ABI with host buffers
+        n_e2e = max(1, min(args.steps, args.e2e_steps))
+        idx, val, w = ctx.download(0)
+        host_dom = ctx.download_domain(0, grid)
+        h2d = host_dom.idx.nbytes + host_dom.values.nbytes + host_dom.run_start.nbytes + host_dom.run_sign.nbytes
+        ctx2 = Context(args.local_rank, prec)
+        ctx2.set_stream(stream.cuda_stream)
+        ctx2.set_grid(grid)
+        ctx2.set_level_set_count(1)
+        ctx2.set_velocity(vel.descriptor())
+        torch.cuda.synchronize()
+        e2e_updates = 0
+        d2h = 0
+        t0 = time.perf_counter()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        cur = host_dom
+        for _ in range(n_e2e):
+            ctx2.upload(0, cur)
+            r2 = ctx2.advect(p)
+            e2e_updates += r2.point_updates
+            cur = ctx2.download_domain(0, grid)
+            d2h += cur.idx.nbytes + cur.values.nbytes
+        e1.record(stream)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        out["e2e"] = {"value": e2e_updates / wall, "unit": UNIT,
+                      "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h // n_e2e),
+                      "steps": n_e2e, "wall_s_per_step": wall / n_e2e}
+        ctx2.close()
+    ctx.close()
+    return out
+
+
+def cpu_baseline(args, sample_radius, steps=1):
+    """The oracle (FP64 restatement, OpenMP on all host cores) on a bounded
+    sample: the same workload at a smaller radius."""
+    from oracle import oracle as O
+    from viennals_b200.synth import perturbed_sphere, precision_velocity
+
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    grid, dom = perturbed_sphere(radius=sample_radius, grid_delta=args.grid_delta,
+                                 seed=args.seed, device="cuda" if _has_cuda() else "cpu")
+    ls = O.OracleLS(grid, dom)
+    p = params_for(args)
+    updates = 0
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        r = O.advect([ls], p, precision_velocity())
+        updates += r.point_updates
+    dt = time.perf_counter() - t0
+    return {"value": updates / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": (f"perturbed sphere R={sample_radius} at gridDelta {args.grid_delta} "
+                       f"({dom.n_points} band points), WENO5+RK3 CFL 0.4, {steps} step(s), "
+                       f"FP64 oracle restatement (the reference cannot be built here)"),
+            "seconds": dt}
+
+
+def _has_cuda():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+def roofline(out, peaks):
+    """Dominant kernel: device time share; achieved = its algorithmic bytes /
+    its average launch time."""
+    ks = out.get("kernels") or []
+    if not ks:
+        return None
+    top = max(ks, key=lambda k: k["device_ms"])
+    hbm = peaks.get("hbm_gbs") if peaks else None
+    src = "measured" if hbm else "fallback"
+    hbm = hbm or HBM_PEAK_FALLBACK
+    per_launch_ms = top["device_ms"] / max(1, top["launches"])
+    bytes_per_launch = top["bytes"] / max(1, top["launches"])
+    achieved = bytes_per_launch / (per_launch_ms / 1e3) / 1e9 if per_launch_ms > 0 else 0.0
+    total = sum(k["device_ms"] for k in ks)
+    return {"bound": "hbm", "kernel": top["name"], "achieved": achieved, "peak": hbm,
+            "peak_source": src, "unit": "GB/s", "frac": achieved / hbm,
+            "traffic": None, "share": top["device_ms"] / total if total else None,
+            "launch_ms": per_launch_ms}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--radius", type=float, default=40.0)
+    ap.add_argument("--grid-delta", type=float, default=0.05)
+    ap.add_argument("--seed", type=int, default=1234)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-sample-radius", type=float, default=8.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    args.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    cfg = {"workload": f"perturbed sphere R={args.radius} gridDelta={args.grid_delta} "
+                       f"(seed {args.seed}), WENO5+RK3, CFL 0.4, v=1+0.3 n_z",
+           "precision": args.precision, "step": "one RK3 time step (3 FE stages + 2 combines)",
+           "l2": "inputs larger than L2 (band ~10M points)", "parallelism": f"replicas x{world}"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        cb = cpu_baseline(args, args.cpu_sample_radius, steps=max(1, args.steps))
+        line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "impl": "reference",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic", "config": cfg,
+                "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    if world > 1:
+        import torch
+        torch.cuda.set_device(args.local_rank)
+        torch.distributed.init_process_group(
+            "nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    out = run_ours(args, rank, world)
+    if world > 1:
+        import torch
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return
+    peaks = measured_peaks()
+    line = {"metric": METRIC, "value": out["value"], "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": out["ms"] / max(1, args.steps), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if args.precision == "fp32" else "f64",
+            "data": "synthetic", "config": cfg, "gpu_launches": out["launches"],
+            "clocks": out["clocks"], "e2e": out.get("e2e"),
+            "roofline": roofline(out, peaks), "band_points": out["n_points"],
+            "kernels": out.get("kernels")}
+    if not args.no_cpu_baseline:
+        cb = cpu_baseline(args, args.cpu_sample_radius)
+        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

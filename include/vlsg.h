@@ -152,6 +152,10 @@ const char *vlsg_last_error(const vlsg_context *ctx); /* ctx may be NULL */
 int vlsg_create(vlsg_context **out, int32_t device, int32_t precision);
 int vlsg_destroy(vlsg_context *ctx);
 void vlsg_default_params(vlsg_advect_params *p);
+/* The CUDA stream (cudaStream_t) every kernel of the context runs on; a
+ * caller may hand in its own stream (NULL restores the context's own). */
+int vlsg_set_stream(vlsg_context *ctx, void *stream);
+int vlsg_get_stream(vlsg_context *ctx, void **stream);
 
 /* Grid: Domain(bounds, boundaryConditions, gridDelta), lsDomain.hpp:68-78.
  * grid_min/grid_max are INDEX bounds (floor(min/dx), ceil(max/dx)); for a
@@ -172,6 +176,14 @@ int vlsg_upload_levelset(vlsg_context *ctx, int32_t slot, int64_t n_points,
 int vlsg_count_points(vlsg_context *ctx, int32_t slot, int64_t *n_points);
 int vlsg_download_levelset(vlsg_context *ctx, int32_t slot, int64_t capacity,
                            int32_t *indices, double *values, int32_t *width);
+
+/* Values of arbitrary grid points of a level set (indices are mapped through
+ * the boundary conditions): the defined value, or +-DBL_MAX carrying the sign
+ * of the undefined region -- what viennahrle's iterators return for them
+ * (lsDomain.hpp:51-52).  Used to rebuild the undefined runs of a downloaded
+ * level set. */
+int vlsg_get_values(vlsg_context *ctx, int32_t slot, int64_t n,
+                    const int32_t *indices, double *values);
 
 /* Velocity plugin: either a device functor or a host callback. */
 int vlsg_set_velocity_functor(vlsg_context *ctx, const vlsg_velocity_desc *v);

@@ -1,0 +1,262 @@
+"""`Advect` -- the drop-in front of viennals::Advect<T,3> over libvlsgpu.
+
+Same setters, getters and semantics as the reference (lsAdvect.hpp:836-1043,
+bound to Python at python/pyWrap.hpp:324-401): level sets are inserted bottom
+to top, the last one is advected and must wrap the others, and apply()
+writes the results back into the same Domain objects.  Errors that the
+reference logs and returns on raise RuntimeError here.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._abi import (AdvectParams, AdvectResult, KernelStat, Precision,
+                   SpatialSchemeEnum, TemporalSchemeEnum)
+from .domain import Domain, make_runs
+
+
+def _p(a, t):
+    return a.ctypes.data_as(ctypes.POINTER(t))
+
+
+class Context:
+    """One libvlsgpu context (device, precision, CUDA stream)."""
+
+    def __init__(self, device=0, precision=Precision.FP64):
+        self.lib = _lib.load()
+        self.h = ctypes.c_void_p()
+        self._check(self.lib.vlsg_create(ctypes.byref(self.h), int(device), int(precision)), None)
+        self.precision = Precision(precision)
+
+    def _check(self, rc, h="self"):
+        if rc != 0:
+            msg = self.lib.vlsg_last_error(self.h if h == "self" else None)
+            raise RuntimeError(f"vlsg error {rc}: {msg.decode() if msg else ''}")
+
+    def close(self):
+        if self.h:
+            self.lib.vlsg_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------------
+    def set_stream(self, stream_ptr):
+        """Run the context's kernels on an external cudaStream_t (int handle)."""
+        self._check(self.lib.vlsg_set_stream(self.h, ctypes.c_void_p(stream_ptr)))
+
+    def stream(self):
+        s = ctypes.c_void_p()
+        self._check(self.lib.vlsg_get_stream(self.h, ctypes.byref(s)))
+        return s.value
+
+    def set_grid(self, grid):
+        gmin = np.array(grid.min[:3], np.int64)
+        gmax = np.array(grid.max[:3], np.int64)
+        bc = np.array(grid.bc[:3], np.int32)
+        self._check(self.lib.vlsg_set_grid(self.h, grid.dim, _p(gmin, ctypes.c_int64),
+                                           _p(gmax, ctypes.c_int64), _p(bc, ctypes.c_int32),
+                                           float(grid.delta)))
+
+    def set_level_set_count(self, n):
+        self._check(self.lib.vlsg_set_level_set_count(self.h, int(n)))
+
+    def upload(self, slot, dom):
+        idx = np.ascontiguousarray(dom.idx, np.int32)
+        val = np.ascontiguousarray(dom.values, np.float64)
+        rs = np.ascontiguousarray(dom.run_start, np.int32)
+        sg = np.ascontiguousarray(dom.run_sign, np.int8)
+        self._check(self.lib.vlsg_upload_levelset(
+            self.h, int(slot), len(val), _p(idx, ctypes.c_int32), _p(val, ctypes.c_double),
+            len(sg), _p(rs, ctypes.c_int32), _p(sg, ctypes.c_int8), int(dom.width)))
+
+    def count(self, slot):
+        n = ctypes.c_int64()
+        self._check(self.lib.vlsg_count_points(self.h, int(slot), ctypes.byref(n)))
+        return n.value
+
+    def download(self, slot):
+        """(idx, values, width) of the defined points in HRLE order."""
+        n = self.count(slot)
+        idx = np.zeros((n, 3), np.int32)
+        val = np.zeros(n)
+        w = ctypes.c_int32()
+        self._check(self.lib.vlsg_download_levelset(self.h, int(slot), n, _p(idx, ctypes.c_int32),
+                                                    _p(val, ctypes.c_double), ctypes.byref(w)))
+        return idx, val, w.value
+
+    def values_at(self, slot, idx):
+        idx = np.ascontiguousarray(idx, np.int32)
+        out = np.zeros(len(idx))
+        self._check(self.lib.vlsg_get_values(self.h, int(slot), len(idx), _p(idx, ctypes.c_int32),
+                                             _p(out, ctypes.c_double)))
+        return out
+
+    def set_velocity(self, desc):
+        self._check(self.lib.vlsg_set_velocity_functor(self.h, ctypes.byref(desc)))
+
+    def advect(self, params):
+        res = AdvectResult()
+        self._check(self.lib.vlsg_advect(self.h, ctypes.byref(params), ctypes.byref(res)))
+        return res
+
+    def set_profiling(self, on):
+        self._check(self.lib.vlsg_set_profiling(self.h, int(bool(on))))
+
+    def kernel_stats(self):
+        cnt = ctypes.c_int32()
+        self._check(self.lib.vlsg_get_kernel_stats(self.h, 0, None, ctypes.byref(cnt)))
+        arr = (KernelStat * max(1, cnt.value))()
+        self._check(self.lib.vlsg_get_kernel_stats(self.h, cnt.value, arr, ctypes.byref(cnt)))
+        return [dict(name=arr[i].name.decode(), launches=arr[i].launches,
+                     device_ms=arr[i].device_ms, bytes=arr[i].algorithmic_bytes)
+                for i in range(cnt.value)]
+
+    def download_domain(self, slot, grid):
+        """Domain with the defined points and the undefined runs rebuilt from
+        the device's signs."""
+        idx, val, w = self.download(slot)
+        if len(idx):
+            lo = idx.min(0) - 1
+            hi = idx.max(0) + 1
+        else:
+            lo = np.zeros(3, np.int64)
+            hi = np.zeros(3, np.int64)
+
+        def sign_fn(x, y, z):
+            q = np.stack([np.asarray(x), np.asarray(y), np.asarray(z)], 1).astype(np.int32)
+            v = self.values_at(slot, q)
+            return np.where(v < 0, -1, 1)
+
+        rs, sg = make_runs(idx, sign_fn, lo, hi)
+        return Domain(grid, idx, val, rs, sg, width=w)
+
+
+class Advect:
+    """Mirror of viennals::Advect<T,3> running on the GPU."""
+
+    velocityLabel = "AdvectionVelocities"
+    dissipationLabel = "Dissipation"
+
+    def __init__(self, levelSets=None, velocities=None, precision=Precision.FP64, device=0):
+        if isinstance(levelSets, Domain):
+            levelSets = [levelSets]
+        self.levelSets = list(levelSets) if levelSets else []
+        self.velocities = velocities
+        self.params = AdvectParams.defaults()
+        self.precision = Precision(precision)
+        self.device = device
+        self.ctx = None
+        self.result = AdvectResult()
+        self.result.current_time_step = -1.0
+        self._resident = None  # (ids, fingerprints) of the level sets on the device
+
+    # setters, lsAdvect.hpp:856-969 ---------------------------------------
+    def insertNextLevelSet(self, ls):
+        self.levelSets.append(ls)
+
+    def clearLevelSets(self):
+        self.levelSets = []
+
+    def setVelocityField(self, v):
+        self.velocities = v
+
+    def setAdvectionTime(self, t):
+        self.params.advection_time = float(t)
+
+    def setSingleStep(self, b):
+        self.params.single_step = int(bool(b))
+
+    def setTimeStepRatio(self, cfl):
+        self.params.time_step_ratio = float(cfl)
+
+    def setCalculateNormalVectors(self, b):
+        self.params.calculate_normal_vectors = int(bool(b))
+
+    def setIgnoreVoids(self, b):
+        self.params.ignore_voids = int(bool(b))
+
+    def setAdaptiveTimeStepping(self, b=True, subdivisions=20):
+        self.params.adaptive_time_stepping = int(bool(b))
+        self.params.adaptive_subdivisions = max(1, int(subdivisions))
+
+    def setSaveAdvectionVelocities(self, b):
+        self.params.save_advection_velocities = int(bool(b))
+
+    def setSpatialScheme(self, s):
+        self.params.spatial_scheme = int(SpatialSchemeEnum(s))
+
+    setIntegrationScheme = setSpatialScheme  # deprecated name, lsAdvect.hpp:940-946
+
+    def setTemporalScheme(self, s):
+        self.params.temporal_scheme = int(TemporalSchemeEnum(s))
+
+    def setDissipationAlpha(self, a):
+        self.params.dissipation_alpha = float(a)
+
+    def setCheckDissipation(self, b):
+        self.params.check_dissipation = int(bool(b))
+
+    def setUpdatePointData(self, b):
+        self.params.update_point_data = int(bool(b))
+
+    def setVelocityUpdateCallback(self, cb):
+        raise RuntimeError("setVelocityUpdateCallback is not supported by the GPU front")
+
+    # getters, lsAdvect.hpp:920-932 ---------------------------------------
+    def getAdvectedTime(self):
+        return self.result.advected_time
+
+    def getCurrentTimeStep(self):
+        return self.result.current_time_step
+
+    def getNumberOfTimeSteps(self):
+        return self.result.number_of_time_steps
+
+    def getTimeStepRatio(self):
+        return self.params.time_step_ratio
+
+    def getCalculateNormalVectors(self):
+        return bool(self.params.calculate_normal_vectors)
+
+    # ---------------------------------------------------------------------
+    @staticmethod
+    def _fingerprint(d):
+        return (d.n_points, d.width, hash(d.idx.tobytes()), hash(d.values.tobytes()))
+
+    def _sync_to_device(self):
+        if not self.levelSets:
+            raise RuntimeError("No level sets passed to Advect. Not advecting.")
+        if self.velocities is None:
+            raise RuntimeError("No velocity field passed to Advect. Not advecting.")
+        desc = self.velocities.descriptor()
+        if desc is None:
+            raise RuntimeError("the velocity field must be a FunctorVelocity on the GPU")
+        if self.ctx is None:
+            self.ctx = Context(self.device, self.precision)
+        key = [id(d) for d in self.levelSets]
+        fps = [self._fingerprint(d) for d in self.levelSets]
+        if self._resident is None or self._resident != (key, fps):
+            grid = self.levelSets[-1].grid
+            self.ctx.set_grid(grid)
+            self.ctx.set_level_set_count(len(self.levelSets))
+            for i, d in enumerate(self.levelSets):
+                self.ctx.upload(i, d)
+        self.ctx.set_velocity(desc)
+
+    def apply(self):
+        """Advect::apply, lsAdvect.hpp:1017-1043; results written back."""
+        self._sync_to_device()
+        self.result = self.ctx.advect(self.params)
+        for i, d in enumerate(self.levelSets):
+            nd = self.ctx.download_domain(i, d.grid)
+            d.idx, d.values, d.run_start, d.run_sign, d.width = (
+                nd.idx, nd.values, nd.run_start, nd.run_sign, nd.width)
+        self._resident = ([id(d) for d in self.levelSets],
+                          [self._fingerprint(d) for d in self.levelSets])
+        return self.result

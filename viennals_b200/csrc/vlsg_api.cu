@@ -1,0 +1,344 @@
+// vlsg_api.cu -- the C ABI of libvlsgpu.so (declared in include/vlsg.h).
+#include <algorithm>
+#include <climits>
+#include <cstdio>
+#include <memory>
+#include <mutex>
+#include <string>
+
+#include "vlsg_engine.cuh"
+
+using namespace vlsg;
+
+struct vlsg_context {
+  int device = 0;
+  int precision = VLSG_FP64;
+  cudaStream_t stream = nullptr;    // stream in use
+  cudaStream_t ownStream = nullptr; // stream created with the context
+  std::string err;
+  bool hasGrid = false;
+  GridDev grid{};
+  std::vector<StagedLS> staged;
+  bool dirty = true;
+  bool hasVel = false;
+  vlsg_velocity_desc vel{};
+  bool profiling = false;
+  std::unique_ptr<Engine<double>> e64;
+  std::unique_ptr<Engine<float>> e32;
+};
+
+namespace {
+std::mutex g_errMutex;
+std::string g_lastError;
+
+int fail(vlsg_context *ctx, int code, const std::string &msg) {
+  if (ctx) ctx->err = msg;
+  std::lock_guard<std::mutex> lk(g_errMutex);
+  g_lastError = msg;
+  return code;
+}
+
+template <class F> int guarded(vlsg_context *ctx, F f) {
+  try {
+    if (ctx) {
+      cudaError_t e = cudaSetDevice(ctx->device);
+      if (e != cudaSuccess) return fail(ctx, VLSG_ERR_CUDA, cudaGetErrorString(e));
+    }
+    return f();
+  } catch (const CudaError &e) {
+    return fail(ctx, e.code, e.what());
+  } catch (const std::exception &e) {
+    return fail(ctx, VLSG_ERR_ARGUMENT, e.what());
+  }
+}
+
+template <class F> auto withEngine(vlsg_context *ctx, F f) {
+  if (ctx->precision == VLSG_FP64) return f(*ctx->e64);
+  return f(*ctx->e32);
+}
+
+void ensureBuilt(vlsg_context *ctx) {
+  if (!ctx->hasGrid) throw CudaError("no grid set (vlsg_set_grid)", VLSG_ERR_STATE);
+  if (ctx->staged.empty()) throw CudaError("no level set uploaded", VLSG_ERR_STATE);
+  if (!ctx->dirty) return;
+  const int margin = 4;
+  if (ctx->precision == VLSG_FP64) {
+    if (!ctx->e64) ctx->e64.reset(new Engine<double>());
+    ctx->e64->stream = ctx->stream;
+    ctx->e64->build(ctx->grid, ctx->staged, margin);
+  } else {
+    if (!ctx->e32) ctx->e32.reset(new Engine<float>());
+    ctx->e32->stream = ctx->stream;
+    ctx->e32->build(ctx->grid, ctx->staged, margin);
+  }
+  ctx->dirty = false;
+}
+} // namespace
+
+extern "C" {
+
+int vlsg_version(void) { return 100; }
+
+const char *vlsg_last_error(const vlsg_context *ctx) {
+  if (ctx) return ctx->err.c_str();
+  return g_lastError.c_str();
+}
+
+void vlsg_default_params(vlsg_advect_params *p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->spatial_scheme = VLSG_ENGQUIST_OSHER_1ST_ORDER;
+  p->temporal_scheme = VLSG_FORWARD_EULER;
+  p->time_step_ratio = 0.4999;
+  p->dissipation_alpha = 1.0;
+  p->advection_time = 0.;
+  p->calculate_normal_vectors = 1;
+  p->adaptive_subdivisions = 20;
+  p->check_dissipation = 1;
+  p->update_point_data = 1;
+}
+
+int vlsg_create(vlsg_context **out, int32_t device, int32_t precision) {
+  if (!out) return fail(nullptr, VLSG_ERR_ARGUMENT, "vlsg_create: out is NULL");
+  if (precision != VLSG_FP64 && precision != VLSG_FP32)
+    return fail(nullptr, VLSG_ERR_ARGUMENT, "vlsg_create: unknown precision");
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || device < 0 || device >= n)
+    return fail(nullptr, VLSG_ERR_CUDA,
+                std::string("vlsg_create: no CUDA device ") + std::to_string(device) +
+                    (e != cudaSuccess ? std::string(": ") + cudaGetErrorString(e) : ""));
+  auto *ctx = new vlsg_context();
+  ctx->device = device;
+  ctx->precision = precision;
+  int rc = guarded(ctx, [&] {
+    VLSG_CUDA(cudaStreamCreateWithFlags(&ctx->ownStream, cudaStreamNonBlocking));
+    ctx->stream = ctx->ownStream;
+    return VLSG_OK;
+  });
+  if (rc != VLSG_OK) {
+    delete ctx;
+    return rc;
+  }
+  *out = ctx;
+  return VLSG_OK;
+}
+
+int vlsg_destroy(vlsg_context *ctx) {
+  if (!ctx) return VLSG_OK;
+  cudaSetDevice(ctx->device);
+  ctx->e64.reset();
+  ctx->e32.reset();
+  if (ctx->ownStream) cudaStreamDestroy(ctx->ownStream);
+  delete ctx;
+  return VLSG_OK;
+}
+
+int vlsg_set_stream(vlsg_context *ctx, void *stream) {
+  if (!ctx) return fail(nullptr, VLSG_ERR_ARGUMENT, "NULL context");
+  return guarded(ctx, [&] {
+    VLSG_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->stream = stream ? (cudaStream_t)stream : ctx->ownStream;
+    if (ctx->e64) ctx->e64->stream = ctx->stream;
+    if (ctx->e32) ctx->e32->stream = ctx->stream;
+    return VLSG_OK;
+  });
+}
+
+int vlsg_get_stream(vlsg_context *ctx, void **stream) {
+  if (!ctx || !stream) return fail(ctx, VLSG_ERR_ARGUMENT, "bad argument");
+  *stream = (void *)ctx->stream;
+  return VLSG_OK;
+}
+
+int vlsg_set_grid(vlsg_context *ctx, int32_t dim, const int64_t *gmin, const int64_t *gmax,
+                  const int32_t *bc, double delta) {
+  if (!ctx) return fail(nullptr, VLSG_ERR_ARGUMENT, "NULL context");
+  if (dim != 3) return fail(ctx, VLSG_ERR_ARGUMENT, "only D = 3 is supported on the GPU");
+  if (!gmin || !gmax || !bc || !(delta > 0))
+    return fail(ctx, VLSG_ERR_ARGUMENT, "vlsg_set_grid: bad argument");
+  GridDev g{};
+  for (int d = 0; d < 3; ++d) {
+    if (bc[d] < 0 || bc[d] > 4) return fail(ctx, VLSG_ERR_ARGUMENT, "unknown boundary condition");
+    if (gmin[d] < -(1 << 19) || gmax[d] > (1 << 19))
+      return fail(ctx, VLSG_ERR_ARGUMENT, "grid index bounds exceed +-2^19");
+    g.gmin[d] = (int)gmin[d];
+    g.gmax[d] = (int)gmax[d];
+    g.bc[d] = bc[d];
+    if ((bc[d] == VLSG_PERIODIC_BOUNDARY && gmax[d] - gmin[d] < 1) ||
+        (bc[d] == VLSG_REFLECTIVE_BOUNDARY && gmax[d] < gmin[d]))
+      return fail(ctx, VLSG_ERR_ARGUMENT, "empty bounded direction");
+  }
+  g.delta = delta;
+  ctx->grid = g;
+  ctx->hasGrid = true;
+  ctx->dirty = true;
+  return VLSG_OK;
+}
+
+int vlsg_set_level_set_count(vlsg_context *ctx, int32_t n) {
+  if (!ctx) return fail(nullptr, VLSG_ERR_ARGUMENT, "NULL context");
+  if (n < 1 || n > VLSG_MAX_LEVEL_SETS)
+    return fail(ctx, VLSG_ERR_ARGUMENT, "level set count out of range");
+  ctx->staged.resize(n);
+  ctx->dirty = true;
+  return VLSG_OK;
+}
+
+int vlsg_upload_levelset(vlsg_context *ctx, int32_t slot, int64_t n, const int32_t *idx,
+                         const double *values, int64_t nRuns, const int32_t *runStart,
+                         const int8_t *runSign, int32_t width) {
+  if (!ctx) return fail(nullptr, VLSG_ERR_ARGUMENT, "NULL context");
+  return guarded(ctx, [&] {
+    if (!ctx->hasGrid) return fail(ctx, VLSG_ERR_STATE, "vlsg_set_grid must come first");
+    if (slot < 0 || slot >= VLSG_MAX_LEVEL_SETS)
+      return fail(ctx, VLSG_ERR_ARGUMENT, "level set slot out of range");
+    if (n < 0 || nRuns < 0 || (n > 0 && (!idx || !values)) ||
+        (nRuns > 0 && (!runStart || !runSign)))
+      return fail(ctx, VLSG_ERR_ARGUMENT, "vlsg_upload_levelset: bad arrays");
+    if (n > INT_MAX / 4) return fail(ctx, VLSG_ERR_ARGUMENT, "too many points");
+    if ((int)ctx->staged.size() <= slot) ctx->staged.resize(slot + 1);
+    StagedLS &s = ctx->staged[slot];
+    s.idx.resize(3 * n);
+    s.vals.resize(n);
+    const GridDev &g = ctx->grid;
+    for (int64_t i = 0; i < n; ++i) {
+      for (int d = 0; d < 3; ++d) {
+        const int c = mapCoord(g, d, idx[3 * i + d]);
+        if (c < -(1 << 19) || c > (1 << 19))
+          return fail(ctx, VLSG_ERR_ARGUMENT, "point index out of the supported range");
+        s.idx[3 * i + d] = c;
+      }
+      s.vals[i] = values[i];
+    }
+    std::vector<std::pair<uint64_t, int8_t>> runs(nRuns);
+    for (int64_t i = 0; i < nRuns; ++i) {
+      int c[3];
+      for (int d = 0; d < 3; ++d) {
+        c[d] = runStart[3 * i + d];
+        c[d] = std::max(-(1 << 20) + 1, std::min((1 << 20) - 1, c[d]));
+      }
+      runs[i] = {hostCellKey(c[0], c[1], c[2]), runSign[i] < 0 ? (int8_t)-1 : (int8_t)1};
+    }
+    std::stable_sort(runs.begin(), runs.end(),
+                     [](const auto &a, const auto &b) { return a.first < b.first; });
+    s.runKeys.resize(nRuns);
+    s.runSign.resize(nRuns);
+    for (int64_t i = 0; i < nRuns; ++i) s.runKeys[i] = runs[i].first, s.runSign[i] = runs[i].second;
+    s.width = width;
+    ctx->dirty = true;
+    return VLSG_OK;
+  });
+}
+
+int vlsg_count_points(vlsg_context *ctx, int32_t slot, int64_t *n) {
+  if (!ctx || !n) return fail(ctx, VLSG_ERR_ARGUMENT, "bad argument");
+  return guarded(ctx, [&] {
+    ensureBuilt(ctx);
+    if (slot < 0 || slot >= (int)ctx->staged.size())
+      return fail(ctx, VLSG_ERR_ARGUMENT, "level set slot out of range");
+    *n = withEngine(ctx, [&](auto &e) { return e.countDefined(slot); });
+    return VLSG_OK;
+  });
+}
+
+int vlsg_download_levelset(vlsg_context *ctx, int32_t slot, int64_t capacity, int32_t *idx,
+                           double *values, int32_t *width) {
+  if (!ctx) return fail(nullptr, VLSG_ERR_ARGUMENT, "NULL context");
+  return guarded(ctx, [&] {
+    ensureBuilt(ctx);
+    if (slot < 0 || slot >= (int)ctx->staged.size())
+      return fail(ctx, VLSG_ERR_ARGUMENT, "level set slot out of range");
+    const int64_t n = withEngine(ctx, [&](auto &e) {
+      if (width) *width = e.buf[slot].width;
+      return e.compact(slot, idx, values, capacity);
+    });
+    if (n > capacity) return fail(ctx, VLSG_ERR_CAPACITY, "download capacity too small");
+    return VLSG_OK;
+  });
+}
+
+int vlsg_get_values(vlsg_context *ctx, int32_t slot, int64_t n, const int32_t *idx,
+                    double *values) {
+  if (!ctx || n < 0 || (n > 0 && (!idx || !values)))
+    return fail(ctx, VLSG_ERR_ARGUMENT, "bad argument");
+  return guarded(ctx, [&] {
+    ensureBuilt(ctx);
+    if (slot < 0 || slot >= (int)ctx->staged.size())
+      return fail(ctx, VLSG_ERR_ARGUMENT, "level set slot out of range");
+    if (n > INT_MAX / 4) return fail(ctx, VLSG_ERR_ARGUMENT, "too many queries");
+    withEngine(ctx, [&](auto &e) {
+      e.queryValues(slot, n, idx, values);
+      return 0;
+    });
+    return VLSG_OK;
+  });
+}
+
+int vlsg_set_velocity_functor(vlsg_context *ctx, const vlsg_velocity_desc *v) {
+  if (!ctx || !v) return fail(ctx, VLSG_ERR_ARGUMENT, "bad argument");
+  if (v->n_materials < 1 || v->n_materials > VLSG_MAX_MATERIALS)
+    return fail(ctx, VLSG_ERR_ARGUMENT, "n_materials out of range");
+  ctx->vel = *v;
+  ctx->hasVel = true;
+  return VLSG_OK;
+}
+
+int vlsg_set_velocity_callback(vlsg_context *ctx, vlsg_velocity_cb cb, void *user) {
+  (void)cb;
+  (void)user;
+  return fail(ctx, VLSG_ERR_ARGUMENT,
+              "host velocity callbacks are not supported by this build; use a device functor");
+}
+
+int vlsg_advect(vlsg_context *ctx, const vlsg_advect_params *p, vlsg_advect_result *r) {
+  if (!ctx || !p || !r) return fail(ctx, VLSG_ERR_ARGUMENT, "bad argument");
+  // Advect::apply validation, lsAdvect.hpp:1019-1027
+  if (ctx->staged.empty()) return fail(ctx, VLSG_ERR_STATE, "No level sets passed to Advect. Not advecting.");
+  if (!ctx->hasVel)
+    return fail(ctx, VLSG_ERR_STATE, "No velocity field passed to Advect. Not advecting.");
+  if (p->ignore_voids) return fail(ctx, VLSG_ERR_ARGUMENT, "setIgnoreVoids(true) is not supported");
+  if (schemeWidth(p->spatial_scheme) < 0)
+    return fail(ctx, VLSG_ERR_ARGUMENT, "Advect: Discretization scheme not found.");
+  if (p->temporal_scheme < 0 || p->temporal_scheme > 2)
+    return fail(ctx, VLSG_ERR_ARGUMENT, "unknown temporal scheme");
+  return guarded(ctx, [&] {
+    ensureBuilt(ctx);
+    withEngine(ctx, [&](auto &e) {
+      e.vel = ctx->vel;
+      e.profiling = ctx->profiling;
+      if (ctx->profiling) e.timers.clear();
+      e.apply(*p, *r);
+      return 0;
+    });
+    return VLSG_OK;
+  });
+}
+
+int vlsg_set_profiling(vlsg_context *ctx, int32_t on) {
+  if (!ctx) return fail(nullptr, VLSG_ERR_ARGUMENT, "NULL context");
+  ctx->profiling = on != 0;
+  return VLSG_OK;
+}
+
+int vlsg_get_kernel_stats(vlsg_context *ctx, int32_t capacity, vlsg_kernel_stat *out,
+                          int32_t *count) {
+  if (!ctx || !count) return fail(ctx, VLSG_ERR_ARGUMENT, "bad argument");
+  auto fill = [&](auto &e) {
+    *count = (int32_t)e.timers.size();
+    for (int i = 0; i < (int)e.timers.size() && i < capacity && out; ++i) {
+      std::memset(&out[i], 0, sizeof(out[i]));
+      std::snprintf(out[i].name, sizeof(out[i].name), "%s", e.timers[i].name.c_str());
+      out[i].launches = e.timers[i].launches;
+      out[i].device_ms = e.timers[i].ms;
+      out[i].algorithmic_bytes = e.timers[i].bytes;
+    }
+    return 0;
+  };
+  if (ctx->precision == VLSG_FP64 && ctx->e64) fill(*ctx->e64);
+  else if (ctx->precision == VLSG_FP32 && ctx->e32) fill(*ctx->e32);
+  else *count = 0;
+  return VLSG_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,153 @@
+// vlsg_common.cuh -- device data layout and helpers of libvlsgpu.
+//
+// Layout in HBM (per context):
+//   * brick map: dense int32 array over a box of 8^3-cell bricks covering the
+//     domain (bounded directions) or the band plus a margin (infinite
+//     directions).  Entry >= 0: slot of an allocated brick; -1: not allocated.
+//   * per level-set buffer and brick: int8 sign of an unallocated brick
+//     (every cell undefined with that sign).
+//   * slot pool: per buffer two value arrays (ping-pong) of slots x 512 cells
+//     (x fastest, then y, then z inside a brick) holding the value in grid
+//     units or +-max for undefined cells, and a state byte per slot
+//     (DENSE, or UNIFORM_POS / UNIFORM_NEG when every cell is undefined with
+//     one sign, so its cells are neither read nor written).
+//   * slot list: compact list of allocated slots, and slot -> brick index.
+// Undefined cells carry the reference's sentinels +-numeric_limits<T>::max()
+// (lsDomain.hpp:51-52) so every rule compares exactly as the reference does.
+#pragma once
+
+#include <cfloat>
+#include <cstdint>
+
+#include "../../include/vlsg.h"
+
+namespace vlsg {
+
+constexpr int BS = 8;           // brick edge
+constexpr int BV = BS * BS * BS; // cells per brick
+constexpr int MAXB = 2 * VLSG_MAX_LEVEL_SETS; // current + initial copies
+
+enum : uint8_t { ST_DENSE = 0, ST_UPOS = 1, ST_UNEG = 2 };
+
+template <class T> struct Lim;
+template <> struct Lim<double> {
+  static __host__ __device__ constexpr double max() { return DBL_MAX; }
+  static __host__ __device__ constexpr double lowest() { return -DBL_MAX; }
+  static __host__ __device__ constexpr double eps() { return DBL_EPSILON; }
+};
+template <> struct Lim<float> {
+  static __host__ __device__ constexpr float max() { return FLT_MAX; }
+  static __host__ __device__ constexpr float lowest() { return -FLT_MAX; }
+  static __host__ __device__ constexpr float eps() { return FLT_EPSILON; }
+};
+
+template <class T> __host__ __device__ inline bool isDef(T v) {
+  return v != Lim<T>::max() && v != Lim<T>::lowest();
+}
+
+// Grid and brick-map geometry, passed by value to kernels.
+struct GridDev {
+  int gmin[3], gmax[3]; // index bounds of the grid
+  int bc[3];            // vlsg_boundary
+  int org[3];           // global cell index of brick (0,0,0), cell (0,0,0)
+  int nb[3];            // bricks per direction in the map box
+  double delta;
+};
+
+__host__ __device__ inline int mapCoord(const GridDev &g, int d, int c) {
+  const int lo = g.gmin[d], hi = g.gmax[d];
+  switch (g.bc[d]) {
+  case VLSG_PERIODIC_BOUNDARY: {
+    const int n = hi - lo;
+    if (c >= lo && c < hi) return c;
+    int r = (c - lo) % n;
+    if (r < 0) r += n;
+    return lo + r;
+  }
+  case VLSG_REFLECTIVE_BOUNDARY:
+    for (int k = 0; k < 4; ++k) {
+      if (c < lo) c = 2 * lo - c;
+      else if (c > hi) c = 2 * hi - c;
+      else break;
+    }
+    return c;
+  case VLSG_POS_INFINITE_BOUNDARY:
+    return c < lo ? 2 * lo - c : c;
+  case VLSG_NEG_INFINITE_BOUNDARY:
+    return c > hi ? 2 * hi - c : c;
+  default:
+    return c;
+  }
+}
+
+// Buffer view: one level set (a current one or an RK initial copy).
+template <class T> struct Buf {
+  const T *vals;          // slot pool values
+  const uint8_t *state;   // per-slot state
+  const int8_t *farSign;  // per-brick sign of unallocated bricks
+};
+
+struct MapView {
+  const int *brickMap;  // brick -> slot or -1
+  const int *slotBrick; // slot -> linear brick index
+};
+
+__device__ inline int brickIndex(const GridDev &g, int bx, int by, int bz) {
+  return (bz * g.nb[1] + by) * g.nb[0] + bx;
+}
+
+// Value of global cell (x,y,z) (already mapped through the boundary
+// conditions).  Cells outside the map box take the value of the nearest box
+// cell: the box keeps a margin of undefined bricks around every band.
+template <class T>
+__device__ inline T cellValue(const GridDev &g, const MapView &m, const Buf<T> &b,
+                              int x, int y, int z) {
+  int rx = x - g.org[0], ry = y - g.org[1], rz = z - g.org[2];
+  const int ex = g.nb[0] * BS - 1, ey = g.nb[1] * BS - 1, ez = g.nb[2] * BS - 1;
+  rx = rx < 0 ? 0 : (rx > ex ? ex : rx);
+  ry = ry < 0 ? 0 : (ry > ey ? ey : ry);
+  rz = rz < 0 ? 0 : (rz > ez ? ez : rz);
+  const int bi = brickIndex(g, rx >> 3, ry >> 3, rz >> 3);
+  const int slot = m.brickMap[bi];
+  if (slot < 0) return b.farSign[bi] < 0 ? Lim<T>::lowest() : Lim<T>::max();
+  const uint8_t st = b.state[slot];
+  if (st != ST_DENSE) return st == ST_UNEG ? Lim<T>::lowest() : Lim<T>::max();
+  return b.vals[(size_t)slot * BV + ((rz & 7) * 64 + (ry & 7) * 8 + (rx & 7))];
+}
+
+template <class T>
+__device__ inline T cellValueRaw(const GridDev &g, const MapView &m,
+                                 const Buf<T> &b, int x, int y, int z) {
+  return cellValue<T>(g, m, b, mapCoord(g, 0, x), mapCoord(g, 1, y),
+                      mapCoord(g, 2, z));
+}
+
+__device__ inline void brickCoords(const GridDev &g, int bi, int &bx, int &by,
+                                   int &bz) {
+  bx = bi % g.nb[0];
+  const int t = bi / g.nb[0];
+  by = t % g.nb[1];
+  bz = t / g.nb[1];
+}
+
+// A cell that exists in the grid (bounded directions have a fixed number of
+// points; the last brick of a direction may hang over the end).
+__device__ inline bool cellExists(const GridDev &g, int x, int y, int z) {
+  const int c[3] = {x, y, z};
+  for (int d = 0; d < 3; ++d) {
+    if (g.bc[d] == VLSG_PERIODIC_BOUNDARY && (c[d] < g.gmin[d] || c[d] >= g.gmax[d]))
+      return false;
+    if (g.bc[d] == VLSG_REFLECTIVE_BOUNDARY && (c[d] < g.gmin[d] || c[d] > g.gmax[d]))
+      return false;
+    if (g.bc[d] == VLSG_POS_INFINITE_BOUNDARY && c[d] < g.gmin[d]) return false;
+    if (g.bc[d] == VLSG_NEG_INFINITE_BOUNDARY && c[d] > g.gmax[d]) return false;
+  }
+  return true;
+}
+
+// Order-preserving 64-bit image of a non-negative double, for atomicMin/Max.
+__device__ inline unsigned long long orderedBits(double v) {
+  return (unsigned long long)__double_as_longlong(v);
+}
+
+} // namespace vlsg

@@ -1,0 +1,873 @@
+// vlsg_engine.cuh -- host orchestration of one context (templated on the
+// storage type T = double or float).  Follows viennals::Advect::apply and
+// the AdvectTimeIntegration schemes (lsAdvect.hpp:199-830,
+// lsAdvectIntegrationSchemes.hpp:46-168) stage by stage, with every
+// level-set operation running as kernels on the context stream.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "vlsg_common.cuh"
+#include "vlsg_maint.cuh"
+#include "vlsg_passes.cuh"
+#include "vlsg_rates.cuh"
+
+namespace vlsg {
+
+struct CudaError : std::runtime_error {
+  int code;
+  CudaError(const std::string &m, int c) : std::runtime_error(m), code(c) {}
+};
+
+#define VLSG_CUDA(x)                                                           \
+  do {                                                                         \
+    cudaError_t e_ = (x);                                                      \
+    if (e_ != cudaSuccess)                                                     \
+      throw vlsg::CudaError(std::string(#x) + ": " + cudaGetErrorString(e_),   \
+                            VLSG_ERR_CUDA);                                    \
+  } while (0)
+
+struct StagedLS {
+  std::vector<int32_t> idx;
+  std::vector<double> vals;
+  std::vector<uint64_t> runKeys;
+  std::vector<int8_t> runSign;
+  int width = 1;
+};
+
+inline uint64_t hostCellKey(int x, int y, int z) {
+  const uint64_t off = 1ull << 20;
+  return ((uint64_t)(z + (int)off) << 42) | ((uint64_t)(y + (int)off) << 21) |
+         (uint64_t)(x + (int)off);
+}
+
+struct KernelTimer {
+  std::string name;
+  uint64_t launches = 0;
+  double ms = 0;
+  double bytes = 0;
+};
+
+// Expand width of each scheme's prepareLS (lsEngquistOsher.hpp:31,
+// lsLaxFriedrichs.hpp:225, lsLocalLocalLaxFriedrichs.hpp:288,
+// lsLocalLaxFriedrichs.hpp:55, lsWENO.hpp:44).
+inline int schemeWidth(int s) {
+  switch (s) {
+  case VLSG_ENGQUIST_OSHER_1ST_ORDER: return 3;
+  case VLSG_ENGQUIST_OSHER_2ND_ORDER: return 5;
+  case VLSG_LAX_FRIEDRICHS_1ST_ORDER: return 3;
+  case VLSG_LAX_FRIEDRICHS_2ND_ORDER: return 5;
+  case VLSG_LOCAL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER: return 3;
+  case VLSG_LOCAL_LOCAL_LAX_FRIEDRICHS_2ND_ORDER: return 5;
+  case VLSG_LOCAL_LAX_FRIEDRICHS_1ST_ORDER: return 7;
+  case VLSG_LOCAL_LAX_FRIEDRICHS_2ND_ORDER: return 9;
+  case VLSG_WENO_3RD_ORDER: return 5;
+  case VLSG_WENO_5TH_ORDER: return 7;
+  default: return -1;
+  }
+}
+
+template <class T> class Engine {
+public:
+  cudaStream_t stream = nullptr;
+  GridDev g{};
+  int L = 0;
+  int nBricks = 0;
+  int cap = 0;      // slot capacity
+  size_t activeCap = 0;
+  // device arrays
+  int *brickMap = nullptr, *slotBrick = nullptr, *slotList = nullptr;
+  int *freeStack = nullptr;
+  int *counters = nullptr; // 0 nSlots, 1 freeCount, 2 nActive, 3 err, 4 flag, 5 nOut
+  uint8_t *needed = nullptr;
+  unsigned long long *scal = nullptr; // 0 minStep, 1..3 alphas
+  struct DBuf {
+    T *vals[2] = {nullptr, nullptr};
+    uint8_t *state[2] = {nullptr, nullptr};
+    int cur = 0;
+    uint8_t *hasDef = nullptr;
+    int8_t *farSign = nullptr;
+    int width = 1;
+    bool live = false;
+    int64_t nDef = 0; // defined cells (kept up to date in profiling mode)
+  };
+  DBuf buf[MAXB];
+  T *rateV = nullptr, *rateStop = nullptr;
+  uint8_t *rateLen = nullptr;
+  uint32_t *active = nullptr;
+  // host mirrors
+  int hCounters[8];
+  unsigned long long hScal[4];
+  int *pinCounters = nullptr;
+  unsigned long long *pinScal = nullptr;
+  // bookkeeping
+  uint64_t launches = 0;
+  int64_t lastBand = 0, lastActive = 0; // profiling: band / active cells of the stage
+  uint64_t pointUpdates = 0;
+  uint32_t stages = 0;
+  double currentTimeStep = -1.;
+  vlsg_velocity_desc vel{};
+  bool profiling = false;
+  std::vector<KernelTimer> timers;
+  int blocksPass = 148 * 8;
+
+  ~Engine() { release(); }
+
+  void release() {
+    auto f = [](void *p) { if (p) cudaFree(p); };
+    f(brickMap); f(slotBrick); f(slotList); f(freeStack); f(counters); f(needed);
+    f(scal); f(rateV); f(rateStop); f(rateLen); f(active);
+    for (auto &b : buf) {
+      f(b.vals[0]); f(b.vals[1]); f(b.state[0]); f(b.state[1]); f(b.hasDef); f(b.farSign);
+      b = DBuf();
+    }
+    if (pinCounters) cudaFreeHost(pinCounters);
+    if (pinScal) cudaFreeHost(pinScal);
+    brickMap = slotBrick = slotList = freeStack = counters = nullptr;
+    needed = nullptr; scal = nullptr; rateV = rateStop = nullptr; rateLen = nullptr;
+    active = nullptr; pinCounters = nullptr; pinScal = nullptr;
+  }
+
+  MapView mapView() const { return MapView{brickMap, slotBrick}; }
+  Buf<T> view(int b) const {
+    return Buf<T>{buf[b].vals[buf[b].cur], buf[b].state[buf[b].cur], buf[b].farSign};
+  }
+  PassOut<T> outOf(int b) {
+    const int o = 1 - buf[b].cur;
+    return PassOut<T>{buf[b].vals[o], buf[b].state[o], buf[b].hasDef, defCounter()};
+  }
+  void flip(int b) { buf[b].cur = 1 - buf[b].cur; }
+  int *nSlotsPtr() { return counters + 0; }
+  int *freeCountPtr() { return counters + 1; }
+  int *nActivePtr() { return counters + 2; }
+  int *errPtr() { return counters + 3; }
+  int *flagPtr() { return counters + 4; }
+  int *nOutPtr() { return counters + 5; }
+
+  // ---------------------------------------------------------------- timing
+  // One kernel launch.  With profiling on it is bracketed by CUDA events on
+  // the context stream and, after the kernel finished, `bytesFn` turns the
+  // device counters into the launch's algorithmic bytes.
+  struct Scope {
+    Engine *e;
+    int idx;
+    cudaEvent_t a, b;
+    std::function<double()> bytesFn;
+    Scope(Engine *eng, const char *name, std::function<double()> fn = nullptr)
+        : e(eng), idx(-1), bytesFn(std::move(fn)) {
+      ++e->launches;
+      if (!e->profiling) return;
+      for (size_t i = 0; i < e->timers.size(); ++i)
+        if (e->timers[i].name == name) idx = (int)i;
+      if (idx < 0) {
+        e->timers.push_back(KernelTimer{name});
+        idx = (int)e->timers.size() - 1;
+      }
+      e->timers[idx].launches++;
+      cudaMemsetAsync(e->counters + 6, 0, 2 * sizeof(unsigned long long), e->stream);
+      cudaEventCreate(&a);
+      cudaEventCreate(&b);
+      cudaEventRecord(a, e->stream);
+    }
+    ~Scope() {
+      if (!e->profiling || idx < 0) return;
+      cudaEventRecord(b, e->stream);
+      cudaEventSynchronize(b);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, a, b);
+      e->timers[idx].ms += ms;
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
+      if (bytesFn) e->timers[idx].bytes += bytesFn();
+    }
+  };
+  // Defined cells counted by the last launch (profiling mode only).
+  unsigned long long defCounted() {
+    unsigned long long v = 0;
+    cudaMemcpy(&v, counters + 6, sizeof(v), cudaMemcpyDeviceToHost);
+    return v;
+  }
+  unsigned long long bandCounted() {
+    unsigned long long v = 0;
+    cudaMemcpy(&v, counters + 8, sizeof(v), cudaMemcpyDeviceToHost);
+    return v;
+  }
+  unsigned long long *defCounter() { return (unsigned long long *)(counters + 6); }
+  unsigned long long *bandCounter() { return (unsigned long long *)(counters + 8); }
+  // Bytes of a band pass in the survey's accounting: value + 64-bit key,
+  // read once and written once per band point.
+  double bandPassBytes(int64_t nIn, int64_t nOut) const {
+    return double(sizeof(T) + 8) * double(nIn + nOut);
+  }
+  void checkLaunch() { VLSG_CUDA(cudaGetLastError()); }
+
+  // ------------------------------------------------------------- layout
+  void allocBuffers(int nb) {
+    const size_t cells = (size_t)cap * BV;
+    for (int b = 0; b < nb; ++b) {
+      auto &B = buf[b];
+      if (B.vals[0]) continue;
+      VLSG_CUDA(cudaMalloc(&B.vals[0], cells * sizeof(T)));
+      VLSG_CUDA(cudaMalloc(&B.vals[1], cells * sizeof(T)));
+      VLSG_CUDA(cudaMalloc(&B.state[0], cap));
+      VLSG_CUDA(cudaMalloc(&B.state[1], cap));
+      VLSG_CUDA(cudaMalloc(&B.hasDef, cap));
+      VLSG_CUDA(cudaMalloc(&B.farSign, nBricks));
+      VLSG_CUDA(cudaMemsetAsync(B.hasDef, 0, cap, stream));
+      VLSG_CUDA(cudaMemsetAsync(B.state[0], ST_UPOS, cap, stream));
+      VLSG_CUDA(cudaMemsetAsync(B.state[1], ST_UPOS, cap, stream));
+      B.cur = 0;
+    }
+  }
+
+  // The live buffers (current level sets and the RK copies in use).
+  BufSet bufSet() {
+    BufSet s{};
+    s.elem = sizeof(T);
+    int k = 0;
+    for (int b = 0; b < 2 * L; ++b) {
+      if (!buf[b].live || !buf[b].vals[0]) continue;
+      s.hasDef[k] = buf[b].hasDef;
+      s.hasDefW[k] = buf[b].hasDef;
+      s.state[k] = buf[b].state[buf[b].cur];
+      s.farSign[k] = buf[b].farSign;
+      s.vals[k] = buf[b].vals[buf[b].cur];
+      ++k;
+    }
+    s.nBuf = k;
+    return s;
+  }
+
+  void build(const GridDev &grid, std::vector<StagedLS> &ls, int margin) {
+    release();
+    VLSG_CUDA(cudaHostAlloc(&pinCounters, 8 * sizeof(int), cudaHostAllocDefault));
+    VLSG_CUDA(cudaHostAlloc(&pinScal, 4 * sizeof(unsigned long long), cudaHostAllocDefault));
+    g = grid;
+    L = (int)ls.size();
+    // box: bounded directions cover the grid, infinite ones the points + margin
+    long long lo[3], hi[3];
+    for (int d = 0; d < 3; ++d) lo[d] = LLONG_MAX, hi[d] = LLONG_MIN;
+    for (auto &s : ls)
+      for (size_t i = 0; i < s.vals.size(); ++i)
+        for (int d = 0; d < 3; ++d) {
+          lo[d] = std::min<long long>(lo[d], s.idx[3 * i + d]);
+          hi[d] = std::max<long long>(hi[d], s.idx[3 * i + d]);
+        }
+    for (int d = 0; d < 3; ++d) {
+      const bool bounded = g.bc[d] == VLSG_PERIODIC_BOUNDARY || g.bc[d] == VLSG_REFLECTIVE_BOUNDARY;
+      if (bounded) {
+        g.org[d] = g.gmin[d];
+        const int n = g.bc[d] == VLSG_PERIODIC_BOUNDARY ? g.gmax[d] - g.gmin[d]
+                                                       : g.gmax[d] - g.gmin[d] + 1;
+        g.nb[d] = (n + BS - 1) / BS;
+      } else {
+        if (lo[d] > hi[d]) lo[d] = hi[d] = 0;
+        const long long a = lo[d] - (long long)margin * BS;
+        const long long b = hi[d] + (long long)margin * BS;
+        const long long a8 = (a >= 0) ? (a / BS) * BS : -(((-a) + BS - 1) / BS) * BS;
+        g.org[d] = (int)a8;
+        g.nb[d] = (int)((b - a8) / BS + 1);
+      }
+    }
+    nBricks = g.nb[0] * g.nb[1] * g.nb[2];
+    VLSG_CUDA(cudaMalloc(&brickMap, nBricks * sizeof(int)));
+    VLSG_CUDA(cudaMalloc(&needed, nBricks));
+    VLSG_CUDA(cudaMalloc(&counters, 16 * sizeof(int)));
+    VLSG_CUDA(cudaMemsetAsync(counters, 0, 16 * sizeof(int), stream));
+    VLSG_CUDA(cudaMalloc(&scal, 4 * sizeof(unsigned long long)));
+    VLSG_CUDA(cudaMemsetAsync(counters, 0, 8 * sizeof(int), stream));
+    VLSG_CUDA(cudaMemsetAsync(brickMap, 0xff, nBricks * sizeof(int), stream));
+    VLSG_CUDA(cudaMemsetAsync(needed, 0, nBricks, stream));
+    // mark point bricks of every level set, dilate
+    uint8_t *core = nullptr;
+    VLSG_CUDA(cudaMalloc(&core, nBricks));
+    VLSG_CUDA(cudaMemsetAsync(core, 0, nBricks, stream));
+    std::vector<int *> dIdx(L, nullptr);
+    std::vector<double *> dVal(L, nullptr);
+    std::vector<uint64_t *> dRunK(L, nullptr);
+    std::vector<int8_t *> dRunS(L, nullptr);
+    for (int l = 0; l < L; ++l) {
+      auto &s = ls[l];
+      const size_t n = s.vals.size();
+      VLSG_CUDA(cudaMalloc(&dIdx[l], std::max<size_t>(1, n) * 3 * sizeof(int)));
+      VLSG_CUDA(cudaMalloc(&dVal[l], std::max<size_t>(1, n) * sizeof(double)));
+      VLSG_CUDA(cudaMalloc(&dRunK[l], std::max<size_t>(1, s.runKeys.size()) * sizeof(uint64_t)));
+      VLSG_CUDA(cudaMalloc(&dRunS[l], std::max<size_t>(1, s.runSign.size())));
+      if (n) {
+        VLSG_CUDA(cudaMemcpyAsync(dIdx[l], s.idx.data(), n * 3 * sizeof(int), cudaMemcpyHostToDevice, stream));
+        VLSG_CUDA(cudaMemcpyAsync(dVal[l], s.vals.data(), n * sizeof(double), cudaMemcpyHostToDevice, stream));
+      }
+      if (!s.runKeys.empty()) {
+        VLSG_CUDA(cudaMemcpyAsync(dRunK[l], s.runKeys.data(), s.runKeys.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, stream));
+        VLSG_CUDA(cudaMemcpyAsync(dRunS[l], s.runSign.data(), s.runSign.size(), cudaMemcpyHostToDevice, stream));
+      }
+      if (n) {
+        Scope sc(this, "upload_mark");
+        kMarkPointBricks<<<grid1(n), 256, 0, stream>>>(g, (int)n, dIdx[l], core, errPtr());
+        checkLaunch();
+      }
+    }
+    {
+      Scope sc(this, "upload_dilate");
+      kDilateBricks<<<grid1(nBricks), 256, 0, stream>>>(g, nBricks, core, needed, errPtr());
+      checkLaunch();
+    }
+    // count needed bricks to size the pool
+    std::vector<uint8_t> hNeeded(nBricks);
+    VLSG_CUDA(cudaMemcpyAsync(hNeeded.data(), needed, nBricks, cudaMemcpyDeviceToHost, stream));
+    syncErr("upload");
+    long long nNeeded = 0;
+    for (auto v : hNeeded) nNeeded += v;
+    cap = (int)std::max<long long>(1024, nNeeded * 2 + 256);
+    activeCap = (size_t)cap * 160;
+    VLSG_CUDA(cudaMalloc(&slotBrick, cap * sizeof(int)));
+    VLSG_CUDA(cudaMalloc(&slotList, cap * sizeof(int)));
+    VLSG_CUDA(cudaMalloc(&freeStack, cap * sizeof(int)));
+    VLSG_CUDA(cudaMemsetAsync(slotBrick, 0xff, cap * sizeof(int), stream));
+    {
+      std::vector<int> fs(cap);
+      for (int i = 0; i < cap; ++i) fs[i] = cap - 1 - i;
+      VLSG_CUDA(cudaMemcpyAsync(freeStack, fs.data(), cap * sizeof(int), cudaMemcpyHostToDevice, stream));
+      int c[2] = {0, cap};
+      VLSG_CUDA(cudaMemcpyAsync(counters, c, 2 * sizeof(int), cudaMemcpyHostToDevice, stream));
+      VLSG_CUDA(cudaStreamSynchronize(stream));
+    }
+    allocBuffers(L);
+    for (int l = 0; l < L; ++l) {
+      Scope sc(this, "upload_farsign");
+      kFarSignFromRuns<<<grid1(nBricks), 256, 0, stream>>>(
+          g, nBricks, dRunK[l], dRunS[l], (int)ls[l].runKeys.size(), buf[l].farSign);
+      checkLaunch();
+      buf[l].width = ls[l].width;
+      buf[l].live = true;
+    }
+    {
+      Scope sc(this, "alloc");
+      kAllocNeeded<<<grid1(nBricks), 256, 0, stream>>>(nBricks, brickMap, slotBrick, needed,
+                                                       bufSet(), freeStack, freeCountPtr(), errPtr());
+      checkLaunch();
+    }
+    rebuildSlotList();
+    for (int l = 0; l < L; ++l) {
+      auto &s = ls[l];
+      {
+        Scope sc(this, "upload_fill");
+        kFillFromRuns<T><<<blocksPass, 256, 0, stream>>>(g, slotList, nSlotsPtr(), slotBrick, dRunK[l],
+                                                         dRunS[l], (int)s.runKeys.size(),
+                                                         buf[l].vals[buf[l].cur]);
+        checkLaunch();
+      }
+      if (!s.vals.empty()) {
+        Scope sc(this, "upload_scatter");
+        kScatterPoints<T><<<grid1(s.vals.size()), 256, 0, stream>>>(
+            g, (int)s.vals.size(), dIdx[l], dVal[l], brickMap, buf[l].vals[buf[l].cur], errPtr());
+        checkLaunch();
+      }
+      {
+        VLSG_CUDA(cudaMemsetAsync(defCounter(), 0, sizeof(unsigned long long), stream));
+        Scope sc(this, "upload_normalize");
+        kNormalize<T><<<blocksPass, 256, 0, stream>>>(g, slotList, nSlotsPtr(), slotBrick,
+                                                      buf[l].vals[buf[l].cur],
+                                                      buf[l].state[buf[l].cur], buf[l].hasDef,
+                                                      defCounter());
+        checkLaunch();
+      }
+      VLSG_CUDA(cudaStreamSynchronize(stream));
+      buf[l].nDef = (int64_t)defCounted();
+    }
+    syncErr("upload");
+    for (int l = 0; l < L; ++l) {
+      cudaFree(dIdx[l]);
+      cudaFree(dVal[l]);
+      cudaFree(dRunK[l]);
+      cudaFree(dRunS[l]);
+    }
+    cudaFree(core);
+    const size_t cells = (size_t)cap * BV;
+    VLSG_CUDA(cudaMalloc(&rateV, cells * sizeof(T) * L));
+    VLSG_CUDA(cudaMalloc(&rateStop, cells * sizeof(T) * L));
+    VLSG_CUDA(cudaMalloc(&rateLen, cells));
+    VLSG_CUDA(cudaMalloc(&active, activeCap * sizeof(uint32_t)));
+  }
+
+  static int grid1(size_t n) {
+    size_t b = (n + 255) / 256;
+    if (b < 1) b = 1;
+    if (b > 148 * 32) b = 148 * 32;
+    return (int)b;
+  }
+
+  void syncErr(const char *where) {
+    VLSG_CUDA(cudaMemcpyAsync(pinCounters, counters, 8 * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    VLSG_CUDA(cudaStreamSynchronize(stream));
+    std::memcpy(hCounters, pinCounters, sizeof(hCounters));
+    const int e = hCounters[3];
+    if (e) {
+      std::string m = std::string(where) + ": device check failed:";
+      if (e & 1) m += " band reached the edge of the brick box (infinite direction);";
+      if (e & 2) m += " stop chain overran;";
+      if (e & 4) m += " brick pool capacity exceeded;";
+      if (e & 8) m += " freed brick held a defined point;";
+      if (e & 16) m += " active list capacity exceeded;";
+      int z = 0;
+      cudaMemcpy(errPtr(), &z, sizeof(int), cudaMemcpyHostToDevice);
+      throw CudaError(m, (e & (4 | 16)) ? VLSG_ERR_CAPACITY : VLSG_ERR_DEVICE_CHECK);
+    }
+  }
+
+  void rebuildSlotList() {
+    VLSG_CUDA(cudaMemsetAsync(nSlotsPtr(), 0, sizeof(int), stream));
+    Scope sc(this, "slot_list");
+    kBuildSlotList<<<grid1(nBricks), 256, 0, stream>>>(nBricks, brickMap, slotList, nSlotsPtr());
+    checkLaunch();
+  }
+
+  // Bring the allocated bricks back to dilate(core) of the live buffers.
+  void maintain() {
+    VLSG_CUDA(cudaMemsetAsync(needed, 0, nBricks, stream));
+    {
+      Scope sc(this, "maint_mark");
+      kMarkNeeded<<<grid1(cap), 256, 0, stream>>>(g, slotBrick, slotList, nSlotsPtr(),
+                                                  bufSet(), needed, errPtr());
+      checkLaunch();
+    }
+    {
+      Scope sc(this, "maint_free");
+      kFreeUnneeded<T><<<grid1(cap), 256, 0, stream>>>(slotList, nSlotsPtr(), brickMap, slotBrick,
+                                                       needed, bufSet(), freeStack,
+                                                       freeCountPtr(), errPtr());
+      checkLaunch();
+    }
+    {
+      Scope sc(this, "maint_alloc");
+      kAllocNeeded<<<grid1(nBricks), 256, 0, stream>>>(nBricks, brickMap, slotBrick, needed,
+                                                       bufSet(), freeStack, freeCountPtr(),
+                                                       errPtr());
+      checkLaunch();
+    }
+    rebuildSlotList();
+  }
+
+  // --------------------------------------------------------------- passes
+  template <class Rule> void starPass(int b, Rule rule, const char *name) {
+    const int64_t nIn = buf[b].nDef;
+    {
+      Scope sc(this, name, [this, b, nIn] {
+        buf[b].nDef = (int64_t)defCounted();
+        return bandPassBytes(nIn, buf[b].nDef);
+      });
+      kStarPass<T, Rule><<<blocksPass, PASS_THREADS, 0, stream>>>(g, mapView(), slotList, nSlotsPtr(),
+                                                                  view(b), outOf(b), rule);
+      checkLaunch();
+    }
+    flip(b);
+  }
+
+  // Expand::apply (lsExpand.hpp:44-172)
+  void expand(int b, int width) {
+    if (width <= buf[b].width) return;
+    const int startWidth = buf[b].width;
+    const T totalLimit = T(width * 0.5);
+    for (int c = 0; c < width - startWidth; ++c) {
+      ExpandRule<T> r{totalLimit, T((startWidth + c + 1) * T(0.5))};
+      starPass(b, r, "expand");
+    }
+    buf[b].width = width;
+  }
+  void prune(int b, bool rsz) {
+    starPass(b, PruneRule<T>{rsz}, "prune");
+    buf[b].width = 2;
+  }
+  void rebuild(int b) {
+    starPass(b, RebuildRule<T>{1.0}, "rebuild");
+    buf[b].width = 2;
+  }
+  template <class Comp> void pointwise(int a, int bb, Comp comp, int *flag) {
+    {
+      const int64_t nA = buf[a].nDef, nB = buf[bb].nDef;
+      Scope sc(this, "boolean", [this, a, nA, nB] {
+        buf[a].nDef = (int64_t)defCounted();
+        return bandPassBytes(nA + nB, buf[a].nDef);
+      });
+      kPointwise2<T, Comp><<<blocksPass, PASS_THREADS, 0, stream>>>(g, mapView(), slotList, nSlotsPtr(),
+                                                                    view(a), view(bb), outOf(a), comp, flag);
+      checkLaunch();
+    }
+    {
+      Scope sc(this, "boolean_far");
+      kPointwise2FarSign<T, Comp><<<grid1(nBricks), 256, 0, stream>>>(nBricks, buf[a].farSign,
+                                                                      buf[bb].farSign, buf[a].farSign, comp);
+      checkLaunch();
+    }
+    flip(a);
+  }
+  // BooleanOperation + Prune x2 (lsBooleanOperation.hpp:199-212)
+  template <class Comp> void booleanOp(int a, int bb, Comp comp, int *flag = nullptr) {
+    pointwise(a, bb, comp, flag);
+    prune(a, true);
+    prune(a, false);
+  }
+
+  void copyBuffer(int src, int dst) {
+    allocBuffers(dst + 1);
+    auto &S = buf[src];
+    auto &D = buf[dst];
+    {
+      Scope sc(this, "copy");
+      kCopySlots<T><<<blocksPass, 256, 0, stream>>>(slotList, nSlotsPtr(), S.vals[S.cur], S.state[S.cur],
+                                                    S.hasDef, D.vals[D.cur], D.state[D.cur], D.hasDef);
+      checkLaunch();
+    }
+    VLSG_CUDA(cudaMemcpyAsync(D.farSign, S.farSign, nBricks, cudaMemcpyDeviceToDevice, stream));
+    D.width = S.width;
+    D.nDef = S.nDef;
+    D.live = true;
+  }
+
+  // --------------------------------------------------------- one FE stage
+  // integrateTime + findGlobalAlphas + reduceTimeStepHamiltonJacobi
+  double computeRates(const vlsg_advect_params &P, double maxTimeStep) {
+    const int top = L - 1;
+    const int w = schemeWidth(P.spatial_scheme);
+    if (w < 0) throw CudaError("Advect: Discretization scheme not found.", VLSG_ERR_ARGUMENT);
+    expand(top, w); // prepareLS
+    VLSG_CUDA(cudaMemsetAsync(nActivePtr(), 0, sizeof(int), stream));
+    {
+      Scope sc(this, "compact_active", [this] {
+        lastBand = (int64_t)bandCounted();
+        return double(sizeof(T)) * double(lastBand);
+      });
+      kCompactActive<T><<<blocksPass, RATE_THREADS, 0, stream>>>(slotList, nSlotsPtr(), view(top),
+                                                                 active, nActivePtr(),
+                                                                 (int)activeCap, errPtr(),
+                                                                 bandCounter());
+      checkLaunch();
+    }
+    RateArgs<T> A{};
+    A.g = g;
+    A.m = mapView();
+    for (int l = 0; l < L; ++l) A.ls[l] = view(l);
+    A.L = L;
+    A.active = active;
+    A.nActive = nActivePtr();
+    A.activeCap = (int)activeCap;
+    A.scheme = P.spatial_scheme;
+    A.cfl = P.time_step_ratio;
+    A.dissipationAlpha = P.dissipation_alpha;
+    A.calcNormals = P.calculate_normal_vectors;
+    A.adaptive = P.adaptive_time_stepping;
+    A.adaptiveFactor = 1.0 / (P.adaptive_subdivisions < 1 ? 1u : P.adaptive_subdivisions);
+    A.checkDiss = P.check_dissipation;
+    A.rateV = rateV;
+    A.rateStop = rateStop;
+    A.rateLen = rateLen;
+    A.poolCells = (size_t)cap * BV;
+    A.minStep = scal;
+    A.err = errPtr();
+    const int s = P.spatial_scheme;
+    const bool globalLF = s == VLSG_LAX_FRIEDRICHS_1ST_ORDER || s == VLSG_LAX_FRIEDRICHS_2ND_ORDER;
+    const bool lfFamily = !(s == VLSG_ENGQUIST_OSHER_1ST_ORDER || s == VLSG_ENGQUIST_OSHER_2ND_ORDER ||
+                            s == VLSG_WENO_3RD_ORDER || s == VLSG_WENO_5TH_ORDER);
+    unsigned long long init[4] = {~0ull, 0, 0, 0};
+    VLSG_CUDA(cudaMemcpyAsync(scal, init, sizeof(init), cudaMemcpyHostToDevice, stream));
+    double alphas[3] = {0, 0, 0};
+    const int rateBlocks = 148 * 8;
+    if (globalLF) {
+      A.alphaMax = scal + 1;
+      {
+        Scope sc(this, "global_alphas");
+        kGlobalAlphas<T><<<rateBlocks, RATE_THREADS, 0, stream>>>(A, vel);
+        checkLaunch();
+      }
+      VLSG_CUDA(cudaMemcpyAsync(pinScal, scal, sizeof(init), cudaMemcpyDeviceToHost, stream));
+      VLSG_CUDA(cudaStreamSynchronize(stream));
+      for (int k = 0; k < 3; ++k) {
+        double a;
+        std::memcpy(&a, &pinScal[1 + k], 8);
+        alphas[k] = a;
+        A.globalAlpha[k] = T(a);
+      }
+      A.alphaMax = nullptr;
+    } else if (lfFamily) {
+      A.alphaMax = scal + 1;
+    } else {
+      A.alphaMax = nullptr;
+    }
+    {
+      // stencil input (each band value once) + output per active point
+      Scope sc(this, "rates", [this] {
+        int nAct = 0;
+        cudaMemcpy(&nAct, nActivePtr(), sizeof(int), cudaMemcpyDeviceToHost);
+        lastActive = nAct;
+        return double(sizeof(T)) * double(lastBand + nAct);
+      });
+      kRates<T><<<rateBlocks, RATE_THREADS, 0, stream>>>(A, vel);
+      checkLaunch();
+    }
+    VLSG_CUDA(cudaMemcpyAsync(pinScal, scal, sizeof(init), cudaMemcpyDeviceToHost, stream));
+    syncErr("rates");
+    std::memcpy(hScal, pinScal, sizeof(hScal));
+    if ((size_t)hCounters[2] > activeCap)
+      throw CudaError("active list capacity exceeded", VLSG_ERR_CAPACITY);
+    pointUpdates += (uint64_t)hCounters[2];
+    double tempMax = maxTimeStep;
+    if (hScal[0] != ~0ull) {
+      double m;
+      std::memcpy(&m, &hScal[0], 8);
+      if (m < tempMax) tempMax = m;
+    }
+    if (lfFamily) {
+      double fa[3];
+      if (globalLF) {
+        for (int k = 0; k < 3; ++k) fa[k] = alphas[k];
+      } else {
+        for (int k = 0; k < 3; ++k) std::memcpy(&fa[k], &hScal[1 + k], 8);
+      }
+      double timeStep = 0;
+      for (int i = 0; i < 3; ++i) timeStep += fa[i] / g.delta;
+      timeStep = 1.0 / timeStep;
+      tempMax = (tempMax < timeStep) ? tempMax : timeStep;
+    }
+    if (tempMax < maxTimeStep) maxTimeStep = tempMax;
+    currentTimeStep = maxTimeStep;
+    return maxTimeStep;
+  }
+
+  void updateLevelSet(double dt) {
+    const int top = L - 1;
+    UpdateArgs<T> U{};
+    U.g = g;
+    U.m = mapView();
+    U.slotList = slotList;
+    U.nSlots = nSlotsPtr();
+    U.vals = buf[top].vals[buf[top].cur];
+    U.state = buf[top].state[buf[top].cur];
+    U.hasDef = buf[top].hasDef;
+    U.rateV = rateV;
+    U.rateStop = rateStop;
+    U.rateLen = rateLen;
+    U.poolCells = (size_t)cap * BV;
+    U.L = L;
+    U.dt = dt;
+    U.err = errPtr();
+    U.defCount = defCounter();
+    {
+      // active values read and written, their rates read
+      Scope sc(this, "update", [this, top] {
+        buf[top].nDef = (int64_t)defCounted();
+        return 3.0 * double(sizeof(T)) * double(lastActive);
+      });
+      kUpdate<T><<<blocksPass, RATE_THREADS, 0, stream>>>(U);
+      checkLaunch();
+    }
+    if (buf[top].width > 1) buf[top].width = 1; // Reduce(1), lsReduce.hpp:241-242
+    ++stages;
+  }
+
+  void adjustLowerLayers(const vlsg_advect_params &P) {
+    if (P.spatial_scheme == VLSG_STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER) return;
+    for (int i = 0; i + 1 < L; ++i) booleanOp(i, L - 1, MaxComp<T>{});
+  }
+
+  double evolveForwardEuler(const vlsg_advect_params &P, double maxTimeStep,
+                            bool updateLowerLayers) {
+    const double dt = computeRates(P, maxTimeStep);
+    updateLevelSet(dt);
+    rebuild(L - 1);
+    maintain();
+    if (updateLowerLayers) adjustLowerLayers(P);
+    return dt;
+  }
+
+  bool combineLevelSets(const vlsg_advect_params &P, double wTarget, double wSource) {
+    int steps = 1;
+    if (P.temporal_scheme == VLSG_RUNGE_KUTTA_2ND_ORDER) steps = 2;
+    else if (P.temporal_scheme == VLSG_RUNGE_KUTTA_3RD_ORDER) steps = 3;
+    const int expansionWidth = (int)std::ceil(2.0 * steps * P.time_step_ratio + 1);
+    const int top = L - 1, init = 2 * L - 1;
+    expand(top, expansionWidth);
+    expand(init, expansionWidth);
+    VLSG_CUDA(cudaMemsetAsync(flagPtr(), 0, sizeof(int), stream));
+    CombineComp<T> comp{wTarget, wSource};
+    pointwise(top, init, comp, flagPtr());
+    prune(top, true);
+    prune(top, false);
+    rebuild(top);
+    maintain();
+    if (L > 1) {
+      VLSG_CUDA(cudaMemcpyAsync(pinCounters, counters, 8 * sizeof(int), cudaMemcpyDeviceToHost, stream));
+      VLSG_CUDA(cudaStreamSynchronize(stream));
+      return pinCounters[4] != 0;
+    }
+    return false;
+  }
+
+  void saveInitial(bool all) {
+    for (int l = all ? 0 : L - 1; l < L; ++l) copyBuffer(l, L + l);
+  }
+  void restoreLower() {
+    for (int l = 0; l + 1 < L; ++l) {
+      // copy initial back into the current buffer
+      auto &S = buf[L + l];
+      auto &D = buf[l];
+      Scope sc(this, "copy");
+      kCopySlots<T><<<blocksPass, 256, 0, stream>>>(slotList, nSlotsPtr(), S.vals[S.cur], S.state[S.cur],
+                                                    S.hasDef, D.vals[D.cur], D.state[D.cur], D.hasDef);
+      checkLaunch();
+      VLSG_CUDA(cudaMemcpyAsync(D.farSign, S.farSign, nBricks, cudaMemcpyDeviceToDevice, stream));
+      D.width = S.width;
+      D.nDef = S.nDef;
+    }
+  }
+
+  // Recount the defined cells of every live buffer (profiling bookkeeping).
+  void recountDefined() {
+    for (int b = 0; b < 2 * L; ++b) {
+      if (!buf[b].live || !buf[b].vals[0]) continue;
+      VLSG_CUDA(cudaMemsetAsync(defCounter(), 0, sizeof(unsigned long long), stream));
+      kCountDefined<T><<<blocksPass, 256, 0, stream>>>(slotList, nSlotsPtr(), buf[b].vals[buf[b].cur],
+                                                       buf[b].state[buf[b].cur], defCounter());
+      checkLaunch();
+      VLSG_CUDA(cudaStreamSynchronize(stream));
+      buf[b].nDef = (int64_t)defCounted();
+    }
+  }
+
+  double evolveRungeKutta2(const vlsg_advect_params &P, double maxTimeStep) {
+    saveInitial(false);
+    const double dt1 = evolveForwardEuler(P, maxTimeStep, false);
+    if (dt1 <= 0.) return 0.;
+    const double dt2 = evolveForwardEuler(P, dt1, false);
+    combineLevelSets(P, 0.5, 0.5);
+    adjustLowerLayers(P);
+    return 0.5 * dt1 + 0.5 * dt2;
+  }
+  double evolveRungeKutta3(const vlsg_advect_params &P, double maxTimeStep) {
+    saveInitial(true);
+    const double dt1 = evolveForwardEuler(P, maxTimeStep, false);
+    if (dt1 <= 0.) return 0.;
+    const double dt2 = evolveForwardEuler(P, dt1, false);
+    combineLevelSets(P, 0.75, 0.25);
+    adjustLowerLayers(P);
+    const double dt3 = evolveForwardEuler(P, dt1, false);
+    const bool etched2 = combineLevelSets(P, 1.0 / 3.0, 2.0 / 3.0);
+    if (etched2) restoreLower();
+    adjustLowerLayers(P);
+    return (dt1 + dt2 + 4.0 * dt3) / 6.0;
+  }
+  double advect(const vlsg_advect_params &P, double maxTimeStep) {
+    switch (P.temporal_scheme) {
+    case VLSG_RUNGE_KUTTA_2ND_ORDER: return evolveRungeKutta2(P, maxTimeStep);
+    case VLSG_RUNGE_KUTTA_3RD_ORDER: return evolveRungeKutta3(P, maxTimeStep);
+    default: return evolveForwardEuler(P, maxTimeStep, true);
+    }
+  }
+
+  void apply(const vlsg_advect_params &P, vlsg_advect_result &r) {
+    if (profiling) recountDefined();
+    pointUpdates = 0;
+    stages = 0;
+    const uint64_t l0 = launches;
+    double advectedTime = 0.;
+    unsigned steps = 0;
+    const uint32_t maxSteps = P.max_steps ? P.max_steps : 10000000u;
+    if (P.advection_time == 0.) {
+      advectedTime = advect(P, std::numeric_limits<double>::max());
+      steps = 1;
+    } else {
+      double currentTime = 0.0;
+      while (currentTime < P.advection_time) {
+        currentTime += advect(P, P.advection_time - currentTime);
+        ++steps;
+        if (P.single_step) break;
+        if (steps >= maxSteps) throw CudaError("step limit reached", VLSG_ERR_NUMERIC);
+      }
+      advectedTime = currentTime;
+    }
+    VLSG_CUDA(cudaStreamSynchronize(stream));
+    r.advected_time = advectedTime;
+    r.current_time_step = currentTimeStep;
+    r.number_of_time_steps = steps;
+    r.number_of_stages = stages;
+    r.point_updates = pointUpdates;
+    r.kernel_launches = launches - l0;
+  }
+
+  // ------------------------------------------------------------ download
+  int64_t countDefined(int b) { return compact(b, nullptr, nullptr, 0); }
+
+  void queryValues(int b, int64_t n, const int32_t *idx, double *out) {
+    if (n <= 0) return;
+    int *di = nullptr;
+    double *dv = nullptr;
+    VLSG_CUDA(cudaMalloc(&di, n * 3 * sizeof(int)));
+    VLSG_CUDA(cudaMalloc(&dv, n * sizeof(double)));
+    VLSG_CUDA(cudaMemcpyAsync(di, idx, n * 3 * sizeof(int), cudaMemcpyHostToDevice, stream));
+    {
+      Scope sc(this, "query");
+      kQueryValues<T><<<grid1(n), 256, 0, stream>>>(g, mapView(), view(b), (int)n, di, dv);
+      checkLaunch();
+    }
+    VLSG_CUDA(cudaMemcpyAsync(out, dv, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    VLSG_CUDA(cudaStreamSynchronize(stream));
+    cudaFree(di);
+    cudaFree(dv);
+  }
+
+  // Defined points of buffer b in HRLE order (keys sorted on the host).
+  int64_t compact(int b, int32_t *idxOut, double *valOut, int64_t capOut) {
+    VLSG_CUDA(cudaMemsetAsync(nOutPtr(), 0, sizeof(int), stream));
+    uint64_t *dk = nullptr;
+    double *dv = nullptr;
+    // count first
+    const size_t maxPts = (size_t)cap * BV;
+    size_t room = std::min<size_t>(maxPts, (size_t)cap * 256);
+    VLSG_CUDA(cudaMalloc(&dk, room * sizeof(uint64_t)));
+    VLSG_CUDA(cudaMalloc(&dv, room * sizeof(double)));
+    {
+      Scope sc(this, "download_compact");
+      kCompactDefined<T><<<blocksPass, 256, 0, stream>>>(g, slotList, nSlotsPtr(), slotBrick,
+                                                         buf[b].vals[buf[b].cur],
+                                                         buf[b].state[buf[b].cur], dk, dv, nOutPtr(),
+                                                         (int)room);
+      checkLaunch();
+    }
+    syncErr("download");
+    const int64_t n = hCounters[5];
+    if ((size_t)n > room) {
+      cudaFree(dk);
+      cudaFree(dv);
+      throw CudaError("download buffer too small", VLSG_ERR_CAPACITY);
+    }
+    if (idxOut && valOut && n <= capOut) {
+      std::vector<uint64_t> hk(n);
+      std::vector<double> hv(n);
+      VLSG_CUDA(cudaMemcpyAsync(hk.data(), dk, n * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream));
+      VLSG_CUDA(cudaMemcpyAsync(hv.data(), dv, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+      VLSG_CUDA(cudaStreamSynchronize(stream));
+      std::vector<int64_t> order(n);
+      for (int64_t i = 0; i < n; ++i) order[i] = i;
+      std::sort(order.begin(), order.end(), [&](int64_t a, int64_t c) { return hk[a] < hk[c]; });
+      const int64_t off = 1ll << 20;
+      for (int64_t i = 0; i < n; ++i) {
+        const uint64_t k = hk[order[i]];
+        idxOut[3 * i + 0] = (int32_t)((int64_t)(k & 0x1fffff) - off);
+        idxOut[3 * i + 1] = (int32_t)((int64_t)((k >> 21) & 0x1fffff) - off);
+        idxOut[3 * i + 2] = (int32_t)((int64_t)((k >> 42) & 0x1fffff) - off);
+        valOut[i] = hv[order[i]];
+      }
+    }
+    cudaFree(dk);
+    cudaFree(dv);
+    return n;
+  }
+};
+
+} // namespace vlsg

@@ -65,3 +65,85 @@ def make_sphere(grid, origin, radius):
     rs, sg = make_runs(idx, sign_fn, [lo[0] - 1, lo[1] - 1, lo[2] - 1],
                        [hi[0] + 1, hi[1] + 1, hi[2] + 1])
     return Domain(grid, idx.astype(np.int32), vals, rs, sg, width=2)
+
+
+def sdf_levelset(grid, sdf, lo, hi, lipschitz=1.0):
+    """Width-2 band of a signed distance function (physical units).
+
+    Every cell of the index box [lo, hi] with |sdf| <= gridDelta is defined
+    with value sdf / gridDelta; undefined runs carry the sign of sdf.  Bricks
+    of 8^3 cells whose centre is further than their half diagonal (times
+    `lipschitz`) plus one cell from the surface are skipped unevaluated.
+    sdf(x, y, z) takes float arrays of coordinates.
+    """
+    gd = grid.delta
+    lo = [int(v) for v in lo]
+    hi = [int(v) for v in hi]
+    B = 8
+    nb = [(hi[d] - lo[d]) // B + 1 for d in range(3)]
+    bz, by, bx = np.meshgrid(np.arange(nb[2]), np.arange(nb[1]), np.arange(nb[0]), indexing="ij")
+    cx = (lo[0] + bx * B + 3.5) * gd
+    cy = (lo[1] + by * B + 3.5) * gd
+    cz = (lo[2] + bz * B + 3.5) * gd
+    dc = sdf(cx.ravel(), cy.ravel(), cz.ravel())
+    reach = (np.sqrt(3.0) * 4.0 * lipschitz + 1.5) * gd
+    near = np.nonzero(np.abs(dc) <= reach)[0]
+    off = np.arange(B)
+    oz, oy, ox = np.meshgrid(off, off, off, indexing="ij")
+    ox, oy, oz = ox.ravel(), oy.ravel(), oz.ravel()
+    idx_parts, val_parts = [], []
+    chunk = 1 << 14
+    for s in range(0, len(near), chunk):
+        nbk = near[s:s + chunk]
+        X = (lo[0] + bx.ravel()[nbk, None] * B + ox[None, :]).ravel()
+        Y = (lo[1] + by.ravel()[nbk, None] * B + oy[None, :]).ravel()
+        Z = (lo[2] + bz.ravel()[nbk, None] * B + oz[None, :]).ravel()
+        inside = (X <= hi[0]) & (Y <= hi[1]) & (Z <= hi[2])
+        X, Y, Z = X[inside], Y[inside], Z[inside]
+        v = sdf(X * gd, Y * gd, Z * gd) / gd
+        keep = np.abs(v) <= 1.0
+        idx_parts.append(np.stack([X[keep], Y[keep], Z[keep]], 1))
+        val_parts.append(v[keep])
+    idx = np.concatenate(idx_parts) if idx_parts else np.zeros((0, 3), np.int64)
+    vals = np.concatenate(val_parts) if val_parts else np.zeros(0)
+    for d in range(3):
+        if grid.is_periodic(d):
+            idx[:, d] = grid.map_index(d, idx[:, d])
+    if len(idx):
+        key = (idx[:, 2].astype(np.int64) << 42) + (idx[:, 1].astype(np.int64) << 21) + idx[:, 0]
+        _, first = np.unique(key, return_index=True)
+        idx, vals = idx[first], vals[first]
+
+    def sign_fn(x, y, z):
+        return np.where(sdf(np.asarray(x) * gd, np.asarray(y) * gd, np.asarray(z) * gd) < 0, -1, 1)
+
+    rs, sg = make_runs(idx, sign_fn, [lo[0] - 1, lo[1] - 1, lo[2] - 1], [hi[0] + 1, hi[1] + 1, hi[2] + 1])
+    return Domain(grid, idx.astype(np.int32), vals, rs, sg, width=2)
+
+
+# signed distance helpers (physical units) ----------------------------------
+def sdf_box(p, lo, hi):
+    q = [np.maximum(lo[d] - p[d], p[d] - hi[d]) for d in range(3)]
+    outside = np.sqrt(sum(np.maximum(qd, 0.0) ** 2 for qd in q))
+    inside = np.minimum(np.maximum(np.maximum(q[0], q[1]), q[2]), 0.0)
+    return outside + inside
+
+
+def trench_etch_level_sets(grid, mask_thickness=0.5, opening=4.0):
+    """Mask (material 0) and substrate-wrapping top (material 1) of a square
+    trench etch: substrate below z = 0, a mask slab 0 < z < thickness with a
+    centred square opening of the given width (periodic in x/y)."""
+    h = opening / 2.0
+    big = 1e9
+
+    def mask(x, y, z):
+        slab = np.maximum(-z, z - mask_thickness)
+        hole = sdf_box((x, y, z), (-h, -h, -big), (h, h, big))
+        return np.maximum(slab, -hole)
+
+    def top(x, y, z):
+        return np.minimum(z, mask(x, y, z))
+
+    lo = [grid.min[0], grid.min[1], grid.min[2]]
+    hi = [grid.max[0] - 1, grid.max[1] - 1, grid.max[2]]
+    return sdf_levelset(grid, mask, lo, hi), sdf_levelset(grid, top, lo, hi)

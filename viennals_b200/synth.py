@@ -1,0 +1,148 @@
+"""Seeded synthetic workloads of the benchmark (inputs only).
+
+`perturbed_sphere` builds the precision-form geometry: a sphere of radius R
+whose radius is modulated by real spherical harmonics of degree l <= lmax
+with coefficients ~ N(0, rel_sigma * R) drawn from a fixed seed;
+phi = (|x| - r(theta, varphi)) / gridDelta is kept where |phi| <= 1 (a
+width-2 band) and the undefined runs take the sign of phi.  The field is
+evaluated with torch on `device` (the GPU for the full-size case).
+"""
+import math
+
+import numpy as np
+
+from ._abi import BoundaryConditionEnum as BC
+from .domain import Domain, Grid, make_runs
+
+
+def sh_coefficients(lmax, sigma, seed):
+    rng = np.random.default_rng(seed)
+    return [(l, m, float(rng.normal(0.0, sigma))) for l in range(lmax + 1)
+            for m in range(-l, l + 1)]
+
+
+def _radius_torch(torch, coeffs, ct, st, phi, radius):
+    """r(theta, phi) = R + sum c_lm Y_lm (real, orthonormal)."""
+    lmax = max(l for l, _, _ in coeffs)
+    # associated Legendre P_l^m(cos t) without Condon-Shortley phase
+    P = {}
+    P[(0, 0)] = torch.ones_like(ct)
+    for m in range(1, lmax + 1):
+        P[(m, m)] = P[(m - 1, m - 1)] * (2 * m - 1) * st
+    for m in range(0, lmax):
+        P[(m + 1, m)] = (2 * m + 1) * ct * P[(m, m)]
+    for m in range(0, lmax + 1):
+        for l in range(m + 2, lmax + 1):
+            P[(l, m)] = ((2 * l - 1) * ct * P[(l - 1, m)] - (l + m - 1) * P[(l - 2, m)]) / (l - m)
+    r = torch.full_like(ct, radius)
+    for l, m, c in coeffs:
+        am = abs(m)
+        norm = math.sqrt((2 * l + 1) / (4 * math.pi) * math.factorial(l - am) / math.factorial(l + am))
+        if m == 0:
+            y = norm * P[(l, 0)]
+        elif m > 0:
+            y = math.sqrt(2.0) * norm * P[(l, am)] * torch.cos(am * phi)
+        else:
+            y = math.sqrt(2.0) * norm * P[(l, am)] * torch.sin(am * phi)
+        r = r + c * y
+    return r
+
+
+def perturbed_sphere(radius=40.0, grid_delta=0.05, lmax=8, rel_sigma=0.02, seed=1234,
+                     device="cpu"):
+    import torch
+
+    grid = Grid(None, [BC.INFINITE_BOUNDARY] * 3, grid_delta)
+    coeffs = sh_coefficients(lmax, rel_sigma * radius, seed)
+    gd = grid_delta
+    dev = torch.device(device)
+    # range of r(theta, phi) from a fine angular sample
+    th = torch.linspace(0, math.pi, 721, device=dev, dtype=torch.float64)
+    pp = torch.linspace(-math.pi, math.pi, 1441, device=dev, dtype=torch.float64)
+    T_, P_ = torch.meshgrid(th, pp, indexing="ij")
+    rs_ = _radius_torch(torch, coeffs, torch.cos(T_).reshape(-1), torch.sin(T_).reshape(-1),
+                        P_.reshape(-1), radius)
+    span = float(rs_.max() - rs_.min())
+    rmin = max(0.0, (float(rs_.min()) - 0.05 * span) / gd - 3.0)
+    rmax = (float(rs_.max()) + 0.05 * span) / gd + 3.0
+    n = int(math.ceil(rmax))
+
+    def raw(x, y, z):
+        """|x| - r(theta, phi) in physical units; x, y, z in index units."""
+        rho = torch.sqrt(x * x + y * y + z * z)
+        safe = torch.where(rho > 0, rho, torch.ones_like(rho))
+        ct = z / safe
+        st = torch.sqrt(torch.clamp(1 - ct * ct, min=0.0))
+        ph = torch.atan2(y, x)
+        return rho * gd - _radius_torch(torch, coeffs, ct, st, ph, radius)
+
+    def phi_at(x, y, z):
+        # first-order distance: (|x| - r) / |grad(|x| - r)|, in grid units
+        f = raw(x, y, z)
+        h = 1e-3
+        g2 = torch.zeros_like(f)
+        for d in range(3):
+            o = [0.0, 0.0, 0.0]
+            o[d] = h
+            fp = raw(x + o[0], y + o[1], z + o[2])
+            fm = raw(x - o[0], y - o[1], z - o[2])
+            g2 = g2 + ((fp - fm) / (2 * h * gd)) ** 2
+        return f / torch.sqrt(g2) / gd
+
+    # 1. bricks of 8^3 cells whose centre lies near the surface
+    B = 8
+    nbk = (2 * n + 1) // B + 2
+    base = -(nbk * B) // 2
+    bax = torch.arange(nbk, device=dev, dtype=torch.float64)
+    keep_b = []
+    reach = 4.0 * math.sqrt(3.0) * 2.0 + 2.0  # half diagonal x Lipschitz bound + margin
+    for bz in range(nbk):
+        cz = base + bz * B + 3.5
+        BY, BX = torch.meshgrid(bax, bax, indexing="ij")
+        cx = base + BX.reshape(-1) * B + 3.5
+        cy = base + BY.reshape(-1) * B + 3.5
+        rr = torch.sqrt(cx * cx + cy * cy + cz * cz)
+        near = (rr >= rmin - 8) & (rr <= rmax + 8)
+        if not bool(near.any()):
+            continue
+        cx, cy = cx[near], cy[near]
+        czt = torch.full_like(cx, cz)
+        f = raw(cx, cy, czt) / gd
+        sel = torch.abs(f) <= reach
+        keep_b.append(torch.stack([cx[sel], cy[sel], czt[sel]], 1) - 3.5)
+    bricks = torch.cat(keep_b)
+    off = torch.arange(B, device=dev, dtype=torch.float64)
+    OZ, OY, OX = torch.meshgrid(off, off, off, indexing="ij")
+    offs = torch.stack([OX.reshape(-1), OY.reshape(-1), OZ.reshape(-1)], 1)
+    # 2. cells of those bricks, evaluated in chunks
+    idx_parts, val_parts = [], []
+    per = max(1, (1 << 23) // (B ** 3))
+    for s0 in range(0, len(bricks), per):
+        cells = (bricks[s0:s0 + per, None, :] + offs[None, :, :]).reshape(-1, 3)
+        v = phi_at(cells[:, 0], cells[:, 1], cells[:, 2])
+        keep = torch.abs(v) <= 1.0
+        idx_parts.append(cells[keep].to(torch.int32).cpu().numpy())
+        val_parts.append(v[keep].cpu().numpy())
+    idx = np.concatenate(idx_parts)
+    vals = np.concatenate(val_parts)
+
+    def sign_fn(x, y, z):
+        out = np.empty(len(x), np.int64)
+        step = 1 << 22
+        for s in range(0, len(x), step):
+            t = [torch.as_tensor(np.asarray(a[s:s + step], np.float64), device=dev) for a in (x, y, z)]
+            out[s:s + step] = np.where(phi_at(*t).cpu().numpy() < 0, -1, 1)
+        return out
+
+    rs, sg = make_runs(idx, sign_fn, [-n - 1] * 3, [n + 1] * 3)
+    return grid, Domain(grid, idx, vals, rs, sg, width=2)
+
+
+def precision_velocity():
+    """v = 1.0 + 0.3 n_z on the single material."""
+    from .velocity import FunctorVelocity
+
+    v = FunctorVelocity(1)
+    v.set_rate(0, 1.0)
+    v.set_linear(0, 2, 0.3)
+    return v
