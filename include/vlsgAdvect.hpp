@@ -1,0 +1,232 @@
+// vlsgAdvect.hpp -- header-only C++ front of libvlsgpu with the interface of
+// viennals::Advect<T,D> (include/viennals/lsAdvect.hpp:836-1043 of ViennaLS
+// 5.8.3): the same setters and getters, level sets inserted bottom to top,
+// apply() writing the results back into the same level-set objects, and
+// errors logged and swallowed like VIENNACORE_LOG_ERROR + return.
+//
+// `vlsg::LevelSet` holds what crosses the C ABI for one level set: the grid,
+// the defined points with their values (grid units) and the undefined runs,
+// all in HRLE order.  With ViennaLS available, define VLSG_WITH_VIENNALS
+// before including this header to get conversions from and to
+// viennals::Domain<T,3> (they iterate the HRLE domain the way
+// lsReduce.hpp:281-296 does).
+#pragma once
+
+#include <array>
+#include <cstdint>
+#include <cstdio>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "vlsg.h"
+
+namespace vlsg {
+
+enum class SpatialSchemeEnum : unsigned {
+  ENGQUIST_OSHER_1ST_ORDER = 0,
+  ENGQUIST_OSHER_2ND_ORDER = 1,
+  LAX_FRIEDRICHS_1ST_ORDER = 2,
+  LAX_FRIEDRICHS_2ND_ORDER = 3,
+  LOCAL_LAX_FRIEDRICHS_ANALYTICAL_1ST_ORDER = 4,
+  LOCAL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER = 5,
+  LOCAL_LOCAL_LAX_FRIEDRICHS_2ND_ORDER = 6,
+  LOCAL_LAX_FRIEDRICHS_1ST_ORDER = 7,
+  LOCAL_LAX_FRIEDRICHS_2ND_ORDER = 8,
+  STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER = 9,
+  WENO_3RD_ORDER = 10,
+  WENO_5TH_ORDER = 11
+};
+enum class TemporalSchemeEnum : unsigned {
+  FORWARD_EULER = 0,
+  RUNGE_KUTTA_2ND_ORDER = 1,
+  RUNGE_KUTTA_3RD_ORDER = 2
+};
+
+struct Grid {
+  std::array<int64_t, 3> min{}, max{};
+  std::array<int32_t, 3> boundary{VLSG_INFINITE_BOUNDARY, VLSG_INFINITE_BOUNDARY,
+                                   VLSG_INFINITE_BOUNDARY};
+  double gridDelta = 1.0;
+};
+
+struct LevelSet {
+  Grid grid;
+  std::vector<int32_t> indices; // 3 per point, HRLE order
+  std::vector<double> values;
+  std::vector<int32_t> runStart; // 3 per undefined run
+  std::vector<int8_t> runSign;
+  int width = 2;
+  int64_t numberOfPoints() const { return (int64_t)values.size(); }
+};
+
+// Device velocity field: per-material polynomial in the normal (vlsg.h).
+struct VelocityFunctor {
+  vlsg_velocity_desc desc{};
+  explicit VelocityFunctor(int materials = 1) { desc.n_materials = materials; }
+  VelocityFunctor &rate(int m, double v) { desc.rate[m] = v; return *this; }
+  VelocityFunctor &linear(int m, int k, double pos, double neg) {
+    desc.lin_pos[m][k] = pos, desc.lin_neg[m][k] = neg;
+    return *this;
+  }
+  VelocityFunctor &absolute(int m, int k, double pos, double neg) {
+    desc.abs_pos[m][k] = pos, desc.abs_neg[m][k] = neg;
+    return *this;
+  }
+  VelocityFunctor &square(int m, int k, double pos, double neg) {
+    desc.sq_pos[m][k] = pos, desc.sq_neg[m][k] = neg;
+    return *this;
+  }
+  VelocityFunctor &vector(int m, double x, double y, double z) {
+    desc.vec[m][0] = x, desc.vec[m][1] = y, desc.vec[m][2] = z;
+    return *this;
+  }
+};
+
+template <class T> class Advect {
+  std::vector<std::shared_ptr<LevelSet>> levelSets;
+  std::shared_ptr<VelocityFunctor> velocities;
+  vlsg_advect_params params{};
+  vlsg_advect_result result{};
+  vlsg_context *ctx = nullptr;
+  int device = 0;
+
+  static void logError(const std::string &m) { std::fprintf(stderr, "[vlsg] %s\n", m.c_str()); }
+  bool check(int rc) {
+    if (rc == VLSG_OK) return true;
+    logError(vlsg_last_error(ctx));
+    return false;
+  }
+
+public:
+  Advect() { vlsg_default_params(&params), result.current_time_step = -1.; }
+  explicit Advect(std::shared_ptr<LevelSet> ls) : Advect() { levelSets.push_back(ls); }
+  Advect(std::shared_ptr<LevelSet> ls, std::shared_ptr<VelocityFunctor> v) : Advect() {
+    levelSets.push_back(ls);
+    velocities = v;
+  }
+  Advect(std::vector<std::shared_ptr<LevelSet>> lss, std::shared_ptr<VelocityFunctor> v)
+      : Advect() {
+    levelSets = lss;
+    velocities = v;
+  }
+  ~Advect() {
+    if (ctx) vlsg_destroy(ctx);
+  }
+  Advect(const Advect &) = delete;
+  Advect &operator=(const Advect &) = delete;
+
+  void setDevice(int d) { device = d; }
+  void insertNextLevelSet(std::shared_ptr<LevelSet> ls) { levelSets.push_back(ls); }
+  void clearLevelSets() { levelSets.clear(); }
+  void setVelocityField(std::shared_ptr<VelocityFunctor> v) { velocities = v; }
+  void setAdvectionTime(double t) { params.advection_time = t; }
+  void setSingleStep(bool b) { params.single_step = b; }
+  void setTimeStepRatio(const double &cfl) { params.time_step_ratio = cfl; }
+  void setCalculateNormalVectors(bool b) { params.calculate_normal_vectors = b; }
+  void setIgnoreVoids(bool b) { params.ignore_voids = b; }
+  void setAdaptiveTimeStepping(bool b = true, unsigned subdivisions = 20) {
+    params.adaptive_time_stepping = b;
+    params.adaptive_subdivisions = subdivisions < 1 ? 1 : subdivisions;
+  }
+  void setSaveAdvectionVelocities(bool b) { params.save_advection_velocities = b; }
+  void setSpatialScheme(SpatialSchemeEnum s) { params.spatial_scheme = (int32_t)s; }
+  void setTemporalScheme(TemporalSchemeEnum s) { params.temporal_scheme = (int32_t)s; }
+  void setDissipationAlpha(const double &a) { params.dissipation_alpha = a; }
+  void setCheckDissipation(bool b) { params.check_dissipation = b; }
+  void setUpdatePointData(bool b) { params.update_point_data = b; }
+
+  double getAdvectedTime() const { return result.advected_time; }
+  double getCurrentTimeStep() const { return result.current_time_step; }
+  unsigned getNumberOfTimeSteps() const { return result.number_of_time_steps; }
+  double getTimeStepRatio() const { return params.time_step_ratio; }
+  bool getCalculateNormalVectors() const { return params.calculate_normal_vectors; }
+  const vlsg_advect_result &getResult() const { return result; }
+
+  // Advect::apply, lsAdvect.hpp:1017-1043
+  void apply() {
+    if (levelSets.empty()) return logError("No level sets passed to Advect. Not advecting.");
+    if (!velocities) return logError("No velocity field passed to Advect. Not advecting.");
+    if (!ctx) {
+      const int precision = sizeof(T) == 4 ? VLSG_FP32 : VLSG_FP64;
+      if (!check(vlsg_create(&ctx, device, precision))) return;
+    }
+    const Grid &g = levelSets.back()->grid;
+    if (!check(vlsg_set_grid(ctx, 3, g.min.data(), g.max.data(), g.boundary.data(), g.gridDelta)))
+      return;
+    if (!check(vlsg_set_level_set_count(ctx, (int32_t)levelSets.size()))) return;
+    for (size_t i = 0; i < levelSets.size(); ++i) {
+      const LevelSet &ls = *levelSets[i];
+      if (!check(vlsg_upload_levelset(ctx, (int32_t)i, ls.numberOfPoints(), ls.indices.data(),
+                                      ls.values.data(), (int64_t)ls.runSign.size(),
+                                      ls.runStart.data(), ls.runSign.data(), ls.width)))
+        return;
+    }
+    if (!check(vlsg_set_velocity_functor(ctx, &velocities->desc))) return;
+    if (!check(vlsg_advect(ctx, &params, &result))) return;
+    for (size_t i = 0; i < levelSets.size(); ++i) {
+      LevelSet &ls = *levelSets[i];
+      int64_t n = 0;
+      if (!check(vlsg_count_points(ctx, (int32_t)i, &n))) return;
+      ls.indices.resize(3 * n);
+      ls.values.resize(n);
+      int32_t w = 0;
+      if (!check(vlsg_download_levelset(ctx, (int32_t)i, n, ls.indices.data(), ls.values.data(), &w)))
+        return;
+      ls.width = w;
+      rebuildRuns(i, ls);
+    }
+  }
+
+private:
+  // Undefined runs of a downloaded level set (HRLE order): one before the
+  // bounding box of the points, one after it, one per row of the box without
+  // points, and in rows with points one at the row head and one after every
+  // point not followed by a defined neighbour.  Each run's sign is read back
+  // from the device at a cell inside the run.
+  void rebuildRuns(size_t slot, LevelSet &ls) {
+    const int64_t n = ls.numberOfPoints();
+    const int32_t NI = -((1 << 20) - 2);
+    std::array<int32_t, 3> lo{0, 0, 0}, hi{0, 0, 0};
+    for (int64_t i = 0; i < n; ++i)
+      for (int d = 0; d < 3; ++d) {
+        const int32_t c = ls.indices[3 * i + d];
+        if (i == 0 || c < lo[d]) lo[d] = c;
+        if (i == 0 || c > hi[d]) hi[d] = c;
+      }
+    std::vector<int32_t> starts, probe;
+    auto add = [&](int32_t x, int32_t y, int32_t z, int32_t px, int32_t py, int32_t pz) {
+      starts.insert(starts.end(), {x, y, z});
+      probe.insert(probe.end(), {px, py, pz});
+    };
+    add(NI, NI, NI, lo[0], lo[1], lo[2] - 1);
+    int64_t i = 0;
+    for (int32_t z = lo[2]; z <= hi[2]; ++z) {
+      add(NI, NI, z, lo[0], lo[1] - 1, z);
+      for (int32_t y = lo[1]; y <= hi[1]; ++y) {
+        if (i >= n || ls.indices[3 * i + 1] != y || ls.indices[3 * i + 2] != z) {
+          add(NI, y, z, lo[0], y, z); // row without points
+          continue;
+        }
+        add(NI, y, z, ls.indices[3 * i] - 1, y, z);
+        for (; i < n && ls.indices[3 * i + 1] == y && ls.indices[3 * i + 2] == z; ++i) {
+          const int32_t x = ls.indices[3 * i];
+          const bool adjacent = i + 1 < n && ls.indices[3 * (i + 1)] == x + 1 &&
+                                ls.indices[3 * (i + 1) + 1] == y && ls.indices[3 * (i + 1) + 2] == z;
+          if (!adjacent) add(x + 1, y, z, x + 1, y, z);
+        }
+      }
+      add(NI, hi[1] + 1, z, lo[0], hi[1] + 1, z);
+    }
+    add(NI, NI, hi[2] + 1, lo[0], lo[1], hi[2] + 1);
+    const int64_t m = (int64_t)starts.size() / 3;
+    std::vector<double> v(m);
+    if (!check(vlsg_get_values(ctx, (int32_t)slot, m, probe.data(), v.data()))) return;
+    ls.runStart = starts;
+    ls.runSign.resize(m);
+    for (int64_t j = 0; j < m; ++j) ls.runSign[j] = v[j] < 0 ? -1 : 1;
+  }
+};
+
+} // namespace vlsg

@@ -66,6 +66,19 @@ def test_trench_two_materials_periodic(spatial, temporal):
     _parity(g, lss, v, p)
 
 
+def test_periodic_extent_not_multiple_of_brick():
+    # 50 x 46 points: the last brick of x and y hangs over the periodic end
+    from viennals_b200.geometry import trench_etch_level_sets
+
+    g = Grid([-2.5, 2.5, -2.3, 2.3, -1.6, 1.6],
+             [BC.PERIODIC_BOUNDARY, BC.PERIODIC_BOUNDARY, BC.INFINITE_BOUNDARY], 0.1)
+    m, t = trench_etch_level_sets(g, 0.5, 1.6)
+    v = FunctorVelocity(2)
+    v.set_rate(1, -1.0)
+    v.set_linear(1, 2, -0.3)
+    _parity(g, [m, t], v, params(11, 2, 0.15))
+
+
 def test_multi_material_union_rk3():
     from oracle import oracle as O
 

@@ -18,6 +18,7 @@
 #include "vlsg_maint.cuh"
 #include "vlsg_passes.cuh"
 #include "vlsg_rates.cuh"
+#include "vlsg_fused.cuh"
 
 namespace vlsg {
 
@@ -102,6 +103,9 @@ public:
   T *rateV = nullptr, *rateStop = nullptr;
   uint8_t *rateLen = nullptr;
   uint32_t *active = nullptr;
+  // brick-aligned domains: 27-neighbour table per slot and per-pass work list
+  bool aligned = false;
+  int *nbr = nullptr, *work = nullptr;
   // host mirrors
   int hCounters[8];
   unsigned long long hScal[4];
@@ -123,7 +127,8 @@ public:
   void release() {
     auto f = [](void *p) { if (p) cudaFree(p); };
     f(brickMap); f(slotBrick); f(slotList); f(freeStack); f(counters); f(needed);
-    f(scal); f(rateV); f(rateStop); f(rateLen); f(active);
+    f(scal); f(rateV); f(rateStop); f(rateLen); f(active); f(nbr); f(work);
+    nbr = work = nullptr;
     for (auto &b : buf) {
       f(b.vals[0]); f(b.vals[1]); f(b.state[0]); f(b.state[1]); f(b.hasDef); f(b.farSign);
       b = DBuf();
@@ -330,6 +335,16 @@ public:
     VLSG_CUDA(cudaMalloc(&slotBrick, cap * sizeof(int)));
     VLSG_CUDA(cudaMalloc(&slotList, cap * sizeof(int)));
     VLSG_CUDA(cudaMalloc(&freeStack, cap * sizeof(int)));
+    aligned = true;
+    for (int d = 0; d < 3; ++d) {
+      if (g.bc[d] == VLSG_INFINITE_BOUNDARY) continue;
+      if (g.bc[d] == VLSG_PERIODIC_BOUNDARY && (g.gmax[d] - g.gmin[d]) % BS == 0) continue;
+      aligned = false;
+    }
+    if (aligned) {
+      VLSG_CUDA(cudaMalloc(&nbr, (size_t)cap * 27 * sizeof(int)));
+      VLSG_CUDA(cudaMalloc(&work, (size_t)cap * sizeof(int)));
+    }
     VLSG_CUDA(cudaMemsetAsync(slotBrick, 0xff, cap * sizeof(int), stream));
     {
       std::vector<int> fs(cap);
@@ -424,9 +439,73 @@ public:
 
   void rebuildSlotList() {
     VLSG_CUDA(cudaMemsetAsync(nSlotsPtr(), 0, sizeof(int), stream));
-    Scope sc(this, "slot_list");
-    kBuildSlotList<<<grid1(nBricks), 256, 0, stream>>>(nBricks, brickMap, slotList, nSlotsPtr());
+    {
+      Scope sc(this, "slot_list");
+      kBuildSlotList<<<grid1(nBricks), 256, 0, stream>>>(nBricks, brickMap, slotList, nSlotsPtr());
+      checkLaunch();
+    }
+    if (aligned) {
+      Scope sc(this, "neighbours");
+      kBuildNeighbours<<<grid1(cap), 256, 0, stream>>>(g, brickMap, slotBrick, slotList,
+                                                       nSlotsPtr(), nbr);
+      checkLaunch();
+    }
+  }
+
+  int *nWorkPtr() { return counters + 10; }
+  // Work list of a pass over buffer b (aligned domains).
+  void buildWork(int b) {
+    VLSG_CUDA(cudaMemsetAsync(nWorkPtr(), 0, sizeof(int), stream));
+    Scope sc(this, "work_list");
+    const int o = 1 - buf[b].cur;
+    kBuildWork<T><<<grid1(cap), 256, 0, stream>>>(slotList, nSlotsPtr(), nbr, view(b),
+                                                  buf[b].state[o], buf[b].hasDef, work, nWorkPtr());
     checkLaunch();
+  }
+  template <int R> void launchExpandFused(int b, const ExpandCycles<T> &cyc) {
+    constexpr int S = BS + 2 * R;
+    const size_t smem = 2 * (size_t)S * S * S * sizeof(T);
+    static bool attr = false;
+    if (!attr) {
+      VLSG_CUDA(cudaFuncSetAttribute(kExpandFused<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+      attr = true;
+    }
+    kExpandFused<T, R><<<blocksPass, FUSED_THREADS, smem, stream>>>(g, work, nWorkPtr(), nbr,
+                                                                    view(b), outOf(b), cyc);
+  }
+  // `n` (<= MAX_FUSED_CYCLES) Expand cycles in one sweep of the pool.
+  void expandFused(int b, const ExpandCycles<T> &cyc) {
+    buildWork(b);
+    const int64_t nIn = buf[b].nDef;
+    {
+      Scope sc(this, "expand", [this, b, nIn, cyc] {
+        buf[b].nDef = (int64_t)defCounted();
+        return bandPassBytes(nIn, buf[b].nDef);
+      });
+      switch (cyc.n) {
+      case 1: launchExpandFused<1>(b, cyc); break;
+      case 2: launchExpandFused<2>(b, cyc); break;
+      case 3: launchExpandFused<3>(b, cyc); break;
+      default: launchExpandFused<4>(b, cyc); break;
+      }
+      checkLaunch();
+    }
+    flip(b);
+  }
+  template <class Rule> void starTable(int b, Rule rule, const char *name) {
+    buildWork(b);
+    const int64_t nIn = buf[b].nDef;
+    {
+      Scope sc(this, name, [this, b, nIn] {
+        buf[b].nDef = (int64_t)defCounted();
+        return bandPassBytes(nIn, buf[b].nDef);
+      });
+      kStarTable<T, Rule><<<blocksPass, FUSED_THREADS, 0, stream>>>(work, nWorkPtr(), nbr, view(b),
+                                                                   outOf(b), rule);
+      checkLaunch();
+    }
+    flip(b);
   }
 
   // Bring the allocated bricks back to dilate(core) of the live buffers.
@@ -475,19 +554,51 @@ public:
     if (width <= buf[b].width) return;
     const int startWidth = buf[b].width;
     const T totalLimit = T(width * 0.5);
-    for (int c = 0; c < width - startWidth; ++c) {
-      ExpandRule<T> r{totalLimit, T((startWidth + c + 1) * T(0.5))};
-      starPass(b, r, "expand");
+    const int cycles = width - startWidth;
+    if (aligned) {
+      for (int c0 = 0; c0 < cycles; c0 += MAX_FUSED_CYCLES) {
+        ExpandCycles<T> cyc{};
+        cyc.n = std::min(MAX_FUSED_CYCLES, cycles - c0);
+        cyc.totalLimit = totalLimit;
+        for (int k = 0; k < cyc.n; ++k) cyc.limit[k] = T((startWidth + c0 + k + 1) * T(0.5));
+        expandFused(b, cyc);
+      }
+    } else {
+      for (int c = 0; c < cycles; ++c) {
+        ExpandRule<T> r{totalLimit, T((startWidth + c + 1) * T(0.5))};
+        starPass(b, r, "expand");
+      }
     }
     buf[b].width = width;
   }
   void prune(int b, bool rsz) {
-    starPass(b, PruneRule<T>{rsz}, "prune");
+    if (aligned) starTable(b, PruneRule<T>{rsz}, "prune");
+    else starPass(b, PruneRule<T>{rsz}, "prune");
     buf[b].width = 2;
   }
   void rebuild(int b) {
-    starPass(b, RebuildRule<T>{1.0}, "rebuild");
+    if (aligned) starTable(b, RebuildRule<T>{1.0}, "rebuild");
+    else starPass(b, RebuildRule<T>{1.0}, "rebuild");
     buf[b].width = 2;
+  }
+  // updateLevelSet (Reduce(1) + update) and rebuildLS in one sweep
+  void updateRebuildFused(double dt) {
+    const int top = L - 1;
+    buildWork(top);
+    {
+      Scope sc(this, "update_rebuild", [this, top] {
+        buf[top].nDef = (int64_t)defCounted();
+        // stage: band values + rates of the active points; out: new band
+        return double(sizeof(T)) * double(lastBand + lastActive) + bandPassBytes(0, buf[top].nDef);
+      });
+      kUpdateRebuild<T><<<blocksPass, FUSED_THREADS, 0, stream>>>(
+          g, work, nWorkPtr(), nbr, view(top), outOf(top), rateV, rateStop, rateLen,
+          (size_t)cap * BV, L, currentTimeStep, 1.0, errPtr());
+      checkLaunch();
+    }
+    flip(top);
+    buf[top].width = 2;
+    ++stages;
   }
   template <class Comp> void pointwise(int a, int bb, Comp comp, int *flag) {
     {
@@ -538,16 +649,23 @@ public:
     const int w = schemeWidth(P.spatial_scheme);
     if (w < 0) throw CudaError("Advect: Discretization scheme not found.", VLSG_ERR_ARGUMENT);
     expand(top, w); // prepareLS
+    const int s = P.spatial_scheme;
+    const bool globalLF = s == VLSG_LAX_FRIEDRICHS_1ST_ORDER || s == VLSG_LAX_FRIEDRICHS_2ND_ORDER;
+    const bool lfFamily = !(s == VLSG_ENGQUIST_OSHER_1ST_ORDER || s == VLSG_ENGQUIST_OSHER_2ND_ORDER ||
+                            s == VLSG_WENO_3RD_ORDER || s == VLSG_WENO_5TH_ORDER);
+    // the brick-staged rate kernel finds the active points itself; the list
+    // is needed by the generic path and by the global-alpha pre-pass
+    const bool useList = !aligned || globalLF;
     VLSG_CUDA(cudaMemsetAsync(nActivePtr(), 0, sizeof(int), stream));
-    {
+    if (useList) {
       Scope sc(this, "compact_active", [this] {
         lastBand = (int64_t)bandCounted();
         return double(sizeof(T)) * double(lastBand);
       });
-      kCompactActive<T><<<blocksPass, RATE_THREADS, 0, stream>>>(slotList, nSlotsPtr(), view(top),
-                                                                 active, nActivePtr(),
-                                                                 (int)activeCap, errPtr(),
-                                                                 bandCounter());
+      kCompactActiveWarp<T><<<blocksPass, RATE_THREADS, 0, stream>>>(slotList, nSlotsPtr(), view(top),
+                                                                     active, nActivePtr(),
+                                                                     (int)activeCap, errPtr(),
+                                                                     bandCounter());
       checkLaunch();
     }
     RateArgs<T> A{};
@@ -571,10 +689,6 @@ public:
     A.poolCells = (size_t)cap * BV;
     A.minStep = scal;
     A.err = errPtr();
-    const int s = P.spatial_scheme;
-    const bool globalLF = s == VLSG_LAX_FRIEDRICHS_1ST_ORDER || s == VLSG_LAX_FRIEDRICHS_2ND_ORDER;
-    const bool lfFamily = !(s == VLSG_ENGQUIST_OSHER_1ST_ORDER || s == VLSG_ENGQUIST_OSHER_2ND_ORDER ||
-                            s == VLSG_WENO_3RD_ORDER || s == VLSG_WENO_5TH_ORDER);
     unsigned long long init[4] = {~0ull, 0, 0, 0};
     VLSG_CUDA(cudaMemcpyAsync(scal, init, sizeof(init), cudaMemcpyHostToDevice, stream));
     double alphas[3] = {0, 0, 0};
@@ -600,8 +714,21 @@ public:
     } else {
       A.alphaMax = nullptr;
     }
-    {
+    if (aligned) {
+      VLSG_CUDA(cudaMemsetAsync(nActivePtr(), 0, sizeof(int), stream));
+      if (profiling) VLSG_CUDA(cudaMemsetAsync(bandCounter(), 0, 8, stream));
       // stencil input (each band value once) + output per active point
+      Scope sc(this, "rates", [this] {
+        int nAct = 0;
+        cudaMemcpy(&nAct, nActivePtr(), sizeof(int), cudaMemcpyDeviceToHost);
+        lastActive = nAct;
+        lastBand = (int64_t)bandCounted();
+        return double(sizeof(T)) * double(lastBand + nAct);
+      });
+      kRatesBrick<T><<<blocksPass, FUSED_THREADS, 0, stream>>>(A, vel, slotList, nSlotsPtr(), nbr,
+                                                                nActivePtr(), bandCounter());
+      checkLaunch();
+    } else {
       Scope sc(this, "rates", [this] {
         int nAct = 0;
         cudaMemcpy(&nAct, nActivePtr(), sizeof(int), cudaMemcpyDeviceToHost);
@@ -679,8 +806,12 @@ public:
   double evolveForwardEuler(const vlsg_advect_params &P, double maxTimeStep,
                             bool updateLowerLayers) {
     const double dt = computeRates(P, maxTimeStep);
-    updateLevelSet(dt);
-    rebuild(L - 1);
+    if (aligned) {
+      updateRebuildFused(dt);
+    } else {
+      updateLevelSet(dt);
+      rebuild(L - 1);
+    }
     maintain();
     if (updateLowerLayers) adjustLowerLayers(P);
     return dt;

@@ -100,8 +100,19 @@ template <class T> struct Stencil {
   }
 };
 
-template <class T>
-__device__ inline void oneSided(const Stencil<T> &S, int i, T phi0, T gridDelta,
+// Reader of a brick staged in shared memory with a halo of H cells.
+template <class T, int H> struct BoxStencil {
+  static constexpr int S = BS + 2 * H;
+  const T *box;
+  int o; // index of the centre cell
+  __device__ T at(int dx, int dy, int dz) const { return box[o + (dz * S + dy) * S + dx]; }
+  __device__ T axis(int d, int off) const {
+    return box[o + off * (d == 0 ? 1 : (d == 1 ? S : S * S))];
+  }
+};
+
+template <class T, class St>
+__device__ inline void oneSided(const St &S, int i, T phi0, T gridDelta,
                                 int order, T &diffPos, T &diffNeg) {
   const T deltaPos = gridDelta;
   const T deltaNeg = -gridDelta;
@@ -191,9 +202,9 @@ __device__ inline T weno5(const T *x, T dx, bool plus) {
 }
 
 // One scheme evaluation (Hamiltonian, dissipation) for `material`.
-template <class T>
+template <class T, class St>
 __device__ void evalScheme(const RateArgs<T> &A, const vlsg_velocity_desc &vel,
-                           const Stencil<T> &S, T C, int material, T *alphas,
+                           const St &S, T C, int material, T *alphas,
                            T &outG, T &outD) {
   const T gridDelta = T(A.g.delta);
   const int sch = A.scheme;
@@ -411,6 +422,64 @@ __device__ inline void atomicMaxAlpha(unsigned long long *dst, double v) {
   if ((threadIdx.x & 31) == 0 && b != 0ull) atomicMax(dst, b);
 }
 
+// integrateTime for one active point (lsAdvect.hpp:501-592): the material
+// chain, the stored rates (velocity as updateLevelSet applies it,
+// lsAdvect.hpp:738-744, and the stop value) and the point's time budget.
+template <class T, class St>
+__device__ inline double ratePoint(const RateArgs<T> &A, const vlsg_velocity_desc &vel,
+                                   const St &S, int slot, int c, T C, T *alphas) {
+  const int L = A.L;
+  const size_t q = (size_t)slot * BV + c;
+  T value = C;
+  double maxStepTime = 0;
+  double cfl = A.cfl;
+  int len = 0;
+  for (int cur = L - 1; cur >= 0; --cur) {
+    T g = 0, d = 0;
+    for (int lower = 0; lower < L; ++lower) {
+      const T lv = lower == L - 1 ? C : lsValueAt<T>(A.ls[lower], slot, c);
+      if ((double)lv <= (double)value + 1e-4) {
+        evalScheme<T>(A, vel, S, C, lower, alphas, g, d);
+        break;
+      }
+    }
+    const T velocity = g - d;
+    T veff = velocity;
+    if ((A.checkDiss && (g < 0 && velocity > 0)) || (g > 0 && velocity < 0)) veff = 0;
+    T stop;
+    bool done = true;
+    if (velocity > 0.) {
+      maxStepTime += cfl / velocity;
+      stop = Lim<T>::lowest();
+    } else if (velocity == 0.) {
+      maxStepTime = (double)Lim<T>::max();
+      stop = Lim<T>::max();
+    } else {
+      const T valueBelow = cur > 0 ? lsValueAt<T>(A.ls[cur - 1], slot, c) : Lim<T>::max();
+      const T difference = fabs(valueBelow - value);
+      if ((double)difference >= cfl) {
+        maxStepTime -= cfl / velocity;
+        stop = Lim<T>::max();
+      } else if (A.adaptive && (double)difference > A.adaptiveFactor * cfl) {
+        maxStepTime -= A.adaptiveFactor * cfl / velocity;
+        stop = Lim<T>::max();
+      } else {
+        cfl -= difference;
+        value = valueBelow;
+        maxStepTime -= difference / velocity;
+        stop = valueBelow;
+        done = false;
+      }
+    }
+    A.rateV[(size_t)len * A.poolCells + q] = veff;
+    A.rateStop[(size_t)len * A.poolCells + q] = stop;
+    ++len;
+    if (done) break;
+  }
+  A.rateLen[q] = (uint8_t)len;
+  return maxStepTime;
+}
+
 template <class T>
 __global__ void __launch_bounds__(RATE_THREADS)
     kRates(RateArgs<T> A, const vlsg_velocity_desc vel) {
@@ -431,55 +500,7 @@ __global__ void __launch_bounds__(RATE_THREADS)
                          A.g.org[0] + bx * BS, A.g.org[1] + by * BS,
                          A.g.org[2] + bz * BS};
       const T C = top.vals[(size_t)slot * BV + c];
-      T value = C;
-      maxStepTime = 0;
-      double cfl = A.cfl;
-      int len = 0;
-      for (int cur = L - 1; cur >= 0; --cur) {
-        T g = 0, d = 0;
-        for (int lower = 0; lower < L; ++lower) {
-          const T lv = lower == L - 1 ? C : lsValueAt<T>(A.ls[lower], slot, c);
-          if ((double)lv <= (double)value + 1e-4) {
-            evalScheme<T>(A, vel, S, C, lower, alphas, g, d);
-            break;
-          }
-        }
-        const T velocity = g - d;
-        // velocity applied by updateLevelSet (lsAdvect.hpp:738-744)
-        T veff = velocity;
-        if ((A.checkDiss && (g < 0 && velocity > 0)) || (g > 0 && velocity < 0))
-          veff = 0;
-        T stop;
-        bool done = true;
-        if (velocity > 0.) {
-          maxStepTime += cfl / velocity;
-          stop = Lim<T>::lowest();
-        } else if (velocity == 0.) {
-          maxStepTime = (double)Lim<T>::max();
-          stop = Lim<T>::max();
-        } else {
-          const T valueBelow = cur > 0 ? lsValueAt<T>(A.ls[cur - 1], slot, c) : Lim<T>::max();
-          const T difference = fabs(valueBelow - value);
-          if ((double)difference >= cfl) {
-            maxStepTime -= cfl / velocity;
-            stop = Lim<T>::max();
-          } else if (A.adaptive && (double)difference > A.adaptiveFactor * cfl) {
-            maxStepTime -= A.adaptiveFactor * cfl / velocity;
-            stop = Lim<T>::max();
-          } else {
-            cfl -= difference;
-            value = valueBelow;
-            maxStepTime -= difference / velocity;
-            stop = valueBelow;
-            done = false;
-          }
-        }
-        A.rateV[(size_t)len * A.poolCells + q] = veff;
-        A.rateStop[(size_t)len * A.poolCells + q] = stop;
-        ++len;
-        if (done) break;
-      }
-      A.rateLen[q] = (uint8_t)len;
+      maxStepTime = ratePoint<T>(A, vel, S, slot, c, C, alphas);
     }
     atomicMinStep(A.minStep, maxStepTime);
     if (A.alphaMax) {
