@@ -185,6 +185,33 @@ int vlsg_download_levelset(vlsg_context *ctx, int32_t slot, int64_t capacity,
 int vlsg_get_values(vlsg_context *ctx, int32_t slot, int64_t n,
                     const int32_t *indices, double *values);
 
+/* vlsg_get_values without any device allocation.  It has no counterpart in
+ * the reference.  It serves callers that may not allocate device memory once
+ * their set-up is done: an application whose memory pool (a framework's
+ * caching allocator, a fixed budget shared with other GPU work) already holds
+ * the device's free memory, or a loop that must not stall the other streams
+ * of the device, which cudaMalloc and cudaFree can do.  vlsg_get_values
+ * stages the query indices and the returned values in device buffers it
+ * allocates and frees on every call; this entry point stages them instead in
+ * one static device array of the library, sized for VLSG_NOALLOC_MAX_QUERIES
+ * queries (1.25 MiB, held on every GPU that loads the library until the
+ * process exits).
+ *   - n > VLSG_NOALLOC_MAX_QUERIES is rejected with VLSG_ERR_CAPACITY.
+ *   - The level sets must already be on the device (after vlsg_advect,
+ *     vlsg_count_points, vlsg_download_levelset or vlsg_get_values), because
+ *     moving them there allocates; otherwise VLSG_ERR_STATE.
+ *   - The first call on a device looks up the array's device address (once
+ *     per device, with the context's device current); make that first call
+ *     before any stream capture on that device.
+ *   - All calls share the array.  Calls that overlap on the GPU (contexts on
+ *     the same device driven from several host threads at once) race on it.
+ *     Each call writes every byte it reads, so nothing needs clearing between
+ *     calls.
+ * Same arguments, results and synchronisation as vlsg_get_values. */
+#define VLSG_NOALLOC_MAX_QUERIES 65536
+int vlsg_get_values_noalloc(vlsg_context *ctx, int32_t slot, int64_t n,
+                            const int32_t *indices, double *values);
+
 /* Velocity plugin: either a device functor or a host callback. */
 int vlsg_set_velocity_functor(vlsg_context *ctx, const vlsg_velocity_desc *v);
 int vlsg_set_velocity_callback(vlsg_context *ctx, vlsg_velocity_cb cb,

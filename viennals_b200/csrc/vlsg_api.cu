@@ -57,6 +57,53 @@ template <class F> auto withEngine(vlsg_context *ctx, F f) {
   return f(*ctx->e32);
 }
 
+// Staging of vlsg_get_values_noalloc: the query indices (3 x int32 each) of
+// at most VLSG_NOALLOC_MAX_QUERIES queries, then their values (double each).
+constexpr size_t kNoAllocIdxBytes = (size_t)VLSG_NOALLOC_MAX_QUERIES * 3 * sizeof(int32_t);
+constexpr size_t kNoAllocBytes = kNoAllocIdxBytes + (size_t)VLSG_NOALLOC_MAX_QUERIES * sizeof(double);
+static_assert(kNoAllocIdxBytes % 256 == 0, "value staging must stay 256-byte aligned");
+} // namespace
+
+// The array itself.  In host code this name is only a stand-in for the
+// symbol; its device address comes from cudaGetSymbolAddress.
+static __device__ __align__(256) unsigned char vlsg_noalloc_scratch[kNoAllocBytes];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_scratchMutex;
+unsigned char *g_scratchAddr[kMaxDevices] = {}; // device address per device
+
+// Device address of the staging array on `device` (the current device);
+// looked up on the first call per device.
+int noallocScratch(vlsg_context *ctx, int device, unsigned char **out) {
+  if (device < 0 || device >= kMaxDevices)
+    return fail(ctx, VLSG_ERR_ARGUMENT, "device ordinal out of range for vlsg_get_values_noalloc");
+  std::lock_guard<std::mutex> lk(g_scratchMutex);
+  if (!g_scratchAddr[device]) {
+    unsigned char *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress((void **)&p, vlsg_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(ctx, VLSG_ERR_CUDA,
+                  std::string("vlsg_get_values_noalloc: cudaGetSymbolAddress failed: ") +
+                      cudaGetErrorString(e));
+    g_scratchAddr[device] = p;
+  }
+  *out = g_scratchAddr[device];
+  return VLSG_OK;
+}
+
+// Query kernel of vlsg_get_values on caller-provided staging (di, dv).
+template <class T>
+void queryStaged(Engine<T> &e, int slot, int64_t n, const int32_t *idx, double *values,
+                 int32_t *di, double *dv) {
+  VLSG_CUDA(cudaMemcpyAsync(di, idx, n * 3 * sizeof(int32_t), cudaMemcpyHostToDevice, e.stream));
+  kQueryValues<T><<<Engine<T>::grid1(n), 256, 0, e.stream>>>(e.g, e.mapView(), e.view(slot),
+                                                              (int)n, di, dv);
+  e.checkLaunch();
+  VLSG_CUDA(cudaMemcpyAsync(values, dv, n * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
+  VLSG_CUDA(cudaStreamSynchronize(e.stream));
+}
+
 void ensureBuilt(vlsg_context *ctx) {
   if (!ctx->hasGrid) throw CudaError("no grid set (vlsg_set_grid)", VLSG_ERR_STATE);
   if (ctx->staged.empty()) throw CudaError("no level set uploaded", VLSG_ERR_STATE);
@@ -271,6 +318,35 @@ int vlsg_get_values(vlsg_context *ctx, int32_t slot, int64_t n, const int32_t *i
       e.queryValues(slot, n, idx, values);
       return 0;
     });
+    return VLSG_OK;
+  });
+}
+
+// Same queries as vlsg_get_values, staged in the library's static device
+// array instead of per-call device buffers: no cudaMalloc, no cudaFree.
+int vlsg_get_values_noalloc(vlsg_context *ctx, int32_t slot, int64_t n, const int32_t *idx,
+                            double *values) {
+  if (!ctx || n < 0 || (n > 0 && (!idx || !values)))
+    return fail(ctx, VLSG_ERR_ARGUMENT, "bad argument");
+  if (n > VLSG_NOALLOC_MAX_QUERIES)
+    return fail(ctx, VLSG_ERR_CAPACITY,
+                "vlsg_get_values_noalloc: " + std::to_string(n) + " queries exceed the maximum of " +
+                    std::to_string(VLSG_NOALLOC_MAX_QUERIES) + " per call");
+  return guarded(ctx, [&] {
+    if (!ctx->hasGrid || ctx->staged.empty() || ctx->dirty)
+      return fail(ctx, VLSG_ERR_STATE,
+                  "vlsg_get_values_noalloc: the level sets are not on the device yet (moving them "
+                  "there allocates); call vlsg_count_points or vlsg_advect first");
+    if (slot < 0 || slot >= (int)ctx->staged.size())
+      return fail(ctx, VLSG_ERR_ARGUMENT, "level set slot out of range");
+    unsigned char *scratch = nullptr;
+    const int rc = noallocScratch(ctx, ctx->device, &scratch);
+    if (rc != VLSG_OK) return rc;
+    if (n == 0) return VLSG_OK;
+    int32_t *di = (int32_t *)scratch;
+    double *dv = (double *)(scratch + kNoAllocIdxBytes);
+    if (ctx->precision == VLSG_FP64) queryStaged(*ctx->e64, slot, n, idx, values, di, dv);
+    else queryStaged(*ctx->e32, slot, n, idx, values, di, dv);
     return VLSG_OK;
   });
 }
