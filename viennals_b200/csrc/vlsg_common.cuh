@@ -6,12 +6,12 @@
 //     directions).  Entry >= 0: slot of an allocated brick; -1: not allocated.
 //   * per level-set buffer and brick: int8 sign of an unallocated brick
 //     (every cell undefined with that sign).
-//   * slot pool: per buffer two value arrays (ping-pong) of slots x 512 cells
-//     (x fastest, then y, then z inside a brick) holding the value in grid
-//     units or +-max for undefined cells, and a state byte per slot
-//     (DENSE, or UNIFORM_POS / UNIFORM_NEG when every cell is undefined with
-//     one sign, so its cells are neither read nor written).
-//   * slot list: compact list of allocated slots, and slot -> brick index.
+//   * slot pool: per buffer one value array of slots x 512 cells (x fastest,
+//     then y, then z inside a brick) holding the value in grid units or
+//     +-max for undefined cells, updated in place, and per slot a 512-bit
+//     mask of the defined cells (8 words, one per z-plane, bit y*8+x).
+//   * slot list: compact list of allocated slots, slot -> brick index, and
+//     per slot its 27 neighbours (slot, or -1-brick when not allocated).
 // Undefined cells carry the reference's sentinels +-numeric_limits<T>::max()
 // (lsDomain.hpp:51-52) so every rule compares exactly as the reference does.
 #pragma once
@@ -26,8 +26,6 @@ namespace vlsg {
 constexpr int BS = 8;           // brick edge
 constexpr int BV = BS * BS * BS; // cells per brick
 constexpr int MAXB = 2 * VLSG_MAX_LEVEL_SETS; // current + initial copies
-
-enum : uint8_t { ST_DENSE = 0, ST_UPOS = 1, ST_UNEG = 2 };
 
 template <class T> struct Lim;
 template <> struct Lim<double> {
@@ -83,7 +81,6 @@ __host__ __device__ inline int mapCoord(const GridDev &g, int d, int c) {
 // Buffer view: one level set (a current one or an RK initial copy).
 template <class T> struct Buf {
   const T *vals;          // slot pool values
-  const uint8_t *state;   // per-slot state
   const int8_t *farSign;  // per-brick sign of unallocated bricks
 };
 
@@ -110,8 +107,6 @@ __device__ inline T cellValue(const GridDev &g, const MapView &m, const Buf<T> &
   const int bi = brickIndex(g, rx >> 3, ry >> 3, rz >> 3);
   const int slot = m.brickMap[bi];
   if (slot < 0) return b.farSign[bi] < 0 ? Lim<T>::lowest() : Lim<T>::max();
-  const uint8_t st = b.state[slot];
-  if (st != ST_DENSE) return st == ST_UNEG ? Lim<T>::lowest() : Lim<T>::max();
   return b.vals[(size_t)slot * BV + ((rz & 7) * 64 + (ry & 7) * 8 + (rx & 7))];
 }
 

@@ -7,18 +7,21 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <functional>
+#include <limits>
 #include <stdexcept>
 #include <string>
 #include <vector>
 
 #include "vlsg_common.cuh"
+#include "vlsg_frontier.cuh"
 #include "vlsg_maint.cuh"
 #include "vlsg_passes.cuh"
 #include "vlsg_rates.cuh"
-#include "vlsg_fused.cuh"
 
 namespace vlsg {
 
@@ -81,33 +84,36 @@ public:
   GridDev g{};
   int L = 0;
   int nBricks = 0;
-  int cap = 0;      // slot capacity
-  size_t activeCap = 0;
+  int cap = 0; // slot capacity
+  size_t poolCells = 0; // cap * 512
   // device arrays
   int *brickMap = nullptr, *slotBrick = nullptr, *slotList = nullptr;
-  int *freeStack = nullptr;
-  int *counters = nullptr; // 0 nSlots, 1 freeCount, 2 nActive, 3 err, 4 flag, 5 nOut
+  int *freeStack = nullptr, *newList = nullptr;
+  int *counters = nullptr; // see the *Ptr() accessors
   uint8_t *needed = nullptr;
-  unsigned long long *scal = nullptr; // 0 minStep, 1..3 alphas
+  unsigned long long *scal = nullptr;   // 0 minStep, 1..3 alphas
+  unsigned long long *defCnt = nullptr; // defined cells per buffer (counted on demand)
+  unsigned long long *rateCounts = nullptr; // active cells, band cells of the last rates
+  int *nbr = nullptr;                   // 27 per slot
+  uint8_t *cflag = nullptr;             // CF_* per slot
   struct DBuf {
-    T *vals[2] = {nullptr, nullptr};
-    uint8_t *state[2] = {nullptr, nullptr};
+    T *vals = nullptr;
+    uint64_t *def[2] = {nullptr, nullptr};
     int cur = 0;
-    uint8_t *hasDef = nullptr;
     int8_t *farSign = nullptr;
     int width = 1;
     bool live = false;
-    int64_t nDef = 0; // defined cells (kept up to date in profiling mode)
+    double bound = 0;  // upper bound of |value| over the defined cells
+    int64_t nDef = 0;  // defined cells (profiling mode)
   };
   DBuf buf[MAXB];
-  T *rateV = nullptr, *rateStop = nullptr;
+  T *rateV = nullptr, *rateStop = nullptr; // pool shaped, L chain entries
   uint8_t *rateLen = nullptr;
-  uint32_t *active = nullptr;
-  // brick-aligned domains: 27-neighbour table per slot and per-pass work list
-  bool aligned = false;
-  int *nbr = nullptr, *work = nullptr;
+  uint64_t *act = nullptr;  // active masks of the top level set
+  T *next = nullptr;        // new values of the cells a pass changes
+  uint64_t *chg = nullptr;  // change masks of the last pass
   // host mirrors
-  int hCounters[8];
+  int hCounters[16];
   unsigned long long hScal[4];
   int *pinCounters = nullptr;
   unsigned long long *pinScal = nullptr;
@@ -126,35 +132,36 @@ public:
 
   void release() {
     auto f = [](void *p) { if (p) cudaFree(p); };
-    f(brickMap); f(slotBrick); f(slotList); f(freeStack); f(counters); f(needed);
-    f(scal); f(rateV); f(rateStop); f(rateLen); f(active); f(nbr); f(work);
-    nbr = work = nullptr;
+    f(brickMap); f(slotBrick); f(slotList); f(freeStack); f(newList); f(counters); f(needed);
+    f(scal); f(defCnt); f(rateCounts); f(nbr); f(cflag); f(rateV); f(rateStop); f(rateLen);
+    f(act); f(next); f(chg);
     for (auto &b : buf) {
-      f(b.vals[0]); f(b.vals[1]); f(b.state[0]); f(b.state[1]); f(b.hasDef); f(b.farSign);
+      f(b.vals); f(b.def[0]); f(b.def[1]); f(b.farSign);
       b = DBuf();
     }
     if (pinCounters) cudaFreeHost(pinCounters);
     if (pinScal) cudaFreeHost(pinScal);
-    brickMap = slotBrick = slotList = freeStack = counters = nullptr;
-    needed = nullptr; scal = nullptr; rateV = rateStop = nullptr; rateLen = nullptr;
-    active = nullptr; pinCounters = nullptr; pinScal = nullptr;
+    brickMap = slotBrick = slotList = freeStack = newList = counters = nullptr;
+    needed = nullptr; scal = defCnt = rateCounts = nullptr; nbr = nullptr; cflag = nullptr;
+    rateV = rateStop = nullptr; rateLen = nullptr; act = nullptr; next = nullptr; chg = nullptr;
+    pinCounters = nullptr; pinScal = nullptr;
   }
 
-  MapView mapView() const { return MapView{brickMap, slotBrick}; }
-  Buf<T> view(int b) const {
-    return Buf<T>{buf[b].vals[buf[b].cur], buf[b].state[buf[b].cur], buf[b].farSign};
-  }
-  PassOut<T> outOf(int b) {
-    const int o = 1 - buf[b].cur;
-    return PassOut<T>{buf[b].vals[o], buf[b].state[o], buf[b].hasDef, defCounter()};
-  }
-  void flip(int b) { buf[b].cur = 1 - buf[b].cur; }
   int *nSlotsPtr() { return counters + 0; }
   int *freeCountPtr() { return counters + 1; }
   int *nActivePtr() { return counters + 2; }
   int *errPtr() { return counters + 3; }
   int *flagPtr() { return counters + 4; }
   int *nOutPtr() { return counters + 5; }
+  int *nNewPtr() { return counters + 10; }
+
+  MapView mapView() const { return MapView{brickMap, slotBrick}; }
+  Buf<T> view(int b) const { return Buf<T>{buf[b].vals, buf[b].farSign}; }
+  Topo topo() { return Topo{g, brickMap, slotBrick, slotList, nSlotsPtr(), nbr, cflag, errPtr()}; }
+  LsView<T> lsView(int b) {
+    auto &B = buf[b];
+    return LsView<T>{B.vals, B.def[B.cur], B.def[1 - B.cur], B.farSign, next, chg};
+  }
 
   // ---------------------------------------------------------------- timing
   // One kernel launch.  With profiling on it is bracketed by CUDA events on
@@ -176,7 +183,6 @@ public:
         idx = (int)e->timers.size() - 1;
       }
       e->timers[idx].launches++;
-      cudaMemsetAsync(e->counters + 6, 0, 2 * sizeof(unsigned long long), e->stream);
       cudaEventCreate(&a);
       cudaEventCreate(&b);
       cudaEventRecord(a, e->stream);
@@ -193,19 +199,26 @@ public:
       if (bytesFn) e->timers[idx].bytes += bytesFn();
     }
   };
-  // Defined cells counted by the last launch (profiling mode only).
-  unsigned long long defCounted() {
-    unsigned long long v = 0;
-    cudaMemcpy(&v, counters + 6, sizeof(v), cudaMemcpyDeviceToHost);
-    return v;
+  // Stream-ordered reads of device counters (synchronous).
+  unsigned long long readU64(const unsigned long long *p) {
+    VLSG_CUDA(cudaMemcpyAsync(pinScal + 7, p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream));
+    VLSG_CUDA(cudaStreamSynchronize(stream));
+    return pinScal[7];
   }
-  unsigned long long bandCounted() {
-    unsigned long long v = 0;
-    cudaMemcpy(&v, counters + 8, sizeof(v), cudaMemcpyDeviceToHost);
-    return v;
+  int readI32(const int *p) {
+    VLSG_CUDA(cudaMemcpyAsync(pinCounters + 31, p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    VLSG_CUDA(cudaStreamSynchronize(stream));
+    return pinCounters[31];
   }
-  unsigned long long *defCounter() { return (unsigned long long *)(counters + 6); }
-  unsigned long long *bandCounter() { return (unsigned long long *)(counters + 8); }
+  // Defined cells of buffer b, counted from its masks (synchronous; for the
+  // download and the profiling byte counts).
+  int64_t defined(int b) {
+    VLSG_CUDA(cudaMemsetAsync(defCnt + b, 0, sizeof(unsigned long long), stream));
+    kCountDefined<<<grid1(cap), 256, 0, stream>>>(slotList, nSlotsPtr(), buf[b].def[buf[b].cur],
+                                                  defCnt + b);
+    checkLaunch();
+    return (int64_t)readU64(defCnt + b);
+  }
   // Bytes of a band pass in the survey's accounting: value + 64-bit key,
   // read once and written once per band point.
   double bandPassBytes(int64_t nIn, int64_t nOut) const {
@@ -213,21 +226,25 @@ public:
   }
   void checkLaunch() { VLSG_CUDA(cudaGetLastError()); }
 
+  static int grid1(size_t n) {
+    size_t b = (n + 255) / 256;
+    if (b < 1) b = 1;
+    if (b > 148 * 32) b = 148 * 32;
+    return (int)b;
+  }
+
   // ------------------------------------------------------------- layout
   void allocBuffers(int nb) {
     const size_t cells = (size_t)cap * BV;
     for (int b = 0; b < nb; ++b) {
       auto &B = buf[b];
-      if (B.vals[0]) continue;
-      VLSG_CUDA(cudaMalloc(&B.vals[0], cells * sizeof(T)));
-      VLSG_CUDA(cudaMalloc(&B.vals[1], cells * sizeof(T)));
-      VLSG_CUDA(cudaMalloc(&B.state[0], cap));
-      VLSG_CUDA(cudaMalloc(&B.state[1], cap));
-      VLSG_CUDA(cudaMalloc(&B.hasDef, cap));
+      if (B.vals) continue;
+      VLSG_CUDA(cudaMalloc(&B.vals, cells * sizeof(T)));
+      VLSG_CUDA(cudaMalloc(&B.def[0], (size_t)cap * 8 * sizeof(uint64_t)));
+      VLSG_CUDA(cudaMalloc(&B.def[1], (size_t)cap * 8 * sizeof(uint64_t)));
       VLSG_CUDA(cudaMalloc(&B.farSign, nBricks));
-      VLSG_CUDA(cudaMemsetAsync(B.hasDef, 0, cap, stream));
-      VLSG_CUDA(cudaMemsetAsync(B.state[0], ST_UPOS, cap, stream));
-      VLSG_CUDA(cudaMemsetAsync(B.state[1], ST_UPOS, cap, stream));
+      VLSG_CUDA(cudaMemsetAsync(B.def[0], 0, (size_t)cap * 8 * sizeof(uint64_t), stream));
+      VLSG_CUDA(cudaMemsetAsync(B.farSign, 1, nBricks, stream));
       B.cur = 0;
     }
   }
@@ -235,15 +252,12 @@ public:
   // The live buffers (current level sets and the RK copies in use).
   BufSet bufSet() {
     BufSet s{};
-    s.elem = sizeof(T);
     int k = 0;
     for (int b = 0; b < 2 * L; ++b) {
-      if (!buf[b].live || !buf[b].vals[0]) continue;
-      s.hasDef[k] = buf[b].hasDef;
-      s.hasDefW[k] = buf[b].hasDef;
-      s.state[k] = buf[b].state[buf[b].cur];
+      if (!buf[b].live || !buf[b].vals) continue;
+      s.vals[k] = buf[b].vals;
+      s.def[k] = buf[b].def[buf[b].cur];
       s.farSign[k] = buf[b].farSign;
-      s.vals[k] = buf[b].vals[buf[b].cur];
       ++k;
     }
     s.nBuf = k;
@@ -252,8 +266,8 @@ public:
 
   void build(const GridDev &grid, std::vector<StagedLS> &ls, int margin) {
     release();
-    VLSG_CUDA(cudaHostAlloc(&pinCounters, 8 * sizeof(int), cudaHostAllocDefault));
-    VLSG_CUDA(cudaHostAlloc(&pinScal, 4 * sizeof(unsigned long long), cudaHostAllocDefault));
+    VLSG_CUDA(cudaHostAlloc(&pinCounters, 32 * sizeof(int), cudaHostAllocDefault));
+    VLSG_CUDA(cudaHostAlloc(&pinScal, 8 * sizeof(unsigned long long), cudaHostAllocDefault));
     g = grid;
     L = (int)ls.size();
     // box: bounded directions cover the grid, infinite ones the points + margin
@@ -285,9 +299,11 @@ public:
     VLSG_CUDA(cudaMalloc(&brickMap, nBricks * sizeof(int)));
     VLSG_CUDA(cudaMalloc(&needed, nBricks));
     VLSG_CUDA(cudaMalloc(&counters, 16 * sizeof(int)));
-    VLSG_CUDA(cudaMemsetAsync(counters, 0, 16 * sizeof(int), stream));
     VLSG_CUDA(cudaMalloc(&scal, 4 * sizeof(unsigned long long)));
-    VLSG_CUDA(cudaMemsetAsync(counters, 0, 8 * sizeof(int), stream));
+    VLSG_CUDA(cudaMalloc(&defCnt, MAXB * sizeof(unsigned long long)));
+    VLSG_CUDA(cudaMalloc(&rateCounts, 2 * sizeof(unsigned long long)));
+    VLSG_CUDA(cudaMemsetAsync(counters, 0, 16 * sizeof(int), stream));
+    VLSG_CUDA(cudaMemsetAsync(defCnt, 0, MAXB * sizeof(unsigned long long), stream));
     VLSG_CUDA(cudaMemsetAsync(brickMap, 0xff, nBricks * sizeof(int), stream));
     VLSG_CUDA(cudaMemsetAsync(needed, 0, nBricks, stream));
     // mark point bricks of every level set, dilate
@@ -295,19 +311,19 @@ public:
     VLSG_CUDA(cudaMalloc(&core, nBricks));
     VLSG_CUDA(cudaMemsetAsync(core, 0, nBricks, stream));
     std::vector<int *> dIdx(L, nullptr);
-    std::vector<double *> dVal(L, nullptr);
+    std::vector<double *> dPtVal(L, nullptr);
     std::vector<uint64_t *> dRunK(L, nullptr);
     std::vector<int8_t *> dRunS(L, nullptr);
     for (int l = 0; l < L; ++l) {
       auto &s = ls[l];
       const size_t n = s.vals.size();
       VLSG_CUDA(cudaMalloc(&dIdx[l], std::max<size_t>(1, n) * 3 * sizeof(int)));
-      VLSG_CUDA(cudaMalloc(&dVal[l], std::max<size_t>(1, n) * sizeof(double)));
+      VLSG_CUDA(cudaMalloc(&dPtVal[l], std::max<size_t>(1, n) * sizeof(double)));
       VLSG_CUDA(cudaMalloc(&dRunK[l], std::max<size_t>(1, s.runKeys.size()) * sizeof(uint64_t)));
       VLSG_CUDA(cudaMalloc(&dRunS[l], std::max<size_t>(1, s.runSign.size())));
       if (n) {
         VLSG_CUDA(cudaMemcpyAsync(dIdx[l], s.idx.data(), n * 3 * sizeof(int), cudaMemcpyHostToDevice, stream));
-        VLSG_CUDA(cudaMemcpyAsync(dVal[l], s.vals.data(), n * sizeof(double), cudaMemcpyHostToDevice, stream));
+        VLSG_CUDA(cudaMemcpyAsync(dPtVal[l], s.vals.data(), n * sizeof(double), cudaMemcpyHostToDevice, stream));
       }
       if (!s.runKeys.empty()) {
         VLSG_CUDA(cudaMemcpyAsync(dRunK[l], s.runKeys.data(), s.runKeys.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, stream));
@@ -331,20 +347,19 @@ public:
     long long nNeeded = 0;
     for (auto v : hNeeded) nNeeded += v;
     cap = (int)std::max<long long>(1024, nNeeded * 2 + 256);
-    activeCap = (size_t)cap * 160;
+    poolCells = (size_t)cap * BV;
     VLSG_CUDA(cudaMalloc(&slotBrick, cap * sizeof(int)));
     VLSG_CUDA(cudaMalloc(&slotList, cap * sizeof(int)));
     VLSG_CUDA(cudaMalloc(&freeStack, cap * sizeof(int)));
-    aligned = true;
-    for (int d = 0; d < 3; ++d) {
-      if (g.bc[d] == VLSG_INFINITE_BOUNDARY) continue;
-      if (g.bc[d] == VLSG_PERIODIC_BOUNDARY && (g.gmax[d] - g.gmin[d]) % BS == 0) continue;
-      aligned = false;
-    }
-    if (aligned) {
-      VLSG_CUDA(cudaMalloc(&nbr, (size_t)cap * 27 * sizeof(int)));
-      VLSG_CUDA(cudaMalloc(&work, (size_t)cap * sizeof(int)));
-    }
+    VLSG_CUDA(cudaMalloc(&newList, cap * sizeof(int)));
+    VLSG_CUDA(cudaMalloc(&nbr, (size_t)cap * 27 * sizeof(int)));
+    VLSG_CUDA(cudaMalloc(&cflag, cap));
+    VLSG_CUDA(cudaMalloc(&act, (size_t)cap * 8 * sizeof(uint64_t)));
+    VLSG_CUDA(cudaMalloc(&chg, (size_t)cap * 8 * sizeof(uint64_t)));
+    VLSG_CUDA(cudaMalloc(&next, poolCells * sizeof(T)));
+    VLSG_CUDA(cudaMalloc(&rateV, poolCells * sizeof(T) * L));
+    VLSG_CUDA(cudaMalloc(&rateStop, poolCells * sizeof(T) * L));
+    VLSG_CUDA(cudaMalloc(&rateLen, poolCells));
     VLSG_CUDA(cudaMemsetAsync(slotBrick, 0xff, cap * sizeof(int), stream));
     {
       std::vector<int> fs(cap);
@@ -366,7 +381,8 @@ public:
     {
       Scope sc(this, "alloc");
       kAllocNeeded<<<grid1(nBricks), 256, 0, stream>>>(nBricks, brickMap, slotBrick, needed,
-                                                       bufSet(), freeStack, freeCountPtr(), errPtr());
+                                                       freeStack, freeCountPtr(), nullptr,
+                                                       nNewPtr(), errPtr());
       checkLaunch();
     }
     rebuildSlotList();
@@ -375,52 +391,41 @@ public:
       {
         Scope sc(this, "upload_fill");
         kFillFromRuns<T><<<blocksPass, 256, 0, stream>>>(g, slotList, nSlotsPtr(), slotBrick, dRunK[l],
-                                                         dRunS[l], (int)s.runKeys.size(),
-                                                         buf[l].vals[buf[l].cur]);
+                                                         dRunS[l], (int)s.runKeys.size(), buf[l].vals);
         checkLaunch();
       }
       if (!s.vals.empty()) {
         Scope sc(this, "upload_scatter");
         kScatterPoints<T><<<grid1(s.vals.size()), 256, 0, stream>>>(
-            g, (int)s.vals.size(), dIdx[l], dVal[l], brickMap, buf[l].vals[buf[l].cur], errPtr());
+            g, (int)s.vals.size(), dIdx[l], dPtVal[l], brickMap, buf[l].vals, errPtr());
         checkLaunch();
       }
       {
-        VLSG_CUDA(cudaMemsetAsync(defCounter(), 0, sizeof(unsigned long long), stream));
-        Scope sc(this, "upload_normalize");
-        kNormalize<T><<<blocksPass, 256, 0, stream>>>(g, slotList, nSlotsPtr(), slotBrick,
-                                                      buf[l].vals[buf[l].cur],
-                                                      buf[l].state[buf[l].cur], buf[l].hasDef,
-                                                      defCounter());
+        Scope sc(this, "upload_masks");
+        kMasksFromValues<T><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(
+            g, slotBrick, slotList, nSlotsPtr(), buf[l].vals, buf[l].def[buf[l].cur], nullptr);
         checkLaunch();
       }
-      VLSG_CUDA(cudaStreamSynchronize(stream));
-      buf[l].nDef = (int64_t)defCounted();
+      double bound = 0;
+      for (double v : s.vals) {
+        const double a = std::fabs((double)(T)v);
+        if (a > bound) bound = a;
+      }
+      buf[l].bound = bound;
     }
     syncErr("upload");
     for (int l = 0; l < L; ++l) {
       cudaFree(dIdx[l]);
-      cudaFree(dVal[l]);
+      cudaFree(dPtVal[l]);
       cudaFree(dRunK[l]);
       cudaFree(dRunS[l]);
+      buf[l].nDef = defined(l);
     }
     cudaFree(core);
-    const size_t cells = (size_t)cap * BV;
-    VLSG_CUDA(cudaMalloc(&rateV, cells * sizeof(T) * L));
-    VLSG_CUDA(cudaMalloc(&rateStop, cells * sizeof(T) * L));
-    VLSG_CUDA(cudaMalloc(&rateLen, cells));
-    VLSG_CUDA(cudaMalloc(&active, activeCap * sizeof(uint32_t)));
-  }
-
-  static int grid1(size_t n) {
-    size_t b = (n + 255) / 256;
-    if (b < 1) b = 1;
-    if (b > 148 * 32) b = 148 * 32;
-    return (int)b;
   }
 
   void syncErr(const char *where) {
-    VLSG_CUDA(cudaMemcpyAsync(pinCounters, counters, 8 * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    VLSG_CUDA(cudaMemcpyAsync(pinCounters, counters, 16 * sizeof(int), cudaMemcpyDeviceToHost, stream));
     VLSG_CUDA(cudaStreamSynchronize(stream));
     std::memcpy(hCounters, pinCounters, sizeof(hCounters));
     const int e = hCounters[3];
@@ -430,10 +435,10 @@ public:
       if (e & 2) m += " stop chain overran;";
       if (e & 4) m += " brick pool capacity exceeded;";
       if (e & 8) m += " freed brick held a defined point;";
-      if (e & 16) m += " active list capacity exceeded;";
+      if (e & 64) m += " band reached an unallocated brick;";
       int z = 0;
       cudaMemcpy(errPtr(), &z, sizeof(int), cudaMemcpyHostToDevice);
-      throw CudaError(m, (e & (4 | 16)) ? VLSG_ERR_CAPACITY : VLSG_ERR_DEVICE_CHECK);
+      throw CudaError(m, (e & 4) ? VLSG_ERR_CAPACITY : VLSG_ERR_DEVICE_CHECK);
     }
   }
 
@@ -444,68 +449,12 @@ public:
       kBuildSlotList<<<grid1(nBricks), 256, 0, stream>>>(nBricks, brickMap, slotList, nSlotsPtr());
       checkLaunch();
     }
-    if (aligned) {
+    {
       Scope sc(this, "neighbours");
       kBuildNeighbours<<<grid1(cap), 256, 0, stream>>>(g, brickMap, slotBrick, slotList,
-                                                       nSlotsPtr(), nbr);
+                                                       nSlotsPtr(), nbr, cflag);
       checkLaunch();
     }
-  }
-
-  int *nWorkPtr() { return counters + 10; }
-  // Work list of a pass over buffer b (aligned domains).
-  void buildWork(int b) {
-    VLSG_CUDA(cudaMemsetAsync(nWorkPtr(), 0, sizeof(int), stream));
-    Scope sc(this, "work_list");
-    const int o = 1 - buf[b].cur;
-    kBuildWork<T><<<grid1(cap), 256, 0, stream>>>(slotList, nSlotsPtr(), nbr, view(b),
-                                                  buf[b].state[o], buf[b].hasDef, work, nWorkPtr());
-    checkLaunch();
-  }
-  template <int R> void launchExpandFused(int b, const ExpandCycles<T> &cyc) {
-    constexpr int S = BS + 2 * R;
-    const size_t smem = 2 * (size_t)S * S * S * sizeof(T);
-    static bool attr = false;
-    if (!attr) {
-      VLSG_CUDA(cudaFuncSetAttribute(kExpandFused<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem));
-      attr = true;
-    }
-    kExpandFused<T, R><<<blocksPass, FUSED_THREADS, smem, stream>>>(g, work, nWorkPtr(), nbr,
-                                                                    view(b), outOf(b), cyc);
-  }
-  // `n` (<= MAX_FUSED_CYCLES) Expand cycles in one sweep of the pool.
-  void expandFused(int b, const ExpandCycles<T> &cyc) {
-    buildWork(b);
-    const int64_t nIn = buf[b].nDef;
-    {
-      Scope sc(this, "expand", [this, b, nIn, cyc] {
-        buf[b].nDef = (int64_t)defCounted();
-        return bandPassBytes(nIn, buf[b].nDef);
-      });
-      switch (cyc.n) {
-      case 1: launchExpandFused<1>(b, cyc); break;
-      case 2: launchExpandFused<2>(b, cyc); break;
-      case 3: launchExpandFused<3>(b, cyc); break;
-      default: launchExpandFused<4>(b, cyc); break;
-      }
-      checkLaunch();
-    }
-    flip(b);
-  }
-  template <class Rule> void starTable(int b, Rule rule, const char *name) {
-    buildWork(b);
-    const int64_t nIn = buf[b].nDef;
-    {
-      Scope sc(this, name, [this, b, nIn] {
-        buf[b].nDef = (int64_t)defCounted();
-        return bandPassBytes(nIn, buf[b].nDef);
-      });
-      kStarTable<T, Rule><<<blocksPass, FUSED_THREADS, 0, stream>>>(work, nWorkPtr(), nbr, view(b),
-                                                                   outOf(b), rule);
-      checkLaunch();
-    }
-    flip(b);
   }
 
   // Bring the allocated bricks back to dilate(core) of the live buffers.
@@ -519,34 +468,51 @@ public:
     }
     {
       Scope sc(this, "maint_free");
-      kFreeUnneeded<T><<<grid1(cap), 256, 0, stream>>>(slotList, nSlotsPtr(), brickMap, slotBrick,
-                                                       needed, bufSet(), freeStack,
+      kFreeUnneeded<T><<<grid1(cap), 256, 0, stream>>>(g, slotList, nSlotsPtr(), brickMap,
+                                                       slotBrick, needed, bufSet(), freeStack,
                                                        freeCountPtr(), errPtr());
       checkLaunch();
     }
+    VLSG_CUDA(cudaMemsetAsync(nNewPtr(), 0, sizeof(int), stream));
     {
       Scope sc(this, "maint_alloc");
       kAllocNeeded<<<grid1(nBricks), 256, 0, stream>>>(nBricks, brickMap, slotBrick, needed,
-                                                       bufSet(), freeStack, freeCountPtr(),
-                                                       errPtr());
+                                                       freeStack, freeCountPtr(), newList,
+                                                       nNewPtr(), errPtr());
+      checkLaunch();
+    }
+    {
+      Scope sc(this, "maint_init");
+      kInitNewSlots<T><<<blocksPass, 128, 0, stream>>>(g, newList, nNewPtr(), slotBrick, bufSet());
       checkLaunch();
     }
     rebuildSlotList();
   }
 
   // --------------------------------------------------------------- passes
-  template <class Rule> void starPass(int b, Rule rule, const char *name) {
-    const int64_t nIn = buf[b].nDef;
+  void applyChanges(int b) {
+    Scope sc(this, "apply_changes");
+    kApplyChanges<T><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(topo(), buf[b].vals, next, chg);
+    checkLaunch();
+  }
+
+  // One star pass of `rule` over buffer b: candidates, changes, write-back.
+  template <int MODE, class Rule> void frontierPass(int b, Rule rule, const char *name) {
+    const int64_t nIn = profiling ? defined(b) : 0;
     {
       Scope sc(this, name, [this, b, nIn] {
-        buf[b].nDef = (int64_t)defCounted();
+        // the output band is known once the new masks are current
+        buf[b].cur ^= 1;
+        buf[b].nDef = defined(b);
+        buf[b].cur ^= 1;
         return bandPassBytes(nIn, buf[b].nDef);
       });
-      kStarPass<T, Rule><<<blocksPass, PASS_THREADS, 0, stream>>>(g, mapView(), slotList, nSlotsPtr(),
-                                                                  view(b), outOf(b), rule);
+      kFrontierPass<T, MODE, Rule><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(topo(), lsView(b),
+                                                                                 rule);
       checkLaunch();
     }
-    flip(b);
+    applyChanges(b);
+    buf[b].cur ^= 1;
   }
 
   // Expand::apply (lsExpand.hpp:44-172)
@@ -555,60 +521,62 @@ public:
     const int startWidth = buf[b].width;
     const T totalLimit = T(width * 0.5);
     const int cycles = width - startWidth;
-    if (aligned) {
-      for (int c0 = 0; c0 < cycles; c0 += MAX_FUSED_CYCLES) {
-        ExpandCycles<T> cyc{};
-        cyc.n = std::min(MAX_FUSED_CYCLES, cycles - c0);
-        cyc.totalLimit = totalLimit;
-        for (int k = 0; k < cyc.n; ++k) cyc.limit[k] = T((startWidth + c0 + k + 1) * T(0.5));
-        expandFused(b, cyc);
-      }
-    } else {
-      for (int c = 0; c < cycles; ++c) {
-        ExpandRule<T> r{totalLimit, T((startWidth + c + 1) * T(0.5))};
-        starPass(b, r, "expand");
-      }
+    // defined cells with |value| <= totalLimit keep their value
+    const bool onlyUndefined = buf[b].bound <= (double)totalLimit;
+    for (int c = 0; c < cycles; ++c) {
+      ExpandRule<T> r{totalLimit, T((startWidth + c + 1) * T(0.5))};
+      if (onlyUndefined) frontierPass<FP_EXPAND>(b, r, "expand");
+      else frontierPass<FP_ALL>(b, r, "expand");
     }
     buf[b].width = width;
+    buf[b].bound = (double)totalLimit;
   }
   void prune(int b, bool rsz) {
-    if (aligned) starTable(b, PruneRule<T>{rsz}, "prune");
-    else starPass(b, PruneRule<T>{rsz}, "prune");
+    frontierPass<FP_PRUNE>(b, PruneRule<T>{rsz}, "prune");
     buf[b].width = 2;
   }
   void rebuild(int b) {
-    if (aligned) starTable(b, RebuildRule<T>{1.0}, "rebuild");
-    else starPass(b, RebuildRule<T>{1.0}, "rebuild");
+    frontierPass<FP_ALL>(b, RebuildRule<T>{1.0}, "rebuild");
     buf[b].width = 2;
+    buf[b].bound = 1.0;
   }
-  // updateLevelSet (Reduce(1) + update) and rebuildLS in one sweep
-  void updateRebuildFused(double dt) {
+  // updateLevelSet (value update + Reduce(1)) followed by rebuildLS
+  void updateRebuild(double dt) {
     const int top = L - 1;
-    buildWork(top);
     {
-      Scope sc(this, "update_rebuild", [this, top] {
-        buf[top].nDef = (int64_t)defCounted();
-        // stage: band values + rates of the active points; out: new band
-        return double(sizeof(T)) * double(lastBand + lastActive) + bandPassBytes(0, buf[top].nDef);
-      });
-      kUpdateRebuild<T><<<blocksPass, FUSED_THREADS, 0, stream>>>(
-          g, work, nWorkPtr(), nbr, view(top), outOf(top), rateV, rateStop, rateLen,
-          (size_t)cap * BV, L, currentTimeStep, 1.0, errPtr());
+      // active values read and written, their rates read
+      Scope sc(this, "update", [this] { return 3.0 * double(sizeof(T)) * double(lastActive); });
+      kUpdate<T><<<blocksPass, RATE_THREADS, 0, stream>>>(slotList, nSlotsPtr(), act, buf[top].vals,
+                                                          rateV, rateStop, rateLen, poolCells, L,
+                                                          dt, errPtr());
       checkLaunch();
     }
-    flip(top);
+    {
+      Scope sc(this, "update_rebuild", [this, top] {
+        buf[top].cur ^= 1;
+        buf[top].nDef = defined(top);
+        buf[top].cur ^= 1;
+        // in: the active band; out: the new band
+        return bandPassBytes(lastActive, buf[top].nDef);
+      });
+      kUpdateRebuild<T><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(topo(), lsView(top), act, 1.0);
+      checkLaunch();
+    }
+    applyChanges(top);
+    buf[top].cur ^= 1;
     buf[top].width = 2;
+    buf[top].bound = 1.0;
     ++stages;
   }
   template <class Comp> void pointwise(int a, int bb, Comp comp, int *flag) {
     {
-      const int64_t nA = buf[a].nDef, nB = buf[bb].nDef;
+      const int64_t nA = profiling ? defined(a) : 0, nB = profiling ? defined(bb) : 0;
       Scope sc(this, "boolean", [this, a, nA, nB] {
-        buf[a].nDef = (int64_t)defCounted();
+        buf[a].nDef = defined(a);
         return bandPassBytes(nA + nB, buf[a].nDef);
       });
-      kPointwise2<T, Comp><<<blocksPass, PASS_THREADS, 0, stream>>>(g, mapView(), slotList, nSlotsPtr(),
-                                                                    view(a), view(bb), outOf(a), comp, flag);
+      kPointwise<T, Comp><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(
+          topo(), buf[a].vals, buf[a].def[buf[a].cur], buf[bb].vals, comp, flag);
       checkLaunch();
     }
     {
@@ -617,7 +585,7 @@ public:
                                                                       buf[bb].farSign, buf[a].farSign, comp);
       checkLaunch();
     }
-    flip(a);
+    buf[a].bound = std::max(buf[a].bound, buf[bb].bound);
   }
   // BooleanOperation + Prune x2 (lsBooleanOperation.hpp:199-212)
   template <class Comp> void booleanOp(int a, int bb, Comp comp, int *flag = nullptr) {
@@ -632,12 +600,13 @@ public:
     auto &D = buf[dst];
     {
       Scope sc(this, "copy");
-      kCopySlots<T><<<blocksPass, 256, 0, stream>>>(slotList, nSlotsPtr(), S.vals[S.cur], S.state[S.cur],
-                                                    S.hasDef, D.vals[D.cur], D.state[D.cur], D.hasDef);
+      kCopySlots<T><<<blocksPass, 256, 0, stream>>>(slotList, nSlotsPtr(), S.vals, S.def[S.cur],
+                                                    D.vals, D.def[D.cur]);
       checkLaunch();
     }
     VLSG_CUDA(cudaMemcpyAsync(D.farSign, S.farSign, nBricks, cudaMemcpyDeviceToDevice, stream));
     D.width = S.width;
+    D.bound = S.bound;
     D.nDef = S.nDef;
     D.live = true;
   }
@@ -653,29 +622,18 @@ public:
     const bool globalLF = s == VLSG_LAX_FRIEDRICHS_1ST_ORDER || s == VLSG_LAX_FRIEDRICHS_2ND_ORDER;
     const bool lfFamily = !(s == VLSG_ENGQUIST_OSHER_1ST_ORDER || s == VLSG_ENGQUIST_OSHER_2ND_ORDER ||
                             s == VLSG_WENO_3RD_ORDER || s == VLSG_WENO_5TH_ORDER);
-    // the brick-staged rate kernel finds the active points itself; the list
-    // is needed by the generic path and by the global-alpha pre-pass
-    const bool useList = !aligned || globalLF;
-    VLSG_CUDA(cudaMemsetAsync(nActivePtr(), 0, sizeof(int), stream));
-    if (useList) {
-      Scope sc(this, "compact_active", [this] {
-        lastBand = (int64_t)bandCounted();
-        return double(sizeof(T)) * double(lastBand);
-      });
-      kCompactActiveWarp<T><<<blocksPass, RATE_THREADS, 0, stream>>>(slotList, nSlotsPtr(), view(top),
-                                                                     active, nActivePtr(),
-                                                                     (int)activeCap, errPtr(),
-                                                                     bandCounter());
-      checkLaunch();
-    }
+    double alphas[3] = {0, 0, 0};
     RateArgs<T> A{};
     A.g = g;
     A.m = mapView();
     for (int l = 0; l < L; ++l) A.ls[l] = view(l);
     A.L = L;
-    A.active = active;
-    A.nActive = nActivePtr();
-    A.activeCap = (int)activeCap;
+    A.slotList = slotList;
+    A.nSlots = nSlotsPtr();
+    A.nbr = nbr;
+    A.cflag = cflag;
+    A.def = buf[top].def[buf[top].cur];
+    A.act = act;
     A.scheme = P.spatial_scheme;
     A.cfl = P.time_step_ratio;
     A.dissipationAlpha = P.dissipation_alpha;
@@ -686,18 +644,18 @@ public:
     A.rateV = rateV;
     A.rateStop = rateStop;
     A.rateLen = rateLen;
-    A.poolCells = (size_t)cap * BV;
+    A.poolCells = poolCells;
     A.minStep = scal;
+    A.counts = rateCounts;
     A.err = errPtr();
     unsigned long long init[4] = {~0ull, 0, 0, 0};
     VLSG_CUDA(cudaMemcpyAsync(scal, init, sizeof(init), cudaMemcpyHostToDevice, stream));
-    double alphas[3] = {0, 0, 0};
-    const int rateBlocks = 148 * 8;
+    VLSG_CUDA(cudaMemsetAsync(rateCounts, 0, 2 * sizeof(unsigned long long), stream));
     if (globalLF) {
       A.alphaMax = scal + 1;
       {
         Scope sc(this, "global_alphas");
-        kGlobalAlphas<T><<<rateBlocks, RATE_THREADS, 0, stream>>>(A, vel);
+        kRates<T, 1><<<blocksPass, RATE_THREADS, 0, stream>>>(A, vel);
         checkLaunch();
       }
       VLSG_CUDA(cudaMemcpyAsync(pinScal, scal, sizeof(init), cudaMemcpyDeviceToHost, stream));
@@ -714,36 +672,24 @@ public:
     } else {
       A.alphaMax = nullptr;
     }
-    if (aligned) {
-      VLSG_CUDA(cudaMemsetAsync(nActivePtr(), 0, sizeof(int), stream));
-      if (profiling) VLSG_CUDA(cudaMemsetAsync(bandCounter(), 0, 8, stream));
+    {
       // stencil input (each band value once) + output per active point
       Scope sc(this, "rates", [this] {
-        int nAct = 0;
-        cudaMemcpy(&nAct, nActivePtr(), sizeof(int), cudaMemcpyDeviceToHost);
-        lastActive = nAct;
-        lastBand = (int64_t)bandCounted();
-        return double(sizeof(T)) * double(lastBand + nAct);
+        lastActive = (int64_t)readU64(rateCounts + 0);
+        lastBand = (int64_t)readU64(rateCounts + 1);
+        return double(sizeof(T)) * double(lastBand + lastActive);
       });
-      kRatesBrick<T><<<blocksPass, FUSED_THREADS, 0, stream>>>(A, vel, slotList, nSlotsPtr(), nbr,
-                                                                nActivePtr(), bandCounter());
-      checkLaunch();
-    } else {
-      Scope sc(this, "rates", [this] {
-        int nAct = 0;
-        cudaMemcpy(&nAct, nActivePtr(), sizeof(int), cudaMemcpyDeviceToHost);
-        lastActive = nAct;
-        return double(sizeof(T)) * double(lastBand + nAct);
-      });
-      kRates<T><<<rateBlocks, RATE_THREADS, 0, stream>>>(A, vel);
+      kRates<T, 0><<<blocksPass, RATE_THREADS, 0, stream>>>(A, vel);
       checkLaunch();
     }
     VLSG_CUDA(cudaMemcpyAsync(pinScal, scal, sizeof(init), cudaMemcpyDeviceToHost, stream));
+    VLSG_CUDA(cudaMemcpyAsync(pinScal + 4, rateCounts, 2 * sizeof(unsigned long long),
+                              cudaMemcpyDeviceToHost, stream));
     syncErr("rates");
     std::memcpy(hScal, pinScal, sizeof(hScal));
-    if ((size_t)hCounters[2] > activeCap)
-      throw CudaError("active list capacity exceeded", VLSG_ERR_CAPACITY);
-    pointUpdates += (uint64_t)hCounters[2];
+    lastActive = (int64_t)pinScal[4];
+    lastBand = (int64_t)pinScal[5];
+    pointUpdates += (uint64_t)lastActive;
     double tempMax = maxTimeStep;
     if (hScal[0] != ~0ull) {
       double m;
@@ -767,37 +713,6 @@ public:
     return maxTimeStep;
   }
 
-  void updateLevelSet(double dt) {
-    const int top = L - 1;
-    UpdateArgs<T> U{};
-    U.g = g;
-    U.m = mapView();
-    U.slotList = slotList;
-    U.nSlots = nSlotsPtr();
-    U.vals = buf[top].vals[buf[top].cur];
-    U.state = buf[top].state[buf[top].cur];
-    U.hasDef = buf[top].hasDef;
-    U.rateV = rateV;
-    U.rateStop = rateStop;
-    U.rateLen = rateLen;
-    U.poolCells = (size_t)cap * BV;
-    U.L = L;
-    U.dt = dt;
-    U.err = errPtr();
-    U.defCount = defCounter();
-    {
-      // active values read and written, their rates read
-      Scope sc(this, "update", [this, top] {
-        buf[top].nDef = (int64_t)defCounted();
-        return 3.0 * double(sizeof(T)) * double(lastActive);
-      });
-      kUpdate<T><<<blocksPass, RATE_THREADS, 0, stream>>>(U);
-      checkLaunch();
-    }
-    if (buf[top].width > 1) buf[top].width = 1; // Reduce(1), lsReduce.hpp:241-242
-    ++stages;
-  }
-
   void adjustLowerLayers(const vlsg_advect_params &P) {
     if (P.spatial_scheme == VLSG_STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER) return;
     for (int i = 0; i + 1 < L; ++i) booleanOp(i, L - 1, MaxComp<T>{});
@@ -806,12 +721,7 @@ public:
   double evolveForwardEuler(const vlsg_advect_params &P, double maxTimeStep,
                             bool updateLowerLayers) {
     const double dt = computeRates(P, maxTimeStep);
-    if (aligned) {
-      updateRebuildFused(dt);
-    } else {
-      updateLevelSet(dt);
-      rebuild(L - 1);
-    }
+    updateRebuild(dt);
     maintain();
     if (updateLowerLayers) adjustLowerLayers(P);
     return dt;
@@ -833,7 +743,7 @@ public:
     rebuild(top);
     maintain();
     if (L > 1) {
-      VLSG_CUDA(cudaMemcpyAsync(pinCounters, counters, 8 * sizeof(int), cudaMemcpyDeviceToHost, stream));
+      VLSG_CUDA(cudaMemcpyAsync(pinCounters, counters, 16 * sizeof(int), cudaMemcpyDeviceToHost, stream));
       VLSG_CUDA(cudaStreamSynchronize(stream));
       return pinCounters[4] != 0;
     }
@@ -848,26 +758,16 @@ public:
       // copy initial back into the current buffer
       auto &S = buf[L + l];
       auto &D = buf[l];
-      Scope sc(this, "copy");
-      kCopySlots<T><<<blocksPass, 256, 0, stream>>>(slotList, nSlotsPtr(), S.vals[S.cur], S.state[S.cur],
-                                                    S.hasDef, D.vals[D.cur], D.state[D.cur], D.hasDef);
-      checkLaunch();
+      {
+        Scope sc(this, "copy");
+        kCopySlots<T><<<blocksPass, 256, 0, stream>>>(slotList, nSlotsPtr(), S.vals, S.def[S.cur],
+                                                      D.vals, D.def[D.cur]);
+        checkLaunch();
+      }
       VLSG_CUDA(cudaMemcpyAsync(D.farSign, S.farSign, nBricks, cudaMemcpyDeviceToDevice, stream));
       D.width = S.width;
+      D.bound = S.bound;
       D.nDef = S.nDef;
-    }
-  }
-
-  // Recount the defined cells of every live buffer (profiling bookkeeping).
-  void recountDefined() {
-    for (int b = 0; b < 2 * L; ++b) {
-      if (!buf[b].live || !buf[b].vals[0]) continue;
-      VLSG_CUDA(cudaMemsetAsync(defCounter(), 0, sizeof(unsigned long long), stream));
-      kCountDefined<T><<<blocksPass, 256, 0, stream>>>(slotList, nSlotsPtr(), buf[b].vals[buf[b].cur],
-                                                       buf[b].state[buf[b].cur], defCounter());
-      checkLaunch();
-      VLSG_CUDA(cudaStreamSynchronize(stream));
-      buf[b].nDef = (int64_t)defCounted();
     }
   }
 
@@ -902,7 +802,6 @@ public:
   }
 
   void apply(const vlsg_advect_params &P, vlsg_advect_result &r) {
-    if (profiling) recountDefined();
     pointUpdates = 0;
     stages = 0;
     const uint64_t l0 = launches;
@@ -922,7 +821,7 @@ public:
       }
       advectedTime = currentTime;
     }
-    VLSG_CUDA(cudaStreamSynchronize(stream));
+    syncErr("advect");
     r.advected_time = advectedTime;
     r.current_time_step = currentTimeStep;
     r.number_of_time_steps = steps;
@@ -954,49 +853,45 @@ public:
 
   // Defined points of buffer b in HRLE order (keys sorted on the host).
   int64_t compact(int b, int32_t *idxOut, double *valOut, int64_t capOut) {
+    const int64_t n = defined(b);
+    if (!idxOut || !valOut || n > capOut) return n;
     VLSG_CUDA(cudaMemsetAsync(nOutPtr(), 0, sizeof(int), stream));
     uint64_t *dk = nullptr;
     double *dv = nullptr;
-    // count first
-    const size_t maxPts = (size_t)cap * BV;
-    size_t room = std::min<size_t>(maxPts, (size_t)cap * 256);
+    const size_t room = std::max<int64_t>(1, n);
     VLSG_CUDA(cudaMalloc(&dk, room * sizeof(uint64_t)));
     VLSG_CUDA(cudaMalloc(&dv, room * sizeof(double)));
     {
       Scope sc(this, "download_compact");
-      kCompactDefined<T><<<blocksPass, 256, 0, stream>>>(g, slotList, nSlotsPtr(), slotBrick,
-                                                         buf[b].vals[buf[b].cur],
-                                                         buf[b].state[buf[b].cur], dk, dv, nOutPtr(),
-                                                         (int)room);
+      kCompactDefined<T><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(
+          g, slotList, nSlotsPtr(), slotBrick, buf[b].vals, buf[b].def[buf[b].cur], dk, dv,
+          nOutPtr(), (int)room);
       checkLaunch();
     }
     syncErr("download");
-    const int64_t n = hCounters[5];
-    if ((size_t)n > room) {
+    if ((int64_t)hCounters[5] != n) {
       cudaFree(dk);
       cudaFree(dv);
-      throw CudaError("download buffer too small", VLSG_ERR_CAPACITY);
+      throw CudaError("download: defined-cell count mismatch", VLSG_ERR_DEVICE_CHECK);
     }
-    if (idxOut && valOut && n <= capOut) {
-      std::vector<uint64_t> hk(n);
-      std::vector<double> hv(n);
-      VLSG_CUDA(cudaMemcpyAsync(hk.data(), dk, n * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream));
-      VLSG_CUDA(cudaMemcpyAsync(hv.data(), dv, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
-      VLSG_CUDA(cudaStreamSynchronize(stream));
-      std::vector<int64_t> order(n);
-      for (int64_t i = 0; i < n; ++i) order[i] = i;
-      std::sort(order.begin(), order.end(), [&](int64_t a, int64_t c) { return hk[a] < hk[c]; });
-      const int64_t off = 1ll << 20;
-      for (int64_t i = 0; i < n; ++i) {
-        const uint64_t k = hk[order[i]];
-        idxOut[3 * i + 0] = (int32_t)((int64_t)(k & 0x1fffff) - off);
-        idxOut[3 * i + 1] = (int32_t)((int64_t)((k >> 21) & 0x1fffff) - off);
-        idxOut[3 * i + 2] = (int32_t)((int64_t)((k >> 42) & 0x1fffff) - off);
-        valOut[i] = hv[order[i]];
-      }
-    }
+    std::vector<uint64_t> hk(n);
+    std::vector<double> hv(n);
+    VLSG_CUDA(cudaMemcpyAsync(hk.data(), dk, n * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream));
+    VLSG_CUDA(cudaMemcpyAsync(hv.data(), dv, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    VLSG_CUDA(cudaStreamSynchronize(stream));
     cudaFree(dk);
     cudaFree(dv);
+    std::vector<int64_t> order(n);
+    for (int64_t i = 0; i < n; ++i) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](int64_t a, int64_t c) { return hk[a] < hk[c]; });
+    const int64_t off = 1ll << 20;
+    for (int64_t i = 0; i < n; ++i) {
+      const uint64_t k = hk[order[i]];
+      idxOut[3 * i + 0] = (int32_t)((int64_t)(k & 0x1fffff) - off);
+      idxOut[3 * i + 1] = (int32_t)((int64_t)((k >> 21) & 0x1fffff) - off);
+      idxOut[3 * i + 2] = (int32_t)((int64_t)((k >> 42) & 0x1fffff) - off);
+      valOut[i] = hv[order[i]];
+    }
     return n;
   }
 };

@@ -1,11 +1,12 @@
 // vlsg_maint.cuh -- slot-pool maintenance, upload and download kernels.
 //
-// After every pass that can move the band, the set of allocated bricks is
-// brought back to "every brick holding a defined cell of any live level set,
-// plus its 26 neighbours": a band moves at most one cell per pass and at most
-// a few cells between two maintenances, so reads never reach a brick whose
-// cells are unknown.  A freed brick records its (uniform) sign per level set
-// in the far-sign map; a new brick starts UNIFORM with that sign.
+// After every stage the set of allocated bricks is brought back to "every
+// brick holding a defined cell of any live level set, plus its 26
+// neighbours": the band moves at most one cell per pass and at most a few
+// cells between two maintenances, so every cell a pass can change lies in an
+// allocated brick.  A freed brick records its (uniform) sign per level set in
+// the far-sign map; a new brick starts with every cell undefined with that
+// sign.
 #pragma once
 
 #include "vlsg_common.cuh"
@@ -13,14 +14,16 @@
 namespace vlsg {
 
 struct BufSet {
-  const uint8_t *hasDef[MAXB];
-  uint8_t *state[MAXB];   // current side
+  void *vals[MAXB];
+  uint64_t *def[MAXB]; // current defined masks
   int8_t *farSign[MAXB];
-  uint8_t *hasDefW[MAXB];
-  const void *vals[MAXB]; // current side
   int nBuf;
-  int elem; // sizeof(T)
 };
+
+__device__ inline bool slotHasDef(const uint64_t *def, int slot) {
+  const uint64_t *w = def + (size_t)slot * 8;
+  return (w[0] | w[1] | w[2] | w[3] | w[4] | w[5] | w[6] | w[7]) != 0ull;
+}
 
 __device__ inline bool neighbourBrick(const GridDev &g, int &x, int &y, int &z) {
   int c[3] = {x, y, z};
@@ -34,6 +37,22 @@ __device__ inline bool neighbourBrick(const GridDev &g, int &x, int &y, int &z) 
   return true;
 }
 
+__device__ inline void markDilated(const GridDev &g, int bi, uint8_t *needed, int *err) {
+  int bx, by, bz;
+  brickCoords(g, bi, bx, by, bz);
+  const int c[3] = {bx, by, bz};
+  for (int d = 0; d < 3; ++d)
+    if (g.bc[d] != VLSG_PERIODIC_BOUNDARY && g.bc[d] != VLSG_REFLECTIVE_BOUNDARY &&
+        (c[d] <= 0 || c[d] >= g.nb[d] - 1))
+      atomicOr(err, 1);
+  for (int dz = -1; dz <= 1; ++dz)
+    for (int dy = -1; dy <= 1; ++dy)
+      for (int dx = -1; dx <= 1; ++dx) {
+        int x = bx + dx, y = by + dy, z = bz + dz;
+        if (neighbourBrick(g, x, y, z)) needed[brickIndex(g, x, y, z)] = 1;
+      }
+}
+
 // err bits: 1 box too small (infinite direction), 4 pool capacity,
 // 8 a freed brick still held a defined cell
 __global__ void kMarkNeeded(GridDev g, const int *slotBrick, const int *slotList,
@@ -42,47 +61,31 @@ __global__ void kMarkNeeded(GridDev g, const int *slotBrick, const int *slotList
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int slot = slotList[i];
     bool core = false;
-    for (int b = 0; b < B.nBuf; ++b) core |= B.hasDef[b][slot] != 0;
-    if (!core) continue;
-    int bx, by, bz;
-    brickCoords(g, slotBrick[slot], bx, by, bz);
-    const int c[3] = {bx, by, bz};
-    for (int d = 0; d < 3; ++d)
-      if (g.bc[d] != VLSG_PERIODIC_BOUNDARY && g.bc[d] != VLSG_REFLECTIVE_BOUNDARY &&
-          (c[d] <= 0 || c[d] >= g.nb[d] - 1))
-        atomicOr(err, 1);
-    for (int dz = -1; dz <= 1; ++dz)
-      for (int dy = -1; dy <= 1; ++dy)
-        for (int dx = -1; dx <= 1; ++dx) {
-          int x = bx + dx, y = by + dy, z = bz + dz;
-          if (neighbourBrick(g, x, y, z)) needed[brickIndex(g, x, y, z)] = 1;
-        }
+    for (int b = 0; b < B.nBuf; ++b) core |= slotHasDef(B.def[b], slot);
+    if (core) markDilated(g, slotBrick[slot], needed, err);
   }
 }
 
 __global__ void kDilateBricks(GridDev g, int nBricks, const uint8_t *core,
                               uint8_t *needed, int *err) {
   for (int bi = blockIdx.x * blockDim.x + threadIdx.x; bi < nBricks;
-       bi += gridDim.x * blockDim.x) {
-    if (!core[bi]) continue;
-    int bx, by, bz;
-    brickCoords(g, bi, bx, by, bz);
-    const int c[3] = {bx, by, bz};
-    for (int d = 0; d < 3; ++d)
-      if (g.bc[d] != VLSG_PERIODIC_BOUNDARY && g.bc[d] != VLSG_REFLECTIVE_BOUNDARY &&
-          (c[d] <= 0 || c[d] >= g.nb[d] - 1))
-        atomicOr(err, 1);
-    for (int dz = -1; dz <= 1; ++dz)
-      for (int dy = -1; dy <= 1; ++dy)
-        for (int dx = -1; dx <= 1; ++dx) {
-          int x = bx + dx, y = by + dy, z = bz + dz;
-          if (neighbourBrick(g, x, y, z)) needed[brickIndex(g, x, y, z)] = 1;
-        }
-  }
+       bi += gridDim.x * blockDim.x)
+    if (core[bi]) markDilated(g, bi, needed, err);
+}
+
+// First cell of a brick that exists in the grid (cells of the last brick of
+// a bounded direction may lie past its end).
+__device__ inline int firstExistingCell(const GridDev &g, int bi) {
+  int bx, by, bz;
+  brickCoords(g, bi, bx, by, bz);
+  const int x0 = g.org[0] + bx * BS, y0 = g.org[1] + by * BS, z0 = g.org[2] + bz * BS;
+  for (int c = 0; c < BV; ++c)
+    if (cellExists(g, x0 + (c & 7), y0 + ((c >> 3) & 7), z0 + (c >> 6))) return c;
+  return 0;
 }
 
 template <class T>
-__global__ void kFreeUnneeded(const int *slotList, const int *nSlots, int *brickMap,
+__global__ void kFreeUnneeded(GridDev g, const int *slotList, const int *nSlots, int *brickMap,
                               int *slotBrick, const uint8_t *needed, BufSet B,
                               int *freeStack, int *freeCount, int *err) {
   const int n = *nSlots;
@@ -90,17 +93,11 @@ __global__ void kFreeUnneeded(const int *slotList, const int *nSlots, int *brick
     const int slot = slotList[i];
     const int bi = slotBrick[slot];
     if (needed[bi]) continue;
+    const int c = firstExistingCell(g, bi);
     for (int b = 0; b < B.nBuf; ++b) {
-      const uint8_t st = B.state[b][slot];
-      int8_t s;
-      if (st == ST_DENSE) {
-        const T v = ((const T *)B.vals[b])[(size_t)slot * BV];
-        if (isDef(v)) atomicOr(err, 8);
-        s = v < 0 ? -1 : 1;
-      } else {
-        s = st == ST_UNEG ? -1 : 1;
-      }
-      B.farSign[b][bi] = s;
+      if (slotHasDef(B.def[b], slot)) atomicOr(err, 8);
+      const T v = ((const T *)B.vals[b])[(size_t)slot * BV + c];
+      B.farSign[b][bi] = v < 0 ? -1 : 1;
     }
     brickMap[bi] = -1;
     slotBrick[slot] = -1;
@@ -108,9 +105,10 @@ __global__ void kFreeUnneeded(const int *slotList, const int *nSlots, int *brick
   }
 }
 
-__global__ void kAllocNeeded(int nBricks, int *brickMap, int *slotBrick,
-                             const uint8_t *needed, BufSet B, int *freeStack,
-                             int *freeCount, int *err) {
+// Allocate a slot for every needed brick without one; list the new slots.
+__global__ void kAllocNeeded(int nBricks, int *brickMap, int *slotBrick, const uint8_t *needed,
+                             int *freeStack, int *freeCount, int *newList, int *nNew,
+                             int *err) {
   for (int bi = blockIdx.x * blockDim.x + threadIdx.x; bi < nBricks;
        bi += gridDim.x * blockDim.x) {
     if (!needed[bi] || brickMap[bi] >= 0) continue;
@@ -123,9 +121,30 @@ __global__ void kAllocNeeded(int nBricks, int *brickMap, int *slotBrick,
     const int slot = freeStack[k];
     brickMap[bi] = slot;
     slotBrick[slot] = bi;
+    if (newList) newList[atomicAdd(nNew, 1)] = slot;
+  }
+}
+
+// New slots: every cell undefined with the brick's far sign, no defined cell.
+// Cells past the end of a bounded direction hold +max.
+template <class T>
+__global__ void kInitNewSlots(GridDev g, const int *newList, const int *nNew,
+                              const int *slotBrick, BufSet B) {
+  const int n = *nNew;
+  for (int it = blockIdx.x; it < n; it += gridDim.x) {
+    const int slot = newList[it];
+    const int bi = slotBrick[slot];
+    int bx, by, bz;
+    brickCoords(g, bi, bx, by, bz);
     for (int b = 0; b < B.nBuf; ++b) {
-      B.state[b][slot] = B.farSign[b][bi] < 0 ? ST_UNEG : ST_UPOS;
-      B.hasDefW[b][slot] = 0;
+      const T s = B.farSign[b][bi] < 0 ? Lim<T>::lowest() : Lim<T>::max();
+      T *v = (T *)B.vals[b] + (size_t)slot * BV;
+      for (int c = threadIdx.x; c < BV; c += blockDim.x) {
+        const bool ex = cellExists(g, g.org[0] + bx * BS + (c & 7),
+                                   g.org[1] + by * BS + ((c >> 3) & 7), g.org[2] + bz * BS + (c >> 6));
+        v[c] = ex ? s : Lim<T>::max();
+      }
+      if (threadIdx.x < 8) B.def[b][(size_t)slot * 8 + threadIdx.x] = 0ull;
     }
   }
 }
@@ -230,73 +249,78 @@ __global__ void kScatterPoints(GridDev g, int n, const int *idx, const double *v
   }
 }
 
-// Set state / hasDef of every slot from its cells.
+
+// Defined masks and defined-cell count of a buffer from its values (after an
+// upload); cells past the end of a bounded direction are set to +max.
 template <class T>
-__global__ void kNormalize(GridDev g, const int *slotList, const int *nSlots,
-                           const int *slotBrick, T *vals, uint8_t *state,
-                           uint8_t *hasDef, unsigned long long *defCount) {
+__global__ void kMasksFromValues(GridDev g, const int *slotBrick, const int *slotList,
+                                 const int *nSlots, T *vals, uint64_t *def,
+                                 unsigned long long *cnt) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nWarps = (gridDim.x * blockDim.x) >> 5;
   const int n = *nSlots;
-  for (int it = blockIdx.x; it < n; it += gridDim.x) {
-    const int slot = slotList[it];
+  for (int w = warp; w < n; w += nWarps) {
+    const int slot = slotList[w];
     int bx, by, bz;
     brickCoords(g, slotBrick[slot], bx, by, bz);
-    bool anyDef = false, allPos = true, allNeg = true;
-    for (int c = threadIdx.x; c < BV; c += blockDim.x) {
-      const int x = g.org[0] + bx * BS + (c & 7), y = g.org[1] + by * BS + ((c >> 3) & 7),
-                z = g.org[2] + bz * BS + (c >> 6);
-      T v = vals[(size_t)slot * BV + c];
-      if (!cellExists(g, x, y, z)) {
-        vals[(size_t)slot * BV + c] = Lim<T>::max();
-        continue;
-      }
-      if (isDef(v)) anyDef = true;
-      else if (v < 0) allPos = false;
-      else allNeg = false;
-    }
     int nd = 0;
-    for (int c = 0; c < BV; c += blockDim.x) {
-      const int cc = c + threadIdx.x;
-      const bool d = cc < BV && isDef(vals[(size_t)slot * BV + cc]);
-      nd += __syncthreads_count(d);
+    uint64_t mine = 0;
+    for (int z = 0; z < 8; ++z) {
+      uint64_t bits = 0;
+      for (int half = 0; half < 2; ++half) {
+        const int c = z * 64 + half * 32 + lane;
+        T v = vals[(size_t)slot * BV + c];
+        if (!cellExists(g, g.org[0] + bx * BS + (c & 7), g.org[1] + by * BS + ((c >> 3) & 7),
+                        g.org[2] + bz * BS + (c >> 6))) {
+          v = Lim<T>::max();
+          vals[(size_t)slot * BV + c] = v;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, isDef(v));
+        bits |= (uint64_t)m << (32 * half);
+        nd += lane == 0 ? __popc(m) : 0;
+      }
+      if (lane == z) mine = bits;
     }
-    if (threadIdx.x == 0 && nd) atomicAdd(defCount, (unsigned long long)nd);
-    const int any = __syncthreads_or(anyDef);
-    const int ap = __syncthreads_and(allPos);
-    const int an = __syncthreads_and(allNeg);
-    if (threadIdx.x == 0) {
-      state[slot] = (!any && ap) ? ST_UPOS : ((!any && an) ? ST_UNEG : ST_DENSE);
-      hasDef[slot] = any ? 1 : 0;
-    }
+    if (lane < 8) def[(size_t)slot * 8 + lane] = mine;
+    if (lane == 0 && nd && cnt) atomicAdd(cnt, (unsigned long long)nd);
   }
 }
 
-// Defined cells of a buffer as (HRLE key, value) pairs.
+// Defined cells of a buffer as (HRLE key, value) pairs (one warp per slot,
+// walking the set bits of its mask).
 template <class T>
 __global__ void kCompactDefined(GridDev g, const int *slotList, const int *nSlots,
-                                const int *slotBrick, const T *vals,
-                                const uint8_t *state, uint64_t *keys, double *out,
-                                int *nOut, int room) {
+                                const int *slotBrick, const T *vals, const uint64_t *def,
+                                uint64_t *keys, double *out, int *nOut, int room) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nWarps = (gridDim.x * blockDim.x) >> 5;
   const int n = *nSlots;
-  for (int it = blockIdx.x; it < n; it += gridDim.x) {
-    const int slot = slotList[it];
-    if (state[slot] != ST_DENSE) continue;
+  for (int w = warp; w < n; w += nWarps) {
+    const int slot = slotList[w];
     int bx, by, bz;
     brickCoords(g, slotBrick[slot], bx, by, bz);
-    for (int k = 0; k < BV / 256; ++k) {
-      const int c = threadIdx.x + k * 256;
-      const int x = g.org[0] + bx * BS + (c & 7), y = g.org[1] + by * BS + ((c >> 3) & 7),
-                z = g.org[2] + bz * BS + (c >> 6);
-      const T v = vals[(size_t)slot * BV + c];
-      const bool d = isDef(v) && cellExists(g, x, y, z);
-      const unsigned mask = __ballot_sync(0xffffffffu, d);
-      const int lane = threadIdx.x & 31;
-      int off = 0;
-      if (lane == 0 && mask) off = atomicAdd(nOut, __popc(mask));
-      off = __shfl_sync(0xffffffffu, off, 0);
-      const int p = off + __popc(mask & ((1u << lane) - 1));
-      if (d && p < room) {
-        keys[p] = cellKey(x, y, z);
-        out[p] = (double)v;
+    for (int z = 0; z < 8; ++z) {
+      const uint64_t m = def[(size_t)slot * 8 + z];
+      if (!m) continue;
+      const unsigned lo = (unsigned)m, hi = (unsigned)(m >> 32);
+      const int nlo = __popc(lo), cnt = nlo + __popc(hi);
+      for (int base = 0; base < cnt; base += 32) {
+        const int k = base + lane;
+        const bool has = k < cnt;
+        int c = 0;
+        if (has) c = z * 64 + (k < nlo ? __fns(lo, 0, k + 1) : 32 + __fns(hi, 0, k - nlo + 1));
+        const unsigned mask = __ballot_sync(0xffffffffu, has);
+        int off = 0;
+        if (lane == 0) off = atomicAdd(nOut, __popc(mask));
+        off = __shfl_sync(0xffffffffu, off, 0);
+        const int p = off + lane;
+        if (has && p < room) {
+          keys[p] = cellKey(g.org[0] + bx * BS + (c & 7), g.org[1] + by * BS + ((c >> 3) & 7),
+                            g.org[2] + bz * BS + (c >> 6));
+          out[p] = (double)vals[(size_t)slot * BV + c];
+        }
       }
     }
   }
@@ -311,36 +335,34 @@ __global__ void kQueryValues(GridDev g, MapView m, Buf<T> b, int n, const int *i
   }
 }
 
-template <class T>
-__global__ void kCountDefined(const int *slotList, const int *nSlots, const T *vals,
-                              const uint8_t *state, unsigned long long *cnt) {
+
+// Defined cells of a buffer, from its masks.
+__global__ void kCountDefined(const int *slotList, const int *nSlots, const uint64_t *def,
+                              unsigned long long *cnt) {
   const int n = *nSlots;
-  for (int it = blockIdx.x; it < n; it += gridDim.x) {
-    const int slot = slotList[it];
-    if (state[slot] != ST_DENSE) continue;
+  for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    const int i = base + threadIdx.x;
     int nd = 0;
-    for (int c = 0; c < BV; c += blockDim.x)
-      nd += __syncthreads_count(isDef(vals[(size_t)slot * BV + c + threadIdx.x]));
-    if (threadIdx.x == 0 && nd) atomicAdd(cnt, (unsigned long long)nd);
+    if (i < n) {
+      const uint64_t *w = def + (size_t)slotList[i] * 8;
+      for (int k = 0; k < 8; ++k) nd += __popcll(w[k]);
+    }
+    for (int o = 16; o > 0; o >>= 1) nd += __shfl_xor_sync(0xffffffffu, nd, o);
+    if ((threadIdx.x & 31) == 0 && nd) atomicAdd(cnt, (unsigned long long)nd);
   }
 }
 
-// Copy the listed slots of one buffer into another (RK initial copies).
+// Copy the listed slots of one buffer (values and masks) into another.
 template <class T>
 __global__ void kCopySlots(const int *slotList, const int *nSlots, const T *sv,
-                           const uint8_t *ss, const uint8_t *sh, T *dv, uint8_t *ds,
-                           uint8_t *dh) {
-  const int n = *nSlots;
-  for (int it = blockIdx.x; it < n; it += gridDim.x) {
-    const int slot = slotList[it];
-    const uint8_t st = ss[slot];
-    if (threadIdx.x == 0) {
-      ds[slot] = st;
-      dh[slot] = sh[slot];
-    }
-    if (st == ST_DENSE)
-      for (int c = threadIdx.x; c < BV; c += blockDim.x)
-        dv[(size_t)slot * BV + c] = sv[(size_t)slot * BV + c];
+                           const uint64_t *sd, T *dv, uint64_t *dd) {
+  const size_t n = (size_t)*nSlots * BV;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const size_t slot = slotList[i >> 9];
+    const int c = i & (BV - 1);
+    dv[slot * BV + c] = sv[slot * BV + c];
+    if (c < 8) dd[slot * 8 + c] = sd[slot * 8 + c];
   }
 }
 

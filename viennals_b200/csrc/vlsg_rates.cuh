@@ -12,11 +12,16 @@
 // Expressions keep the reference's evaluation order; the library is compiled
 // with -fmad=false so FP64 results are bit-identical to the CPU restatement.
 //
-// One thread per active point.  Neighbours inside the point's own brick are
-// read directly from the slot; the rest go through the brick map.
+// One warp per brick: the brick's active cells are found from its defined
+// mask and taken 32 at a time, one thread per active point.  Stencil values
+// come through the slot's 27-neighbour table, or through the brick map and
+// the boundary mapping for bricks within 8 cells of a boundary that remaps
+// cells.  Outputs are pool shaped (cell q of chain entry j at
+// j * poolCells + q).
 #pragma once
 
 #include "vlsg_common.cuh"
+#include "vlsg_frontier.cuh"
 #include "vlsg_passes.cuh"
 
 namespace vlsg {
@@ -61,9 +66,11 @@ template <class T> struct RateArgs {
   MapView m;
   Buf<T> ls[VLSG_MAX_LEVEL_SETS];
   int L;
-  const uint32_t *active;
-  const int *nActive;
-  int activeCap;
+  const int *slotList, *nSlots;
+  const int *nbr;       // 27-neighbour table per slot
+  const uint8_t *cflag; // CF_* per slot
+  const uint64_t *def;  // defined masks of the top level set
+  uint64_t *act;        // out: active masks of the top level set
   int scheme;
   double cfl;
   double dissipationAlpha;
@@ -72,13 +79,14 @@ template <class T> struct RateArgs {
   double adaptiveFactor;
   int checkDiss;
   T globalAlpha[3];
-  // outputs (pool shaped: entry j of cell q at j * poolCells + q)
+  // outputs: chain entry j of cell q at j * poolCells + q
   T *rateV;
   T *rateStop;
   uint8_t *rateLen;
   size_t poolCells;
   unsigned long long *minStep;  // bits of the smallest non-negative step
   unsigned long long *alphaMax; // bits of the LLF/LLLF alphas
+  unsigned long long *counts;   // out: active cells, band cells
   int *err;
 };
 
@@ -100,14 +108,22 @@ template <class T> struct Stencil {
   }
 };
 
-// Reader of a brick staged in shared memory with a halo of H cells.
-template <class T, int H> struct BoxStencil {
-  static constexpr int S = BS + 2 * H;
-  const T *box;
-  int o; // index of the centre cell
-  __device__ T at(int dx, int dy, int dz) const { return box[o + (dz * S + dy) * S + dx]; }
+// Reader of the top level set around one active point through the slot's
+// 27-neighbour table (offsets up to 8 cells; every cell it reaches exists and
+// is not remapped by a boundary).
+template <class T> struct TableStencil {
+  const T *vals;
+  const int8_t *farSign;
+  const int *nb27;
+  int lx, ly, lz;
+  __device__ T at(int dx, int dy, int dz) const {
+    const int nx = lx + dx, ny = ly + dy, nz = lz + dz;
+    const int ref = nb27[((nz >> 3) + 1) * 9 + ((ny >> 3) + 1) * 3 + ((nx >> 3) + 1)];
+    if (ref < 0) return farSign[-1 - ref] < 0 ? Lim<T>::lowest() : Lim<T>::max();
+    return vals[(size_t)ref * BV + ((nz & 7) * 64 + (ny & 7) * 8 + (nx & 7))];
+  }
   __device__ T axis(int d, int off) const {
-    return box[o + off * (d == 0 ? 1 : (d == 1 ? S : S * S))];
+    return d == 0 ? at(off, 0, 0) : (d == 1 ? at(0, off, 0) : at(0, 0, off));
   }
 };
 
@@ -398,28 +414,30 @@ __device__ void evalScheme(const RateArgs<T> &A, const vlsg_velocity_desc &vel,
 
 template <class T>
 __device__ inline T lsValueAt(const Buf<T> &b, int slot, int c) {
-  const uint8_t st = b.state[slot];
-  if (st == ST_DENSE) return b.vals[(size_t)slot * BV + c];
-  return st == ST_UNEG ? Lim<T>::lowest() : Lim<T>::max();
+  return b.vals[(size_t)slot * BV + c];
 }
 
-// Warp + block reduction of the per-point minima / maxima into global atomics.
-__device__ inline void atomicMinStep(unsigned long long *dst, double v) {
-  // v >= 0 or NaN; NaN never lowers the minimum (lsAdvect.hpp:591)
-  unsigned long long b = (v >= 0.0) ? orderedBits(v + 0.0) : ~0ull;
+// Bits of a per-point step for the minimum (v >= 0; NaN or "no point" -1
+// never lowers the minimum, lsAdvect.hpp:591) and of an alpha for the maximum.
+__device__ inline unsigned long long stepBits(double v) {
+  return (v >= 0.0) ? orderedBits(v + 0.0) : ~0ull;
+}
+__device__ inline unsigned long long alphaBits(double v) {
+  return (v > 0.0) ? orderedBits(v) : 0ull;
+}
+__device__ inline unsigned long long warpMinU64(unsigned long long b) {
   for (int o = 16; o > 0; o >>= 1) {
     const unsigned long long t = __shfl_xor_sync(0xffffffffu, b, o);
     b = t < b ? t : b;
   }
-  if ((threadIdx.x & 31) == 0 && b != ~0ull) atomicMin(dst, b);
+  return b;
 }
-__device__ inline void atomicMaxAlpha(unsigned long long *dst, double v) {
-  unsigned long long b = (v > 0.0) ? orderedBits(v) : 0ull;
+__device__ inline unsigned long long warpMaxU64(unsigned long long b) {
   for (int o = 16; o > 0; o >>= 1) {
     const unsigned long long t = __shfl_xor_sync(0xffffffffu, b, o);
     b = t > b ? t : b;
   }
-  if ((threadIdx.x & 31) == 0 && b != 0ull) atomicMax(dst, b);
+  return b;
 }
 
 // integrateTime for one active point (lsAdvect.hpp:501-592): the material
@@ -480,196 +498,181 @@ __device__ inline double ratePoint(const RateArgs<T> &A, const vlsg_velocity_des
   return maxStepTime;
 }
 
+// Stencil of local cell c of `slot`: the table reader, or the global one
+// near a boundary that remaps cells; fn(stencil, centre value).
+template <class T, class Fn>
+__device__ inline void withStencil(const RateArgs<T> &A, int slot, int c, Fn fn) {
+  const Buf<T> &top = A.ls[A.L - 1];
+  const T C = top.vals[(size_t)slot * BV + c];
+  if (A.cflag[slot] & CF_NEAR) {
+    int bx, by, bz;
+    brickCoords(A.g, A.m.slotBrick[slot], bx, by, bz);
+    const Stencil<T> S{A.g, A.m, top, slot, c & 7, (c >> 3) & 7, c >> 6,
+                       A.g.org[0] + bx * BS, A.g.org[1] + by * BS, A.g.org[2] + bz * BS};
+    fn(S, C);
+  } else {
+    const TableStencil<T> S{top.vals, top.farSign, A.nbr + (size_t)slot * 27, c & 7,
+                            (c >> 3) & 7, c >> 6};
+    fn(S, C);
+  }
+}
+
+// Active mask of a brick (defined cells with |phi| <= 0.5, lsAdvect.hpp:498;
+// lane z returns plane z); `words` is the warp's shared scratch.
 template <class T>
+__device__ inline uint64_t activePlanes(const T *vals, int slot, uint64_t own,
+                                        unsigned long long *words) {
+  const int lane = threadIdx.x & 31;
+  if (lane < 8) words[lane] = 0ull;
+  __syncwarp();
+  const PlaneEnum pe(own);
+  for (int base = 0; base < pe.total; base += 32) {
+    const int k = base + lane;
+    const int c = pe.cell(own, k < pe.total ? k : pe.total - 1);
+    if (k < pe.total) {
+      const T v = vals[(size_t)slot * BV + c];
+      if (isDef(v) && fabs(v) <= T(0.5)) markCell(words, c);
+    }
+  }
+  __syncwarp();
+  const uint64_t a = lane < 8 ? words[lane] : 0ull;
+  __syncwarp();
+  return a;
+}
+
+// integrateTime over every active point (MODE 0), or findGlobalAlphas
+// (lsAdvect.hpp:90-195, MODE 1).  Minima, maxima and counts are kept per
+// thread and reach global memory once per warp.
+template <class T, int MODE>
 __global__ void __launch_bounds__(RATE_THREADS)
     kRates(RateArgs<T> A, const vlsg_velocity_desc vel) {
-  const int n = min(*A.nActive, A.activeCap);
+  __shared__ unsigned long long sAct[RATE_THREADS / 32][8];
+  unsigned long long *words = sAct[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nWarps = (gridDim.x * blockDim.x) >> 5;
+  const int n = *A.nSlots;
   const int L = A.L;
   const Buf<T> &top = A.ls[L - 1];
-  for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-    const int i = base + threadIdx.x;
-    double maxStepTime = -1.0; // "no point"
-    T alphas[3] = {0, 0, 0};
-    if (i < n) {
-      const uint32_t q = A.active[i];
-      const int slot = q >> 9, c = q & 511;
-      const int bi = A.m.slotBrick[slot];
-      int bx, by, bz;
-      brickCoords(A.g, bi, bx, by, bz);
-      const Stencil<T> S{A.g, A.m, top, slot, c & 7, (c >> 3) & 7, c >> 6,
-                         A.g.org[0] + bx * BS, A.g.org[1] + by * BS,
-                         A.g.org[2] + bz * BS};
-      const T C = top.vals[(size_t)slot * BV + c];
-      maxStepTime = ratePoint<T>(A, vel, S, slot, c, C, alphas);
+  unsigned long long minBits = ~0ull, alphaMax[3] = {0, 0, 0}, nAct = 0, nBand = 0;
+  for (int w = warp; w < n; w += nWarps) {
+    const int slot = A.slotList[w];
+    const uint64_t own = lane < 8 ? A.def[(size_t)slot * 8 + lane] : 0ull;
+    uint64_t a = 0ull;
+    if (__any_sync(0xffffffffu, own != 0ull)) a = activePlanes<T>(top.vals, slot, own, words);
+    if (lane < 8) {
+      if (MODE == 0) A.act[(size_t)slot * 8 + lane] = a;
+      nAct += __popcll(a);
+      nBand += __popcll(own);
     }
-    atomicMinStep(A.minStep, maxStepTime);
-    if (A.alphaMax) {
-      for (int k = 0; k < 3; ++k) atomicMaxAlpha(&A.alphaMax[k], (double)alphas[k]);
-    }
-  }
-}
-
-// findGlobalAlphas, lsAdvect.hpp:90-195.
-template <class T>
-__global__ void __launch_bounds__(RATE_THREADS)
-    kGlobalAlphas(RateArgs<T> A, const vlsg_velocity_desc vel) {
-  const int n = min(*A.nActive, A.activeCap);
-  const int L = A.L;
-  const Buf<T> &top = A.ls[L - 1];
-  for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-    const int i = base + threadIdx.x;
-    T la[3] = {0, 0, 0};
-    if (i < n) {
-      const uint32_t q = A.active[i];
-      const int slot = q >> 9, c = q & 511;
-      const int bi = A.m.slotBrick[slot];
-      int bx, by, bz;
-      brickCoords(A.g, bi, bx, by, bz);
-      const Stencil<T> S{A.g, A.m, top, slot, c & 7, (c >> 3) & 7, c >> 6,
-                         A.g.org[0] + bx * BS, A.g.org[1] + by * BS,
-                         A.g.org[2] + bz * BS};
-      const T value = top.vals[(size_t)slot * BV + c];
-      for (int lower = 0; lower < L; ++lower) {
-        const T lv = lower == L - 1 ? value : lsValueAt<T>(A.ls[lower], slot, c);
-        if ((double)lv <= (double)value + 1e-4) {
-          T normal[3];
-          T normalModulus = 0.;
-          for (int k = 0; k < 3; ++k) {
-            const T phiPos = S.axis(k, 1);
-            const T phiNeg = S.axis(k, -1);
-            normal[k] = phiPos - phiNeg;
-            normalModulus += normal[k] * normal[k];
+    const PlaneEnum pa(a);
+    for (int base = 0; base < pa.total; base += 32) {
+      const int k = base + lane;
+      const int c = pa.cell(a, k < pa.total ? k : pa.total - 1);
+      if (k >= pa.total) continue;
+      withStencil<T>(A, slot, c, [&](const auto &S, T value) {
+        if (MODE == 0) {
+          T alphas[3] = {0, 0, 0};
+          const double step = ratePoint<T>(A, vel, S, slot, c, value, alphas);
+          const unsigned long long sb = stepBits(step);
+          minBits = sb < minBits ? sb : minBits;
+          for (int d = 0; d < 3; ++d) {
+            const unsigned long long ab = alphaBits((double)alphas[d]);
+            alphaMax[d] = ab > alphaMax[d] ? ab : alphaMax[d];
           }
-          normalModulus = T(1.) / sqrt(normalModulus);
-          for (int k = 0; k < 3; ++k) normal[k] *= normalModulus;
-          const T scaVel = scalarVelocity<T>(vel, lower, normal);
-          T vecVel[3];
-          vectorVelocity<T>(vel, lower, vecVel);
-          for (int k = 0; k < 3; ++k) {
-            const T tempAlpha = fabs((scaVel + vecVel[k]) * normal[k]);
-            la[k] = stdMax(la[k], tempAlpha);
-          }
-          break;
+          return;
         }
-      }
-    }
-    for (int k = 0; k < 3; ++k) atomicMaxAlpha(&A.alphaMax[k], (double)la[k]);
-  }
-}
-
-// Reduce(1) + value update of updateLevelSet, in place on the top level set.
-template <class T> struct UpdateArgs {
-  GridDev g;
-  MapView m;
-  const int *slotList;
-  const int *nSlots;
-  T *vals;
-  uint8_t *state;
-  uint8_t *hasDef;
-  const T *rateV;
-  const T *rateStop;
-  const uint8_t *rateLen;
-  size_t poolCells;
-  int L;
-  double dt;
-  int *err;
-  unsigned long long *defCount;
-};
-
-template <class T>
-__global__ void __launch_bounds__(RATE_THREADS) kUpdate(UpdateArgs<T> U) {
-  const int n = *U.nSlots;
-  for (int it = blockIdx.x; it < n; it += gridDim.x) {
-    const int slot = U.slotList[it];
-    const uint8_t st = U.state[slot];
-    if (st != ST_DENSE) continue; // uniform: Reduce keeps it as it is
-    const int bi = U.m.slotBrick[slot];
-    int bx, by, bz;
-    brickCoords(U.g, bi, bx, by, bz);
-    T res[2];
-    bool anyDef = false, allPos = true, allNeg = true;
-    for (int k = 0; k < 2; ++k) {
-      const int c = threadIdx.x + k * RATE_THREADS;
-      const size_t q = (size_t)slot * BV + c;
-      T value = U.vals[q];
-      if (isDef(value) && fabs(value) <= T(0.5)) {
-        int len = U.rateLen[q];
-        if (len < 1 || len > U.L) {
-          atomicOr(U.err, 2);
-          len = 1;
-        }
-        double time = U.dt;
-        int j = 0;
-        T velocity = U.rateV[q];
-        T rate = T(time * velocity);
-        while (fabs(U.rateStop[(size_t)j * U.poolCells + q] - value) < fabs(rate)) {
-          const T stop = U.rateStop[(size_t)j * U.poolCells + q];
-          time -= fabs((stop - value) / velocity);
-          value = stop;
-          ++j;
-          if (j >= len) {
-            atomicOr(U.err, 2);
+        for (int lower = 0; lower < L; ++lower) {
+          const T lv = lower == L - 1 ? value : lsValueAt<T>(A.ls[lower], slot, c);
+          if ((double)lv <= (double)value + 1e-4) {
+            T normal[3];
+            T normalModulus = 0.;
+            for (int d = 0; d < 3; ++d) {
+              const T phiPos = S.axis(d, 1);
+              const T phiNeg = S.axis(d, -1);
+              normal[d] = phiPos - phiNeg;
+              normalModulus += normal[d] * normal[d];
+            }
+            normalModulus = T(1.) / sqrt(normalModulus);
+            for (int d = 0; d < 3; ++d) normal[d] *= normalModulus;
+            const T scaVel = scalarVelocity<T>(vel, lower, normal);
+            T vecVel[3];
+            vectorVelocity<T>(vel, lower, vecVel);
+            for (int d = 0; d < 3; ++d) {
+              const unsigned long long ab =
+                  alphaBits((double)fabs((scaVel + vecVel[d]) * normal[d]));
+              alphaMax[d] = ab > alphaMax[d] ? ab : alphaMax[d];
+            }
             break;
           }
-          velocity = U.rateV[(size_t)j * U.poolCells + q];
-          rate = T(time * velocity);
         }
-        value -= rate;
-      } else {
-        value = value < 0 ? Lim<T>::lowest() : Lim<T>::max();
-      }
-      const int lx = c & 7, ly = (c >> 3) & 7, lz = c >> 6;
-      if (!cellExists(U.g, U.g.org[0] + bx * BS + lx, U.g.org[1] + by * BS + ly,
-                      U.g.org[2] + bz * BS + lz))
-        value = Lim<T>::max();
-      else if (isDef(value)) anyDef = true;
-      else if (value < 0) allPos = false;
-      else allNeg = false;
-      res[k] = value;
+      });
     }
-    countDefined<T>(res, U.defCount);
-    const int any = __syncthreads_or(anyDef);
-    const int ap = __syncthreads_and(allPos);
-    const int an = __syncthreads_and(allNeg);
-    if (!any && (ap || an)) {
-      if (threadIdx.x == 0) {
-        U.state[slot] = ap ? ST_UPOS : ST_UNEG;
-        U.hasDef[slot] = 0;
-      }
-    } else {
-      for (int k = 0; k < 2; ++k) U.vals[(size_t)slot * BV + threadIdx.x + k * RATE_THREADS] = res[k];
-      if (threadIdx.x == 0) U.hasDef[slot] = any ? 1 : 0;
+  }
+  minBits = warpMinU64(minBits);
+  for (int d = 0; d < 3; ++d) alphaMax[d] = warpMaxU64(alphaMax[d]);
+  for (int o = 16; o > 0; o >>= 1) {
+    nAct += __shfl_xor_sync(0xffffffffu, nAct, o);
+    nBand += __shfl_xor_sync(0xffffffffu, nBand, o);
+  }
+  if (lane == 0) {
+    if (MODE == 0 && minBits != ~0ull) atomicMin(A.minStep, minBits);
+    if (A.alphaMax)
+      for (int d = 0; d < 3; ++d)
+        if (alphaMax[d]) atomicMax(&A.alphaMax[d], alphaMax[d]);
+    if (MODE == 0 && A.counts) {
+      if (nAct) atomicAdd(&A.counts[0], nAct);
+      if (nBand) atomicAdd(&A.counts[1], nBand);
     }
-    __syncthreads();
   }
 }
 
-// Compact the active points (defined, |phi| <= 0.5) of the top level set.
+// Value update of updateLevelSet (lsAdvect.hpp:725-777) for every active
+// point, in place on the top level set (the Reduce(1) part is applied by the
+// rebuild pass that follows).
 template <class T>
 __global__ void __launch_bounds__(RATE_THREADS)
-    kCompactActive(const int *slotList, const int *nSlots, Buf<T> top,
-                   uint32_t *active, int *nActive, int activeCap, int *err,
-                   unsigned long long *bandCount) {
+    kUpdate(const int *slotList, const int *nSlots, const uint64_t *act, T *vals,
+            const T *rateV, const T *rateStop, const uint8_t *rateLen, size_t poolCells, int L,
+            double dt, int *err) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nWarps = (gridDim.x * blockDim.x) >> 5;
   const int n = *nSlots;
-  for (int it = blockIdx.x; it < n; it += gridDim.x) {
-    const int slot = slotList[it];
-    if (top.state[slot] != ST_DENSE) continue;
-    for (int k = 0; k < 2; ++k) {
-      const int c = threadIdx.x + k * RATE_THREADS;
-      const T v = top.vals[(size_t)slot * BV + c];
-      const bool act = isDef(v) && fabs(v) <= T(0.5);
-      const int nd = __syncthreads_count(isDef(v));
-      if (threadIdx.x == 0 && nd) atomicAdd(bandCount, (unsigned long long)nd);
-      const unsigned mask = __ballot_sync(0xffffffffu, act);
-      const int lane = threadIdx.x & 31;
-      int base = 0;
-      if (lane == 0 && mask) base = atomicAdd(nActive, __popc(mask));
-      base = __shfl_sync(0xffffffffu, base, 0);
-      const int pos = base + __popc(mask & ((1u << lane) - 1));
-      if (act) {
-        if (pos < activeCap) active[pos] = ((uint32_t)slot << 9) | c;
-        else atomicOr(err, 16);
+  for (int w = warp; w < n; w += nWarps) {
+    const int slot = slotList[w];
+    const uint64_t a = lane < 8 ? act[(size_t)slot * 8 + lane] : 0ull;
+    if (!__any_sync(0xffffffffu, a != 0ull)) continue;
+    const PlaneEnum pa(a);
+    for (int base = 0; base < pa.total; base += 32) {
+      const int k = base + lane;
+      const int c = pa.cell(a, k < pa.total ? k : pa.total - 1);
+      if (k >= pa.total) continue;
+      const size_t q = (size_t)slot * BV + c;
+      T value = vals[q];
+      int len = rateLen[q];
+      if (len < 1 || len > L) {
+        atomicOr(err, 2);
+        len = 1;
       }
+      double time = dt;
+      int j = 0;
+      T velocity = rateV[q];
+      T rate = T(time * velocity);
+      while (fabs(rateStop[(size_t)j * poolCells + q] - value) < fabs(rate)) {
+        const T stop = rateStop[(size_t)j * poolCells + q];
+        time -= fabs((stop - value) / velocity);
+        value = stop;
+        ++j;
+        if (j >= len) {
+          atomicOr(err, 2);
+          break;
+        }
+        velocity = rateV[(size_t)j * poolCells + q];
+        rate = T(time * velocity);
+      }
+      value -= rate;
+      vals[q] = value;
     }
   }
 }
