@@ -177,6 +177,19 @@ int vlsg_count_points(vlsg_context *ctx, int32_t slot, int64_t *n_points);
 int vlsg_download_levelset(vlsg_context *ctx, int32_t slot, int64_t capacity,
                            int32_t *indices, double *values, int32_t *width);
 
+/* Undefined runs of a level set in HRLE order -- what viennahrle's sparse
+ * iterators yield besides the defined points (lsDomain.hpp:51-52: an
+ * undefined run carries +-max with its sign) -- over the box [min - 1,
+ * max + 1] of the defined points: one run before the box, per z-plane one
+ * run before and one after its rows, per row a run at its head (or one for
+ * a row without points) and one after every point not followed by its +x
+ * neighbour, one run after the box; a run with the previous run's sign and
+ * no defined point between them is merged into it.  Start indices below the
+ * box are -(2^20 - 2).  Writes *n_runs; with capacity < *n_runs nothing is
+ * written and VLSG_ERR_CAPACITY is returned (call with capacity 0 to ask). */
+int vlsg_download_runs(vlsg_context *ctx, int32_t slot, int64_t capacity,
+                       int32_t *run_start, int8_t *run_sign, int64_t *n_runs);
+
 /* Values of arbitrary grid points of a level set (indices are mapped through
  * the boundary conditions): the defined value, or +-DBL_MAX carrying the sign
  * of the undefined region -- what viennahrle's iterators return for them

@@ -41,6 +41,7 @@ def load(build_if_missing=True):
     L.vlsg_count_points.argtypes = [vp, i32, P(i64)]
     L.vlsg_download_levelset.argtypes = [vp, i32, i64, P(i32), P(ctypes.c_double), P(i32)]
     L.vlsg_get_values.argtypes = [vp, i32, i64, P(i32), P(ctypes.c_double)]
+    L.vlsg_download_runs.argtypes = [vp, i32, i64, P(i32), P(ctypes.c_int8), P(i64)]
     L.vlsg_get_values_noalloc.argtypes = [vp, i32, i64, P(i32), P(ctypes.c_double)]
     L.vlsg_set_velocity_functor.argtypes = [vp, P(VelocityDesc)]
     L.vlsg_set_velocity_callback.argtypes = [vp, VELOCITY_CALLBACK, vp]
@@ -55,7 +56,7 @@ EXPORTED = [
     "vlsg_version", "vlsg_last_error", "vlsg_create", "vlsg_destroy",
     "vlsg_default_params", "vlsg_set_stream", "vlsg_get_stream",
     "vlsg_set_grid", "vlsg_set_level_set_count",
-    "vlsg_upload_levelset", "vlsg_count_points", "vlsg_download_levelset",
+    "vlsg_upload_levelset", "vlsg_count_points", "vlsg_download_levelset", "vlsg_download_runs",
     "vlsg_get_values", "vlsg_get_values_noalloc",
     "vlsg_set_velocity_functor", "vlsg_set_velocity_callback", "vlsg_advect",
     "vlsg_set_profiling", "vlsg_get_kernel_stats",

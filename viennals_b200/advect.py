@@ -117,9 +117,29 @@ class Context:
                      device_ms=arr[i].device_ms, bytes=arr[i].algorithmic_bytes)
                 for i in range(cnt.value)]
 
+    def download_runs(self, slot):
+        """(run_start (K,3) int32, run_sign (K,) int8) of the undefined runs in
+        HRLE order, built on the device (vlsg_download_runs)."""
+        n = ctypes.c_int64()
+        rc = self.lib.vlsg_download_runs(self.h, int(slot), 0, None, None, ctypes.byref(n))
+        if rc not in (0, -3):
+            self._check(rc)
+        starts = np.zeros((n.value, 3), np.int32)
+        signs = np.zeros(n.value, np.int8)
+        self._check(self.lib.vlsg_download_runs(self.h, int(slot), n.value, _p(starts, ctypes.c_int32),
+                                                _p(signs, ctypes.c_int8), ctypes.byref(n)))
+        return starts, signs
+
     def download_domain(self, slot, grid):
-        """Domain with the defined points and the undefined runs rebuilt from
-        the device's signs."""
+        """Domain with the defined points and the undefined runs, both in HRLE
+        order from the device."""
+        idx, val, w = self.download(slot)
+        rs, sg = self.download_runs(slot)
+        return Domain(grid, idx, val, rs, sg, width=w)
+
+    def download_domain_host_runs(self, slot, grid):
+        """Same as download_domain with the runs rebuilt on the host from
+        point queries (the reference layout the device builder follows)."""
         idx, val, w = self.download(slot)
         if len(idx):
             lo = idx.min(0) - 1

@@ -305,6 +305,24 @@ int vlsg_download_levelset(vlsg_context *ctx, int32_t slot, int64_t capacity, in
   });
 }
 
+int vlsg_download_runs(vlsg_context *ctx, int32_t slot, int64_t capacity, int32_t *runStart,
+                       int8_t *runSign, int64_t *nRuns) {
+  if (!ctx || !nRuns || capacity < 0 || (capacity > 0 && (!runStart || !runSign)))
+    return fail(ctx, VLSG_ERR_ARGUMENT, "bad argument");
+  return guarded(ctx, [&] {
+    ensureBuilt(ctx);
+    if (slot < 0 || slot >= (int)ctx->staged.size())
+      return fail(ctx, VLSG_ERR_ARGUMENT, "level set slot out of range");
+    const int64_t n = withEngine(ctx, [&](auto &e) {
+      return e.runs(slot, capacity > 0 ? runStart : nullptr, capacity > 0 ? runSign : nullptr,
+                    capacity);
+    });
+    *nRuns = n;
+    if (n > capacity) return fail(ctx, VLSG_ERR_CAPACITY, "run capacity too small");
+    return VLSG_OK;
+  });
+}
+
 int vlsg_get_values(vlsg_context *ctx, int32_t slot, int64_t n, const int32_t *idx,
                     double *values) {
   if (!ctx || n < 0 || (n > 0 && (!idx || !values)))

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "vlsg_common.cuh"
+#include "vlsg_exchange.cuh"
 #include "vlsg_frontier.cuh"
 #include "vlsg_maint.cuh"
 #include "vlsg_passes.cuh"
@@ -127,8 +128,26 @@ public:
   bool profiling = false;
   std::vector<KernelTimer> timers;
   int blocksPass = 148 * 8;
+  // exchange format (points and runs in HRLE order), cached per buffer until
+  // the level sets change
+  struct Scratch {
+    void *p = nullptr;
+    size_t bytes = 0;
+  };
+  enum { X_FLAGS, X_POS, X_OB, X_BOUNDS, X_C, X_P, X_SUMS, X_BOX, X_IDX, X_VAL, X_GC, X_GE,
+         X_ROWC, X_ROWG, X_PB, X_GB, X_RSTART, X_RSIGN, X_RPB, X_KEEP, X_KPOS, X_OSTART,
+         X_OSIGN, X_COUNT };
+  Scratch xs[X_COUNT];
+  uint64_t generation = 0;
+  int xBuf = -1;
+  uint64_t xGen = ~0ull;
+  int64_t xPoints = 0, xRuns = 0;
 
-  ~Engine() { release(); }
+  ~Engine() {
+    release();
+    for (auto &x : xs)
+      if (x.p) cudaFree(x.p);
+  }
 
   void release() {
     auto f = [](void *p) { if (p) cudaFree(p); };
@@ -266,6 +285,7 @@ public:
 
   void build(const GridDev &grid, std::vector<StagedLS> &ls, int margin) {
     release();
+    ++generation;
     VLSG_CUDA(cudaHostAlloc(&pinCounters, 32 * sizeof(int), cudaHostAllocDefault));
     VLSG_CUDA(cudaHostAlloc(&pinScal, 8 * sizeof(unsigned long long), cudaHostAllocDefault));
     g = grid;
@@ -802,6 +822,7 @@ public:
   }
 
   void apply(const vlsg_advect_params &P, vlsg_advect_result &r) {
+    ++generation;
     pointUpdates = 0;
     stages = 0;
     const uint64_t l0 = launches;
@@ -831,7 +852,7 @@ public:
   }
 
   // ------------------------------------------------------------ download
-  int64_t countDefined(int b) { return compact(b, nullptr, nullptr, 0); }
+  int64_t countDefined(int b) { return defined(b); }
 
   void queryValues(int b, int64_t n, const int32_t *idx, double *out) {
     if (n <= 0) return;
@@ -851,48 +872,147 @@ public:
     cudaFree(dv);
   }
 
-  // Defined points of buffer b in HRLE order (keys sorted on the host).
-  int64_t compact(int b, int32_t *idxOut, double *valOut, int64_t capOut) {
-    const int64_t n = defined(b);
-    if (!idxOut || !valOut || n > capOut) return n;
-    VLSG_CUDA(cudaMemsetAsync(nOutPtr(), 0, sizeof(int), stream));
-    uint64_t *dk = nullptr;
-    double *dv = nullptr;
-    const size_t room = std::max<int64_t>(1, n);
-    VLSG_CUDA(cudaMalloc(&dk, room * sizeof(uint64_t)));
-    VLSG_CUDA(cudaMalloc(&dv, room * sizeof(double)));
-    {
-      Scope sc(this, "download_compact");
-      kCompactDefined<T><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(
-          g, slotList, nSlotsPtr(), slotBrick, buf[b].vals, buf[b].def[buf[b].cur], dk, dv,
-          nOutPtr(), (int)room);
-      checkLaunch();
+  // ------------------------------------------------------------ exchange
+  template <class V> V *scratch(int k, size_t n) {
+    const size_t bytes = std::max<size_t>(n, 1) * sizeof(V);
+    if (xs[k].bytes < bytes) {
+      if (xs[k].p) VLSG_CUDA(cudaFree(xs[k].p));
+      xs[k].p = nullptr;
+      xs[k].bytes = 0;
+      const size_t grown = bytes + bytes / 4;
+      VLSG_CUDA(cudaMalloc(&xs[k].p, grown));
+      xs[k].bytes = grown;
     }
-    syncErr("download");
-    if ((int64_t)hCounters[5] != n) {
-      cudaFree(dk);
-      cudaFree(dv);
-      throw CudaError("download: defined-cell count mismatch", VLSG_ERR_DEVICE_CHECK);
+    return (V *)xs[k].p;
+  }
+  // Exclusive scan of n counts; the total lands in sums[(n + tile - 1) / tile].
+  void scanExclusive(const uint32_t *in, uint32_t *out, size_t n, uint32_t *sums) {
+    const size_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
+    if (nb > (size_t)SCAN_TOP_THREADS * SCAN_TOP_ITEMS)
+      throw CudaError("exchange: too many elements for the scan", VLSG_ERR_CAPACITY);
+    if (nb == 0) {
+      VLSG_CUDA(cudaMemsetAsync(sums, 0, sizeof(uint32_t), stream));
+      return;
     }
-    std::vector<uint64_t> hk(n);
-    std::vector<double> hv(n);
-    VLSG_CUDA(cudaMemcpyAsync(hk.data(), dk, n * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream));
-    VLSG_CUDA(cudaMemcpyAsync(hv.data(), dv, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    kScanReduce<<<(unsigned)nb, SCAN_THREADS, 0, stream>>>(in, n, sums);
+    kScanTop<<<1, SCAN_TOP_THREADS, 0, stream>>>(sums, (int)nb);
+    kScanApply<<<(unsigned)nb, SCAN_THREADS, 0, stream>>>(in, n, sums, out);
+    checkLaunch();
+  }
+  uint32_t scanTotal(const uint32_t *sums, size_t n) {
+    const size_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
+    VLSG_CUDA(cudaMemcpyAsync(pinCounters + 30, sums + nb, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                              stream));
     VLSG_CUDA(cudaStreamSynchronize(stream));
-    cudaFree(dk);
-    cudaFree(dv);
-    std::vector<int64_t> order(n);
-    for (int64_t i = 0; i < n; ++i) order[i] = i;
-    std::sort(order.begin(), order.end(), [&](int64_t a, int64_t c) { return hk[a] < hk[c]; });
-    const int64_t off = 1ll << 20;
-    for (int64_t i = 0; i < n; ++i) {
-      const uint64_t k = hk[order[i]];
-      idxOut[3 * i + 0] = (int32_t)((int64_t)(k & 0x1fffff) - off);
-      idxOut[3 * i + 1] = (int32_t)((int64_t)((k >> 21) & 0x1fffff) - off);
-      idxOut[3 * i + 2] = (int32_t)((int64_t)((k >> 42) & 0x1fffff) - off);
-      valOut[i] = hv[order[i]];
+    return (uint32_t)pinCounters[30];
+  }
+
+  // Points (HRLE order) and runs of buffer b on the device, in the scratch
+  // arrays X_IDX / X_VAL / X_OSTART / X_OSIGN.
+  void buildExchange(int b) {
+    if (xBuf == b && xGen == generation) return;
+    Scope sc(this, "exchange");
+    const int nAlloc = readI32(nSlotsPtr());
+    uint32_t *flags = scratch<uint32_t>(X_FLAGS, nBricks);
+    uint32_t *pos = scratch<uint32_t>(X_POS, nBricks);
+    uint32_t *sums = scratch<uint32_t>(X_SUMS, scanScratch((size_t)std::max(nBricks, nAlloc * 64)) + 64);
+    kAllocFlags<<<grid1(nBricks), 256, 0, stream>>>(brickMap, nBricks, flags);
+    scanExclusive(flags, pos, nBricks, sums);
+    int *ob = scratch<int>(X_OB, nAlloc);
+    kOrderedBricks<<<grid1(nBricks), 256, 0, stream>>>(brickMap, nBricks, pos, ob);
+    int4 *bounds = scratch<int4>(X_BOUNDS, nAlloc);
+    kBrickBounds<<<grid1(nAlloc), 256, 0, stream>>>(g, ob, nAlloc, bounds);
+    const size_t nSeg = (size_t)nAlloc * 64;
+    uint32_t *C = scratch<uint32_t>(X_C, nSeg);
+    uint32_t *P = scratch<uint32_t>(X_P, nSeg);
+    int *box = scratch<int>(X_BOX, 8);
+    const int boxInit[6] = {INT_MAX, INT_MAX, INT_MAX, INT_MIN, INT_MIN, INT_MIN};
+    std::memcpy(pinCounters + 16, boxInit, sizeof(boxInit));
+    VLSG_CUDA(cudaMemcpyAsync(box, pinCounters + 16, sizeof(boxInit), cudaMemcpyHostToDevice, stream));
+    const uint64_t *def = buf[b].def[buf[b].cur];
+    kSegCounts<<<grid1(nSeg), 256, 0, stream>>>(g, ob, nAlloc, brickMap, bounds, def, C, box);
+    scanExclusive(C, P, nSeg, sums);
+    const uint32_t nPts = scanTotal(sums, nSeg);
+    int hbox[6];
+    VLSG_CUDA(cudaMemcpyAsync(pinCounters + 16, box, sizeof(hbox), cudaMemcpyDeviceToHost, stream));
+    VLSG_CUDA(cudaStreamSynchronize(stream));
+    std::memcpy(hbox, pinCounters + 16, sizeof(hbox));
+    checkLaunch();
+    RunBox rb{};
+    for (int d = 0; d < 3; ++d) {
+      rb.lo[d] = nPts ? hbox[d] - 1 : 0;
+      rb.hi[d] = nPts ? hbox[3 + d] + 1 : 0;
     }
-    return n;
+    rb.ny = rb.hi[1] - rb.lo[1] + 1;
+    rb.nz = rb.hi[2] - rb.lo[2] + 1;
+    const size_t rows = (size_t)rb.ny * rb.nz;
+    int32_t *idx = scratch<int32_t>(X_IDX, 3 * (size_t)nPts);
+    double *val = scratch<double>(X_VAL, nPts);
+    uint32_t *GC = scratch<uint32_t>(X_GC, nSeg);
+    uint32_t *GE = scratch<uint32_t>(X_GE, nSeg);
+    uint32_t *rowC = scratch<uint32_t>(X_ROWC, rows);
+    uint32_t *rowG = scratch<uint32_t>(X_ROWG, rows);
+    uint32_t *PB = scratch<uint32_t>(X_PB, rows);
+    uint32_t *GB = scratch<uint32_t>(X_GB, rows);
+    uint32_t *sums2 = scratch<uint32_t>(X_KPOS, scanScratch(rows) + 64);
+    VLSG_CUDA(cudaMemsetAsync(rowC, 0, rows * sizeof(uint32_t), stream));
+    VLSG_CUDA(cudaMemsetAsync(rowG, 0, rows * sizeof(uint32_t), stream));
+    kSegScatter<T><<<grid1(nSeg), 256, 0, stream>>>(g, ob, nAlloc, brickMap, nbr, bounds, def,
+                                                    buf[b].vals, P, rb, idx, val, GC, rowC, rowG);
+    scanExclusive(GC, GE, nSeg, sums);
+    scanExclusive(rowC, PB, rows, sums2);
+    scanExclusive(rowG, GB, rows, sums2);
+    const uint32_t gaps = scanTotal(sums2, rows);
+    const size_t nRuns = 2 + 2 * (size_t)rb.nz + rows + gaps;
+    if (nRuns >= (size_t)UINT32_MAX || (size_t)nPts >= (size_t)INT32_MAX)
+      throw CudaError("exchange: level set too large", VLSG_ERR_CAPACITY);
+    RunSink<T> sink{scratch<int32_t>(X_RSTART, 3 * nRuns), scratch<int8_t>(X_RSIGN, nRuns),
+                    scratch<uint32_t>(X_RPB, nRuns), g, mapView(), view(b)};
+    kRunsRows<T><<<grid1(rows), 256, 0, stream>>>(rb, rowC, rowG, PB, GB, idx, nPts,
+                                                  (uint32_t)nRuns, sink);
+    kRunsGaps<T><<<grid1(nSeg), 256, 0, stream>>>(g, ob, nAlloc, brickMap, nbr, bounds, def, P, GE,
+                                                  rb, sink);
+    uint32_t *keep = scratch<uint32_t>(X_KEEP, nRuns);
+    uint32_t *kpos = scratch<uint32_t>(X_POS, std::max<size_t>(nRuns, nBricks));
+    uint32_t *sums3 = scratch<uint32_t>(X_SUMS, scanScratch(std::max<size_t>(nRuns, std::max(nBricks, nAlloc * 64))) + 64);
+    kRunKeep<<<grid1(nRuns), 256, 0, stream>>>(sink.sign, sink.pb, (uint32_t)nRuns, keep);
+    scanExclusive(keep, kpos, nRuns, sums3);
+    const uint32_t kept = scanTotal(sums3, nRuns);
+    kRunCompact<<<grid1(nRuns), 256, 0, stream>>>(sink.start, sink.sign, keep, kpos,
+                                                  (uint32_t)nRuns, scratch<int32_t>(X_OSTART, 3 * (size_t)kept),
+                                                  scratch<int8_t>(X_OSIGN, kept));
+    checkLaunch();
+    syncErr("exchange");
+    xBuf = b;
+    xGen = generation;
+    xPoints = nPts;
+    xRuns = kept;
+  }
+
+  // Defined points of buffer b in HRLE order; returns their number.
+  int64_t compact(int b, int32_t *idxOut, double *valOut, int64_t capOut) {
+    buildExchange(b);
+    if (!idxOut || !valOut || xPoints > capOut) return xPoints;
+    if (xPoints) {
+      VLSG_CUDA(cudaMemcpyAsync(idxOut, xs[X_IDX].p, 3 * sizeof(int32_t) * xPoints,
+                                cudaMemcpyDeviceToHost, stream));
+      VLSG_CUDA(cudaMemcpyAsync(valOut, xs[X_VAL].p, sizeof(double) * xPoints,
+                                cudaMemcpyDeviceToHost, stream));
+      VLSG_CUDA(cudaStreamSynchronize(stream));
+    }
+    return xPoints;
+  }
+  // Undefined runs of buffer b (HRLE order); returns their number.
+  int64_t runs(int b, int32_t *startOut, int8_t *signOut, int64_t capOut) {
+    buildExchange(b);
+    if (!startOut || !signOut || xRuns > capOut) return xRuns;
+    if (xRuns) {
+      VLSG_CUDA(cudaMemcpyAsync(startOut, xs[X_OSTART].p, 3 * sizeof(int32_t) * xRuns,
+                                cudaMemcpyDeviceToHost, stream));
+      VLSG_CUDA(cudaMemcpyAsync(signOut, xs[X_OSIGN].p, xRuns, cudaMemcpyDeviceToHost, stream));
+      VLSG_CUDA(cudaStreamSynchronize(stream));
+    }
+    return xRuns;
   }
 };
 

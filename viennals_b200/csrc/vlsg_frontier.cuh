@@ -35,6 +35,12 @@
 namespace vlsg {
 
 constexpr int FRONTIER_THREADS = 256;
+// Resident blocks per SM the passes are compiled for (40 registers per
+// thread): the passes are bound by latency and issue, so occupancy pays more
+// than the few spilled registers cost.
+#ifndef VLSG_PASS_MIN_BLOCKS
+#define VLSG_PASS_MIN_BLOCKS 6
+#endif
 constexpr uint64_t XLO = 0x0101010101010101ull; // cells with x = 0
 constexpr uint64_t XHI = 0x8080808080808080ull; // cells with x = 7
 // 27-neighbour table entries of the six faces (index (dz+1)*9+(dy+1)*3+dx+1)
@@ -225,7 +231,7 @@ enum : int { FP_EXPAND = 0, FP_PRUNE = 1, FP_ALL = 2 };
 // cells next to a defined one, FP_PRUNE the defined cells, FP_ALL the
 // defined cells and their neighbours.
 template <class T, int MODE, class Rule>
-__global__ void __launch_bounds__(FRONTIER_THREADS)
+__global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
     kFrontierPass(Topo t, LsView<T> v, Rule rule) {
   __shared__ WarpMasks sm[FRONTIER_THREADS / 32];
   WarpMasks &wm = sm[threadIdx.x >> 5];
@@ -308,7 +314,7 @@ __device__ inline T reducedValue(const T *vals, const uint64_t *act, const int8_
 // place): candidates are the active cells and their neighbours; every other
 // defined cell becomes undefined with its sign.
 template <class T>
-__global__ void __launch_bounds__(FRONTIER_THREADS)
+__global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
     kUpdateRebuild(Topo t, LsView<T> v, const uint64_t *act, double cutoff) {
   __shared__ WarpMasks sm[FRONTIER_THREADS / 32];
   WarpMasks &wm = sm[threadIdx.x >> 5];

@@ -518,36 +518,31 @@ __device__ inline void withStencil(const RateArgs<T> &A, int slot, int c, Fn fn)
 }
 
 // Active mask of a brick (defined cells with |phi| <= 0.5, lsAdvect.hpp:498;
-// lane z returns plane z); `words` is the warp's shared scratch.
+// lane z returns plane z): one coalesced read of the brick's 512 values.
 template <class T>
-__device__ inline uint64_t activePlanes(const T *vals, int slot, uint64_t own,
-                                        unsigned long long *words) {
+__device__ inline uint64_t activePlanes(const T *vals, int slot) {
   const int lane = threadIdx.x & 31;
-  if (lane < 8) words[lane] = 0ull;
-  __syncwarp();
-  const PlaneEnum pe(own);
-  for (int base = 0; base < pe.total; base += 32) {
-    const int k = base + lane;
-    const int c = pe.cell(own, k < pe.total ? k : pe.total - 1);
-    if (k < pe.total) {
-      const T v = vals[(size_t)slot * BV + c];
-      if (isDef(v) && fabs(v) <= T(0.5)) markCell(words, c);
-    }
+  const T *p = vals + (size_t)slot * BV + lane;
+  T v[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = p[32 * i];
+  uint64_t mine = 0;
+#pragma unroll
+  for (int z = 0; z < 8; ++z) {
+    const unsigned lo = __ballot_sync(0xffffffffu, isDef(v[2 * z]) && fabs(v[2 * z]) <= T(0.5));
+    const unsigned hi =
+        __ballot_sync(0xffffffffu, isDef(v[2 * z + 1]) && fabs(v[2 * z + 1]) <= T(0.5));
+    if (lane == z) mine = (uint64_t)lo | ((uint64_t)hi << 32);
   }
-  __syncwarp();
-  const uint64_t a = lane < 8 ? words[lane] : 0ull;
-  __syncwarp();
-  return a;
+  return mine;
 }
 
-// integrateTime over every active point (MODE 0), or findGlobalAlphas
-// (lsAdvect.hpp:90-195, MODE 1).  Minima, maxima and counts are kept per
-// thread and reach global memory once per warp.
+// Resident blocks per SM: 3 for float (80 registers), 2 for double (the
+// FP64 stencils need 128 registers to stay out of local memory).
+template <class T> constexpr int rateMinBlocks() { return sizeof(T) == 4 ? 3 : 2; }
 template <class T, int MODE>
-__global__ void __launch_bounds__(RATE_THREADS)
+__global__ void __launch_bounds__(RATE_THREADS, rateMinBlocks<T>())
     kRates(RateArgs<T> A, const vlsg_velocity_desc vel) {
-  __shared__ unsigned long long sAct[RATE_THREADS / 32][8];
-  unsigned long long *words = sAct[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nWarps = (gridDim.x * blockDim.x) >> 5;
@@ -559,7 +554,7 @@ __global__ void __launch_bounds__(RATE_THREADS)
     const int slot = A.slotList[w];
     const uint64_t own = lane < 8 ? A.def[(size_t)slot * 8 + lane] : 0ull;
     uint64_t a = 0ull;
-    if (__any_sync(0xffffffffu, own != 0ull)) a = activePlanes<T>(top.vals, slot, own, words);
+    if (__any_sync(0xffffffffu, own != 0ull)) a = activePlanes<T>(top.vals, slot);
     if (lane < 8) {
       if (MODE == 0) A.act[(size_t)slot * 8 + lane] = a;
       nAct += __popcll(a);
@@ -571,7 +566,7 @@ __global__ void __launch_bounds__(RATE_THREADS)
       const int c = pa.cell(a, k < pa.total ? k : pa.total - 1);
       if (k >= pa.total) continue;
       withStencil<T>(A, slot, c, [&](const auto &S, T value) {
-        if (MODE == 0) {
+        if constexpr (MODE == 0) {
           T alphas[3] = {0, 0, 0};
           const double step = ratePoint<T>(A, vel, S, slot, c, value, alphas);
           const unsigned long long sb = stepBits(step);
@@ -580,8 +575,7 @@ __global__ void __launch_bounds__(RATE_THREADS)
             const unsigned long long ab = alphaBits((double)alphas[d]);
             alphaMax[d] = ab > alphaMax[d] ? ab : alphaMax[d];
           }
-          return;
-        }
+        } else {
         for (int lower = 0; lower < L; ++lower) {
           const T lv = lower == L - 1 ? value : lsValueAt<T>(A.ls[lower], slot, c);
           if ((double)lv <= (double)value + 1e-4) {
@@ -605,6 +599,7 @@ __global__ void __launch_bounds__(RATE_THREADS)
             }
             break;
           }
+        }
         }
       });
     }
