@@ -243,35 +243,28 @@ int vlsg_upload_levelset(vlsg_context *ctx, int32_t slot, int64_t n, const int32
     if (n < 0 || nRuns < 0 || (n > 0 && (!idx || !values)) ||
         (nRuns > 0 && (!runStart || !runSign)))
       return fail(ctx, VLSG_ERR_ARGUMENT, "vlsg_upload_levelset: bad arrays");
-    if (n > INT_MAX / 4) return fail(ctx, VLSG_ERR_ARGUMENT, "too many points");
+    if (n > INT_MAX / 4 || nRuns > INT_MAX / 4)
+      return fail(ctx, VLSG_ERR_ARGUMENT, "too many points or runs");
     if ((int)ctx->staged.size() <= slot) ctx->staged.resize(slot + 1);
+    // straight to the device; the index mapping, the range check and the run
+    // order are handled there when the context builds
     StagedLS &s = ctx->staged[slot];
-    s.idx.resize(3 * n);
-    s.vals.resize(n);
-    const GridDev &g = ctx->grid;
-    for (int64_t i = 0; i < n; ++i) {
-      for (int d = 0; d < 3; ++d) {
-        const int c = mapCoord(g, d, idx[3 * i + d]);
-        if (c < -(1 << 19) || c > (1 << 19))
-          return fail(ctx, VLSG_ERR_ARGUMENT, "point index out of the supported range");
-        s.idx[3 * i + d] = c;
-      }
-      s.vals[i] = values[i];
+    growDevice(s.idx, s.capIdx, 3 * (size_t)n);
+    growDevice(s.vals, s.capVals, (size_t)n);
+    growDevice(s.runStart, s.capRunStart, 3 * (size_t)nRuns);
+    growDevice(s.runSign, s.capRunSign, (size_t)nRuns);
+    if (n) {
+      VLSG_CUDA(cudaMemcpyAsync(s.idx, idx, 3 * n * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream));
+      VLSG_CUDA(cudaMemcpyAsync(s.vals, values, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     }
-    std::vector<std::pair<uint64_t, int8_t>> runs(nRuns);
-    for (int64_t i = 0; i < nRuns; ++i) {
-      int c[3];
-      for (int d = 0; d < 3; ++d) {
-        c[d] = runStart[3 * i + d];
-        c[d] = std::max(-(1 << 20) + 1, std::min((1 << 20) - 1, c[d]));
-      }
-      runs[i] = {hostCellKey(c[0], c[1], c[2]), runSign[i] < 0 ? (int8_t)-1 : (int8_t)1};
+    if (nRuns) {
+      VLSG_CUDA(cudaMemcpyAsync(s.runStart, runStart, 3 * nRuns * sizeof(int32_t),
+                                cudaMemcpyHostToDevice, ctx->stream));
+      VLSG_CUDA(cudaMemcpyAsync(s.runSign, runSign, nRuns, cudaMemcpyHostToDevice, ctx->stream));
     }
-    std::stable_sort(runs.begin(), runs.end(),
-                     [](const auto &a, const auto &b) { return a.first < b.first; });
-    s.runKeys.resize(nRuns);
-    s.runSign.resize(nRuns);
-    for (int64_t i = 0; i < nRuns; ++i) s.runKeys[i] = runs[i].first, s.runSign[i] = runs[i].second;
+    VLSG_CUDA(cudaStreamSynchronize(ctx->stream));
+    s.n = n;
+    s.nRuns = nRuns;
     s.width = width;
     ctx->dirty = true;
     return VLSG_OK;

@@ -17,6 +17,7 @@
 #pragma once
 
 #include <cfloat>
+#include <climits>
 #include <cstdint>
 
 #include "../../include/vlsg.h"

@@ -39,12 +39,49 @@ struct CudaError : std::runtime_error {
                             VLSG_ERR_CUDA);                                    \
   } while (0)
 
+// Device array that only grows (contents are not kept when it does).
+template <class V> void growDevice(V *&p, size_t &capacity, size_t n) {
+  if (p && n <= capacity) return;
+  if (p) VLSG_CUDA(cudaFree(p));
+  p = nullptr;
+  capacity = 0;
+  const size_t c = std::max<size_t>(n + n / 4, 16);
+  VLSG_CUDA(cudaMalloc(&p, c * sizeof(V)));
+  capacity = c;
+}
+
+// One uploaded level set, staged on the device until the context builds.
 struct StagedLS {
-  std::vector<int32_t> idx;
-  std::vector<double> vals;
-  std::vector<uint64_t> runKeys;
-  std::vector<int8_t> runSign;
+  int32_t *idx = nullptr;      // 3 per point (as given)
+  double *vals = nullptr;
+  int32_t *runStart = nullptr; // 3 per run
+  int8_t *runSign = nullptr;
+  size_t capIdx = 0, capVals = 0, capRunStart = 0, capRunSign = 0;
+  int64_t n = 0, nRuns = 0;
   int width = 1;
+  StagedLS() = default;
+  StagedLS(const StagedLS &) = delete;
+  StagedLS &operator=(const StagedLS &) = delete;
+  StagedLS(StagedLS &&o) noexcept { *this = std::move(o); }
+  StagedLS &operator=(StagedLS &&o) noexcept {
+    if (this == &o) return *this;
+    release();
+    idx = o.idx, vals = o.vals, runStart = o.runStart, runSign = o.runSign;
+    capIdx = o.capIdx, capVals = o.capVals, capRunStart = o.capRunStart, capRunSign = o.capRunSign;
+    n = o.n, nRuns = o.nRuns, width = o.width;
+    o.idx = nullptr, o.vals = nullptr, o.runStart = nullptr, o.runSign = nullptr;
+    o.capIdx = o.capVals = o.capRunStart = o.capRunSign = 0;
+    return *this;
+  }
+  ~StagedLS() { release(); }
+  void release() {
+    if (idx) cudaFree(idx);
+    if (vals) cudaFree(vals);
+    if (runStart) cudaFree(runStart);
+    if (runSign) cudaFree(runSign);
+    idx = nullptr, vals = nullptr, runStart = nullptr, runSign = nullptr;
+    capIdx = capVals = capRunStart = capRunSign = 0;
+  }
 };
 
 inline uint64_t hostCellKey(int x, int y, int z) {
@@ -97,11 +134,19 @@ public:
   unsigned long long *rateCounts = nullptr; // active cells, band cells of the last rates
   int *nbr = nullptr;                   // 27 per slot
   uint8_t *cflag = nullptr;             // CF_* per slot
+  uint8_t *core = nullptr;              // per brick: holds an uploaded point
+  unsigned long long *small = nullptr;  // 0..5 point box, 6.. |value| bounds per level set
+  uint64_t *runKeys[VLSG_MAX_LEVEL_SETS] = {};
+  size_t capRunKeys[VLSG_MAX_LEVEL_SETS] = {};
+  // allocated sizes: arrays per brick of the map box, per slot, rate chains
+  size_t capBricks = 0, capSlots = 0;
+  int capL = 0;
   struct DBuf {
     T *vals = nullptr;
     uint64_t *def[2] = {nullptr, nullptr};
-    int cur = 0;
     int8_t *farSign = nullptr;
+    size_t capSlots = 0, capBricks = 0;
+    int cur = 0;
     int width = 1;
     bool live = false;
     double bound = 0;  // upper bound of |value| over the defined cells
@@ -152,8 +197,9 @@ public:
   void release() {
     auto f = [](void *p) { if (p) cudaFree(p); };
     f(brickMap); f(slotBrick); f(slotList); f(freeStack); f(newList); f(counters); f(needed);
-    f(scal); f(defCnt); f(rateCounts); f(nbr); f(cflag); f(rateV); f(rateStop); f(rateLen);
-    f(act); f(next); f(chg);
+    f(scal); f(defCnt); f(rateCounts); f(nbr); f(cflag); f(core); f(small); f(rateV);
+    f(rateStop); f(rateLen); f(act); f(next); f(chg);
+    for (auto &k : runKeys) f(k);
     for (auto &b : buf) {
       f(b.vals); f(b.def[0]); f(b.def[1]); f(b.farSign);
       b = DBuf();
@@ -161,9 +207,12 @@ public:
     if (pinCounters) cudaFreeHost(pinCounters);
     if (pinScal) cudaFreeHost(pinScal);
     brickMap = slotBrick = slotList = freeStack = newList = counters = nullptr;
-    needed = nullptr; scal = defCnt = rateCounts = nullptr; nbr = nullptr; cflag = nullptr;
-    rateV = rateStop = nullptr; rateLen = nullptr; act = nullptr; next = nullptr; chg = nullptr;
-    pinCounters = nullptr; pinScal = nullptr;
+    needed = nullptr; scal = defCnt = rateCounts = small = nullptr; nbr = nullptr;
+    cflag = core = nullptr; rateV = rateStop = nullptr; rateLen = nullptr; act = nullptr;
+    next = nullptr; chg = nullptr; pinCounters = nullptr; pinScal = nullptr;
+    for (int l = 0; l < VLSG_MAX_LEVEL_SETS; ++l) runKeys[l] = nullptr, capRunKeys[l] = 0;
+    capBricks = capSlots = 0;
+    capL = 0;
   }
 
   int *nSlotsPtr() { return counters + 0; }
@@ -253,18 +302,27 @@ public:
   }
 
   // ------------------------------------------------------------- layout
+  // Arrays of buffers 0..nb-1 at the current sizes (contents of a grown
+  // array are not kept; every build fills them).
   void allocBuffers(int nb) {
-    const size_t cells = (size_t)cap * BV;
     for (int b = 0; b < nb; ++b) {
       auto &B = buf[b];
-      if (B.vals) continue;
-      VLSG_CUDA(cudaMalloc(&B.vals, cells * sizeof(T)));
-      VLSG_CUDA(cudaMalloc(&B.def[0], (size_t)cap * 8 * sizeof(uint64_t)));
-      VLSG_CUDA(cudaMalloc(&B.def[1], (size_t)cap * 8 * sizeof(uint64_t)));
-      VLSG_CUDA(cudaMalloc(&B.farSign, nBricks));
-      VLSG_CUDA(cudaMemsetAsync(B.def[0], 0, (size_t)cap * 8 * sizeof(uint64_t), stream));
-      VLSG_CUDA(cudaMemsetAsync(B.farSign, 1, nBricks, stream));
-      B.cur = 0;
+      if (B.capSlots < capSlots || !B.vals) {
+        if (B.vals) VLSG_CUDA(cudaFree(B.vals));
+        if (B.def[0]) VLSG_CUDA(cudaFree(B.def[0]));
+        if (B.def[1]) VLSG_CUDA(cudaFree(B.def[1]));
+        B.vals = nullptr, B.def[0] = B.def[1] = nullptr;
+        VLSG_CUDA(cudaMalloc(&B.vals, capSlots * BV * sizeof(T)));
+        VLSG_CUDA(cudaMalloc(&B.def[0], capSlots * 8 * sizeof(uint64_t)));
+        VLSG_CUDA(cudaMalloc(&B.def[1], capSlots * 8 * sizeof(uint64_t)));
+        B.capSlots = capSlots;
+      }
+      if (B.capBricks < capBricks || !B.farSign) {
+        if (B.farSign) VLSG_CUDA(cudaFree(B.farSign));
+        B.farSign = nullptr;
+        VLSG_CUDA(cudaMalloc(&B.farSign, capBricks));
+        B.capBricks = capBricks;
+      }
     }
   }
 
@@ -283,22 +341,95 @@ public:
     return s;
   }
 
-  void build(const GridDev &grid, std::vector<StagedLS> &ls, int margin) {
-    release();
-    ++generation;
+  // Per-brick arrays for nb bricks and per-slot arrays for c slots; cap
+  // becomes the allocated slot count.
+  void ensureLayout(size_t nb, size_t c) {
+    if (nb > capBricks) {
+      for (void *p : {(void *)brickMap, (void *)needed, (void *)core})
+        if (p) VLSG_CUDA(cudaFree(p));
+      brickMap = nullptr, needed = nullptr, core = nullptr;
+      const size_t n = nb + nb / 4 + 64;
+      VLSG_CUDA(cudaMalloc(&brickMap, n * sizeof(int)));
+      VLSG_CUDA(cudaMalloc(&needed, n));
+      VLSG_CUDA(cudaMalloc(&core, n));
+      capBricks = n;
+    }
+    if (c > 0 && (c > capSlots || L > capL)) {
+      for (void *p : {(void *)slotBrick, (void *)slotList, (void *)freeStack, (void *)newList,
+                      (void *)nbr, (void *)cflag, (void *)act, (void *)chg, (void *)next,
+                      (void *)rateV, (void *)rateStop, (void *)rateLen})
+        if (p) VLSG_CUDA(cudaFree(p));
+      slotBrick = slotList = freeStack = newList = nbr = nullptr;
+      cflag = rateLen = nullptr, act = chg = nullptr, next = rateV = rateStop = nullptr;
+      const size_t n = std::max(c, capSlots);
+      const int l = std::max(L, capL);
+      VLSG_CUDA(cudaMalloc(&slotBrick, n * sizeof(int)));
+      VLSG_CUDA(cudaMalloc(&slotList, n * sizeof(int)));
+      VLSG_CUDA(cudaMalloc(&freeStack, n * sizeof(int)));
+      VLSG_CUDA(cudaMalloc(&newList, n * sizeof(int)));
+      VLSG_CUDA(cudaMalloc(&nbr, n * 27 * sizeof(int)));
+      VLSG_CUDA(cudaMalloc(&cflag, n));
+      VLSG_CUDA(cudaMalloc(&act, n * 8 * sizeof(uint64_t)));
+      VLSG_CUDA(cudaMalloc(&chg, n * 8 * sizeof(uint64_t)));
+      VLSG_CUDA(cudaMalloc(&next, n * BV * sizeof(T)));
+      VLSG_CUDA(cudaMalloc(&rateV, n * BV * sizeof(T) * l));
+      VLSG_CUDA(cudaMalloc(&rateStop, n * BV * sizeof(T) * l));
+      VLSG_CUDA(cudaMalloc(&rateLen, n * BV));
+      capSlots = n;
+      capL = l;
+    }
+    cap = (int)capSlots;
+    poolCells = (size_t)cap * BV;
+  }
+
+  void ensureSmall() {
+    if (counters) return;
     VLSG_CUDA(cudaHostAlloc(&pinCounters, 32 * sizeof(int), cudaHostAllocDefault));
-    VLSG_CUDA(cudaHostAlloc(&pinScal, 8 * sizeof(unsigned long long), cudaHostAllocDefault));
+    VLSG_CUDA(cudaHostAlloc(&pinScal, 32 * sizeof(unsigned long long), cudaHostAllocDefault));
+    VLSG_CUDA(cudaMalloc(&counters, 16 * sizeof(int)));
+    VLSG_CUDA(cudaMalloc(&scal, 4 * sizeof(unsigned long long)));
+    VLSG_CUDA(cudaMalloc(&defCnt, MAXB * sizeof(unsigned long long)));
+    VLSG_CUDA(cudaMalloc(&rateCounts, 2 * sizeof(unsigned long long)));
+    VLSG_CUDA(cudaMalloc(&small, 16 * sizeof(unsigned long long)));
+  }
+
+  // Lay the uploaded level sets out on the device (lsDomain's HRLE data
+  // becomes bricks): map box from the points, allocated bricks = the
+  // points' bricks and their neighbours, values from the points and the
+  // runs' signs.  Allocations are reused from the previous build when they
+  // are large enough.
+  void build(const GridDev &grid, std::vector<StagedLS> &ls, int margin) {
+    ++generation;
+    ensureSmall();
     g = grid;
     L = (int)ls.size();
+    VLSG_CUDA(cudaMemsetAsync(counters, 0, 16 * sizeof(int), stream));
+    // point box (through the boundary mapping), run keys, order check
+    const int boxInit[6] = {INT_MAX, INT_MAX, INT_MAX, INT_MIN, INT_MIN, INT_MIN};
+    std::memcpy(pinCounters + 16, boxInit, sizeof(boxInit));
+    int *box = (int *)small;
+    VLSG_CUDA(cudaMemcpyAsync(box, pinCounters + 16, sizeof(boxInit), cudaMemcpyHostToDevice, stream));
+    for (int l = 0; l < L; ++l) {
+      auto &s = ls[l];
+      if (s.n) {
+        Scope sc(this, "upload_points");
+        kStagePoints<<<grid1(s.n), 256, 0, stream>>>(g, (int)s.n, s.idx, box, errPtr());
+        checkLaunch();
+      }
+      growDevice(runKeys[l], capRunKeys[l], (size_t)s.nRuns);
+      if (s.nRuns) {
+        Scope sc(this, "upload_runs");
+        kStageRuns<<<grid1(s.nRuns), 256, 0, stream>>>((int)s.nRuns, s.runStart, runKeys[l],
+                                                       counters + 12 /* unsorted flag */);
+        checkLaunch();
+      }
+    }
+    VLSG_CUDA(cudaMemcpyAsync(pinCounters + 16, box, sizeof(boxInit), cudaMemcpyDeviceToHost, stream));
+    syncErr("upload");
+    int hb[6];
+    std::memcpy(hb, pinCounters + 16, sizeof(hb));
+    if (hCounters[12]) sortRuns(ls);
     // box: bounded directions cover the grid, infinite ones the points + margin
-    long long lo[3], hi[3];
-    for (int d = 0; d < 3; ++d) lo[d] = LLONG_MAX, hi[d] = LLONG_MIN;
-    for (auto &s : ls)
-      for (size_t i = 0; i < s.vals.size(); ++i)
-        for (int d = 0; d < 3; ++d) {
-          lo[d] = std::min<long long>(lo[d], s.idx[3 * i + d]);
-          hi[d] = std::max<long long>(hi[d], s.idx[3 * i + d]);
-        }
     for (int d = 0; d < 3; ++d) {
       const bool bounded = g.bc[d] == VLSG_PERIODIC_BOUNDARY || g.bc[d] == VLSG_REFLECTIVE_BOUNDARY;
       if (bounded) {
@@ -307,93 +438,54 @@ public:
                                                        : g.gmax[d] - g.gmin[d] + 1;
         g.nb[d] = (n + BS - 1) / BS;
       } else {
-        if (lo[d] > hi[d]) lo[d] = hi[d] = 0;
-        const long long a = lo[d] - (long long)margin * BS;
-        const long long b = hi[d] + (long long)margin * BS;
+        long long lo = hb[d], hi = hb[3 + d];
+        if (lo > hi) lo = hi = 0;
+        const long long a = lo - (long long)margin * BS;
+        const long long b = hi + (long long)margin * BS;
         const long long a8 = (a >= 0) ? (a / BS) * BS : -(((-a) + BS - 1) / BS) * BS;
         g.org[d] = (int)a8;
         g.nb[d] = (int)((b - a8) / BS + 1);
       }
     }
-    nBricks = g.nb[0] * g.nb[1] * g.nb[2];
-    VLSG_CUDA(cudaMalloc(&brickMap, nBricks * sizeof(int)));
-    VLSG_CUDA(cudaMalloc(&needed, nBricks));
-    VLSG_CUDA(cudaMalloc(&counters, 16 * sizeof(int)));
-    VLSG_CUDA(cudaMalloc(&scal, 4 * sizeof(unsigned long long)));
-    VLSG_CUDA(cudaMalloc(&defCnt, MAXB * sizeof(unsigned long long)));
-    VLSG_CUDA(cudaMalloc(&rateCounts, 2 * sizeof(unsigned long long)));
-    VLSG_CUDA(cudaMemsetAsync(counters, 0, 16 * sizeof(int), stream));
-    VLSG_CUDA(cudaMemsetAsync(defCnt, 0, MAXB * sizeof(unsigned long long), stream));
+    const long long nb64 = (long long)g.nb[0] * g.nb[1] * g.nb[2];
+    if (nb64 > INT_MAX / 2) throw CudaError("upload: brick box too large", VLSG_ERR_CAPACITY);
+    nBricks = (int)nb64;
+    ensureLayout(nBricks, 0);
     VLSG_CUDA(cudaMemsetAsync(brickMap, 0xff, nBricks * sizeof(int), stream));
     VLSG_CUDA(cudaMemsetAsync(needed, 0, nBricks, stream));
-    // mark point bricks of every level set, dilate
-    uint8_t *core = nullptr;
-    VLSG_CUDA(cudaMalloc(&core, nBricks));
     VLSG_CUDA(cudaMemsetAsync(core, 0, nBricks, stream));
-    std::vector<int *> dIdx(L, nullptr);
-    std::vector<double *> dPtVal(L, nullptr);
-    std::vector<uint64_t *> dRunK(L, nullptr);
-    std::vector<int8_t *> dRunS(L, nullptr);
     for (int l = 0; l < L; ++l) {
-      auto &s = ls[l];
-      const size_t n = s.vals.size();
-      VLSG_CUDA(cudaMalloc(&dIdx[l], std::max<size_t>(1, n) * 3 * sizeof(int)));
-      VLSG_CUDA(cudaMalloc(&dPtVal[l], std::max<size_t>(1, n) * sizeof(double)));
-      VLSG_CUDA(cudaMalloc(&dRunK[l], std::max<size_t>(1, s.runKeys.size()) * sizeof(uint64_t)));
-      VLSG_CUDA(cudaMalloc(&dRunS[l], std::max<size_t>(1, s.runSign.size())));
-      if (n) {
-        VLSG_CUDA(cudaMemcpyAsync(dIdx[l], s.idx.data(), n * 3 * sizeof(int), cudaMemcpyHostToDevice, stream));
-        VLSG_CUDA(cudaMemcpyAsync(dPtVal[l], s.vals.data(), n * sizeof(double), cudaMemcpyHostToDevice, stream));
-      }
-      if (!s.runKeys.empty()) {
-        VLSG_CUDA(cudaMemcpyAsync(dRunK[l], s.runKeys.data(), s.runKeys.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, stream));
-        VLSG_CUDA(cudaMemcpyAsync(dRunS[l], s.runSign.data(), s.runSign.size(), cudaMemcpyHostToDevice, stream));
-      }
-      if (n) {
-        Scope sc(this, "upload_mark");
-        kMarkPointBricks<<<grid1(n), 256, 0, stream>>>(g, (int)n, dIdx[l], core, errPtr());
-        checkLaunch();
-      }
+      if (!ls[l].n) continue;
+      Scope sc(this, "upload_mark");
+      kMarkPointBricks<<<grid1(ls[l].n), 256, 0, stream>>>(g, (int)ls[l].n, ls[l].idx, core, errPtr());
+      checkLaunch();
     }
     {
       Scope sc(this, "upload_dilate");
       kDilateBricks<<<grid1(nBricks), 256, 0, stream>>>(g, nBricks, core, needed, errPtr());
+      kCountFlags<<<grid1(nBricks), 256, 0, stream>>>(needed, nBricks, counters + 13);
       checkLaunch();
     }
-    // count needed bricks to size the pool
-    std::vector<uint8_t> hNeeded(nBricks);
-    VLSG_CUDA(cudaMemcpyAsync(hNeeded.data(), needed, nBricks, cudaMemcpyDeviceToHost, stream));
     syncErr("upload");
-    long long nNeeded = 0;
-    for (auto v : hNeeded) nNeeded += v;
-    cap = (int)std::max<long long>(1024, nNeeded * 2 + 256);
-    poolCells = (size_t)cap * BV;
-    VLSG_CUDA(cudaMalloc(&slotBrick, cap * sizeof(int)));
-    VLSG_CUDA(cudaMalloc(&slotList, cap * sizeof(int)));
-    VLSG_CUDA(cudaMalloc(&freeStack, cap * sizeof(int)));
-    VLSG_CUDA(cudaMalloc(&newList, cap * sizeof(int)));
-    VLSG_CUDA(cudaMalloc(&nbr, (size_t)cap * 27 * sizeof(int)));
-    VLSG_CUDA(cudaMalloc(&cflag, cap));
-    VLSG_CUDA(cudaMalloc(&act, (size_t)cap * 8 * sizeof(uint64_t)));
-    VLSG_CUDA(cudaMalloc(&chg, (size_t)cap * 8 * sizeof(uint64_t)));
-    VLSG_CUDA(cudaMalloc(&next, poolCells * sizeof(T)));
-    VLSG_CUDA(cudaMalloc(&rateV, poolCells * sizeof(T) * L));
-    VLSG_CUDA(cudaMalloc(&rateStop, poolCells * sizeof(T) * L));
-    VLSG_CUDA(cudaMalloc(&rateLen, poolCells));
-    VLSG_CUDA(cudaMemsetAsync(slotBrick, 0xff, cap * sizeof(int), stream));
+    const long long nNeeded = hCounters[13];
+    ensureLayout(nBricks, (size_t)std::max<long long>(1024, nNeeded * 2 + 256));
     {
-      std::vector<int> fs(cap);
-      for (int i = 0; i < cap; ++i) fs[i] = cap - 1 - i;
-      VLSG_CUDA(cudaMemcpyAsync(freeStack, fs.data(), cap * sizeof(int), cudaMemcpyHostToDevice, stream));
-      int c[2] = {0, cap};
-      VLSG_CUDA(cudaMemcpyAsync(counters, c, 2 * sizeof(int), cudaMemcpyHostToDevice, stream));
-      VLSG_CUDA(cudaStreamSynchronize(stream));
+      Scope sc(this, "upload_pool");
+      kInitFreeStack<<<grid1(cap), 256, 0, stream>>>(freeStack, cap);
+      VLSG_CUDA(cudaMemsetAsync(slotBrick, 0xff, (size_t)cap * sizeof(int), stream));
+      checkLaunch();
+    }
+    const int c2[2] = {0, cap};
+    std::memcpy(pinCounters + 24, c2, sizeof(c2));
+    VLSG_CUDA(cudaMemcpyAsync(counters, pinCounters + 24, sizeof(c2), cudaMemcpyHostToDevice, stream));
+    for (auto &B : buf) {
+      B.cur = 0, B.width = 1, B.live = false, B.bound = 0, B.nDef = 0;
     }
     allocBuffers(L);
     for (int l = 0; l < L; ++l) {
       Scope sc(this, "upload_farsign");
-      kFarSignFromRuns<<<grid1(nBricks), 256, 0, stream>>>(
-          g, nBricks, dRunK[l], dRunS[l], (int)ls[l].runKeys.size(), buf[l].farSign);
+      kFarSignFromRuns<<<grid1(nBricks), 256, 0, stream>>>(g, nBricks, runKeys[l], ls[l].runSign,
+                                                           (int)ls[l].nRuns, buf[l].farSign);
       checkLaunch();
       buf[l].width = ls[l].width;
       buf[l].live = true;
@@ -406,42 +498,68 @@ public:
       checkLaunch();
     }
     rebuildSlotList();
+    VLSG_CUDA(cudaMemsetAsync(small + 6, 0, VLSG_MAX_LEVEL_SETS * sizeof(unsigned long long), stream));
     for (int l = 0; l < L; ++l) {
       auto &s = ls[l];
       {
         Scope sc(this, "upload_fill");
-        kFillFromRuns<T><<<blocksPass, 256, 0, stream>>>(g, slotList, nSlotsPtr(), slotBrick, dRunK[l],
-                                                         dRunS[l], (int)s.runKeys.size(), buf[l].vals);
+        kFillRows<T><<<grid1((size_t)cap * 64), 256, 0, stream>>>(
+            g, slotList, nSlotsPtr(), slotBrick, cflag, runKeys[l], s.runSign, (int)s.nRuns,
+            buf[l].vals);
         checkLaunch();
       }
-      if (!s.vals.empty()) {
+      if (s.n) {
         Scope sc(this, "upload_scatter");
-        kScatterPoints<T><<<grid1(s.vals.size()), 256, 0, stream>>>(
-            g, (int)s.vals.size(), dIdx[l], dPtVal[l], brickMap, buf[l].vals, errPtr());
+        kScatterPoints<T><<<grid1(s.n), 256, 0, stream>>>(g, (int)s.n, s.idx, s.vals, brickMap,
+                                                          buf[l].vals, errPtr());
         checkLaunch();
       }
       {
         Scope sc(this, "upload_masks");
         kMasksFromValues<T><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(
-            g, slotBrick, slotList, nSlotsPtr(), buf[l].vals, buf[l].def[buf[l].cur], nullptr);
+            g, slotBrick, slotList, nSlotsPtr(), buf[l].vals, buf[l].def[buf[l].cur], nullptr,
+            small + 6 + l);
         checkLaunch();
       }
-      double bound = 0;
-      for (double v : s.vals) {
-        const double a = std::fabs((double)(T)v);
-        if (a > bound) bound = a;
-      }
-      buf[l].bound = bound;
     }
+    VLSG_CUDA(cudaMemcpyAsync(pinScal + 8, small + 6, VLSG_MAX_LEVEL_SETS * sizeof(unsigned long long),
+                              cudaMemcpyDeviceToHost, stream));
     syncErr("upload");
     for (int l = 0; l < L; ++l) {
-      cudaFree(dIdx[l]);
-      cudaFree(dPtVal[l]);
-      cudaFree(dRunK[l]);
-      cudaFree(dRunS[l]);
-      buf[l].nDef = defined(l);
+      double bound;
+      std::memcpy(&bound, &pinScal[8 + l], sizeof(double));
+      buf[l].bound = bound;
+      buf[l].nDef = profiling ? defined(l) : 0;
     }
-    cudaFree(core);
+  }
+
+  // Runs that arrived out of HRLE order: sort them (stable) on the host.
+  void sortRuns(std::vector<StagedLS> &ls) {
+    for (int l = 0; l < L; ++l) {
+      auto &s = ls[l];
+      if (s.nRuns < 2) continue;
+      std::vector<uint64_t> k(s.nRuns);
+      std::vector<int8_t> sg(s.nRuns);
+      std::vector<int32_t> st(3 * s.nRuns);
+      VLSG_CUDA(cudaMemcpyAsync(k.data(), runKeys[l], s.nRuns * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream));
+      VLSG_CUDA(cudaMemcpyAsync(sg.data(), s.runSign, s.nRuns, cudaMemcpyDeviceToHost, stream));
+      VLSG_CUDA(cudaMemcpyAsync(st.data(), s.runStart, 3 * s.nRuns * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+      VLSG_CUDA(cudaStreamSynchronize(stream));
+      std::vector<int64_t> o(s.nRuns);
+      for (int64_t i = 0; i < s.nRuns; ++i) o[i] = i;
+      std::stable_sort(o.begin(), o.end(), [&](int64_t a, int64_t b) { return k[a] < k[b]; });
+      std::vector<uint64_t> k2(s.nRuns);
+      std::vector<int8_t> sg2(s.nRuns);
+      std::vector<int32_t> st2(3 * s.nRuns);
+      for (int64_t i = 0; i < s.nRuns; ++i) {
+        k2[i] = k[o[i]], sg2[i] = sg[o[i]];
+        for (int d = 0; d < 3; ++d) st2[3 * i + d] = st[3 * o[i] + d];
+      }
+      VLSG_CUDA(cudaMemcpyAsync(runKeys[l], k2.data(), s.nRuns * sizeof(uint64_t), cudaMemcpyHostToDevice, stream));
+      VLSG_CUDA(cudaMemcpyAsync(s.runSign, sg2.data(), s.nRuns, cudaMemcpyHostToDevice, stream));
+      VLSG_CUDA(cudaMemcpyAsync(s.runStart, st2.data(), 3 * s.nRuns * sizeof(int32_t), cudaMemcpyHostToDevice, stream));
+      VLSG_CUDA(cudaStreamSynchronize(stream));
+    }
   }
 
   void syncErr(const char *where) {
@@ -456,6 +574,7 @@ public:
       if (e & 4) m += " brick pool capacity exceeded;";
       if (e & 8) m += " freed brick held a defined point;";
       if (e & 64) m += " band reached an unallocated brick;";
+      if (e & 128) m += " a point index lies outside the supported range (+-2^19);";
       int z = 0;
       cudaMemcpy(errPtr(), &z, sizeof(int), cudaMemcpyHostToDevice);
       throw CudaError(m, (e & 4) ? VLSG_ERR_CAPACITY : VLSG_ERR_DEVICE_CHECK);

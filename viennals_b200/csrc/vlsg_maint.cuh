@@ -229,6 +229,107 @@ __global__ void kFillFromRuns(GridDev g, const int *slotList, const int *nSlots,
   }
 }
 
+// Undefined cells of every allocated brick from the runs' signs (before the
+// points are scattered): one thread per x-row of a brick, one binary search
+// per row and a walk along it; bricks next to a boundary that remaps cells
+// look every cell up through the mapping.
+template <class T>
+__global__ void kFillRows(GridDev g, const int *slotList, const int *nSlots, const int *slotBrick,
+                          const uint8_t *cflag, const uint64_t *keys, const int8_t *sign,
+                          int nRuns, T *vals) {
+  const size_t total = (size_t)*nSlots * 64;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const int slot = slotList[e >> 6];
+    const int lz = (int)(e >> 3) & 7, ly = (int)e & 7;
+    int bx, by, bz;
+    brickCoords(g, slotBrick[slot], bx, by, bz);
+    const int x0 = g.org[0] + bx * BS, y = g.org[1] + by * BS + ly, z = g.org[2] + bz * BS + lz;
+    T *row = vals + (size_t)slot * BV + lz * 64 + ly * 8;
+    if (cflag[slot] & 1) { // CF_STAR
+      for (int lx = 0; lx < 8; ++lx) {
+        const int s = runSignAt(keys, sign, nRuns, cellKey(mapCoord(g, 0, x0 + lx), mapCoord(g, 1, y),
+                                                           mapCoord(g, 2, z)));
+        row[lx] = s < 0 ? Lim<T>::lowest() : Lim<T>::max();
+      }
+      continue;
+    }
+    if (nRuns <= 0) {
+      for (int lx = 0; lx < 8; ++lx) row[lx] = Lim<T>::max();
+      continue;
+    }
+    const uint64_t key0 = cellKey(x0, y, z);
+    int lo = 0, hi = nRuns; // first run starting after key0
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (keys[mid] <= key0) lo = mid + 1;
+      else hi = mid;
+    }
+    int j = lo - 1;
+    for (int lx = 0; lx < 8; ++lx) {
+      const uint64_t key = key0 + lx;
+      while (j + 1 < nRuns && keys[j + 1] <= key) ++j;
+      const int s = j < 0 ? sign[0] : sign[j];
+      row[lx] = s < 0 ? Lim<T>::lowest() : Lim<T>::max();
+    }
+  }
+}
+
+// Uploaded points through the boundary mapping (in place), their index box
+// (atomic min / max into box[0..5]) and the range check (err bit 128).
+__global__ void kStagePoints(GridDev g, int n, int32_t *idx, int *box, int *err) {
+  int mn[3] = {INT_MAX, INT_MAX, INT_MAX}, mx[3] = {INT_MIN, INT_MIN, INT_MIN};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    for (int d = 0; d < 3; ++d) {
+      const int c = mapCoord(g, d, idx[3 * i + d]);
+      if (c < -(1 << 19) || c > (1 << 19)) atomicOr(err, 128);
+      idx[3 * i + d] = c;
+      mn[d] = min(mn[d], c), mx[d] = max(mx[d], c);
+    }
+  }
+  for (int d = 0; d < 3; ++d)
+    for (int o = 16; o > 0; o >>= 1) {
+      mn[d] = min(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o));
+      mx[d] = max(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o));
+    }
+  if ((threadIdx.x & 31) == 0 && mn[0] != INT_MAX)
+    for (int d = 0; d < 3; ++d) {
+      atomicMin(&box[d], mn[d]);
+      atomicMax(&box[3 + d], mx[d]);
+    }
+}
+
+__device__ inline uint64_t runKey(const int32_t *start, int i) {
+  int c[3];
+  for (int d = 0; d < 3; ++d) {
+    const int v = start[3 * i + d];
+    c[d] = v < -(1 << 20) + 1 ? -(1 << 20) + 1 : (v > (1 << 20) - 1 ? (1 << 20) - 1 : v);
+  }
+  return cellKey(c[0], c[1], c[2]);
+}
+
+// HRLE keys of the run starts; *unsorted is set when they are out of order.
+__global__ void kStageRuns(int n, const int32_t *start, uint64_t *keys, int *unsorted) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint64_t k = runKey(start, i);
+    keys[i] = k;
+    if (i > 0 && k < runKey(start, i - 1)) atomicOr(unsorted, 1);
+  }
+}
+
+__global__ void kCountFlags(const uint8_t *f, int n, int *count) {
+  for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    const int i = base + threadIdx.x;
+    const unsigned m = __ballot_sync(0xffffffffu, i < n && f[i]);
+    if ((threadIdx.x & 31) == 0 && m) atomicAdd(count, __popc(m));
+  }
+}
+
+__global__ void kInitFreeStack(int *freeStack, int cap) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += gridDim.x * blockDim.x)
+    freeStack[i] = cap - 1 - i;
+}
+
 template <class T>
 __global__ void kScatterPoints(GridDev g, int n, const int *idx, const double *v,
                                const int *brickMap, T *vals, int *err) {
@@ -255,11 +356,12 @@ __global__ void kScatterPoints(GridDev g, int n, const int *idx, const double *v
 template <class T>
 __global__ void kMasksFromValues(GridDev g, const int *slotBrick, const int *slotList,
                                  const int *nSlots, T *vals, uint64_t *def,
-                                 unsigned long long *cnt) {
+                                 unsigned long long *cnt, unsigned long long *bound) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nWarps = (gridDim.x * blockDim.x) >> 5;
   const int n = *nSlots;
+  double maxAbs = 0.0;
   for (int w = warp; w < n; w += nWarps) {
     const int slot = slotList[w];
     int bx, by, bz;
@@ -279,11 +381,16 @@ __global__ void kMasksFromValues(GridDev g, const int *slotBrick, const int *slo
         const unsigned m = __ballot_sync(0xffffffffu, isDef(v));
         bits |= (uint64_t)m << (32 * half);
         nd += lane == 0 ? __popc(m) : 0;
+        if (isDef(v)) maxAbs = fmax(maxAbs, fabs((double)v));
       }
       if (lane == z) mine = bits;
     }
     if (lane < 8) def[(size_t)slot * 8 + lane] = mine;
     if (lane == 0 && nd && cnt) atomicAdd(cnt, (unsigned long long)nd);
+  }
+  if (bound) {
+    for (int o = 16; o > 0; o >>= 1) maxAbs = fmax(maxAbs, __shfl_xor_sync(0xffffffffu, maxAbs, o));
+    if (lane == 0 && maxAbs > 0.0) atomicMax(bound, (unsigned long long)__double_as_longlong(maxAbs));
   }
 }
 
