@@ -80,11 +80,17 @@ class Context:
         self._check(self.lib.vlsg_count_points(self.h, int(slot), ctypes.byref(n)))
         return n.value
 
-    def download(self, slot):
-        """(idx, values, width) of the defined points in HRLE order."""
+    def download(self, slot, idx_out=None, val_out=None):
+        """(idx, values, width) of the defined points in HRLE order.  With
+        idx_out ((M,3) int32) and val_out ((M,) float64) of capacity M >= n
+        (e.g. pinned host memory), the points land there and views of their
+        first n rows are returned."""
         n = self.count(slot)
-        idx = np.zeros((n, 3), np.int32)
-        val = np.zeros(n)
+        if idx_out is not None and val_out is not None and len(idx_out) >= n and len(val_out) >= n:
+            idx, val = idx_out[:n], val_out[:n]
+        else:
+            idx = np.empty((n, 3), np.int32)
+            val = np.empty(n)
         w = ctypes.c_int32()
         self._check(self.lib.vlsg_download_levelset(self.h, int(slot), n, _p(idx, ctypes.c_int32),
                                                     _p(val, ctypes.c_double), ctypes.byref(w)))
@@ -117,24 +123,40 @@ class Context:
                      device_ms=arr[i].device_ms, bytes=arr[i].algorithmic_bytes)
                 for i in range(cnt.value)]
 
-    def download_runs(self, slot):
+    def download_runs(self, slot, start_out=None, sign_out=None):
         """(run_start (K,3) int32, run_sign (K,) int8) of the undefined runs in
-        HRLE order, built on the device (vlsg_download_runs)."""
+        HRLE order, built on the device (vlsg_download_runs); optional output
+        buffers as for download()."""
         n = ctypes.c_int64()
-        rc = self.lib.vlsg_download_runs(self.h, int(slot), 0, None, None, ctypes.byref(n))
-        if rc not in (0, -3):
-            self._check(rc)
-        starts = np.zeros((n.value, 3), np.int32)
-        signs = np.zeros(n.value, np.int8)
+        cap = 0
+        if start_out is not None and sign_out is not None:
+            cap = min(len(start_out), len(sign_out))
+            rc = self.lib.vlsg_download_runs(self.h, int(slot), cap, _p(start_out, ctypes.c_int32),
+                                             _p(sign_out, ctypes.c_int8), ctypes.byref(n))
+            if rc == 0:
+                return start_out[:n.value], sign_out[:n.value]
+            if rc != -3:
+                self._check(rc)
+        else:
+            rc = self.lib.vlsg_download_runs(self.h, int(slot), 0, None, None, ctypes.byref(n))
+            if rc not in (0, -3):
+                self._check(rc)
+        starts = np.empty((n.value, 3), np.int32)
+        signs = np.empty(n.value, np.int8)
         self._check(self.lib.vlsg_download_runs(self.h, int(slot), n.value, _p(starts, ctypes.c_int32),
                                                 _p(signs, ctypes.c_int8), ctypes.byref(n)))
         return starts, signs
 
-    def download_domain(self, slot, grid):
+    def download_domain(self, slot, grid, out=None):
         """Domain with the defined points and the undefined runs, both in HRLE
-        order from the device."""
-        idx, val, w = self.download(slot)
-        rs, sg = self.download_runs(slot)
+        order from the device.  `out` may be a Domain whose arrays serve as
+        output buffers (capacity permitting)."""
+        if out is not None:
+            idx, val, w = self.download(slot, out.idx, out.values)
+            rs, sg = self.download_runs(slot, out.run_start, out.run_sign)
+        else:
+            idx, val, w = self.download(slot)
+            rs, sg = self.download_runs(slot)
         return Domain(grid, idx, val, rs, sg, width=w)
 
     def download_domain_host_runs(self, slot, grid):

@@ -156,8 +156,12 @@ public:
   T *rateV = nullptr, *rateStop = nullptr; // pool shaped, L chain entries
   uint8_t *rateLen = nullptr;
   uint64_t *act = nullptr;  // active masks of the top level set
-  T *next = nullptr;        // new values of the cells a pass changes
-  uint64_t *chg = nullptr;  // change masks of the last pass
+  // change log of a pass: one segment of logPer entries per warp of the pass
+  uint32_t *logCell = nullptr;
+  T *logVal = nullptr;
+  int *logCount = nullptr;
+  size_t logPer = 0;
+  int logSegments = 0;
   // host mirrors
   int hCounters[16];
   unsigned long long hScal[4];
@@ -198,7 +202,7 @@ public:
     auto f = [](void *p) { if (p) cudaFree(p); };
     f(brickMap); f(slotBrick); f(slotList); f(freeStack); f(newList); f(counters); f(needed);
     f(scal); f(defCnt); f(rateCounts); f(nbr); f(cflag); f(core); f(small); f(rateV);
-    f(rateStop); f(rateLen); f(act); f(next); f(chg);
+    f(rateStop); f(rateLen); f(act); f(logCell); f(logVal); f(logCount);
     for (auto &k : runKeys) f(k);
     for (auto &b : buf) {
       f(b.vals); f(b.def[0]); f(b.def[1]); f(b.farSign);
@@ -209,7 +213,8 @@ public:
     brickMap = slotBrick = slotList = freeStack = newList = counters = nullptr;
     needed = nullptr; scal = defCnt = rateCounts = small = nullptr; nbr = nullptr;
     cflag = core = nullptr; rateV = rateStop = nullptr; rateLen = nullptr; act = nullptr;
-    next = nullptr; chg = nullptr; pinCounters = nullptr; pinScal = nullptr;
+    logCell = nullptr; logVal = nullptr; logCount = nullptr; logPer = 0; logSegments = 0;
+    pinCounters = nullptr; pinScal = nullptr;
     for (int l = 0; l < VLSG_MAX_LEVEL_SETS; ++l) runKeys[l] = nullptr, capRunKeys[l] = 0;
     capBricks = capSlots = 0;
     capL = 0;
@@ -228,8 +233,9 @@ public:
   Topo topo() { return Topo{g, brickMap, slotBrick, slotList, nSlotsPtr(), nbr, cflag, errPtr()}; }
   LsView<T> lsView(int b) {
     auto &B = buf[b];
-    return LsView<T>{B.vals, B.def[B.cur], B.def[1 - B.cur], B.farSign, next, chg};
+    return LsView<T>{B.vals, B.def[B.cur], B.def[1 - B.cur], B.farSign};
   }
+  ChangeLog<T> changeLog() { return ChangeLog<T>{logCell, logVal, logCount, logPer}; }
 
   // ---------------------------------------------------------------- timing
   // One kernel launch.  With profiling on it is bracketed by CUDA events on
@@ -356,11 +362,12 @@ public:
     }
     if (c > 0 && (c > capSlots || L > capL)) {
       for (void *p : {(void *)slotBrick, (void *)slotList, (void *)freeStack, (void *)newList,
-                      (void *)nbr, (void *)cflag, (void *)act, (void *)chg, (void *)next,
-                      (void *)rateV, (void *)rateStop, (void *)rateLen})
+                      (void *)nbr, (void *)cflag, (void *)act, (void *)logCell, (void *)logVal,
+                      (void *)logCount, (void *)rateV, (void *)rateStop, (void *)rateLen})
         if (p) VLSG_CUDA(cudaFree(p));
-      slotBrick = slotList = freeStack = newList = nbr = nullptr;
-      cflag = rateLen = nullptr, act = chg = nullptr, next = rateV = rateStop = nullptr;
+      slotBrick = slotList = freeStack = newList = nbr = logCount = nullptr;
+      cflag = rateLen = nullptr, act = nullptr, logCell = nullptr;
+      logVal = rateV = rateStop = nullptr;
       const size_t n = std::max(c, capSlots);
       const int l = std::max(L, capL);
       VLSG_CUDA(cudaMalloc(&slotBrick, n * sizeof(int)));
@@ -370,8 +377,13 @@ public:
       VLSG_CUDA(cudaMalloc(&nbr, n * 27 * sizeof(int)));
       VLSG_CUDA(cudaMalloc(&cflag, n));
       VLSG_CUDA(cudaMalloc(&act, n * 8 * sizeof(uint64_t)));
-      VLSG_CUDA(cudaMalloc(&chg, n * 8 * sizeof(uint64_t)));
-      VLSG_CUDA(cudaMalloc(&next, n * BV * sizeof(T)));
+      // a pass warp handles at most ceil(n / warps) bricks: its log segment
+      // holds all their cells
+      logSegments = blocksPass * (FRONTIER_THREADS / 32);
+      logPer = (size_t)BV * ((n + logSegments - 1) / logSegments);
+      VLSG_CUDA(cudaMalloc(&logCell, logPer * logSegments * sizeof(uint32_t)));
+      VLSG_CUDA(cudaMalloc(&logVal, logPer * logSegments * sizeof(T)));
+      VLSG_CUDA(cudaMalloc(&logCount, logSegments * sizeof(int)));
       VLSG_CUDA(cudaMalloc(&rateV, n * BV * sizeof(T) * l));
       VLSG_CUDA(cudaMalloc(&rateStop, n * BV * sizeof(T) * l));
       VLSG_CUDA(cudaMalloc(&rateLen, n * BV));
@@ -631,7 +643,8 @@ public:
   // --------------------------------------------------------------- passes
   void applyChanges(int b) {
     Scope sc(this, "apply_changes");
-    kApplyChanges<T><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(topo(), buf[b].vals, next, chg);
+    kApplyChanges<T><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(buf[b].vals, changeLog(),
+                                                                   logSegments);
     checkLaunch();
   }
 
@@ -646,8 +659,8 @@ public:
         buf[b].cur ^= 1;
         return bandPassBytes(nIn, buf[b].nDef);
       });
-      kFrontierPass<T, MODE, Rule><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(topo(), lsView(b),
-                                                                                 rule);
+      kFrontierPass<T, MODE, Rule><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(
+          topo(), lsView(b), rule, changeLog());
       checkLaunch();
     }
     applyChanges(b);
@@ -698,7 +711,8 @@ public:
         // in: the active band; out: the new band
         return bandPassBytes(lastActive, buf[top].nDef);
       });
-      kUpdateRebuild<T><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(topo(), lsView(top), act, 1.0);
+      kUpdateRebuild<T><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(topo(), lsView(top), act, 1.0,
+                                                                     changeLog());
       checkLaunch();
     }
     applyChanges(top);

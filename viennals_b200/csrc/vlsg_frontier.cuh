@@ -6,9 +6,10 @@
 // 64-bit word per z-plane, bit y*8+x).  A pass takes one warp per brick,
 // finds the brick's candidate cells by bit dilation of the masks (neighbour
 // bricks' face planes through the 27-neighbour table), evaluates the
-// reference's rule on the candidates only, writes every value that changes to
-// a scratch array and marks it in a per-slot change mask; kApplyChanges copies
-// the marked cells back afterwards, so every rule reads old values only --
+// reference's rule on the candidates only and appends every (cell, new value)
+// that changes to its warp's own segment of a change log (no atomics: a warp
+// handles at most ceil(slots / warps) bricks of 512 cells); kApplyChanges
+// streams the log back afterwards, so every rule reads old values only --
 // the reference maps the whole old level set to a new one (Jacobi order).
 // The new defined masks go to a second mask array.
 // Candidates per pass:
@@ -62,8 +63,14 @@ template <class T> struct LsView {
   const uint64_t *def;   // current masks, slots x 8 words
   uint64_t *defNext;     // masks after the pass
   const int8_t *farSign; // per brick of the map box
-  T *next;               // scratch: new values of the changed cells
-  uint64_t *chg;         // change masks, slots x 8 words
+};
+
+// Change log: segment w (of `per` entries) belongs to warp w of the pass.
+template <class T> struct ChangeLog {
+  uint32_t *cell; // slot << 9 | cell
+  T *val;
+  int *count;     // entries per segment
+  size_t per;
 };
 
 template <class T> __device__ inline T sentinel(bool neg) {
@@ -200,29 +207,39 @@ struct PlaneEnum {
   }
 };
 
-// Per-warp shared words of the brick in hand: change and flip masks.
+// Per-warp shared words of the brick in hand: cells whose definedness flips.
 struct WarpMasks {
-  unsigned long long chg[8], flip[8];
+  unsigned long long flip[8];
 };
 
 __device__ inline void markCell(unsigned long long *words, int c) {
   atomicOr(&words[c >> 6], 1ull << (c & 63));
 }
 
-// Publish the brick's change mask and its new defined mask (old ^ flips).
-__device__ inline void finishBrick(WarpMasks &m, uint64_t *chg, uint64_t *defNext, int slot,
-                                   int lane, uint64_t own) {
+// Publish the brick's new defined mask (old ^ flips).
+__device__ inline void finishBrick(WarpMasks &m, uint64_t *defNext, int slot, int lane,
+                                   uint64_t own) {
   __syncwarp();
-  if (lane < 8) {
-    chg[(size_t)slot * 8 + lane] = m.chg[lane];
-    defNext[(size_t)slot * 8 + lane] = own ^ m.flip[lane];
-  }
+  if (lane < 8) defNext[(size_t)slot * 8 + lane] = own ^ m.flip[lane];
   __syncwarp();
 }
 
 __device__ inline void clearBrick(WarpMasks &m, int lane) {
-  if (lane < 8) m.chg[lane] = 0ull, m.flip[lane] = 0ull;
+  if (lane < 8) m.flip[lane] = 0ull;
   __syncwarp();
+}
+
+// Append the lanes with `has` to the warp's log segment (warp-uniform call).
+template <class T>
+__device__ inline void logChange(const ChangeLog<T> &lg, size_t base, int &count, bool has,
+                                 uint32_t cell, T val) {
+  const unsigned m = __ballot_sync(0xffffffffu, has);
+  if (has) {
+    const size_t p = base + count + __popc(m & ((1u << (threadIdx.x & 31)) - 1));
+    lg.cell[p] = cell;
+    lg.val[p] = val;
+  }
+  count += __popc(m);
 }
 
 enum : int { FP_EXPAND = 0, FP_PRUNE = 1, FP_ALL = 2 };
@@ -232,13 +249,15 @@ enum : int { FP_EXPAND = 0, FP_PRUNE = 1, FP_ALL = 2 };
 // defined cells and their neighbours.
 template <class T, int MODE, class Rule>
 __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
-    kFrontierPass(Topo t, LsView<T> v, Rule rule) {
+    kFrontierPass(Topo t, LsView<T> v, Rule rule, ChangeLog<T> lg) {
   __shared__ WarpMasks sm[FRONTIER_THREADS / 32];
   WarpMasks &wm = sm[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nWarps = (gridDim.x * blockDim.x) >> 5;
   const int n = *t.nSlots;
+  const size_t logBase = (size_t)warp * lg.per;
+  int logged = 0;
   for (int w = warp; w < n; w += nWarps) {
     const int slot = t.slotList[w];
     const BrickCtx b = loadBrickCtx(t, slot);
@@ -258,6 +277,8 @@ __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
     for (int base = 0; base < pe.total; base += 32) {
       const int k = base + lane;
       const int c = pe.cell(cand, k < pe.total ? k : pe.total - 1);
+      bool changed = false;
+      T out = T(0);
       if (k < pe.total) {
         const size_t q = (size_t)slot * BV + c;
         const T center = v.vals[q];
@@ -266,35 +287,30 @@ __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
         T nb[6];
 #pragma unroll
         for (int j = 0; j < 6; ++j) nb[j] = refValue<T>(v.vals, v.farSign, ref[j], loc[j]);
-        const T out = rule(center, nb);
-        if (out != center || signbit(out) != signbit(center)) {
-          v.next[q] = out;
-          markCell(wm.chg, c);
-          if (isDef(out) != isDef(center)) markCell(wm.flip, c);
-        }
+        out = rule(center, nb);
+        changed = out != center || signbit(out) != signbit(center);
+        if (changed && isDef(out) != isDef(center)) markCell(wm.flip, c);
       }
+      logChange<T>(lg, logBase, logged, changed, ((uint32_t)slot << 9) | (uint32_t)c, out);
     }
-    finishBrick(wm, v.chg, v.defNext, slot, lane, own);
+    finishBrick(wm, v.defNext, slot, lane, own);
   }
+  if (lane == 0) lg.count[warp] = logged;
 }
 
-// Copy the changed cells of every listed slot from the scratch array back.
+// Write a change log back: warp w copies segment w.
 template <class T>
 __global__ void __launch_bounds__(FRONTIER_THREADS)
-    kApplyChanges(Topo t, T *vals, const T *next, const uint64_t *chg) {
+    kApplyChanges(T *vals, ChangeLog<T> lg, int segments) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nWarps = (gridDim.x * blockDim.x) >> 5;
-  const int n = *t.nSlots;
-  for (int w = warp; w < n; w += nWarps) {
-    const int slot = t.slotList[w];
-    const uint64_t m = lane < 8 ? chg[(size_t)slot * 8 + lane] : 0ull;
-    if (!__any_sync(0xffffffffu, m != 0ull)) continue;
-    const PlaneEnum pe(m);
-    for (int base = 0; base < pe.total; base += 32) {
-      const int k = base + lane;
-      const int c = pe.cell(m, k < pe.total ? k : pe.total - 1);
-      if (k < pe.total) vals[(size_t)slot * BV + c] = next[(size_t)slot * BV + c];
+  for (int w = warp; w < segments; w += nWarps) {
+    const int n = lg.count[w];
+    const size_t base = (size_t)w * lg.per;
+    for (int i = lane; i < n; i += 32) {
+      const uint32_t q = lg.cell[base + i];
+      vals[(size_t)(q >> 9) * BV + (q & 511)] = lg.val[base + i];
     }
   }
 }
@@ -315,13 +331,15 @@ __device__ inline T reducedValue(const T *vals, const uint64_t *act, const int8_
 // defined cell becomes undefined with its sign.
 template <class T>
 __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
-    kUpdateRebuild(Topo t, LsView<T> v, const uint64_t *act, double cutoff) {
+    kUpdateRebuild(Topo t, LsView<T> v, const uint64_t *act, double cutoff, ChangeLog<T> lg) {
   __shared__ WarpMasks sm[FRONTIER_THREADS / 32];
   WarpMasks &wm = sm[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nWarps = (gridDim.x * blockDim.x) >> 5;
   const int n = *t.nSlots;
+  const size_t logBase = (size_t)warp * lg.per;
+  int logged = 0;
   const RebuildRule<T> rule{cutoff};
   for (int w = warp; w < n; w += nWarps) {
     const int slot = t.slotList[w];
@@ -336,6 +354,8 @@ __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
     for (int base = 0; base < pe.total; base += 32) {
       const int k = base + lane;
       const int c = pe.cell(cand, k < pe.total ? k : pe.total - 1);
+      bool changed = false;
+      T out = T(0);
       if (k < pe.total) {
         const size_t q = (size_t)slot * BV + c;
         const T mem = v.vals[q];
@@ -345,28 +365,26 @@ __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
         T nb[6];
 #pragma unroll
         for (int j = 0; j < 6; ++j) nb[j] = reducedValue<T>(v.vals, act, v.farSign, ref[j], loc[j]);
-        const T out = rule(center, nb);
-        if (out != mem || signbit(out) != signbit(mem)) {
-          v.next[q] = out;
-          markCell(wm.chg, c);
-          if (isDef(out) != isDef(mem)) markCell(wm.flip, c);
-        }
+        out = rule(center, nb);
+        changed = out != mem || signbit(out) != signbit(mem);
+        if (changed && isDef(out) != isDef(mem)) markCell(wm.flip, c);
       }
+      logChange<T>(lg, logBase, logged, changed, ((uint32_t)slot << 9) | (uint32_t)c, out);
     }
     // defined cells away from the active ones: undefined with their sign
     const PlaneEnum pc(clear);
     for (int base = 0; base < pc.total; base += 32) {
       const int k = base + lane;
       const int c = pc.cell(clear, k < pc.total ? k : pc.total - 1);
-      if (k < pc.total) {
-        const size_t q = (size_t)slot * BV + c;
-        v.next[q] = sentinel<T>(v.vals[q] < 0);
-      }
+      T out = T(0);
+      if (k < pc.total) out = sentinel<T>(v.vals[(size_t)slot * BV + c] < 0);
+      logChange<T>(lg, logBase, logged, k < pc.total, ((uint32_t)slot << 9) | (uint32_t)c, out);
     }
     __syncwarp();
-    if (lane < 8) wm.chg[lane] |= clear, wm.flip[lane] |= clear;
-    finishBrick(wm, v.chg, v.defNext, slot, lane, own);
+    if (lane < 8) wm.flip[lane] |= clear;
+    finishBrick(wm, v.defNext, slot, lane, own);
   }
+  if (lane == 0) lg.count[warp] = logged;
 }
 
 // Pointwise boolean of two level sets, in place on A (booleanOpInternal,
