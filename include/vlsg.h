@@ -225,6 +225,31 @@ int vlsg_get_values(vlsg_context *ctx, int32_t slot, int64_t n,
 int vlsg_get_values_noalloc(vlsg_context *ctx, int32_t slot, int64_t n,
                             const int32_t *indices, double *values);
 
+/* Comparison of two level sets held by contexts on the same device (they may
+ * differ in precision), for the precision report of the FP32 path against
+ * the FP64 path.  No counterpart in Advect itself; the volume and Chamfer
+ * figures restate the rules of lsCompareVolume.hpp:272-287 (a cell is inside
+ * when the average of its 8 corner values is <= 0; counted over the map box)
+ * and lsCompareChamfer.hpp:148-242 (nodes on grid edges between defined
+ * points of opposite sign, interpolated as lsToSurfaceMesh.hpp:339-361, here
+ * without merging close nodes; mean / RMS / max nearest-node distances).
+ * Distances are in grid units (multiply by gridDelta). */
+typedef struct vlsg_compare_result {
+  int64_t points_a, points_b;           /* defined points */
+  int64_t common_points;                /* defined in both */
+  int64_t defined_only_a, defined_only_b;
+  int64_t active_a, active_b;           /* defined with |phi| <= 0.5 */
+  int64_t active_only_a, active_only_b; /* active in one, not active in the other */
+  double max_abs_diff, rms_abs_diff;    /* |phi_a - phi_b| on the common points */
+  int64_t inside_cells_a, inside_cells_b;
+  int64_t nodes_a, nodes_b;
+  double chamfer_ab, chamfer_ba;        /* mean nearest-node distance a->b, b->a */
+  double chamfer_mean, chamfer_rms, chamfer_max;
+  int64_t chamfer_unresolved;           /* nodes with no node within 4 cells */
+} vlsg_compare_result;
+int vlsg_compare(vlsg_context *a, int32_t slot_a, vlsg_context *b, int32_t slot_b,
+                 vlsg_compare_result *out);
+
 /* Velocity plugin: either a device functor or a host callback. */
 int vlsg_set_velocity_functor(vlsg_context *ctx, const vlsg_velocity_desc *v);
 int vlsg_set_velocity_callback(vlsg_context *ctx, vlsg_velocity_cb cb,

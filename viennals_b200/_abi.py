@@ -130,6 +130,27 @@ class KernelStat(ctypes.Structure):
     ]
 
 
+class CompareResult(ctypes.Structure):
+    """vlsg_compare_result (vlsg.h)."""
+    _fields_ = [
+        ("points_a", ctypes.c_int64), ("points_b", ctypes.c_int64),
+        ("common_points", ctypes.c_int64),
+        ("defined_only_a", ctypes.c_int64), ("defined_only_b", ctypes.c_int64),
+        ("active_a", ctypes.c_int64), ("active_b", ctypes.c_int64),
+        ("active_only_a", ctypes.c_int64), ("active_only_b", ctypes.c_int64),
+        ("max_abs_diff", ctypes.c_double), ("rms_abs_diff", ctypes.c_double),
+        ("inside_cells_a", ctypes.c_int64), ("inside_cells_b", ctypes.c_int64),
+        ("nodes_a", ctypes.c_int64), ("nodes_b", ctypes.c_int64),
+        ("chamfer_ab", ctypes.c_double), ("chamfer_ba", ctypes.c_double),
+        ("chamfer_mean", ctypes.c_double), ("chamfer_rms", ctypes.c_double),
+        ("chamfer_max", ctypes.c_double),
+        ("chamfer_unresolved", ctypes.c_int64),
+    ]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 VELOCITY_CALLBACK = ctypes.CFUNCTYPE(
     ctypes.c_int,
     ctypes.c_void_p,

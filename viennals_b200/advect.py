@@ -103,6 +103,14 @@ class Context:
                                              _p(out, ctypes.c_double)))
         return out
 
+    def compare(self, slot, other, other_slot=0):
+        """vlsg_compare of this context's level set (a) against another
+        context's (b) on the same device; a dict of vlsg_compare_result."""
+        from ._abi import CompareResult
+        r = CompareResult()
+        self._check(self.lib.vlsg_compare(self.h, int(slot), other.h, int(other_slot), ctypes.byref(r)))
+        return r.as_dict()
+
     def set_velocity(self, desc):
         self._check(self.lib.vlsg_set_velocity_functor(self.h, ctypes.byref(desc)))
 

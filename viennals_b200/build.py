@@ -14,7 +14,8 @@ LIB = os.path.join(HERE, "libvlsgpu.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 SOURCES = ["vlsg_api.cu"]
 HEADERS = ["vlsg_common.cuh", "vlsg_passes.cuh", "vlsg_frontier.cuh", "vlsg_rates.cuh",
-           "vlsg_maint.cuh", "vlsg_scan.cuh", "vlsg_exchange.cuh", "vlsg_engine.cuh"]
+           "vlsg_maint.cuh", "vlsg_scan.cuh", "vlsg_exchange.cuh", "vlsg_metrics.cuh",
+           "vlsg_engine.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

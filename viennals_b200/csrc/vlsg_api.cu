@@ -7,6 +7,7 @@
 #include <string>
 
 #include "vlsg_engine.cuh"
+#include "vlsg_metrics.cuh"
 
 using namespace vlsg;
 
@@ -102,6 +103,102 @@ void queryStaged(Engine<T> &e, int slot, int64_t n, const int32_t *idx, double *
   e.checkLaunch();
   VLSG_CUDA(cudaMemcpyAsync(values, dv, n * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
   VLSG_CUDA(cudaStreamSynchronize(e.stream));
+}
+
+// Device buffer freed at scope exit (comparison temporaries).
+struct TempBuf {
+  void *p = nullptr;
+  explicit TempBuf(size_t bytes) { VLSG_CUDA(cudaMalloc(&p, bytes ? bytes : 16)); }
+  ~TempBuf() { if (p) cudaFree(p); }
+  template <class V> V *as() const { return (V *)p; }
+};
+
+// Zero-crossing nodes of one engine's exchange points (sorted by cell key).
+template <class T>
+int64_t surfaceNodes(Engine<T> &e, int slot, std::unique_ptr<TempBuf> &nodesOut,
+                     std::unique_ptr<TempBuf> &keysOut) {
+  const int64_t n = e.xPoints;
+  TempBuf cnt(n * sizeof(uint32_t)), off(n * sizeof(uint32_t)),
+      sums((scanScratch(n) + 64) * sizeof(uint32_t));
+  const int32_t *idx = (const int32_t *)e.xs[Engine<T>::X_IDX].p;
+  const double *val = (const double *)e.xs[Engine<T>::X_VAL].p;
+  kSurfaceNodes<T><<<Engine<T>::grid1(n), 256, 0, e.stream>>>(e.g, e.mapView(), e.view(slot), idx,
+                                                               val, n, cnt.as<uint32_t>(), nullptr,
+                                                               nullptr, nullptr);
+  e.scanExclusive(cnt.as<uint32_t>(), off.as<uint32_t>(), n, sums.as<uint32_t>());
+  const int64_t m = e.scanTotal(sums.as<uint32_t>(), n);
+  nodesOut.reset(new TempBuf(3 * m * sizeof(double)));
+  keysOut.reset(new TempBuf(m * sizeof(uint64_t)));
+  kSurfaceNodes<T><<<Engine<T>::grid1(n), 256, 0, e.stream>>>(
+      e.g, e.mapView(), e.view(slot), idx, val, n, cnt.as<uint32_t>(), off.as<uint32_t>(),
+      nodesOut->as<double>(), keysOut->as<uint64_t>());
+  e.checkLaunch();
+  VLSG_CUDA(cudaStreamSynchronize(e.stream));
+  return m;
+}
+
+template <class TA, class TB>
+void compareEngines(Engine<TA> &ea, int sa, Engine<TB> &eb, int sb, vlsg_compare_result *r) {
+  ea.buildExchange(sa);
+  eb.buildExchange(sb);
+  cudaStream_t s = ea.stream;
+  const int64_t na = ea.xPoints, nb = eb.xPoints;
+  const int32_t *ia = (const int32_t *)ea.xs[Engine<TA>::X_IDX].p;
+  const double *va = (const double *)ea.xs[Engine<TA>::X_VAL].p;
+  const int32_t *ib = (const int32_t *)eb.xs[Engine<TB>::X_IDX].p;
+  const double *vb = (const double *)eb.xs[Engine<TB>::X_VAL].p;
+  TempBuf ka(na * sizeof(uint64_t)), kb(nb * sizeof(uint64_t));
+  TempBuf acc(2 * sizeof(CompareAcc) + 2 * sizeof(ChamferAcc) + 2 * sizeof(unsigned long long));
+  VLSG_CUDA(cudaMemsetAsync(acc.p, 0, 2 * sizeof(CompareAcc) + 2 * sizeof(ChamferAcc) +
+                                          2 * sizeof(unsigned long long), s));
+  CompareAcc *accA = acc.as<CompareAcc>(), *accB = accA + 1;
+  ChamferAcc *chA = (ChamferAcc *)(accB + 1), *chB = chA + 1;
+  unsigned long long *inside = (unsigned long long *)(chB + 1);
+  kPointKeys<<<Engine<TA>::grid1(na), 256, 0, s>>>(ia, na, ka.as<uint64_t>());
+  kPointKeys<<<Engine<TA>::grid1(nb), 256, 0, s>>>(ib, nb, kb.as<uint64_t>());
+  kComparePoints<<<Engine<TA>::grid1(na), 256, 0, s>>>(ka.as<uint64_t>(), va, na, kb.as<uint64_t>(),
+                                                       vb, nb, 1, accA);
+  kComparePoints<<<Engine<TA>::grid1(nb), 256, 0, s>>>(kb.as<uint64_t>(), vb, nb, ka.as<uint64_t>(),
+                                                       va, na, 0, accB);
+  kInsideCells<TA><<<ea.blocksPass, 256, 0, s>>>(ea.g, ea.mapView(), ea.view(sa), ea.nBricks, inside);
+  kInsideCells<TB><<<eb.blocksPass, 256, 0, s>>>(eb.g, eb.mapView(), eb.view(sb), eb.nBricks, inside + 1);
+  VLSG_CUDA(cudaGetLastError());
+  VLSG_CUDA(cudaStreamSynchronize(s));
+  std::unique_ptr<TempBuf> nodesA, keysA, nodesB, keysB;
+  const int64_t ma = surfaceNodes(ea, sa, nodesA, keysA);
+  const int64_t mb = surfaceNodes(eb, sb, nodesB, keysB);
+  kNearestNodes<<<Engine<TA>::grid1(ma), 256, 0, s>>>(nodesA->as<double>(), ma, nodesB->as<double>(),
+                                                      keysB->as<uint64_t>(), mb, chA);
+  kNearestNodes<<<Engine<TA>::grid1(mb), 256, 0, s>>>(nodesB->as<double>(), mb, nodesA->as<double>(),
+                                                      keysA->as<uint64_t>(), ma, chB);
+  VLSG_CUDA(cudaGetLastError());
+  CompareAcc h[2];
+  ChamferAcc c[2];
+  unsigned long long in[2];
+  VLSG_CUDA(cudaMemcpyAsync(h, accA, sizeof(h), cudaMemcpyDeviceToHost, s));
+  VLSG_CUDA(cudaMemcpyAsync(c, chA, sizeof(c), cudaMemcpyDeviceToHost, s));
+  VLSG_CUDA(cudaMemcpyAsync(in, inside, sizeof(in), cudaMemcpyDeviceToHost, s));
+  VLSG_CUDA(cudaStreamSynchronize(s));
+  std::memset(r, 0, sizeof(*r));
+  r->points_a = na, r->points_b = nb;
+  r->common_points = (int64_t)h[0].common;
+  r->defined_only_a = (int64_t)h[0].onlyDefined, r->defined_only_b = (int64_t)h[1].onlyDefined;
+  r->active_a = (int64_t)h[0].active, r->active_b = (int64_t)h[1].active;
+  r->active_only_a = (int64_t)h[0].onlyActive, r->active_only_b = (int64_t)h[1].onlyActive;
+  std::memcpy(&r->max_abs_diff, &h[0].maxDiff, sizeof(double));
+  r->rms_abs_diff = h[0].common ? std::sqrt(h[0].sumSq / (double)h[0].common) : 0.0;
+  r->inside_cells_a = (int64_t)in[0], r->inside_cells_b = (int64_t)in[1];
+  r->nodes_a = ma, r->nodes_b = mb;
+  const int64_t ra = ma - (int64_t)c[0].unresolved, rb = mb - (int64_t)c[1].unresolved;
+  r->chamfer_ab = ra ? c[0].sum / ra : 0.0;
+  r->chamfer_ba = rb ? c[1].sum / rb : 0.0;
+  r->chamfer_mean = (ra + rb) ? (c[0].sum + c[1].sum) / double(ra + rb) : 0.0;
+  r->chamfer_rms = (ra + rb) ? std::sqrt((c[0].sumSq + c[1].sumSq) / double(ra + rb)) : 0.0;
+  double mx0, mx1;
+  std::memcpy(&mx0, &c[0].maxBits, sizeof(double));
+  std::memcpy(&mx1, &c[1].maxBits, sizeof(double));
+  r->chamfer_max = std::max(mx0, mx1);
+  r->chamfer_unresolved = (int64_t)(c[0].unresolved + c[1].unresolved);
 }
 
 void ensureBuilt(vlsg_context *ctx) {
@@ -358,6 +455,26 @@ int vlsg_get_values_noalloc(vlsg_context *ctx, int32_t slot, int64_t n, const in
     double *dv = (double *)(scratch + kNoAllocIdxBytes);
     if (ctx->precision == VLSG_FP64) queryStaged(*ctx->e64, slot, n, idx, values, di, dv);
     else queryStaged(*ctx->e32, slot, n, idx, values, di, dv);
+    return VLSG_OK;
+  });
+}
+
+int vlsg_compare(vlsg_context *a, int32_t slotA, vlsg_context *b, int32_t slotB,
+                 vlsg_compare_result *out) {
+  if (!a || !b || !out) return fail(a, VLSG_ERR_ARGUMENT, "bad argument");
+  if (a->device != b->device) return fail(a, VLSG_ERR_ARGUMENT, "contexts on different devices");
+  return guarded(a, [&] {
+    ensureBuilt(a);
+    ensureBuilt(b);
+    if (slotA < 0 || slotA >= (int)a->staged.size() || slotB < 0 || slotB >= (int)b->staged.size())
+      return fail(a, VLSG_ERR_ARGUMENT, "level set slot out of range");
+    if (a->precision == VLSG_FP64) {
+      if (b->precision == VLSG_FP64) compareEngines(*a->e64, slotA, *b->e64, slotB, out);
+      else compareEngines(*a->e64, slotA, *b->e32, slotB, out);
+    } else {
+      if (b->precision == VLSG_FP64) compareEngines(*a->e32, slotA, *b->e64, slotB, out);
+      else compareEngines(*a->e32, slotA, *b->e32, slotB, out);
+    }
     return VLSG_OK;
   });
 }

@@ -1,0 +1,241 @@
+// vlsg_metrics.cuh -- comparison of two level sets on the device, for the
+// precision report of the FP32 path against the FP64 path:
+//   * point sets: defined and active (|phi| <= 0.5) points present in one
+//     level set only, max / RMS |phi_a - phi_b| over the common points;
+//   * volume: cells whose 8-corner average is <= 0 (the inside rule of
+//     lsCompareVolume.hpp:272-287), over the map box;
+//   * Chamfer distance between the zero-crossing node sets: a node on every
+//     grid edge between two defined points of opposite sign, placed as
+//     lsToSurfaceMesh.hpp:339-361 interpolates it (no merging of nodes closer
+//     than the reference's minimum node distance), nearest neighbours found
+//     exactly by searching grid cells in growing Chebyshev shells
+//     (lsCompareChamfer.hpp:148-242 reports the same means / RMS / max).
+// Both level sets are read through their exchange arrays (points in HRLE
+// order, values as double), so they may have different storage types.
+#pragma once
+
+#include "vlsg_common.cuh"
+#include "vlsg_exchange.cuh"
+
+namespace vlsg {
+
+__device__ inline uint64_t keyOf(const int32_t *idx, int64_t i) {
+  return cellKey(idx[3 * i], idx[3 * i + 1], idx[3 * i + 2]);
+}
+
+// Keys of an exchange point list (HRLE order == ascending key order).
+__global__ void kPointKeys(const int32_t *idx, int64_t n, uint64_t *keys) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    keys[i] = keyOf(idx, i);
+}
+
+__device__ inline int64_t findKey(const uint64_t *keys, int64_t n, uint64_t k) {
+  int64_t lo = 0, hi = n;
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (keys[mid] < k) lo = mid + 1;
+    else hi = mid;
+  }
+  return (lo < n && keys[lo] == k) ? lo : -1;
+}
+
+// Accumulators of a comparison (device).
+struct CompareAcc {
+  unsigned long long onlyDefined; // defined here, not in the other
+  unsigned long long onlyActive;  // active here, not active in the other
+  unsigned long long active;      // active points here
+  unsigned long long common;      // points defined in both (counted from A)
+  unsigned long long maxDiff;     // bits of max |a - b|
+  double sumSq;                   // sum of (a - b)^2
+};
+
+// Points of `a` against the sorted keys of `b`.
+__global__ void kComparePoints(const uint64_t *ka, const double *va, int64_t na,
+                               const uint64_t *kb, const double *vb, int64_t nb, int countCommon,
+                               CompareAcc *acc) {
+  unsigned long long onlyDef = 0, onlyAct = 0, act = 0, common = 0, maxBits = 0;
+  double sq = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < na;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double x = va[i];
+    const bool ax = fabs(x) <= 0.5;
+    act += ax;
+    const int64_t j = findKey(kb, nb, ka[i]);
+    if (j < 0) {
+      ++onlyDef;
+      onlyAct += ax;
+      continue;
+    }
+    const double y = vb[j];
+    onlyAct += ax && !(fabs(y) <= 0.5);
+    if (countCommon) {
+      ++common;
+      const double d = fabs(x - y);
+      const unsigned long long b = orderedBits(d);
+      maxBits = b > maxBits ? b : maxBits;
+      sq += d * d;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    onlyDef += __shfl_xor_sync(0xffffffffu, onlyDef, o);
+    onlyAct += __shfl_xor_sync(0xffffffffu, onlyAct, o);
+    act += __shfl_xor_sync(0xffffffffu, act, o);
+    common += __shfl_xor_sync(0xffffffffu, common, o);
+    const unsigned long long t = __shfl_xor_sync(0xffffffffu, maxBits, o);
+    maxBits = t > maxBits ? t : maxBits;
+    sq += __shfl_xor_sync(0xffffffffu, sq, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (onlyDef) atomicAdd(&acc->onlyDefined, onlyDef);
+    if (onlyAct) atomicAdd(&acc->onlyActive, onlyAct);
+    if (act) atomicAdd(&acc->active, act);
+    if (common) atomicAdd(&acc->common, common);
+    if (maxBits) atomicMax(&acc->maxDiff, maxBits);
+    if (sq != 0.0) atomicAdd(&acc->sumSq, sq);
+  }
+}
+
+// Cells of the map box whose corner average is <= 0 (one warp per brick; a
+// brick whose own and +x/+y/+z neighbour bricks are all unallocated with one
+// sign is decided at once).
+template <class T>
+__global__ void kInsideCells(GridDev g, MapView m, Buf<T> b, int nBricks,
+                             unsigned long long *count) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nWarps = (gridDim.x * blockDim.x) >> 5;
+  unsigned long long inside = 0;
+  for (int bi = warp; bi < nBricks; bi += nWarps) {
+    int bx, by, bz;
+    brickCoords(g, bi, bx, by, bz);
+    // uniform test over the brick and the 7 bricks its +1 corners reach
+    int sgn = 0;
+    bool uniform = true;
+    for (int k = 0; k < 8 && uniform; ++k) {
+      int x = bx + (k & 1), y = by + ((k >> 1) & 1), z = bz + (k >> 2);
+      x = x < g.nb[0] ? x : g.nb[0] - 1;
+      y = y < g.nb[1] ? y : g.nb[1] - 1;
+      z = z < g.nb[2] ? z : g.nb[2] - 1;
+      const int nb = brickIndex(g, x, y, z);
+      if (m.brickMap[nb] >= 0) uniform = false;
+      else {
+        const int s = b.farSign[nb] < 0 ? -1 : 1;
+        if (sgn == 0) sgn = s;
+        else if (s != sgn) uniform = false;
+      }
+    }
+    if (uniform && g.bc[0] != VLSG_REFLECTIVE_BOUNDARY && g.bc[1] != VLSG_REFLECTIVE_BOUNDARY &&
+        g.bc[2] != VLSG_REFLECTIVE_BOUNDARY && g.bc[0] != VLSG_PERIODIC_BOUNDARY &&
+        g.bc[1] != VLSG_PERIODIC_BOUNDARY && g.bc[2] != VLSG_PERIODIC_BOUNDARY) {
+      if (lane == 0 && sgn < 0) inside += BV;
+      continue;
+    }
+    const int x0 = g.org[0] + bx * BS, y0 = g.org[1] + by * BS, z0 = g.org[2] + bz * BS;
+    for (int c = lane; c < BV; c += 32) {
+      const int x = x0 + (c & 7), y = y0 + ((c >> 3) & 7), z = z0 + (c >> 6);
+      if (!cellExists(g, x, y, z)) continue;
+      double sum = 0;
+      for (int k = 0; k < 8; ++k)
+        sum += (double)cellValueRaw<T>(g, m, b, x + (k & 1), y + ((k >> 1) & 1), z + (k >> 2));
+      inside += (sum / 8.0 <= 0.0) ? 1 : 0;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) inside += __shfl_xor_sync(0xffffffffu, inside, o);
+  if (lane == 0 && inside) atomicAdd(count, inside);
+}
+
+// Zero-crossing nodes of the +x/+y/+z edges of every point: count pass
+// (nodes == nullptr) or write pass at the scanned offsets.
+template <class T>
+__global__ void kSurfaceNodes(GridDev g, MapView m, Buf<T> b, const int32_t *idx,
+                              const double *val, int64_t n, uint32_t *cnt, const uint32_t *off,
+                              double *nodes, uint64_t *nodeKeys) {
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    const int c[3] = {idx[3 * p], idx[3 * p + 1], idx[3 * p + 2]};
+    const double d0 = val[p];
+    uint32_t k = 0, o = nodes ? off[p] : 0;
+    for (int dir = 0; dir < 3; ++dir) {
+      const T v1 = cellValueRaw<T>(g, m, b, c[0] + (dir == 0), c[1] + (dir == 1), c[2] + (dir == 2));
+      if (!isDef(v1)) continue;
+      const double d1 = (double)v1;
+      if ((d0 >= 0.) == (d1 >= 0.)) continue;
+      if (nodes) {
+        double pos[3] = {(double)c[0], (double)c[1], (double)c[2]};
+        double cc;
+        if (d0 == -d1) cc = c[dir] + 0.5;
+        else if (fabs(d0) <= fabs(d1)) cc = c[dir] + (d0 / (d0 - d1));
+        else cc = (c[dir] + 1) - (d1 / (d1 - d0));
+        cc = fmax(cc, c[dir] + 1e-12);
+        cc = fmin(cc, (c[dir] + 1) - 1e-12);
+        pos[dir] = cc;
+        for (int z = 0; z < 3; ++z) nodes[3 * (size_t)(o + k) + z] = pos[z];
+        nodeKeys[o + k] = cellKey(c[0], c[1], c[2]);
+      }
+      ++k;
+    }
+    if (!nodes) cnt[p] = k;
+  }
+}
+
+struct ChamferAcc {
+  double sum, sumSq;
+  unsigned long long maxBits;
+  unsigned long long unresolved; // nearest node farther than the searched shells
+};
+
+// Distance (grid units) of every query node to the nearest node of `pts`
+// (sorted by cell key); shells of Chebyshev radius 1..4 cells.
+__global__ void kNearestNodes(const double *q, int64_t nq, const double *pts,
+                              const uint64_t *pkeys, int64_t np, ChamferAcc *acc) {
+  double sum = 0, sq = 0;
+  unsigned long long maxBits = 0, unresolved = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nq;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double x = q[3 * i], y = q[3 * i + 1], z = q[3 * i + 2];
+    const int cx = (int)floor(x), cy = (int)floor(y), cz = (int)floor(z);
+    double best = 1e300;
+    for (int r = 1; r <= 4; ++r) {
+      for (int dz = -r; dz <= r; ++dz)
+        for (int dy = -r; dy <= r; ++dy)
+          for (int dx = -r; dx <= r; ++dx) {
+            const int m = max(abs(dx), max(abs(dy), abs(dz)));
+            if (m != r && !(r == 1 && m == 0)) continue; // shell r (r = 1 includes the centre)
+            int64_t j = findKey(pkeys, np, cellKey(cx + dx, cy + dy, cz + dz));
+            if (j < 0) continue;
+            const uint64_t k = pkeys[j];
+            for (; j < np && pkeys[j] == k; ++j) {
+              const double ex = pts[3 * j] - x, ey = pts[3 * j + 1] - y, ez = pts[3 * j + 2] - z;
+              const double d = sqrt(ex * ex + ey * ey + ez * ez);
+              best = d < best ? d : best;
+            }
+          }
+      // every node outside shell r is at least r cells away
+      if (best <= (double)r) break;
+    }
+    if (best > 4.0) {
+      ++unresolved;
+      continue;
+    }
+    sum += best;
+    sq += best * best;
+    const unsigned long long b = orderedBits(best);
+    maxBits = b > maxBits ? b : maxBits;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    sq += __shfl_xor_sync(0xffffffffu, sq, o);
+    const unsigned long long t = __shfl_xor_sync(0xffffffffu, maxBits, o);
+    maxBits = t > maxBits ? t : maxBits;
+    unresolved += __shfl_xor_sync(0xffffffffu, unresolved, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (sum != 0.0) atomicAdd(&acc->sum, sum);
+    if (sq != 0.0) atomicAdd(&acc->sumSq, sq);
+    if (maxBits) atomicMax(&acc->maxBits, maxBits);
+    if (unresolved) atomicAdd(&acc->unresolved, unresolved);
+  }
+}
+
+} // namespace vlsg
