@@ -221,7 +221,66 @@ def run_ours(args, rank, world):
         del t1, t2, t3, t4
         ctx2.close()
     ctx.close()
+    if rank == 0 and args.err_steps > 0:
+        out["precision_report"] = precision_report(args, grid, dom, vel, p, stream)
     return out
+
+
+def precision_report(args, grid, dom, vel, p, stream):
+    """The FP32 path against the FP64 path on the same input after
+    `err_steps` RK3 steps (the precision form runs 50): both timed with CUDA
+    events on the same stream, compared on the device (vlsg_compare).  The
+    FP64 path is the one the parity tests hold bit-identical to the FP64
+    oracle."""
+    import torch
+
+    from viennals_b200.advect import Context
+    from viennals_b200._abi import Precision
+
+    res = {}
+    ctxs = {}
+    for name, prec in (("fp64", Precision.FP64), ("fp32", Precision.FP32)):
+        c = Context(args.local_rank, prec)
+        c.set_stream(stream.cuda_stream)
+        c.set_grid(grid)
+        c.set_level_set_count(1)
+        c.upload(0, dom)
+        c.set_velocity(vel.descriptor())
+        c.count(0)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        upd = 0
+        e0.record(stream)
+        for _ in range(args.err_steps):
+            upd += c.advect(p).point_updates
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        res[name] = {"point_updates_per_s": upd / (ms / 1e3), "ms_per_step": ms / args.err_steps}
+        ctxs[name] = c
+    r = ctxs["fp32"].compare(0, ctxs["fp64"], 0)
+    for c in ctxs.values():
+        c.close()
+    gd = float(grid.delta)
+    vol64, vol32 = r["inside_cells_b"], r["inside_cells_a"]
+    return {
+        "steps": args.err_steps, "against": "FP64 GPU path (bit-identical to the FP64 oracle "
+        "in the parity tests)",
+        "fp32_point_updates_per_s": res["fp32"]["point_updates_per_s"],
+        "fp64_point_updates_per_s": res["fp64"]["point_updates_per_s"],
+        "fp32_ms_per_step": res["fp32"]["ms_per_step"], "fp64_ms_per_step": res["fp64"]["ms_per_step"],
+        "fp32_over_fp64": res["fp32"]["point_updates_per_s"] / res["fp64"]["point_updates_per_s"],
+        "max_abs_dphi_over_gridDelta": r["max_abs_diff"], "rms_abs_dphi_over_gridDelta": r["rms_abs_diff"],
+        "active_points_fp32": r["active_a"], "active_points_fp64": r["active_b"],
+        "active_set_differences": r["active_only_a"] + r["active_only_b"],
+        "defined_set_differences": r["defined_only_a"] + r["defined_only_b"],
+        "inside_cells_fp32": vol32, "inside_cells_fp64": vol64,
+        "rel_volume_error": (vol32 - vol64) / vol64 if vol64 else None,
+        "chamfer_rms": r["chamfer_rms"] * gd, "chamfer_max": r["chamfer_max"] * gd,
+        "chamfer_mean": r["chamfer_mean"] * gd, "chamfer_unit": "length (gridDelta x grid units)",
+        "surface_nodes_fp32": r["nodes_a"], "surface_nodes_fp64": r["nodes_b"],
+    }
 
 
 def cpu_baseline(args, sample_radius, steps=1):
@@ -290,6 +349,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-sample-radius", type=float, default=8.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--err-steps", type=int, default=50,
+                    help="RK3 steps of the FP32-vs-FP64 precision report (0: skip)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -335,6 +396,7 @@ def main():
             "data": "synthetic", "config": cfg, "gpu_launches": out["launches"],
             "clocks": out["clocks"], "e2e": out.get("e2e"),
             "roofline": roofline(out, peaks), "band_points": out["n_points"],
+            "precision_report": out.get("precision_report"),
             "kernels": out.get("kernels")}
     if not args.no_cpu_baseline:
         cb = cpu_baseline(args, args.cpu_sample_radius)
