@@ -1,9 +1,15 @@
 """Build libvlsgpu.so (sm_100a) in-tree with nvcc.
 
-FP64 parity with the reference's double-precision rules needs IEEE division
-and square root (nvcc defaults) and no multiply-add contraction, hence
--fmad=false on the device and -ffp-contract=off on the host.
+Three compilation units, compiled in parallel and linked into one library:
+  vlsg_api.cu       the C ABI and the device comparison of two level sets;
+  vlsg_engine64.cu  the FP64 engine -- parity with the reference's
+                    double-precision rules needs IEEE division and square
+                    root (nvcc defaults) and no multiply-add contraction,
+                    hence -fmad=false (and -ffp-contract=off on the host);
+  vlsg_engine32.cu  the FP32 engine, with multiply-add contraction (its
+                    results are held to a tolerance against the FP64 path).
 """
+import concurrent.futures
 import os
 import subprocess
 import sys
@@ -11,19 +17,23 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libvlsgpu.so")
+OBJ = os.path.join(HERE, "_build")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
-SOURCES = ["vlsg_api.cu"]
-HEADERS = ["vlsg_common.cuh", "vlsg_passes.cuh", "vlsg_frontier.cuh", "vlsg_rates.cuh",
-           "vlsg_maint.cuh", "vlsg_scan.cuh", "vlsg_exchange.cuh", "vlsg_metrics.cuh",
-           "vlsg_engine.cuh"]
+UNITS = {
+    "vlsg_api.cu": ["-fmad=false"],
+    "vlsg_engine64.cu": ["-fmad=false"],
+    "vlsg_engine32.cu": ["-fmad=true"],
+}
+SOURCES = list(UNITS)
+HEADERS = ["vlsg_common.cuh", "vlsg_iface.h", "vlsg_passes.cuh", "vlsg_frontier.cuh",
+           "vlsg_rates.cuh", "vlsg_maint.cuh", "vlsg_scan.cuh", "vlsg_exchange.cuh",
+           "vlsg_metrics.cuh", "vlsg_compare.cuh", "vlsg_engine.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",
-    "-fmad=false",
     "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
     "--expt-relaxed-constexpr",
-    "-shared",
 ]
 
 
@@ -40,13 +50,32 @@ def needs_build():
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+def _compile(src, extra, verbose):
+    obj = os.path.join(OBJ, src.replace(".cu", ".o"))
+    cmd = [nvcc()] + NVCC_FLAGS + UNITS[src] + list(extra) + ["-I", INCLUDE, "-c",
+                                                              os.path.join(CSRC, src), "-o", obj]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    return obj, r
+
+
 def build(force=False, verbose=False, extra=()):
     if not force and not needs_build():
         return LIB
-    cmd = [nvcc()] + NVCC_FLAGS + list(extra) + ["-I", INCLUDE] + \
-          [os.path.join(CSRC, s) for s in SOURCES] + ["-o", LIB + ".tmp"]
+    os.makedirs(OBJ, exist_ok=True)
+    with concurrent.futures.ThreadPoolExecutor(len(UNITS)) as ex:
+        results = list(ex.map(lambda s: _compile(s, extra, verbose), SOURCES))
+    for obj, r in results:
+        if verbose or r.returncode:
+            sys.stdout.write(r.stdout)
+            sys.stderr.write(r.stderr)
+        if r.returncode:
+            raise subprocess.CalledProcessError(r.returncode, r.args)
+    cmd = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a"] + \
+          [obj for obj, _ in results] + ["-o", LIB + ".tmp"]
     if verbose:
-        print(" ".join(cmd))
+        print(" ".join(cmd), flush=True)
     subprocess.check_call(cmd)
     os.replace(LIB + ".tmp", LIB)
     return LIB

@@ -1,13 +1,15 @@
 // vlsg_api.cu -- the C ABI of libvlsgpu.so (declared in include/vlsg.h).
 #include <algorithm>
 #include <climits>
+#include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <memory>
 #include <mutex>
 #include <string>
 
-#include "vlsg_engine.cuh"
-#include "vlsg_metrics.cuh"
+#include "vlsg_compare.cuh"
+#include "vlsg_iface.h"
 
 using namespace vlsg;
 
@@ -24,8 +26,7 @@ struct vlsg_context {
   bool hasVel = false;
   vlsg_velocity_desc vel{};
   bool profiling = false;
-  std::unique_ptr<Engine<double>> e64;
-  std::unique_ptr<Engine<float>> e32;
+  std::unique_ptr<EngineBase> eng; // Engine<double> or Engine<float>
 };
 
 namespace {
@@ -53,9 +54,11 @@ template <class F> int guarded(vlsg_context *ctx, F f) {
   }
 }
 
-template <class F> auto withEngine(vlsg_context *ctx, F f) {
-  if (ctx->precision == VLSG_FP64) return f(*ctx->e64);
-  return f(*ctx->e32);
+int grid1(size_t n) {
+  size_t b = (n + 255) / 256;
+  if (b < 1) b = 1;
+  if (b > 148 * 32) b = 148 * 32;
+  return (int)b;
 }
 
 // Staging of vlsg_get_values_noalloc: the query indices (3 x int32 each) of
@@ -93,18 +96,6 @@ int noallocScratch(vlsg_context *ctx, int device, unsigned char **out) {
   return VLSG_OK;
 }
 
-// Query kernel of vlsg_get_values on caller-provided staging (di, dv).
-template <class T>
-void queryStaged(Engine<T> &e, int slot, int64_t n, const int32_t *idx, double *values,
-                 int32_t *di, double *dv) {
-  VLSG_CUDA(cudaMemcpyAsync(di, idx, n * 3 * sizeof(int32_t), cudaMemcpyHostToDevice, e.stream));
-  kQueryValues<T><<<Engine<T>::grid1(n), 256, 0, e.stream>>>(e.g, e.mapView(), e.view(slot),
-                                                              (int)n, di, dv);
-  e.checkLaunch();
-  VLSG_CUDA(cudaMemcpyAsync(values, dv, n * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
-  VLSG_CUDA(cudaStreamSynchronize(e.stream));
-}
-
 // Device buffer freed at scope exit (comparison temporaries).
 struct TempBuf {
   void *p = nullptr;
@@ -113,71 +104,43 @@ struct TempBuf {
   template <class V> V *as() const { return (V *)p; }
 };
 
-// Zero-crossing nodes of one engine's exchange points (sorted by cell key).
-template <class T>
-int64_t surfaceNodes(Engine<T> &e, int slot, std::unique_ptr<TempBuf> &nodesOut,
-                     std::unique_ptr<TempBuf> &keysOut) {
-  const int64_t n = e.xPoints;
-  TempBuf cnt(n * sizeof(uint32_t)), off(n * sizeof(uint32_t)),
-      sums((scanScratch(n) + 64) * sizeof(uint32_t));
-  const int32_t *idx = (const int32_t *)e.xs[Engine<T>::X_IDX].p;
-  const double *val = (const double *)e.xs[Engine<T>::X_VAL].p;
-  kSurfaceNodes<T><<<Engine<T>::grid1(n), 256, 0, e.stream>>>(e.g, e.mapView(), e.view(slot), idx,
-                                                               val, n, cnt.as<uint32_t>(), nullptr,
-                                                               nullptr, nullptr);
-  e.scanExclusive(cnt.as<uint32_t>(), off.as<uint32_t>(), n, sums.as<uint32_t>());
-  const int64_t m = e.scanTotal(sums.as<uint32_t>(), n);
-  nodesOut.reset(new TempBuf(3 * m * sizeof(double)));
-  keysOut.reset(new TempBuf(m * sizeof(uint64_t)));
-  kSurfaceNodes<T><<<Engine<T>::grid1(n), 256, 0, e.stream>>>(
-      e.g, e.mapView(), e.view(slot), idx, val, n, cnt.as<uint32_t>(), off.as<uint32_t>(),
-      nodesOut->as<double>(), keysOut->as<uint64_t>());
-  e.checkLaunch();
-  VLSG_CUDA(cudaStreamSynchronize(e.stream));
-  return m;
-}
-
-template <class TA, class TB>
-void compareEngines(Engine<TA> &ea, int sa, Engine<TB> &eb, int sb, vlsg_compare_result *r) {
-  ea.buildExchange(sa);
-  eb.buildExchange(sb);
+void compareEngines(EngineBase &ea, int sa, EngineBase &eb, int sb, vlsg_compare_result *r) {
+  const int32_t *ia = nullptr, *ib = nullptr;
+  const double *va = nullptr, *vb = nullptr;
+  int64_t na = 0, nb = 0;
+  ea.exchange(sa, &ia, &va, &na);
+  eb.exchange(sb, &ib, &vb, &nb);
   cudaStream_t s = ea.stream;
-  const int64_t na = ea.xPoints, nb = eb.xPoints;
-  const int32_t *ia = (const int32_t *)ea.xs[Engine<TA>::X_IDX].p;
-  const double *va = (const double *)ea.xs[Engine<TA>::X_VAL].p;
-  const int32_t *ib = (const int32_t *)eb.xs[Engine<TB>::X_IDX].p;
-  const double *vb = (const double *)eb.xs[Engine<TB>::X_VAL].p;
   TempBuf ka(na * sizeof(uint64_t)), kb(nb * sizeof(uint64_t));
-  TempBuf acc(2 * sizeof(CompareAcc) + 2 * sizeof(ChamferAcc) + 2 * sizeof(unsigned long long));
-  VLSG_CUDA(cudaMemsetAsync(acc.p, 0, 2 * sizeof(CompareAcc) + 2 * sizeof(ChamferAcc) +
-                                          2 * sizeof(unsigned long long), s));
+  TempBuf acc(2 * sizeof(CompareAcc) + 2 * sizeof(ChamferAcc));
+  VLSG_CUDA(cudaMemsetAsync(acc.p, 0, 2 * sizeof(CompareAcc) + 2 * sizeof(ChamferAcc), s));
   CompareAcc *accA = acc.as<CompareAcc>(), *accB = accA + 1;
   ChamferAcc *chA = (ChamferAcc *)(accB + 1), *chB = chA + 1;
-  unsigned long long *inside = (unsigned long long *)(chB + 1);
-  kPointKeys<<<Engine<TA>::grid1(na), 256, 0, s>>>(ia, na, ka.as<uint64_t>());
-  kPointKeys<<<Engine<TA>::grid1(nb), 256, 0, s>>>(ib, nb, kb.as<uint64_t>());
-  kComparePoints<<<Engine<TA>::grid1(na), 256, 0, s>>>(ka.as<uint64_t>(), va, na, kb.as<uint64_t>(),
-                                                       vb, nb, 1, accA);
-  kComparePoints<<<Engine<TA>::grid1(nb), 256, 0, s>>>(kb.as<uint64_t>(), vb, nb, ka.as<uint64_t>(),
-                                                       va, na, 0, accB);
-  kInsideCells<TA><<<ea.blocksPass, 256, 0, s>>>(ea.g, ea.mapView(), ea.view(sa), ea.nBricks, inside);
-  kInsideCells<TB><<<eb.blocksPass, 256, 0, s>>>(eb.g, eb.mapView(), eb.view(sb), eb.nBricks, inside + 1);
+  kPointKeys<<<grid1(na), 256, 0, s>>>(ia, na, ka.as<uint64_t>());
+  kPointKeys<<<grid1(nb), 256, 0, s>>>(ib, nb, kb.as<uint64_t>());
+  kComparePoints<<<grid1(na), 256, 0, s>>>(ka.as<uint64_t>(), va, na, kb.as<uint64_t>(), vb, nb,
+                                           1, accA);
+  kComparePoints<<<grid1(nb), 256, 0, s>>>(kb.as<uint64_t>(), vb, nb, ka.as<uint64_t>(), va, na,
+                                           0, accB);
   VLSG_CUDA(cudaGetLastError());
   VLSG_CUDA(cudaStreamSynchronize(s));
-  std::unique_ptr<TempBuf> nodesA, keysA, nodesB, keysB;
-  const int64_t ma = surfaceNodes(ea, sa, nodesA, keysA);
-  const int64_t mb = surfaceNodes(eb, sb, nodesB, keysB);
-  kNearestNodes<<<Engine<TA>::grid1(ma), 256, 0, s>>>(nodesA->as<double>(), ma, nodesB->as<double>(),
-                                                      keysB->as<uint64_t>(), mb, chA);
-  kNearestNodes<<<Engine<TA>::grid1(mb), 256, 0, s>>>(nodesB->as<double>(), mb, nodesA->as<double>(),
-                                                      keysA->as<uint64_t>(), ma, chB);
+  const uint64_t inA = ea.insideCells(sa), inB = eb.insideCells(sb);
+  double *nodesA = nullptr, *nodesB = nullptr;
+  uint64_t *keysA = nullptr, *keysB = nullptr;
+  const int64_t ma = ea.surfaceNodes(sa, &nodesA, &keysA);
+  const int64_t mb = eb.surfaceNodes(sb, &nodesB, &keysB);
+  TempBuf hold(16);
+  struct Free {
+    void *p;
+    ~Free() { if (p) cudaFree(p); }
+  } f1{nodesA}, f2{nodesB}, f3{keysA}, f4{keysB};
+  kNearestNodes<<<grid1(ma), 256, 0, s>>>(nodesA, ma, nodesB, keysB, mb, chA);
+  kNearestNodes<<<grid1(mb), 256, 0, s>>>(nodesB, mb, nodesA, keysA, ma, chB);
   VLSG_CUDA(cudaGetLastError());
   CompareAcc h[2];
   ChamferAcc c[2];
-  unsigned long long in[2];
   VLSG_CUDA(cudaMemcpyAsync(h, accA, sizeof(h), cudaMemcpyDeviceToHost, s));
   VLSG_CUDA(cudaMemcpyAsync(c, chA, sizeof(c), cudaMemcpyDeviceToHost, s));
-  VLSG_CUDA(cudaMemcpyAsync(in, inside, sizeof(in), cudaMemcpyDeviceToHost, s));
   VLSG_CUDA(cudaStreamSynchronize(s));
   std::memset(r, 0, sizeof(*r));
   r->points_a = na, r->points_b = nb;
@@ -187,7 +150,7 @@ void compareEngines(Engine<TA> &ea, int sa, Engine<TB> &eb, int sb, vlsg_compare
   r->active_only_a = (int64_t)h[0].onlyActive, r->active_only_b = (int64_t)h[1].onlyActive;
   std::memcpy(&r->max_abs_diff, &h[0].maxDiff, sizeof(double));
   r->rms_abs_diff = h[0].common ? std::sqrt(h[0].sumSq / (double)h[0].common) : 0.0;
-  r->inside_cells_a = (int64_t)in[0], r->inside_cells_b = (int64_t)in[1];
+  r->inside_cells_a = (int64_t)inA, r->inside_cells_b = (int64_t)inB;
   r->nodes_a = ma, r->nodes_b = mb;
   const int64_t ra = ma - (int64_t)c[0].unresolved, rb = mb - (int64_t)c[1].unresolved;
   r->chamfer_ab = ra ? c[0].sum / ra : 0.0;
@@ -206,15 +169,10 @@ void ensureBuilt(vlsg_context *ctx) {
   if (ctx->staged.empty()) throw CudaError("no level set uploaded", VLSG_ERR_STATE);
   if (!ctx->dirty) return;
   const int margin = 4;
-  if (ctx->precision == VLSG_FP64) {
-    if (!ctx->e64) ctx->e64.reset(new Engine<double>());
-    ctx->e64->stream = ctx->stream;
-    ctx->e64->build(ctx->grid, ctx->staged, margin);
-  } else {
-    if (!ctx->e32) ctx->e32.reset(new Engine<float>());
-    ctx->e32->stream = ctx->stream;
-    ctx->e32->build(ctx->grid, ctx->staged, margin);
-  }
+  if (!ctx->eng)
+    ctx->eng.reset(ctx->precision == VLSG_FP64 ? makeEngineF64() : makeEngineF32());
+  ctx->eng->stream = ctx->stream;
+  ctx->eng->build(ctx->grid, ctx->staged, margin);
   ctx->dirty = false;
 }
 } // namespace
@@ -271,8 +229,7 @@ int vlsg_create(vlsg_context **out, int32_t device, int32_t precision) {
 int vlsg_destroy(vlsg_context *ctx) {
   if (!ctx) return VLSG_OK;
   cudaSetDevice(ctx->device);
-  ctx->e64.reset();
-  ctx->e32.reset();
+  ctx->eng.reset();
   if (ctx->ownStream) cudaStreamDestroy(ctx->ownStream);
   delete ctx;
   return VLSG_OK;
@@ -283,8 +240,7 @@ int vlsg_set_stream(vlsg_context *ctx, void *stream) {
   return guarded(ctx, [&] {
     VLSG_CUDA(cudaStreamSynchronize(ctx->stream));
     ctx->stream = stream ? (cudaStream_t)stream : ctx->ownStream;
-    if (ctx->e64) ctx->e64->stream = ctx->stream;
-    if (ctx->e32) ctx->e32->stream = ctx->stream;
+    if (ctx->eng) ctx->eng->stream = ctx->stream;
     return VLSG_OK;
   });
 }
@@ -374,7 +330,7 @@ int vlsg_count_points(vlsg_context *ctx, int32_t slot, int64_t *n) {
     ensureBuilt(ctx);
     if (slot < 0 || slot >= (int)ctx->staged.size())
       return fail(ctx, VLSG_ERR_ARGUMENT, "level set slot out of range");
-    *n = withEngine(ctx, [&](auto &e) { return e.countDefined(slot); });
+    *n = ctx->eng->countDefined(slot);
     return VLSG_OK;
   });
 }
@@ -386,10 +342,8 @@ int vlsg_download_levelset(vlsg_context *ctx, int32_t slot, int64_t capacity, in
     ensureBuilt(ctx);
     if (slot < 0 || slot >= (int)ctx->staged.size())
       return fail(ctx, VLSG_ERR_ARGUMENT, "level set slot out of range");
-    const int64_t n = withEngine(ctx, [&](auto &e) {
-      if (width) *width = e.buf[slot].width;
-      return e.compact(slot, idx, values, capacity);
-    });
+    if (width) *width = ctx->eng->width(slot);
+    const int64_t n = ctx->eng->compact(slot, idx, values, capacity);
     if (n > capacity) return fail(ctx, VLSG_ERR_CAPACITY, "download capacity too small");
     return VLSG_OK;
   });
@@ -403,10 +357,8 @@ int vlsg_download_runs(vlsg_context *ctx, int32_t slot, int64_t capacity, int32_
     ensureBuilt(ctx);
     if (slot < 0 || slot >= (int)ctx->staged.size())
       return fail(ctx, VLSG_ERR_ARGUMENT, "level set slot out of range");
-    const int64_t n = withEngine(ctx, [&](auto &e) {
-      return e.runs(slot, capacity > 0 ? runStart : nullptr, capacity > 0 ? runSign : nullptr,
-                    capacity);
-    });
+    const int64_t n = ctx->eng->runs(slot, capacity > 0 ? runStart : nullptr,
+                                     capacity > 0 ? runSign : nullptr, capacity);
     *nRuns = n;
     if (n > capacity) return fail(ctx, VLSG_ERR_CAPACITY, "run capacity too small");
     return VLSG_OK;
@@ -422,10 +374,7 @@ int vlsg_get_values(vlsg_context *ctx, int32_t slot, int64_t n, const int32_t *i
     if (slot < 0 || slot >= (int)ctx->staged.size())
       return fail(ctx, VLSG_ERR_ARGUMENT, "level set slot out of range");
     if (n > INT_MAX / 4) return fail(ctx, VLSG_ERR_ARGUMENT, "too many queries");
-    withEngine(ctx, [&](auto &e) {
-      e.queryValues(slot, n, idx, values);
-      return 0;
-    });
+    ctx->eng->queryValues(slot, n, idx, values);
     return VLSG_OK;
   });
 }
@@ -453,8 +402,7 @@ int vlsg_get_values_noalloc(vlsg_context *ctx, int32_t slot, int64_t n, const in
     if (n == 0) return VLSG_OK;
     int32_t *di = (int32_t *)scratch;
     double *dv = (double *)(scratch + kNoAllocIdxBytes);
-    if (ctx->precision == VLSG_FP64) queryStaged(*ctx->e64, slot, n, idx, values, di, dv);
-    else queryStaged(*ctx->e32, slot, n, idx, values, di, dv);
+    ctx->eng->queryStaged(slot, n, idx, values, di, dv);
     return VLSG_OK;
   });
 }
@@ -468,13 +416,7 @@ int vlsg_compare(vlsg_context *a, int32_t slotA, vlsg_context *b, int32_t slotB,
     ensureBuilt(b);
     if (slotA < 0 || slotA >= (int)a->staged.size() || slotB < 0 || slotB >= (int)b->staged.size())
       return fail(a, VLSG_ERR_ARGUMENT, "level set slot out of range");
-    if (a->precision == VLSG_FP64) {
-      if (b->precision == VLSG_FP64) compareEngines(*a->e64, slotA, *b->e64, slotB, out);
-      else compareEngines(*a->e64, slotA, *b->e32, slotB, out);
-    } else {
-      if (b->precision == VLSG_FP64) compareEngines(*a->e32, slotA, *b->e64, slotB, out);
-      else compareEngines(*a->e32, slotA, *b->e32, slotB, out);
-    }
+    compareEngines(*a->eng, slotA, *b->eng, slotB, out);
     return VLSG_OK;
   });
 }
@@ -508,13 +450,11 @@ int vlsg_advect(vlsg_context *ctx, const vlsg_advect_params *p, vlsg_advect_resu
     return fail(ctx, VLSG_ERR_ARGUMENT, "unknown temporal scheme");
   return guarded(ctx, [&] {
     ensureBuilt(ctx);
-    withEngine(ctx, [&](auto &e) {
-      e.vel = ctx->vel;
-      e.profiling = ctx->profiling;
-      if (ctx->profiling) e.timers.clear();
-      e.apply(*p, *r);
-      return 0;
-    });
+    EngineBase &e = *ctx->eng;
+    e.vel = ctx->vel;
+    e.profiling = ctx->profiling;
+    if (ctx->profiling) e.timers.clear();
+    e.apply(*p, *r);
     return VLSG_OK;
   });
 }
@@ -528,7 +468,7 @@ int vlsg_set_profiling(vlsg_context *ctx, int32_t on) {
 int vlsg_get_kernel_stats(vlsg_context *ctx, int32_t capacity, vlsg_kernel_stat *out,
                           int32_t *count) {
   if (!ctx || !count) return fail(ctx, VLSG_ERR_ARGUMENT, "bad argument");
-  auto fill = [&](auto &e) {
+  auto fill = [&](EngineBase &e) {
     *count = (int32_t)e.timers.size();
     for (int i = 0; i < (int)e.timers.size() && i < capacity && out; ++i) {
       std::memset(&out[i], 0, sizeof(out[i]));
@@ -539,8 +479,7 @@ int vlsg_get_kernel_stats(vlsg_context *ctx, int32_t capacity, vlsg_kernel_stat 
     }
     return 0;
   };
-  if (ctx->precision == VLSG_FP64 && ctx->e64) fill(*ctx->e64);
-  else if (ctx->precision == VLSG_FP32 && ctx->e32) fill(*ctx->e32);
+  if (ctx->eng) fill(*ctx->eng);
   else *count = 0;
   return VLSG_OK;
 }

@@ -19,70 +19,15 @@
 
 #include "vlsg_common.cuh"
 #include "vlsg_exchange.cuh"
+#include "vlsg_iface.h"
+#include "vlsg_metrics.cuh"
 #include "vlsg_frontier.cuh"
 #include "vlsg_maint.cuh"
 #include "vlsg_passes.cuh"
 #include "vlsg_rates.cuh"
 
 namespace vlsg {
-
-struct CudaError : std::runtime_error {
-  int code;
-  CudaError(const std::string &m, int c) : std::runtime_error(m), code(c) {}
-};
-
-#define VLSG_CUDA(x)                                                           \
-  do {                                                                         \
-    cudaError_t e_ = (x);                                                      \
-    if (e_ != cudaSuccess)                                                     \
-      throw vlsg::CudaError(std::string(#x) + ": " + cudaGetErrorString(e_),   \
-                            VLSG_ERR_CUDA);                                    \
-  } while (0)
-
-// Device array that only grows (contents are not kept when it does).
-template <class V> void growDevice(V *&p, size_t &capacity, size_t n) {
-  if (p && n <= capacity) return;
-  if (p) VLSG_CUDA(cudaFree(p));
-  p = nullptr;
-  capacity = 0;
-  const size_t c = std::max<size_t>(n + n / 4, 16);
-  VLSG_CUDA(cudaMalloc(&p, c * sizeof(V)));
-  capacity = c;
-}
-
-// One uploaded level set, staged on the device until the context builds.
-struct StagedLS {
-  int32_t *idx = nullptr;      // 3 per point (as given)
-  double *vals = nullptr;
-  int32_t *runStart = nullptr; // 3 per run
-  int8_t *runSign = nullptr;
-  size_t capIdx = 0, capVals = 0, capRunStart = 0, capRunSign = 0;
-  int64_t n = 0, nRuns = 0;
-  int width = 1;
-  StagedLS() = default;
-  StagedLS(const StagedLS &) = delete;
-  StagedLS &operator=(const StagedLS &) = delete;
-  StagedLS(StagedLS &&o) noexcept { *this = std::move(o); }
-  StagedLS &operator=(StagedLS &&o) noexcept {
-    if (this == &o) return *this;
-    release();
-    idx = o.idx, vals = o.vals, runStart = o.runStart, runSign = o.runSign;
-    capIdx = o.capIdx, capVals = o.capVals, capRunStart = o.capRunStart, capRunSign = o.capRunSign;
-    n = o.n, nRuns = o.nRuns, width = o.width;
-    o.idx = nullptr, o.vals = nullptr, o.runStart = nullptr, o.runSign = nullptr;
-    o.capIdx = o.capVals = o.capRunStart = o.capRunSign = 0;
-    return *this;
-  }
-  ~StagedLS() { release(); }
-  void release() {
-    if (idx) cudaFree(idx);
-    if (vals) cudaFree(vals);
-    if (runStart) cudaFree(runStart);
-    if (runSign) cudaFree(runSign);
-    idx = nullptr, vals = nullptr, runStart = nullptr, runSign = nullptr;
-    capIdx = capVals = capRunStart = capRunSign = 0;
-  }
-};
+namespace { // internal linkage: every compilation unit has its own copy
 
 inline uint64_t hostCellKey(int x, int y, int z) {
   const uint64_t off = 1ull << 20;
@@ -90,35 +35,8 @@ inline uint64_t hostCellKey(int x, int y, int z) {
          (uint64_t)(x + (int)off);
 }
 
-struct KernelTimer {
-  std::string name;
-  uint64_t launches = 0;
-  double ms = 0;
-  double bytes = 0;
-};
-
-// Expand width of each scheme's prepareLS (lsEngquistOsher.hpp:31,
-// lsLaxFriedrichs.hpp:225, lsLocalLocalLaxFriedrichs.hpp:288,
-// lsLocalLaxFriedrichs.hpp:55, lsWENO.hpp:44).
-inline int schemeWidth(int s) {
-  switch (s) {
-  case VLSG_ENGQUIST_OSHER_1ST_ORDER: return 3;
-  case VLSG_ENGQUIST_OSHER_2ND_ORDER: return 5;
-  case VLSG_LAX_FRIEDRICHS_1ST_ORDER: return 3;
-  case VLSG_LAX_FRIEDRICHS_2ND_ORDER: return 5;
-  case VLSG_LOCAL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER: return 3;
-  case VLSG_LOCAL_LOCAL_LAX_FRIEDRICHS_2ND_ORDER: return 5;
-  case VLSG_LOCAL_LAX_FRIEDRICHS_1ST_ORDER: return 7;
-  case VLSG_LOCAL_LAX_FRIEDRICHS_2ND_ORDER: return 9;
-  case VLSG_WENO_3RD_ORDER: return 5;
-  case VLSG_WENO_5TH_ORDER: return 7;
-  default: return -1;
-  }
-}
-
-template <class T> class Engine {
+template <class T> class Engine : public EngineBase {
 public:
-  cudaStream_t stream = nullptr;
   GridDev g{};
   int L = 0;
   int nBricks = 0;
@@ -173,10 +91,11 @@ public:
   uint64_t pointUpdates = 0;
   uint32_t stages = 0;
   double currentTimeStep = -1.;
-  vlsg_velocity_desc vel{};
-  bool profiling = false;
-  std::vector<KernelTimer> timers;
-  int blocksPass = 148 * 8;
+  // grids of one wave: every block of a pass (and of the rate kernel) is
+  // resident at once, so no tail of late blocks
+  int numSMs = 148;
+  int blocksPass = 148 * VLSG_PASS_MIN_BLOCKS;
+  int blocksRate = 148 * rateMinBlocks<T>();
   // exchange format (points and runs in HRLE order), cached per buffer until
   // the level sets change
   struct Scratch {
@@ -396,6 +315,11 @@ public:
 
   void ensureSmall() {
     if (counters) return;
+    int dev = 0;
+    VLSG_CUDA(cudaGetDevice(&dev));
+    VLSG_CUDA(cudaDeviceGetAttribute(&numSMs, cudaDevAttrMultiProcessorCount, dev));
+    blocksPass = numSMs * VLSG_PASS_MIN_BLOCKS;
+    blocksRate = numSMs * rateMinBlocks<T>();
     VLSG_CUDA(cudaHostAlloc(&pinCounters, 32 * sizeof(int), cudaHostAllocDefault));
     VLSG_CUDA(cudaHostAlloc(&pinScal, 32 * sizeof(unsigned long long), cudaHostAllocDefault));
     VLSG_CUDA(cudaMalloc(&counters, 16 * sizeof(int)));
@@ -410,7 +334,7 @@ public:
   // points' bricks and their neighbours, values from the points and the
   // runs' signs.  Allocations are reused from the previous build when they
   // are large enough.
-  void build(const GridDev &grid, std::vector<StagedLS> &ls, int margin) {
+  void build(const GridDev &grid, std::vector<StagedLS> &ls, int margin) override {
     ++generation;
     ensureSmall();
     g = grid;
@@ -808,7 +732,7 @@ public:
       A.alphaMax = scal + 1;
       {
         Scope sc(this, "global_alphas");
-        kRates<T, 1><<<blocksPass, RATE_THREADS, 0, stream>>>(A, vel);
+        kRates<T, 1><<<blocksRate, RATE_THREADS, 0, stream>>>(A, vel);
         checkLaunch();
       }
       VLSG_CUDA(cudaMemcpyAsync(pinScal, scal, sizeof(init), cudaMemcpyDeviceToHost, stream));
@@ -832,7 +756,7 @@ public:
         lastBand = (int64_t)readU64(rateCounts + 1);
         return double(sizeof(T)) * double(lastBand + lastActive);
       });
-      kRates<T, 0><<<blocksPass, RATE_THREADS, 0, stream>>>(A, vel);
+      kRates<T, 0><<<blocksRate, RATE_THREADS, 0, stream>>>(A, vel);
       checkLaunch();
     }
     VLSG_CUDA(cudaMemcpyAsync(pinScal, scal, sizeof(init), cudaMemcpyDeviceToHost, stream));
@@ -954,7 +878,7 @@ public:
     }
   }
 
-  void apply(const vlsg_advect_params &P, vlsg_advect_result &r) {
+  void apply(const vlsg_advect_params &P, vlsg_advect_result &r) override {
     ++generation;
     pointUpdates = 0;
     stages = 0;
@@ -985,9 +909,10 @@ public:
   }
 
   // ------------------------------------------------------------ download
-  int64_t countDefined(int b) { return defined(b); }
+  int64_t countDefined(int b) override { return defined(b); }
+  int width(int b) const override { return buf[b].width; }
 
-  void queryValues(int b, int64_t n, const int32_t *idx, double *out) {
+  void queryValues(int b, int64_t n, const int32_t *idx, double *out) override {
     if (n <= 0) return;
     int *di = nullptr;
     double *dv = nullptr;
@@ -1123,7 +1048,7 @@ public:
   }
 
   // Defined points of buffer b in HRLE order; returns their number.
-  int64_t compact(int b, int32_t *idxOut, double *valOut, int64_t capOut) {
+  int64_t compact(int b, int32_t *idxOut, double *valOut, int64_t capOut) override {
     buildExchange(b);
     if (!idxOut || !valOut || xPoints > capOut) return xPoints;
     if (xPoints) {
@@ -1136,7 +1061,7 @@ public:
     return xPoints;
   }
   // Undefined runs of buffer b (HRLE order); returns their number.
-  int64_t runs(int b, int32_t *startOut, int8_t *signOut, int64_t capOut) {
+  int64_t runs(int b, int32_t *startOut, int8_t *signOut, int64_t capOut) override {
     buildExchange(b);
     if (!startOut || !signOut || xRuns > capOut) return xRuns;
     if (xRuns) {
@@ -1147,6 +1072,53 @@ public:
     }
     return xRuns;
   }
+
+  // ------------------------------------------------------ interface extras
+  void queryStaged(int b, int64_t n, const int32_t *idx, double *out, int32_t *di,
+                   double *dv) override {
+    VLSG_CUDA(cudaMemcpyAsync(di, idx, n * 3 * sizeof(int32_t), cudaMemcpyHostToDevice, stream));
+    kQueryValues<T><<<grid1(n), 256, 0, stream>>>(g, mapView(), view(b), (int)n, di, dv);
+    checkLaunch();
+    VLSG_CUDA(cudaMemcpyAsync(out, dv, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    VLSG_CUDA(cudaStreamSynchronize(stream));
+  }
+  void exchange(int b, const int32_t **idx, const double **val, int64_t *n) override {
+    buildExchange(b);
+    *idx = (const int32_t *)xs[X_IDX].p;
+    *val = (const double *)xs[X_VAL].p;
+    *n = xPoints;
+  }
+  uint64_t insideCells(int b) override {
+    VLSG_CUDA(cudaMemsetAsync(small + 15, 0, sizeof(unsigned long long), stream));
+    kInsideCells<T><<<blocksPass, 256, 0, stream>>>(g, mapView(), view(b), nBricks, small + 15);
+    checkLaunch();
+    return readU64(small + 15);
+  }
+  int64_t surfaceNodes(int b, double **nodes, uint64_t **keys) override {
+    buildExchange(b);
+    const int64_t n = xPoints;
+    const int32_t *idx = (const int32_t *)xs[X_IDX].p;
+    const double *val = (const double *)xs[X_VAL].p;
+    uint32_t *cnt = nullptr, *off = nullptr, *sums = nullptr;
+    VLSG_CUDA(cudaMalloc(&cnt, std::max<int64_t>(n, 1) * sizeof(uint32_t)));
+    VLSG_CUDA(cudaMalloc(&off, std::max<int64_t>(n, 1) * sizeof(uint32_t)));
+    VLSG_CUDA(cudaMalloc(&sums, (scanScratch(n) + 64) * sizeof(uint32_t)));
+    kSurfaceNodes<T><<<grid1(n), 256, 0, stream>>>(g, mapView(), view(b), idx, val, n, cnt, nullptr,
+                                                   nullptr, nullptr);
+    scanExclusive(cnt, off, n, sums);
+    const int64_t m = scanTotal(sums, n);
+    VLSG_CUDA(cudaMalloc(nodes, std::max<int64_t>(m, 1) * 3 * sizeof(double)));
+    VLSG_CUDA(cudaMalloc(keys, std::max<int64_t>(m, 1) * sizeof(uint64_t)));
+    kSurfaceNodes<T><<<grid1(n), 256, 0, stream>>>(g, mapView(), view(b), idx, val, n, cnt, off,
+                                                   *nodes, *keys);
+    checkLaunch();
+    VLSG_CUDA(cudaStreamSynchronize(stream));
+    cudaFree(cnt);
+    cudaFree(off);
+    cudaFree(sums);
+    return m;
+  }
 };
 
+} // namespace
 } // namespace vlsg

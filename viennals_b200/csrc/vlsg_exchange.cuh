@@ -29,6 +29,7 @@
 #include "vlsg_scan.cuh"
 
 namespace vlsg {
+namespace { // internal linkage: every compilation unit has its own copy
 
 constexpr int XNI = -((1 << 20) - 2); // start index of runs that begin at -infinity
 
@@ -271,4 +272,5 @@ __global__ void kRunCompact(const int32_t *start, const int8_t *sign, const uint
   }
 }
 
+} // namespace
 } // namespace vlsg

@@ -34,6 +34,7 @@
 #include "vlsg_passes.cuh"
 
 namespace vlsg {
+namespace { // internal linkage: every compilation unit has its own copy
 
 constexpr int FRONTIER_THREADS = 256;
 // Resident blocks per SM the passes are compiled for (40 registers per
@@ -482,4 +483,5 @@ __global__ void kBuildNeighbours(GridDev g, const int *brickMap, const int *slot
   }
 }
 
+} // namespace
 } // namespace vlsg

@@ -12,6 +12,7 @@
 #include "vlsg_common.cuh"
 
 namespace vlsg {
+namespace { // internal linkage: every compilation unit has its own copy
 
 struct BufSet {
   void *vals[MAXB];
@@ -473,4 +474,5 @@ __global__ void kCopySlots(const int *slotList, const int *nSlots, const T *sv,
   }
 }
 
+} // namespace
 } // namespace vlsg

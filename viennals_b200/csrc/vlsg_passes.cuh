@@ -15,6 +15,7 @@
 #include "vlsg_common.cuh"
 
 namespace vlsg {
+namespace { // internal linkage: every compilation unit has its own copy
 
 template <class T> struct ExpandRule {
   T totalLimit, limit;
@@ -151,4 +152,5 @@ template <class T> struct CombineComp {
   }
 };
 
+} // namespace
 } // namespace vlsg

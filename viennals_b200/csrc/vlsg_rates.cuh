@@ -25,6 +25,7 @@
 #include "vlsg_passes.cuh"
 
 namespace vlsg {
+namespace { // internal linkage: every compilation unit has its own copy
 
 constexpr int RATE_THREADS = 256;
 
@@ -672,4 +673,5 @@ __global__ void __launch_bounds__(RATE_THREADS)
   }
 }
 
+} // namespace
 } // namespace vlsg

@@ -6,6 +6,7 @@
 #include <cstdint>
 
 namespace vlsg {
+namespace { // internal linkage: every compilation unit has its own copy
 
 constexpr int SCAN_THREADS = 512;
 constexpr int SCAN_ITEMS = 8;
@@ -104,4 +105,5 @@ __global__ void __launch_bounds__(SCAN_THREADS)
 // Number of block sums (plus one for the total) a scan of n elements needs.
 inline size_t scanScratch(size_t n) { return (n + SCAN_TILE - 1) / SCAN_TILE + 1; }
 
+} // namespace
 } // namespace vlsg
