@@ -175,58 +175,17 @@ public:
       if (!check(vlsg_download_levelset(ctx, (int32_t)i, n, ls.indices.data(), ls.values.data(), &w)))
         return;
       ls.width = w;
-      rebuildRuns(i, ls);
+      // undefined runs in HRLE order, built on the device
+      int64_t m = 0;
+      const int rc = vlsg_download_runs(ctx, (int32_t)i, 0, nullptr, nullptr, &m);
+      if (rc != VLSG_OK && rc != VLSG_ERR_CAPACITY && !check(rc)) return;
+      ls.runStart.resize(3 * m);
+      ls.runSign.resize(m);
+      if (!check(vlsg_download_runs(ctx, (int32_t)i, m, ls.runStart.data(), ls.runSign.data(), &m)))
+        return;
     }
   }
 
-private:
-  // Undefined runs of a downloaded level set (HRLE order): one before the
-  // bounding box of the points, one after it, one per row of the box without
-  // points, and in rows with points one at the row head and one after every
-  // point not followed by a defined neighbour.  Each run's sign is read back
-  // from the device at a cell inside the run.
-  void rebuildRuns(size_t slot, LevelSet &ls) {
-    const int64_t n = ls.numberOfPoints();
-    const int32_t NI = -((1 << 20) - 2);
-    std::array<int32_t, 3> lo{0, 0, 0}, hi{0, 0, 0};
-    for (int64_t i = 0; i < n; ++i)
-      for (int d = 0; d < 3; ++d) {
-        const int32_t c = ls.indices[3 * i + d];
-        if (i == 0 || c < lo[d]) lo[d] = c;
-        if (i == 0 || c > hi[d]) hi[d] = c;
-      }
-    std::vector<int32_t> starts, probe;
-    auto add = [&](int32_t x, int32_t y, int32_t z, int32_t px, int32_t py, int32_t pz) {
-      starts.insert(starts.end(), {x, y, z});
-      probe.insert(probe.end(), {px, py, pz});
-    };
-    add(NI, NI, NI, lo[0], lo[1], lo[2] - 1);
-    int64_t i = 0;
-    for (int32_t z = lo[2]; z <= hi[2]; ++z) {
-      add(NI, NI, z, lo[0], lo[1] - 1, z);
-      for (int32_t y = lo[1]; y <= hi[1]; ++y) {
-        if (i >= n || ls.indices[3 * i + 1] != y || ls.indices[3 * i + 2] != z) {
-          add(NI, y, z, lo[0], y, z); // row without points
-          continue;
-        }
-        add(NI, y, z, ls.indices[3 * i] - 1, y, z);
-        for (; i < n && ls.indices[3 * i + 1] == y && ls.indices[3 * i + 2] == z; ++i) {
-          const int32_t x = ls.indices[3 * i];
-          const bool adjacent = i + 1 < n && ls.indices[3 * (i + 1)] == x + 1 &&
-                                ls.indices[3 * (i + 1) + 1] == y && ls.indices[3 * (i + 1) + 2] == z;
-          if (!adjacent) add(x + 1, y, z, x + 1, y, z);
-        }
-      }
-      add(NI, hi[1] + 1, z, lo[0], hi[1] + 1, z);
-    }
-    add(NI, NI, hi[2] + 1, lo[0], lo[1], hi[2] + 1);
-    const int64_t m = (int64_t)starts.size() / 3;
-    std::vector<double> v(m);
-    if (!check(vlsg_get_values(ctx, (int32_t)slot, m, probe.data(), v.data()))) return;
-    ls.runStart = starts;
-    ls.runSign.resize(m);
-    for (int64_t j = 0; j < m; ++j) ls.runSign[j] = v[j] < 0 ? -1 : 1;
-  }
 };
 
 } // namespace vlsg
