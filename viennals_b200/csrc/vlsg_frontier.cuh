@@ -94,46 +94,59 @@ __device__ inline int locateCell(const GridDev &g, const int *brickMap, int x, i
   return slot >= 0 ? slot : -1 - bi;
 }
 
-// Per-warp context of one brick.
-struct BrickCtx {
-  int slot, nb[6]; // face neighbours -x,+x,-y,+y,-z,+z (slot or -1-brick)
-  bool complex;
-  int x0, y0, z0;
-};
-
-__device__ inline BrickCtx loadBrickCtx(const Topo &t, int slot) {
-  BrickCtx b;
-  b.slot = slot;
-  const int *n = t.nbr + (size_t)slot * 27;
-  b.nb[0] = n[NB_XM], b.nb[1] = n[NB_XP], b.nb[2] = n[NB_YM];
-  b.nb[3] = n[NB_YP], b.nb[4] = n[NB_ZM], b.nb[5] = n[NB_ZP];
-  b.complex = (t.cflag[slot] & CF_STAR) != 0;
-  int bx, by, bz;
-  brickCoords(t.g, t.slotBrick[slot], bx, by, bz);
-  b.x0 = t.g.org[0] + bx * BS, b.y0 = t.g.org[1] + by * BS, b.z0 = t.g.org[2] + bz * BS;
-  return b;
+// Face neighbours of a slot in the 27-table order -x,+x,-y,+y,-z,+z.
+__device__ inline int faceEntry(int f) {
+  return f == 0 ? NB_XM : f == 1 ? NB_XP : f == 2 ? NB_YM : f == 3 ? NB_YP : f == 4 ? NB_ZM : NB_ZP;
 }
 
-// Star neighbours (order +x,+y,+z,-x,-y,-z) of local cell c as (slot or
-// -1-brick, cell) pairs.
-__device__ inline void starRefs(const Topo &t, const BrickCtx &b, int c, int *ref, int *loc) {
+// Per-warp shared scratch of the brick in hand.
+struct WarpScratch {
+  unsigned long long flip[8]; // cells whose definedness flips
+  int nb[6];                  // face neighbours -x,+x,-y,+y,-z,+z (slot or -1-brick)
+  int pad[2];
+  uint16_t list[BV];          // the brick's cells to evaluate, ascending
+};
+
+// Start of a brick: face neighbours to shared memory, flips cleared.
+__device__ inline void beginBrick(const Topo &t, WarpScratch &ws, int slot, int lane) {
+  if (lane < 6) ws.nb[lane] = t.nbr[(size_t)slot * 27 + faceEntry(lane)];
+  if (lane < 8) ws.flip[lane] = 0ull;
+  __syncwarp();
+}
+
+// Publish the brick's new defined mask (old ^ flips).
+__device__ inline void finishBrick(WarpScratch &ws, uint64_t *defNext, int slot, int lane,
+                                   uint64_t own) {
+  __syncwarp();
+  if (lane < 8) defNext[(size_t)slot * 8 + lane] = own ^ ws.flip[lane];
+  __syncwarp();
+}
+
+__device__ inline void brickOrigin(const Topo &t, int slot, int &x0, int &y0, int &z0) {
+  int bx, by, bz;
+  brickCoords(t.g, t.slotBrick[slot], bx, by, bz);
+  x0 = t.g.org[0] + bx * BS, y0 = t.g.org[1] + by * BS, z0 = t.g.org[2] + bz * BS;
+}
+
+// Star neighbour j (order +x,+y,+z,-x,-y,-z) of local cell c as (slot or
+// -1-brick, cell): through the face neighbours, or, for a brick next to a
+// boundary that remaps cells, through the brick map and the mapping.
+__device__ inline int starRef(const Topo &t, const int *nb, int slot, bool complex, int x0,
+                              int y0, int z0, int c, int j, int &loc) {
   const int x = c & 7, y = (c >> 3) & 7, z = c >> 6;
-  if (b.complex) {
-    const int X = b.x0 + x, Y = b.y0 + y, Z = b.z0 + z;
-    ref[0] = locateCell(t.g, t.brickMap, X + 1, Y, Z, loc[0]);
-    ref[1] = locateCell(t.g, t.brickMap, X, Y + 1, Z, loc[1]);
-    ref[2] = locateCell(t.g, t.brickMap, X, Y, Z + 1, loc[2]);
-    ref[3] = locateCell(t.g, t.brickMap, X - 1, Y, Z, loc[3]);
-    ref[4] = locateCell(t.g, t.brickMap, X, Y - 1, Z, loc[4]);
-    ref[5] = locateCell(t.g, t.brickMap, X, Y, Z - 1, loc[5]);
-    return;
+  if (complex) {
+    const int dx = j == 0 ? 1 : j == 3 ? -1 : 0, dy = j == 1 ? 1 : j == 4 ? -1 : 0,
+              dz = j == 2 ? 1 : j == 5 ? -1 : 0;
+    return locateCell(t.g, t.brickMap, x0 + x + dx, y0 + y + dy, z0 + z + dz, loc);
   }
-  ref[0] = x < 7 ? b.slot : b.nb[1], loc[0] = x < 7 ? c + 1 : c - 7;
-  ref[1] = y < 7 ? b.slot : b.nb[3], loc[1] = y < 7 ? c + 8 : c - 56;
-  ref[2] = z < 7 ? b.slot : b.nb[5], loc[2] = z < 7 ? c + 64 : c - 448;
-  ref[3] = x > 0 ? b.slot : b.nb[0], loc[3] = x > 0 ? c - 1 : c + 7;
-  ref[4] = y > 0 ? b.slot : b.nb[2], loc[4] = y > 0 ? c - 8 : c + 56;
-  ref[5] = z > 0 ? b.slot : b.nb[4], loc[5] = z > 0 ? c - 64 : c + 448;
+  switch (j) {
+  case 0: loc = x < 7 ? c + 1 : c - 7; return x < 7 ? slot : nb[1];
+  case 1: loc = y < 7 ? c + 8 : c - 56; return y < 7 ? slot : nb[3];
+  case 2: loc = z < 7 ? c + 64 : c - 448; return z < 7 ? slot : nb[5];
+  case 3: loc = x > 0 ? c - 1 : c + 7; return x > 0 ? slot : nb[0];
+  case 4: loc = y > 0 ? c - 8 : c + 56; return y > 0 ? slot : nb[2];
+  default: loc = z > 0 ? c - 64 : c + 448; return z > 0 ? slot : nb[4];
+  }
 }
 
 template <class T>
@@ -142,11 +155,11 @@ __device__ inline T refValue(const T *vals, const int8_t *farSign, int ref, int 
 }
 
 // Mask of the cells of plane z that exist in the grid.
-__device__ inline uint64_t existPlane(const GridDev &g, const BrickCtx &b, int z) {
+__device__ inline uint64_t existPlane(const GridDev &g, int x0, int y0, int z0, int z) {
   uint64_t m = 0;
   for (int y = 0; y < 8; ++y)
     for (int x = 0; x < 8; ++x)
-      if (cellExists(g, b.x0 + x, b.y0 + y, b.z0 + z)) m |= 1ull << (y * 8 + x);
+      if (cellExists(g, x0 + x, y0 + y, z0 + z)) m |= 1ull << (y * 8 + x);
   return m;
 }
 
@@ -154,80 +167,55 @@ __device__ inline uint64_t existPlane(const GridDev &g, const BrickCtx &b, int z
 // lanes return 0).  Every lane of the warp must call it.  Sets err bit 64
 // when a set cell lies on a face whose neighbour brick is not allocated
 // (its cells could change but are not in the pool).
-__device__ inline uint64_t dilatedMask(const Topo &t, const uint64_t *mask, const BrickCtx &b,
-                                       int lane) {
+__device__ inline uint64_t dilatedMask(const Topo &t, const uint64_t *mask, int slot,
+                                       const int *nb, int lane) {
   const int z = lane & 7;
-  const uint64_t w = lane < 8 ? mask[(size_t)b.slot * 8 + z] : 0ull;
+  const uint64_t w = lane < 8 ? mask[(size_t)slot * 8 + z] : 0ull;
   uint64_t below = __shfl_sync(0xffffffffu, w, (z + 7) & 7);
   uint64_t above = __shfl_sync(0xffffffffu, w, (z + 1) & 7);
   if (lane >= 8) return 0ull;
-  if (z == 0) below = b.nb[4] >= 0 ? mask[(size_t)b.nb[4] * 8 + 7] : 0ull;
-  if (z == 7) above = b.nb[5] >= 0 ? mask[(size_t)b.nb[5] * 8 + 0] : 0ull;
-  const uint64_t nxm = b.nb[0] >= 0 ? mask[(size_t)b.nb[0] * 8 + z] : 0ull;
-  const uint64_t nxp = b.nb[1] >= 0 ? mask[(size_t)b.nb[1] * 8 + z] : 0ull;
-  const uint64_t nym = b.nb[2] >= 0 ? mask[(size_t)b.nb[2] * 8 + z] : 0ull;
-  const uint64_t nyp = b.nb[3] >= 0 ? mask[(size_t)b.nb[3] * 8 + z] : 0ull;
-  const bool open = ((w & XLO) && b.nb[0] < 0) || ((w & XHI) && b.nb[1] < 0) ||
-                    ((w & 0xffull) && b.nb[2] < 0) || ((w >> 56) && b.nb[3] < 0) ||
-                    (z == 0 && w && b.nb[4] < 0) || (z == 7 && w && b.nb[5] < 0);
+  if (z == 0) below = nb[4] >= 0 ? mask[(size_t)nb[4] * 8 + 7] : 0ull;
+  if (z == 7) above = nb[5] >= 0 ? mask[(size_t)nb[5] * 8 + 0] : 0ull;
+  const uint64_t nxm = nb[0] >= 0 ? mask[(size_t)nb[0] * 8 + z] : 0ull;
+  const uint64_t nxp = nb[1] >= 0 ? mask[(size_t)nb[1] * 8 + z] : 0ull;
+  const uint64_t nym = nb[2] >= 0 ? mask[(size_t)nb[2] * 8 + z] : 0ull;
+  const uint64_t nyp = nb[3] >= 0 ? mask[(size_t)nb[3] * 8 + z] : 0ull;
+  const bool open = ((w & XLO) && nb[0] < 0) || ((w & XHI) && nb[1] < 0) ||
+                    ((w & 0xffull) && nb[2] < 0) || ((w >> 56) && nb[3] < 0) ||
+                    (z == 0 && w && nb[4] < 0) || (z == 7 && w && nb[5] < 0);
   if (open) atomicOr(t.err, 64);
   return w | ((w << 1) & ~XLO) | ((w >> 1) & ~XHI) | ((nxm & XHI) >> 7) | ((nxp & XLO) << 7) |
          (w << 8) | (w >> 8) | (nym >> 56) | (nyp << 56) | below | above;
 }
 
-// Enumeration of the set bits of a 512-bit brick mask held as one plane word
-// per lane 0..7 (lane z: plane z): the k-th set bit in (z, y, x) order, so a
-// warp takes 32 cells of the brick per round whatever planes they lie in.
-// Every lane of the warp must construct it and call cell().
-struct PlaneEnum {
-  int incl[8]; // inclusive prefix counts over the planes (in every lane)
-  int total;
-  __device__ explicit PlaneEnum(uint64_t w) {
-    const int lane = threadIdx.x & 31;
-    int cnt = lane < 8 ? __popcll(w) : 0;
+// List the set cells of a brick mask (lane z holds plane z, z < 8) into
+// `list` in ascending order: lane l < 16 walks the 32-bit half l & 1 of plane
+// l >> 1.  Returns the number of cells (every lane).  Every lane of the warp
+// must call it.
+__device__ inline int listCells(uint64_t plane, uint16_t *list) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t pw = __shfl_sync(0xffffffffu, plane, (lane >> 1) & 7);
+  unsigned w = lane < 16 ? (unsigned)(pw >> (32 * (lane & 1))) : 0u;
+  const int cnt = __popc(w);
+  int x = cnt;
 #pragma unroll
-    for (int o = 1; o < 8; o <<= 1) {
-      const int t = __shfl_up_sync(0xffffffffu, cnt, o, 8);
-      if ((lane & 7) >= o) cnt += t;
-    }
-#pragma unroll
-    for (int j = 0; j < 8; ++j) incl[j] = __shfl_sync(0xffffffffu, cnt, j);
-    total = incl[7];
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += t;
   }
-  // Cell index z*64+y*8+x of set bit k (k clamped into range by the caller).
-  __device__ int cell(uint64_t w, int k) const {
-    int z = 0, excl = 0;
-#pragma unroll
-    for (int j = 0; j < 7; ++j)
-      if (k >= incl[j]) z = j + 1, excl = incl[j];
-    const uint64_t m = __shfl_sync(0xffffffffu, w, z);
-    const unsigned lo = (unsigned)m, hi = (unsigned)(m >> 32);
-    const int nlo = __popc(lo), r = k - excl;
-    const int bit = r < nlo ? (int)__fns(lo, 0, r + 1) : 32 + (int)__fns(hi, 0, r - nlo + 1);
-    return z * 64 + bit;
+  int off = x - cnt;
+  const int total = __shfl_sync(0xffffffffu, x, 31);
+  const int base = (lane >> 1) * 64 + (lane & 1) * 32;
+  while (w) {
+    list[off++] = (uint16_t)(base + __ffs(w) - 1);
+    w &= w - 1;
   }
-};
-
-// Per-warp shared words of the brick in hand: cells whose definedness flips.
-struct WarpMasks {
-  unsigned long long flip[8];
-};
+  __syncwarp();
+  return total;
+}
 
 __device__ inline void markCell(unsigned long long *words, int c) {
   atomicOr(&words[c >> 6], 1ull << (c & 63));
-}
-
-// Publish the brick's new defined mask (old ^ flips).
-__device__ inline void finishBrick(WarpMasks &m, uint64_t *defNext, int slot, int lane,
-                                   uint64_t own) {
-  __syncwarp();
-  if (lane < 8) defNext[(size_t)slot * 8 + lane] = own ^ m.flip[lane];
-  __syncwarp();
-}
-
-__device__ inline void clearBrick(WarpMasks &m, int lane) {
-  if (lane < 8) m.flip[lane] = 0ull;
-  __syncwarp();
 }
 
 // Append the lanes with `has` to the warp's log segment (warp-uniform call).
@@ -251,8 +239,8 @@ enum : int { FP_EXPAND = 0, FP_PRUNE = 1, FP_ALL = 2 };
 template <class T, int MODE, class Rule>
 __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
     kFrontierPass(Topo t, LsView<T> v, Rule rule, ChangeLog<T> lg) {
-  __shared__ WarpMasks sm[FRONTIER_THREADS / 32];
-  WarpMasks &wm = sm[threadIdx.x >> 5];
+  __shared__ WarpScratch sm[FRONTIER_THREADS / 32];
+  WarpScratch &ws = sm[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nWarps = (gridDim.x * blockDim.x) >> 5;
@@ -261,40 +249,44 @@ __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
   int logged = 0;
   for (int w = warp; w < n; w += nWarps) {
     const int slot = t.slotList[w];
-    const BrickCtx b = loadBrickCtx(t, slot);
+    beginBrick(t, ws, slot, lane);
+    const bool complex = (t.cflag[slot] & CF_STAR) != 0;
+    int x0 = 0, y0 = 0, z0 = 0;
+    if (complex) brickOrigin(t, slot, x0, y0, z0);
     const uint64_t own = lane < 8 ? v.def[(size_t)slot * 8 + lane] : 0ull;
     uint64_t cand;
     if (MODE == FP_PRUNE) {
       cand = own;
-    } else if (b.complex) {
-      const uint64_t ex = lane < 8 ? existPlane(t.g, b, lane) : 0ull;
+    } else if (complex) {
+      const uint64_t ex = lane < 8 ? existPlane(t.g, x0, y0, z0, lane) : 0ull;
       cand = MODE == FP_EXPAND ? ex & ~own : ex;
     } else {
-      const uint64_t dil = dilatedMask(t, v.def, b, lane);
+      const uint64_t dil = dilatedMask(t, v.def, slot, ws.nb, lane);
       cand = MODE == FP_EXPAND ? dil & ~own : dil;
     }
-    clearBrick(wm, lane);
-    const PlaneEnum pe(cand);
-    for (int base = 0; base < pe.total; base += 32) {
+    const int total = listCells(cand, ws.list);
+    for (int base = 0; base < total; base += 32) {
       const int k = base + lane;
-      const int c = pe.cell(cand, k < pe.total ? k : pe.total - 1);
       bool changed = false;
       T out = T(0);
-      if (k < pe.total) {
-        const size_t q = (size_t)slot * BV + c;
-        const T center = v.vals[q];
-        int ref[6], loc[6];
-        starRefs(t, b, c, ref, loc);
+      int c = 0;
+      if (k < total) {
+        c = ws.list[k];
+        const T center = v.vals[(size_t)slot * BV + c];
         T nb[6];
 #pragma unroll
-        for (int j = 0; j < 6; ++j) nb[j] = refValue<T>(v.vals, v.farSign, ref[j], loc[j]);
+        for (int j = 0; j < 6; ++j) {
+          int loc;
+          const int ref = starRef(t, ws.nb, slot, complex, x0, y0, z0, c, j, loc);
+          nb[j] = refValue<T>(v.vals, v.farSign, ref, loc);
+        }
         out = rule(center, nb);
         changed = out != center || signbit(out) != signbit(center);
-        if (changed && isDef(out) != isDef(center)) markCell(wm.flip, c);
+        if (changed && isDef(out) != isDef(center)) markCell(ws.flip, c);
       }
       logChange<T>(lg, logBase, logged, changed, ((uint32_t)slot << 9) | (uint32_t)c, out);
     }
-    finishBrick(wm, v.defNext, slot, lane, own);
+    finishBrick(ws, v.defNext, slot, lane, own);
   }
   if (lane == 0) lg.count[warp] = logged;
 }
@@ -333,8 +325,8 @@ __device__ inline T reducedValue(const T *vals, const uint64_t *act, const int8_
 template <class T>
 __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
     kUpdateRebuild(Topo t, LsView<T> v, const uint64_t *act, double cutoff, ChangeLog<T> lg) {
-  __shared__ WarpMasks sm[FRONTIER_THREADS / 32];
-  WarpMasks &wm = sm[threadIdx.x >> 5];
+  __shared__ WarpScratch sm[FRONTIER_THREADS / 32];
+  WarpScratch &ws = sm[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nWarps = (gridDim.x * blockDim.x) >> 5;
@@ -344,46 +336,54 @@ __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
   const RebuildRule<T> rule{cutoff};
   for (int w = warp; w < n; w += nWarps) {
     const int slot = t.slotList[w];
-    const BrickCtx b = loadBrickCtx(t, slot);
+    beginBrick(t, ws, slot, lane);
+    const bool complex = (t.cflag[slot] & CF_STAR) != 0;
+    int x0 = 0, y0 = 0, z0 = 0;
+    if (complex) brickOrigin(t, slot, x0, y0, z0);
     const uint64_t own = lane < 8 ? v.def[(size_t)slot * 8 + lane] : 0ull;
     uint64_t cand;
-    if (b.complex) cand = lane < 8 ? existPlane(t.g, b, lane) : 0ull;
-    else cand = dilatedMask(t, act, b, lane);
+    if (complex) cand = lane < 8 ? existPlane(t.g, x0, y0, z0, lane) : 0ull;
+    else cand = dilatedMask(t, act, slot, ws.nb, lane);
     const uint64_t clear = own & ~cand;
-    clearBrick(wm, lane);
-    const PlaneEnum pe(cand);
-    for (int base = 0; base < pe.total; base += 32) {
+    int total = listCells(cand, ws.list);
+    for (int base = 0; base < total; base += 32) {
       const int k = base + lane;
-      const int c = pe.cell(cand, k < pe.total ? k : pe.total - 1);
       bool changed = false;
       T out = T(0);
-      if (k < pe.total) {
-        const size_t q = (size_t)slot * BV + c;
-        const T mem = v.vals[q];
+      int c = 0;
+      if (k < total) {
+        c = ws.list[k];
+        const T mem = v.vals[(size_t)slot * BV + c];
         const T center = reducedValue<T>(v.vals, act, v.farSign, slot, c);
-        int ref[6], loc[6];
-        starRefs(t, b, c, ref, loc);
         T nb[6];
 #pragma unroll
-        for (int j = 0; j < 6; ++j) nb[j] = reducedValue<T>(v.vals, act, v.farSign, ref[j], loc[j]);
+        for (int j = 0; j < 6; ++j) {
+          int loc;
+          const int ref = starRef(t, ws.nb, slot, complex, x0, y0, z0, c, j, loc);
+          nb[j] = reducedValue<T>(v.vals, act, v.farSign, ref, loc);
+        }
         out = rule(center, nb);
         changed = out != mem || signbit(out) != signbit(mem);
-        if (changed && isDef(out) != isDef(mem)) markCell(wm.flip, c);
+        if (changed && isDef(out) != isDef(mem)) markCell(ws.flip, c);
       }
       logChange<T>(lg, logBase, logged, changed, ((uint32_t)slot << 9) | (uint32_t)c, out);
     }
     // defined cells away from the active ones: undefined with their sign
-    const PlaneEnum pc(clear);
-    for (int base = 0; base < pc.total; base += 32) {
+    __syncwarp();
+    total = listCells(clear, ws.list);
+    for (int base = 0; base < total; base += 32) {
       const int k = base + lane;
-      const int c = pc.cell(clear, k < pc.total ? k : pc.total - 1);
       T out = T(0);
-      if (k < pc.total) out = sentinel<T>(v.vals[(size_t)slot * BV + c] < 0);
-      logChange<T>(lg, logBase, logged, k < pc.total, ((uint32_t)slot << 9) | (uint32_t)c, out);
+      int c = 0;
+      if (k < total) {
+        c = ws.list[k];
+        out = sentinel<T>(v.vals[(size_t)slot * BV + c] < 0);
+      }
+      logChange<T>(lg, logBase, logged, k < total, ((uint32_t)slot << 9) | (uint32_t)c, out);
     }
     __syncwarp();
-    if (lane < 8) wm.flip[lane] |= clear;
-    finishBrick(wm, v.defNext, slot, lane, own);
+    if (lane < 8) ws.flip[lane] |= clear;
+    finishBrick(ws, v.defNext, slot, lane, own);
   }
   if (lane == 0) lg.count[warp] = logged;
 }

@@ -544,6 +544,8 @@ template <class T> constexpr int rateMinBlocks() { return sizeof(T) == 4 ? 3 : 2
 template <class T, int MODE>
 __global__ void __launch_bounds__(RATE_THREADS, rateMinBlocks<T>())
     kRates(RateArgs<T> A, const vlsg_velocity_desc vel) {
+  __shared__ uint16_t sList[RATE_THREADS / 32][BV];
+  uint16_t *list = sList[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nWarps = (gridDim.x * blockDim.x) >> 5;
@@ -561,11 +563,11 @@ __global__ void __launch_bounds__(RATE_THREADS, rateMinBlocks<T>())
       nAct += __popcll(a);
       nBand += __popcll(own);
     }
-    const PlaneEnum pa(a);
-    for (int base = 0; base < pa.total; base += 32) {
+    const int total = listCells(a, list);
+    for (int base = 0; base < total; base += 32) {
       const int k = base + lane;
-      const int c = pa.cell(a, k < pa.total ? k : pa.total - 1);
-      if (k >= pa.total) continue;
+      if (k >= total) continue;
+      const int c = list[k];
       withStencil<T>(A, slot, c, [&](const auto &S, T value) {
         if constexpr (MODE == 0) {
           T alphas[3] = {0, 0, 0};
@@ -631,6 +633,8 @@ __global__ void __launch_bounds__(RATE_THREADS)
     kUpdate(const int *slotList, const int *nSlots, const uint64_t *act, T *vals,
             const T *rateV, const T *rateStop, const uint8_t *rateLen, size_t poolCells, int L,
             double dt, int *err) {
+  __shared__ uint16_t sList[RATE_THREADS / 32][BV];
+  uint16_t *list = sList[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nWarps = (gridDim.x * blockDim.x) >> 5;
@@ -639,11 +643,11 @@ __global__ void __launch_bounds__(RATE_THREADS)
     const int slot = slotList[w];
     const uint64_t a = lane < 8 ? act[(size_t)slot * 8 + lane] : 0ull;
     if (!__any_sync(0xffffffffu, a != 0ull)) continue;
-    const PlaneEnum pa(a);
-    for (int base = 0; base < pa.total; base += 32) {
+    const int total = listCells(a, list);
+    for (int base = 0; base < total; base += 32) {
       const int k = base + lane;
-      const int c = pa.cell(a, k < pa.total ? k : pa.total - 1);
-      if (k >= pa.total) continue;
+      if (k >= total) continue;
+      const int c = list[k];
       const size_t q = (size_t)slot * BV + c;
       T value = vals[q];
       int len = rateLen[q];
