@@ -238,8 +238,8 @@ def precision_report(args, grid, dom, vel, p, stream):
     from viennals_b200._abi import Precision
 
     res = {}
-    ctxs = {}
-    for name, prec in (("fp64", Precision.FP64), ("fp32", Precision.FP32)):
+
+    def run(prec):
         c = Context(args.local_rank, prec)
         c.set_stream(stream.cuda_stream)
         c.set_grid(grid)
@@ -257,11 +257,22 @@ def precision_report(args, grid, dom, vel, p, stream):
         e1.record(stream)
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
-        res[name] = {"point_updates_per_s": upd / (ms / 1e3), "ms_per_step": ms / args.err_steps}
-        ctxs[name] = c
-    r = ctxs["fp32"].compare(0, ctxs["fp64"], 0)
-    for c in ctxs.values():
-        c.close()
+        return c, {"point_updates_per_s": upd / (ms / 1e3), "ms_per_step": ms / args.err_steps}
+
+    # each path timed alone on the device; the FP32 result crosses to the
+    # host and back (exact: FP32 values are doubles on the way) so that both
+    # results are resident for the comparison
+    c32, res["fp32"] = run(Precision.FP32)
+    out32 = c32.download_domain(0, grid)
+    c32.close()
+    c64, res["fp64"] = run(Precision.FP64)
+    c32 = Context(args.local_rank, Precision.FP32)
+    c32.set_grid(grid)
+    c32.set_level_set_count(1)
+    c32.upload(0, out32)
+    r = c32.compare(0, c64, 0)
+    c32.close()
+    c64.close()
     gd = float(grid.delta)
     vol64, vol32 = r["inside_cells_b"], r["inside_cells_a"]
     return {

@@ -652,11 +652,16 @@ public:
         buf[a].nDef = defined(a);
         return bandPassBytes(nA + nB, buf[a].nDef);
       });
-      kPointwise<T, Comp><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(
-          topo(), buf[a].vals, buf[a].def[buf[a].cur], buf[bb].vals, comp, flag);
+      if constexpr (Comp::keepsUndefinedA) {
+        kPointwiseDefined<T, Comp><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(
+            topo(), buf[a].vals, buf[a].def[buf[a].cur], buf[bb].vals, comp, flag);
+      } else {
+        kPointwise<T, Comp><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(
+            topo(), buf[a].vals, buf[a].def[buf[a].cur], buf[bb].vals, comp, flag);
+      }
       checkLaunch();
     }
-    {
+    if constexpr (!Comp::keepsUndefinedA) {
       Scope sc(this, "boolean_far");
       kPointwise2FarSign<T, Comp><<<grid1(nBricks), 256, 0, stream>>>(nBricks, buf[a].farSign,
                                                                       buf[bb].farSign, buf[a].farSign, comp);
@@ -677,8 +682,8 @@ public:
     auto &D = buf[dst];
     {
       Scope sc(this, "copy");
-      kCopySlots<T><<<blocksPass, 256, 0, stream>>>(slotList, nSlotsPtr(), S.vals, S.def[S.cur],
-                                                    D.vals, D.def[D.cur]);
+      kCopySlots16<T><<<blocksPass, 256, 0, stream>>>(slotList, nSlotsPtr(), S.vals, S.def[S.cur],
+                                                      D.vals, D.def[D.cur]);
       checkLaunch();
     }
     VLSG_CUDA(cudaMemcpyAsync(D.farSign, S.farSign, nBricks, cudaMemcpyDeviceToDevice, stream));
@@ -837,8 +842,8 @@ public:
       auto &D = buf[l];
       {
         Scope sc(this, "copy");
-        kCopySlots<T><<<blocksPass, 256, 0, stream>>>(slotList, nSlotsPtr(), S.vals, S.def[S.cur],
-                                                      D.vals, D.def[D.cur]);
+        kCopySlots16<T><<<blocksPass, 256, 0, stream>>>(slotList, nSlotsPtr(), S.vals,
+                                                        S.def[S.cur], D.vals, D.def[D.cur]);
         checkLaunch();
       }
       VLSG_CUDA(cudaMemcpyAsync(D.farSign, S.farSign, nBricks, cudaMemcpyDeviceToDevice, stream));

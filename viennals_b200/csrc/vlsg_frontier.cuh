@@ -428,6 +428,62 @@ __global__ void __launch_bounds__(FRONTIER_THREADS)
   }
 }
 
+// Pointwise boolean for comparators that keep every undefined cell of A
+// (combineLevelSets, lsAdvect.hpp:218-230): only A's defined cells are read,
+// in place; A's masks lose the cells that became undefined.
+template <class T, class Comp>
+__global__ void __launch_bounds__(FRONTIER_THREADS)
+    kPointwiseDefined(Topo t, T *av, uint64_t *adef, const T *bv, Comp comp, int *flag) {
+  __shared__ WarpScratch sm[FRONTIER_THREADS / 32];
+  WarpScratch &ws = sm[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nWarps = (gridDim.x * blockDim.x) >> 5;
+  const int n = *t.nSlots;
+  bool moved = false;
+  for (int w = warp; w < n; w += nWarps) {
+    const int slot = t.slotList[w];
+    const uint64_t own = lane < 8 ? adef[(size_t)slot * 8 + lane] : 0ull;
+    if (!__any_sync(0xffffffffu, own != 0ull)) continue;
+    if (lane < 8) ws.flip[lane] = 0ull;
+    const int total = listCells(own, ws.list);
+    for (int base = 0; base < total; base += 32) {
+      const int k = base + lane;
+      if (k >= total) continue;
+      const int c = ws.list[k];
+      const size_t q = (size_t)slot * BV + c;
+      const T a = av[q];
+      bool mv = false;
+      const T o = comp(a, bv[q], mv);
+      moved |= mv;
+      if (o != a || signbit(o) != signbit(a)) {
+        av[q] = o;
+        if (!isDef(o)) markCell(ws.flip, c);
+      }
+    }
+    __syncwarp();
+    if (lane < 8) adef[(size_t)slot * 8 + lane] = own & ~ws.flip[lane];
+    __syncwarp();
+  }
+  if (__any_sync(0xffffffffu, moved) && lane == 0 && flag) atomicOr(flag, 1);
+}
+
+// Copy the listed slots of one buffer (values and masks) into another, 16
+// bytes per thread.
+template <class T>
+__global__ void kCopySlots16(const int *slotList, const int *nSlots, const T *sv,
+                             const uint64_t *sd, T *dv, uint64_t *dd) {
+  constexpr int PER = BV * sizeof(T) / 16; // 16-byte words per slot
+  const size_t n = (size_t)*nSlots * PER;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const size_t slot = slotList[i / PER];
+    const int k = (int)(i % PER);
+    reinterpret_cast<uint4 *>(dv + slot * BV)[k] = reinterpret_cast<const uint4 *>(sv + slot * BV)[k];
+    if (k < 4) reinterpret_cast<uint4 *>(dd + slot * 8)[k] = reinterpret_cast<const uint4 *>(sd + slot * 8)[k];
+  }
+}
+
 // Neighbour table and complexity flags of every listed slot, for any
 // boundary conditions: entry = slot, or -1-brick (unallocated, or outside the
 // map box: the nearest box brick).  CF_STAR: the brick holds a cell whose

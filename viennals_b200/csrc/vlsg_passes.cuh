@@ -127,12 +127,15 @@ __global__ void kPointwise2FarSign(int nBricks, const int8_t *fa,
 }
 
 template <class T> struct MaxComp { // INTERSECT, lsBooleanOperation.hpp:270-276
+  static constexpr bool keepsUndefinedA = false;
   __device__ T operator()(T a, T b, bool &) const { return a > b ? a : b; }
 };
 template <class T> struct MinComp { // UNION, :262-268
+  static constexpr bool keepsUndefinedA = false;
   __device__ T operator()(T a, T b, bool &) const { return a < b ? a : b; }
 };
 template <class T> struct RelComplementComp { // :278-280
+  static constexpr bool keepsUndefinedA = false;
   __device__ T operator()(T a, T b, bool &) const { return a > -b ? a : -b; }
 };
 // combineLevelSets comparator, lsAdvect.hpp:218-230 (a = current, b = saved).
@@ -140,6 +143,8 @@ template <class T> struct RelComplementComp { // :278-280
 // T = double this is the reference's expression, for T = float it is the
 // precision form's FP64 stage combination, rounded once to float.
 template <class T> struct CombineComp {
+  // an undefined current value stays as it is: only defined cells can change
+  static constexpr bool keepsUndefinedA = true;
   double wTarget, wSource;
   __device__ T operator()(T a, T b, bool &moved) const {
     if (isDef(a) && isDef(b)) {
