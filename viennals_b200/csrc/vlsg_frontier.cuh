@@ -194,8 +194,8 @@ __device__ inline uint64_t dilatedMask(const Topo &t, const uint64_t *mask, int 
 // must call it.
 __device__ inline int listCells(uint64_t plane, uint16_t *list) {
   const int lane = threadIdx.x & 31;
-  const uint64_t pw = __shfl_sync(0xffffffffu, plane, (lane >> 1) & 7);
-  unsigned w = lane < 16 ? (unsigned)(pw >> (32 * (lane & 1))) : 0u;
+  const uint64_t pw = __shfl_sync(0xffffffffu, plane, lane >> 2);
+  unsigned w = (unsigned)(pw >> (16 * (lane & 3))) & 0xffffu;
   const int cnt = __popc(w);
   int x = cnt;
 #pragma unroll
@@ -205,7 +205,7 @@ __device__ inline int listCells(uint64_t plane, uint16_t *list) {
   }
   int off = x - cnt;
   const int total = __shfl_sync(0xffffffffu, x, 31);
-  const int base = (lane >> 1) * 64 + (lane & 1) * 32;
+  const int base = (lane >> 2) * 64 + (lane & 3) * 16;
   while (w) {
     list[off++] = (uint16_t)(base + __ffs(w) - 1);
     w &= w - 1;
