@@ -80,6 +80,10 @@ public:
   int *logCount = nullptr;
   size_t logPer = 0;
   int logSegments = 0;
+  // bricks the next frontier pass of buffer visitBuf must visit (written by
+  // the previous pass of that buffer; visitBuf < 0: visit every brick)
+  uint8_t *visit[2] = {nullptr, nullptr};
+  int vcur = 0, visitBuf = -1;
   // host mirrors
   int hCounters[16];
   unsigned long long hScal[4];
@@ -121,7 +125,9 @@ public:
     auto f = [](void *p) { if (p) cudaFree(p); };
     f(brickMap); f(slotBrick); f(slotList); f(freeStack); f(newList); f(counters); f(needed);
     f(scal); f(defCnt); f(rateCounts); f(nbr); f(cflag); f(core); f(small); f(rateV);
-    f(rateStop); f(rateLen); f(act); f(logCell); f(logVal); f(logCount);
+    f(rateStop); f(rateLen); f(act); f(logCell); f(logVal); f(logCount); f(visit[0]); f(visit[1]);
+    visit[0] = visit[1] = nullptr;
+    visitBuf = -1;
     for (auto &k : runKeys) f(k);
     for (auto &b : buf) {
       f(b.vals); f(b.def[0]); f(b.def[1]); f(b.farSign);
@@ -282,7 +288,8 @@ public:
     if (c > 0 && (c > capSlots || L > capL)) {
       for (void *p : {(void *)slotBrick, (void *)slotList, (void *)freeStack, (void *)newList,
                       (void *)nbr, (void *)cflag, (void *)act, (void *)logCell, (void *)logVal,
-                      (void *)logCount, (void *)rateV, (void *)rateStop, (void *)rateLen})
+                      (void *)logCount, (void *)rateV, (void *)rateStop, (void *)rateLen,
+                      (void *)visit[0], (void *)visit[1]})
         if (p) VLSG_CUDA(cudaFree(p));
       slotBrick = slotList = freeStack = newList = nbr = logCount = nullptr;
       cflag = rateLen = nullptr, act = nullptr, logCell = nullptr;
@@ -303,6 +310,9 @@ public:
       VLSG_CUDA(cudaMalloc(&logCell, logPer * logSegments * sizeof(uint32_t)));
       VLSG_CUDA(cudaMalloc(&logVal, logPer * logSegments * sizeof(T)));
       VLSG_CUDA(cudaMalloc(&logCount, logSegments * sizeof(int)));
+      VLSG_CUDA(cudaMalloc(&visit[0], n));
+      VLSG_CUDA(cudaMalloc(&visit[1], n));
+      visitBuf = -1;
       VLSG_CUDA(cudaMalloc(&rateV, n * BV * sizeof(T) * l));
       VLSG_CUDA(cudaMalloc(&rateStop, n * BV * sizeof(T) * l));
       VLSG_CUDA(cudaMalloc(&rateLen, n * BV));
@@ -336,6 +346,7 @@ public:
   // are large enough.
   void build(const GridDev &grid, std::vector<StagedLS> &ls, int margin) override {
     ++generation;
+    visitBuf = -1;
     ensureSmall();
     g = grid;
     L = (int)ls.size();
@@ -534,6 +545,7 @@ public:
 
   // Bring the allocated bricks back to dilate(core) of the live buffers.
   void maintain() {
+    visitBuf = -1; // slots come and go
     VLSG_CUDA(cudaMemsetAsync(needed, 0, nBricks, stream));
     {
       Scope sc(this, "maint_mark");
@@ -583,8 +595,13 @@ public:
         buf[b].cur ^= 1;
         return bandPassBytes(nIn, buf[b].nDef);
       });
+      const uint8_t *visitIn = visitBuf == b ? visit[vcur] : nullptr;
+      uint8_t *visitOut = visit[1 - vcur];
+      VLSG_CUDA(cudaMemsetAsync(visitOut, 0, cap, stream));
       kFrontierPass<T, MODE, Rule><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(
-          topo(), lsView(b), rule, changeLog());
+          topo(), lsView(b), rule, changeLog(), visitIn, visitOut);
+      vcur ^= 1;
+      visitBuf = b;
       checkLaunch();
     }
     applyChanges(b);
@@ -635,8 +652,12 @@ public:
         // in: the active band; out: the new band
         return bandPassBytes(lastActive, buf[top].nDef);
       });
+      uint8_t *visitOut = visit[1 - vcur];
+      VLSG_CUDA(cudaMemsetAsync(visitOut, 0, cap, stream));
       kUpdateRebuild<T><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(topo(), lsView(top), act, 1.0,
-                                                                     changeLog());
+                                                                     changeLog(), visitOut);
+      vcur ^= 1;
+      visitBuf = top;
       checkLaunch();
     }
     applyChanges(top);
@@ -646,6 +667,7 @@ public:
     ++stages;
   }
   template <class Comp> void pointwise(int a, int bb, Comp comp, int *flag) {
+    visitBuf = -1;
     {
       const int64_t nA = profiling ? defined(a) : 0, nB = profiling ? defined(bb) : 0;
       Scope sc(this, "boolean", [this, a, nA, nB] {
@@ -677,6 +699,7 @@ public:
   }
 
   void copyBuffer(int src, int dst) {
+    if (visitBuf == dst) visitBuf = -1;
     allocBuffers(dst + 1);
     auto &S = buf[src];
     auto &D = buf[dst];
@@ -836,6 +859,7 @@ public:
     for (int l = all ? 0 : L - 1; l < L; ++l) copyBuffer(l, L + l);
   }
   void restoreLower() {
+    visitBuf = -1;
     for (int l = 0; l + 1 < L; ++l) {
       // copy initial back into the current buffer
       auto &S = buf[L + l];

@@ -114,11 +114,31 @@ __device__ inline void beginBrick(const Topo &t, WarpScratch &ws, int slot, int 
   __syncwarp();
 }
 
-// Publish the brick's new defined mask (old ^ flips).
+// Publish the brick's new defined mask (old ^ flips) and, when `visit` is
+// given, mark the bricks the next pass of this buffer must visit: this one if
+// it holds a defined cell, and each face neighbour with a defined cell of this
+// brick on the shared face (only those can have candidate cells).
 __device__ inline void finishBrick(WarpScratch &ws, uint64_t *defNext, int slot, int lane,
-                                   uint64_t own) {
+                                   uint64_t own, uint8_t *visit) {
   __syncwarp();
-  if (lane < 8) defNext[(size_t)slot * 8 + lane] = own ^ ws.flip[lane];
+  const uint64_t nw = lane < 8 ? own ^ ws.flip[lane] : 0ull;
+  if (lane < 8) defNext[(size_t)slot * 8 + lane] = nw;
+  if (visit) {
+    const unsigned self = __ballot_sync(0xffffffffu, nw != 0ull);
+    const unsigned xm = __ballot_sync(0xffffffffu, (nw & XLO) != 0ull);
+    const unsigned xp = __ballot_sync(0xffffffffu, (nw & XHI) != 0ull);
+    const unsigned ym = __ballot_sync(0xffffffffu, (nw & 0xffull) != 0ull);
+    const unsigned yp = __ballot_sync(0xffffffffu, (nw >> 56) != 0ull);
+    if (lane == 0 && self) {
+      visit[slot] = 1;
+      if (xm && ws.nb[0] >= 0) visit[ws.nb[0]] = 1;
+      if (xp && ws.nb[1] >= 0) visit[ws.nb[1]] = 1;
+      if (ym && ws.nb[2] >= 0) visit[ws.nb[2]] = 1;
+      if (yp && ws.nb[3] >= 0) visit[ws.nb[3]] = 1;
+      if ((self & 1u) && ws.nb[4] >= 0) visit[ws.nb[4]] = 1;
+      if ((self & 0x80u) && ws.nb[5] >= 0) visit[ws.nb[5]] = 1;
+    }
+  }
   __syncwarp();
 }
 
@@ -238,7 +258,8 @@ enum : int { FP_EXPAND = 0, FP_PRUNE = 1, FP_ALL = 2 };
 // defined cells and their neighbours.
 template <class T, int MODE, class Rule>
 __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
-    kFrontierPass(Topo t, LsView<T> v, Rule rule, ChangeLog<T> lg) {
+    kFrontierPass(Topo t, LsView<T> v, Rule rule, ChangeLog<T> lg, const uint8_t *visitIn,
+                  uint8_t *visitOut) {
   __shared__ WarpScratch sm[FRONTIER_THREADS / 32];
   WarpScratch &ws = sm[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
@@ -249,11 +270,21 @@ __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
   int logged = 0;
   for (int w = warp; w < n; w += nWarps) {
     const int slot = t.slotList[w];
-    beginBrick(t, ws, slot, lane);
     const bool complex = (t.cflag[slot] & CF_STAR) != 0;
+    // a brick the previous pass of this buffer did not mark has no defined
+    // cell and no defined face neighbour cell: nothing to evaluate
+    if (visitIn && !complex && !visitIn[slot]) {
+      if (lane < 8) v.defNext[(size_t)slot * 8 + lane] = 0ull;
+      continue;
+    }
+    const uint64_t own = lane < 8 ? v.def[(size_t)slot * 8 + lane] : 0ull;
+    if (MODE == FP_PRUNE && !complex && !__any_sync(0xffffffffu, own != 0ull)) {
+      if (lane < 8) v.defNext[(size_t)slot * 8 + lane] = 0ull;
+      continue;
+    }
+    beginBrick(t, ws, slot, lane);
     int x0 = 0, y0 = 0, z0 = 0;
     if (complex) brickOrigin(t, slot, x0, y0, z0);
-    const uint64_t own = lane < 8 ? v.def[(size_t)slot * 8 + lane] : 0ull;
     uint64_t cand;
     if (MODE == FP_PRUNE) {
       cand = own;
@@ -286,7 +317,7 @@ __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
       }
       logChange<T>(lg, logBase, logged, changed, ((uint32_t)slot << 9) | (uint32_t)c, out);
     }
-    finishBrick(ws, v.defNext, slot, lane, own);
+    finishBrick(ws, v.defNext, slot, lane, own, visitOut);
   }
   if (lane == 0) lg.count[warp] = logged;
 }
@@ -324,7 +355,8 @@ __device__ inline T reducedValue(const T *vals, const uint64_t *act, const int8_
 // defined cell becomes undefined with its sign.
 template <class T>
 __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
-    kUpdateRebuild(Topo t, LsView<T> v, const uint64_t *act, double cutoff, ChangeLog<T> lg) {
+    kUpdateRebuild(Topo t, LsView<T> v, const uint64_t *act, double cutoff, ChangeLog<T> lg,
+                   uint8_t *visitOut) {
   __shared__ WarpScratch sm[FRONTIER_THREADS / 32];
   WarpScratch &ws = sm[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
@@ -383,7 +415,7 @@ __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
     }
     __syncwarp();
     if (lane < 8) ws.flip[lane] |= clear;
-    finishBrick(ws, v.defNext, slot, lane, own);
+    finishBrick(ws, v.defNext, slot, lane, own, visitOut);
   }
   if (lane == 0) lg.count[warp] = logged;
 }
