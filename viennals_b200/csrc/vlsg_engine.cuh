@@ -415,7 +415,13 @@ public:
     }
     syncErr("upload");
     const long long nNeeded = hCounters[13];
-    ensureLayout(nBricks, (size_t)std::max<long long>(1024, nNeeded * 2 + 256));
+    // the pool keeps room for the band to grow: reallocate only when the
+    // allocated slots fall below 1.25x the needed ones, then to 2x
+    {
+      const size_t minSlots = (size_t)std::max<long long>(1024, nNeeded + nNeeded / 4 + 256);
+      ensureLayout(nBricks, capSlots >= minSlots ? capSlots
+                                                 : (size_t)std::max<long long>(1024, nNeeded * 2 + 256));
+    }
     {
       Scope sc(this, "upload_pool");
       kInitFreeStack<<<grid1(cap), 256, 0, stream>>>(freeStack, cap);
@@ -431,7 +437,7 @@ public:
     allocBuffers(L);
     for (int l = 0; l < L; ++l) {
       Scope sc(this, "upload_farsign");
-      kFarSignFromRuns<<<grid1(nBricks), 256, 0, stream>>>(g, nBricks, runKeys[l], ls[l].runSign,
+      kFarSignRows<<<grid1((size_t)g.nb[1] * g.nb[2]), 256, 0, stream>>>(g, runKeys[l], ls[l].runSign,
                                                            (int)ls[l].nRuns, buf[l].farSign);
       checkLaunch();
       buf[l].width = ls[l].width;

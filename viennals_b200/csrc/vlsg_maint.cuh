@@ -185,15 +185,42 @@ __device__ inline int8_t runSignAt(const uint64_t *keys, const int8_t *sign, int
   return lo == 0 ? sign[0] : sign[lo - 1];
 }
 
-__global__ void kFarSignFromRuns(GridDev g, int nBricks, const uint64_t *runKeys,
-                                 const int8_t *runSign, int nRuns, int8_t *farSign) {
-  for (int bi = blockIdx.x * blockDim.x + threadIdx.x; bi < nBricks;
-       bi += gridDim.x * blockDim.x) {
-    int bx, by, bz;
-    brickCoords(g, bi, bx, by, bz);
-    int x = g.org[0] + bx * BS + 4, y = g.org[1] + by * BS + 4, z = g.org[2] + bz * BS + 4;
-    x = mapCoord(g, 0, x), y = mapCoord(g, 1, y), z = mapCoord(g, 2, z);
-    farSign[bi] = runSignAt(runKeys, runSign, nRuns, cellKey(x, y, z)) < 0 ? -1 : 1;
+// Far signs of all bricks of one brick row (by, bz) from the runs: the sign
+// at each brick's centre cell; one binary search per row, then a walk along
+// the row (the centre cells of a row have increasing keys).  Bounded
+// directions map the centre cells (they lie inside the grid but for the
+// last, partial brick, whose centre may be mapped).
+__global__ void kFarSignRows(GridDev g, const uint64_t *runKeys, const int8_t *runSign, int nRuns,
+                             int8_t *farSign) {
+  const int rows = g.nb[1] * g.nb[2];
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
+    const int by = r % g.nb[1], bz = r / g.nb[1];
+    const int y = mapCoord(g, 1, g.org[1] + by * BS + 4), z = mapCoord(g, 2, g.org[2] + bz * BS + 4);
+    int8_t *row = farSign + (size_t)r * g.nb[0];
+    if (nRuns <= 0) {
+      for (int bx = 0; bx < g.nb[0]; ++bx) row[bx] = 1;
+      continue;
+    }
+    int j = -1, prevX = INT_MIN;
+    for (int bx = 0; bx < g.nb[0]; ++bx) {
+      const int x = mapCoord(g, 0, g.org[0] + bx * BS + 4);
+      const uint64_t key = cellKey(x, y, z);
+      if (x <= prevX || j < 0) { // first brick, or the mapping folded back: search
+        int lo = 0, hi = nRuns;
+        while (lo < hi) {
+          const int mid = (lo + hi) >> 1;
+          if (runKeys[mid] <= key) lo = mid + 1;
+          else hi = mid;
+        }
+        j = lo - 1;
+      } else {
+        while (j + 1 < nRuns && runKeys[j + 1] <= key) ++j;
+      }
+      prevX = x;
+      const int8_t s = j < 0 ? runSign[0] : runSign[j];
+      row[bx] = s < 0 ? -1 : 1;
+      if (j < 0) j = -1;
+    }
   }
 }
 
