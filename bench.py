@@ -289,6 +289,8 @@ def precision_report(args, grid, dom, vel, p, stream):
         "fp32_ms_per_step": res["fp32"]["ms_per_step"], "fp64_ms_per_step": res["fp64"]["ms_per_step"],
         "fp32_over_fp64": res["fp32"]["point_updates_per_s"] / res["fp64"]["point_updates_per_s"],
         "max_abs_dphi_over_gridDelta": r["max_abs_diff"], "rms_abs_dphi_over_gridDelta": r["rms_abs_diff"],
+        "points_with_abs_dphi_above": dict(zip(["1e-6", "1e-5", "1e-4", "1e-3"], r["diff_above"])),
+        "common_points": r["common_points"],
         "active_points_fp32": r["active_a"], "active_points_fp64": r["active_b"],
         "active_set_differences": r["active_only_a"] + r["active_only_b"],
         "defined_set_differences": r["defined_only_a"] + r["defined_only_b"],

@@ -246,6 +246,8 @@ typedef struct vlsg_compare_result {
   double chamfer_ab, chamfer_ba;        /* mean nearest-node distance a->b, b->a */
   double chamfer_mean, chamfer_rms, chamfer_max;
   int64_t chamfer_unresolved;           /* nodes with no node within 4 cells */
+  int64_t diff_above[4];                /* common points with |phi_a - phi_b| above
+                                           1e-6, 1e-5, 1e-4, 1e-3 (grid units) */
 } vlsg_compare_result;
 int vlsg_compare(vlsg_context *a, int32_t slot_a, vlsg_context *b, int32_t slot_b,
                  vlsg_compare_result *out);

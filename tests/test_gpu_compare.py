@@ -62,6 +62,7 @@ def _reference(ia, va, ib, vb):
         "chamfer_ab": float(dab.mean()), "chamfer_ba": float(dba.mean()),
         "chamfer_max": float(max(dab.max(), dba.max())),
         "chamfer_rms": float(np.sqrt((np.sum(dab ** 2) + np.sum(dba ** 2)) / (len(dab) + len(dba)))),
+        "diff_above": [int((diff > t).sum()) for t in (1e-6, 1e-5, 1e-4, 1e-3)],
     }
 
 
@@ -75,7 +76,7 @@ def test_compare_fp32_against_fp64_matches_numpy():
     ib, vb, _ = c64.download(0)
     ref = _reference(ia, va, ib, vb)
     for k in ("common_points", "defined_only_a", "defined_only_b", "active_a", "active_b",
-              "active_only_a", "active_only_b", "nodes_a", "nodes_b"):
+              "active_only_a", "active_only_b", "nodes_a", "nodes_b", "diff_above"):
         assert got[k] == ref[k], k
     assert got["points_a"] == len(va) and got["points_b"] == len(vb)
     assert got["max_abs_diff"] == ref["max_abs_diff"]

@@ -145,10 +145,13 @@ class CompareResult(ctypes.Structure):
         ("chamfer_mean", ctypes.c_double), ("chamfer_rms", ctypes.c_double),
         ("chamfer_max", ctypes.c_double),
         ("chamfer_unresolved", ctypes.c_int64),
+        ("diff_above", ctypes.c_int64 * 4),
     ]
 
     def as_dict(self):
-        return {f: getattr(self, f) for f, _ in self._fields_}
+        d = {f: getattr(self, f) for f, _ in self._fields_}
+        d["diff_above"] = list(self.diff_above)
+        return d
 
 
 VELOCITY_CALLBACK = ctypes.CFUNCTYPE(

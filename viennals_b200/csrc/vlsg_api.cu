@@ -162,6 +162,7 @@ void compareEngines(EngineBase &ea, int sa, EngineBase &eb, int sb, vlsg_compare
   std::memcpy(&mx1, &c[1].maxBits, sizeof(double));
   r->chamfer_max = std::max(mx0, mx1);
   r->chamfer_unresolved = (int64_t)(c[0].unresolved + c[1].unresolved);
+  for (int k = 0; k < 4; ++k) r->diff_above[k] = (int64_t)h[0].above[k];
 }
 
 void ensureBuilt(vlsg_context *ctx) {

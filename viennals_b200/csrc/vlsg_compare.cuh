@@ -45,6 +45,7 @@ struct CompareAcc {
   unsigned long long common;      // points defined in both (counted from A)
   unsigned long long maxDiff;     // bits of max |a - b|
   double sumSq;                   // sum of (a - b)^2
+  unsigned long long above[4];    // |a - b| above 1e-6, 1e-5, 1e-4, 1e-3
 };
 
 // Points of `a` against the sorted keys of `b`.
@@ -52,6 +53,7 @@ __global__ void kComparePoints(const uint64_t *ka, const double *va, int64_t na,
                                const uint64_t *kb, const double *vb, int64_t nb, int countCommon,
                                CompareAcc *acc) {
   unsigned long long onlyDef = 0, onlyAct = 0, act = 0, common = 0, maxBits = 0;
+  unsigned long long above[4] = {0, 0, 0, 0};
   double sq = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < na;
        i += (int64_t)gridDim.x * blockDim.x) {
@@ -72,6 +74,7 @@ __global__ void kComparePoints(const uint64_t *ka, const double *va, int64_t na,
       const unsigned long long b = orderedBits(d);
       maxBits = b > maxBits ? b : maxBits;
       sq += d * d;
+      above[0] += d > 1e-6, above[1] += d > 1e-5, above[2] += d > 1e-4, above[3] += d > 1e-3;
     }
   }
   for (int o = 16; o > 0; o >>= 1) {
@@ -82,8 +85,11 @@ __global__ void kComparePoints(const uint64_t *ka, const double *va, int64_t na,
     const unsigned long long t = __shfl_xor_sync(0xffffffffu, maxBits, o);
     maxBits = t > maxBits ? t : maxBits;
     sq += __shfl_xor_sync(0xffffffffu, sq, o);
+    for (int k = 0; k < 4; ++k) above[k] += __shfl_xor_sync(0xffffffffu, above[k], o);
   }
   if ((threadIdx.x & 31) == 0) {
+    for (int k = 0; k < 4; ++k)
+      if (above[k]) atomicAdd(&acc->above[k], above[k]);
     if (onlyDef) atomicAdd(&acc->onlyDefined, onlyDef);
     if (onlyAct) atomicAdd(&acc->onlyActive, onlyAct);
     if (act) atomicAdd(&acc->active, act);
