@@ -261,6 +261,18 @@ int vlsg_set_velocity_callback(vlsg_context *ctx, vlsg_velocity_cb cb,
 int vlsg_advect(vlsg_context *ctx, const vlsg_advect_params *params,
                 vlsg_advect_result *result);
 
+/* Batching form: advance n independent contexts (each with its own grid,
+ * level sets and velocity functor) with the same parameters.  A pool of
+ * `threads` host threads (0: min(n, 32)) drives them, each context on its own
+ * CUDA stream, so the kernels of many small domains run side by side on the
+ * GPU.  results[i] receives context i's getters; the return value is the
+ * first failing context's status (its message in vlsg_last_error(ctxs[i])).
+ * Results are bit-identical to calling vlsg_advect on each context in turn.
+ * No counterpart in Advect (one Advect per domain); it replaces the loop a
+ * caller would write over many Advect objects. */
+int vlsg_advect_batch(vlsg_context **ctxs, int32_t n, const vlsg_advect_params *params,
+                      vlsg_advect_result *results, int32_t threads);
+
 /* Timing of the last vlsg_advect: per kernel family, device milliseconds and
  * algorithmic bytes, as measured with CUDA events on the context stream
  * (filled only when profiling is switched on with vlsg_set_profiling). */

@@ -1,0 +1,105 @@
+"""The BASELINE configurations other than the bench's, at their full sizes,
+as parity cases:
+  * config 2: square-trench etch, two materials, 128 x 128 x 64 cells at
+    gridDelta 0.1, periodic in x/y, v = -1 on the substrate and 0 on the mask
+    plus -0.3 n_z, local Lax-Friedrichs 2nd order, RK3, double: the FP64 GPU
+    path against the oracle, bit for bit (defined points, values, signs,
+    time steps);
+  * config 3 at a reduced radius (the full 10M-point band is the bench's
+    workload, compared there FP32 against FP64 on the device): FP64 against
+    the oracle.
+"""
+import numpy as np
+import pytest
+
+from parity_cases import compare, params, run_gpu, run_oracle
+from viennals_b200 import BoundaryConditionEnum as BC, Grid
+from viennals_b200.geometry import trench_etch_level_sets
+from viennals_b200.velocity import FunctorVelocity
+
+pytestmark = pytest.mark.gpu
+
+
+def config2(time=0.0):
+    g = Grid([-6.4, 6.4, -6.4, 6.4, -3.2, 3.2],
+             [BC.PERIODIC_BOUNDARY, BC.PERIODIC_BOUNDARY, BC.INFINITE_BOUNDARY], 0.1)
+    mask, top = trench_etch_level_sets(g, 0.5, 4.0)
+    v = FunctorVelocity(2)
+    v.set_rate(0, 0.0)
+    v.set_rate(1, -1.0)
+    v.set_linear(1, 2, -0.3)
+    p = params(8, 2, time)  # LOCAL_LAX_FRIEDRICHS_2ND_ORDER, RUNGE_KUTTA_3RD_ORDER
+    return g, [mask, top], v, p
+
+
+def _parity(grid, lss, vel, p):
+    ols, ro = run_oracle(grid, lss, vel, p)
+    ctx, rg = run_gpu(grid, lss, vel, p)
+    assert rg.number_of_time_steps == ro.number_of_time_steps
+    assert rg.advected_time == ro.advected_time
+    assert rg.current_time_step == ro.current_time_step
+    assert rg.point_updates == ro.point_updates
+    compare(ols, ctx)
+    return ctx
+
+
+def test_config2_trench_full_size_one_step():
+    g, lss, v, p = config2(0.0)
+    ctx = _parity(g, lss, v, p)
+    n = [ctx.count(i) for i in range(2)]
+    # measured at this size: 78k defined points after the step (mask and
+    # substrate bands of width 2 over 128 x 128 columns), not the 1.5M the
+    # configuration text estimates
+    assert sum(n) > 50_000, n
+    print("config 2 defined points after one step:", n)
+
+
+def test_config3_precision_form_reduced_radius_fp64():
+    import torch
+    from viennals_b200.synth import perturbed_sphere, precision_velocity
+
+    grid, dom = perturbed_sphere(8.0, 0.05, seed=1234, device="cuda:0")[:2]
+    p = params(11, 2, 0.0, cfl=0.4)
+    _parity(grid, [dom], precision_velocity(), p)
+
+
+def test_config4_batching_form_matches_loop():
+    """Batching form (FP32, LLF1, RK2): a batch of independent trench / hole
+    domains advanced together equals advancing each alone, bit for bit."""
+    import time
+
+    from viennals_b200._abi import Precision
+    from viennals_b200.advect import Context, advect_batch
+    from viennals_b200.synth import batch_domains
+
+    doms = batch_domains(12, seed=3, points_range=(1e4, 1e5))
+    p = params(7, 1, 0.0)  # LOCAL_LAX_FRIEDRICHS_1ST_ORDER, RUNGE_KUTTA_2ND_ORDER
+
+    def contexts():
+        out = []
+        for grid, dom, vel in doms:
+            c = Context(0, Precision.FP32)
+            c.set_grid(grid)
+            c.set_level_set_count(1)
+            c.upload(0, dom)
+            c.set_velocity(vel.descriptor())
+            c.count(0)
+            out.append(c)
+        return out
+
+    loop = contexts()
+    t0 = time.perf_counter()
+    res_loop = [c.advect(p) for c in loop]
+    t_loop = time.perf_counter() - t0
+    batch = contexts()
+    t0 = time.perf_counter()
+    res_batch = advect_batch(batch, p, threads=8)
+    t_batch = time.perf_counter() - t0
+    for a, b, ca, cb in zip(res_loop, res_batch, loop, batch):
+        assert a.number_of_time_steps == b.number_of_time_steps
+        assert a.current_time_step == b.current_time_step
+        assert a.point_updates == b.point_updates
+        ia, va, _ = ca.download(0)
+        ib, vb, _ = cb.download(0)
+        assert np.array_equal(ia, ib) and np.array_equal(va, vb)
+    print(f"loop {t_loop * 1e3:.1f} ms, batch {t_batch * 1e3:.1f} ms")

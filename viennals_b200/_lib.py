@@ -43,6 +43,7 @@ def load(build_if_missing=True):
     L.vlsg_get_values.argtypes = [vp, i32, i64, P(i32), P(ctypes.c_double)]
     L.vlsg_download_runs.argtypes = [vp, i32, i64, P(i32), P(ctypes.c_int8), P(i64)]
     L.vlsg_compare.argtypes = [vp, i32, vp, i32, P(CompareResult)]
+    L.vlsg_advect_batch.argtypes = [P(vp), i32, P(AdvectParams), P(AdvectResult), i32]
     L.vlsg_get_values_noalloc.argtypes = [vp, i32, i64, P(i32), P(ctypes.c_double)]
     L.vlsg_set_velocity_functor.argtypes = [vp, P(VelocityDesc)]
     L.vlsg_set_velocity_callback.argtypes = [vp, VELOCITY_CALLBACK, vp]
@@ -59,6 +60,6 @@ EXPORTED = [
     "vlsg_set_grid", "vlsg_set_level_set_count",
     "vlsg_upload_levelset", "vlsg_count_points", "vlsg_download_levelset", "vlsg_download_runs",
     "vlsg_get_values", "vlsg_get_values_noalloc",
-    "vlsg_set_velocity_functor", "vlsg_set_velocity_callback", "vlsg_advect",
+    "vlsg_set_velocity_functor", "vlsg_set_velocity_callback", "vlsg_advect", "vlsg_advect_batch",
     "vlsg_set_profiling", "vlsg_get_kernel_stats", "vlsg_compare",
 ]

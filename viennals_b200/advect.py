@@ -187,6 +187,22 @@ class Context:
         return Domain(grid, idx, val, rs, sg, width=w)
 
 
+def advect_batch(contexts, params, threads=0):
+    """vlsg_advect_batch over a list of Contexts; returns their results."""
+    n = len(contexts)
+    handles = (ctypes.c_void_p * n)(*[c.h.value for c in contexts])
+    results = (AdvectResult * n)()
+    lib = _lib.load()
+    rc = lib.vlsg_advect_batch(handles, n, ctypes.byref(params), results, int(threads))
+    if rc != 0:
+        for c in contexts:
+            msg = lib.vlsg_last_error(c.h)
+            if msg:
+                raise RuntimeError(f"vlsg error {rc}: {msg.decode()}")
+        raise RuntimeError(f"vlsg error {rc}")
+    return list(results)
+
+
 class Advect:
     """Mirror of viennals::Advect<T,3> running on the GPU."""
 

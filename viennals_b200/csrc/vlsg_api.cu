@@ -7,6 +7,8 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
+#include <atomic>
 
 #include "vlsg_compare.cuh"
 #include "vlsg_iface.h"
@@ -458,6 +460,28 @@ int vlsg_advect(vlsg_context *ctx, const vlsg_advect_params *p, vlsg_advect_resu
     e.apply(*p, *r);
     return VLSG_OK;
   });
+}
+
+int vlsg_advect_batch(vlsg_context **ctxs, int32_t n, const vlsg_advect_params *params,
+                      vlsg_advect_result *results, int32_t threads) {
+  if (!ctxs || !params || !results || n < 0)
+    return fail(nullptr, VLSG_ERR_ARGUMENT, "vlsg_advect_batch: bad argument");
+  for (int32_t i = 0; i < n; ++i)
+    if (!ctxs[i]) return fail(nullptr, VLSG_ERR_ARGUMENT, "vlsg_advect_batch: NULL context");
+  const int nt = std::max(1, std::min<int>(threads > 0 ? threads : 32, n));
+  std::vector<int> status(n, VLSG_OK);
+  std::atomic<int> next{0};
+  auto worker = [&] {
+    for (int i = next.fetch_add(1); i < n; i = next.fetch_add(1))
+      status[i] = vlsg_advect(ctxs[i], params, &results[i]);
+  };
+  std::vector<std::thread> pool;
+  for (int t = 1; t < nt; ++t) pool.emplace_back(worker);
+  worker();
+  for (auto &th : pool) th.join();
+  for (int32_t i = 0; i < n; ++i)
+    if (status[i] != VLSG_OK) return status[i];
+  return VLSG_OK;
 }
 
 int vlsg_set_profiling(vlsg_context *ctx, int32_t on) {

@@ -146,3 +146,47 @@ def precision_velocity():
     v.set_rate(0, 1.0)
     v.set_linear(0, 2, 0.3)
     return v
+
+
+def batch_domains(n=256, seed=7, points_range=(1e4, 2e6), device=None):
+    """Inputs of the batching form: n independent planes, each with a random
+    trench or cylindrical hole (width 0.5-4.0, depth 1-8), periodic in x/y,
+    gridDelta 0.05-0.2 chosen so the band sizes spread log-uniformly over
+    `points_range`, and a constant etch rate in [0.2, 1.5].  Returns a list
+    of (grid, domain, velocity)."""
+    import numpy as np
+
+    from .geometry import sdf_box, sdf_levelset
+    from .velocity import constant_scalar
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        hole = bool(rng.integers(2))
+        width = float(rng.uniform(0.5, 4.0))
+        depth = float(rng.uniform(1.0, 8.0))
+        rate = float(rng.uniform(0.2, 1.5))
+        target = float(np.exp(rng.uniform(np.log(points_range[0]), np.log(points_range[1]))))
+        lateral = max(2.0 * width, width + 2.0)
+        # band of a plane: ~2.5 layers of (lateral / gd)^2 points, plus walls
+        walls = (4.0 if hole else 2.0) * depth / lateral
+        gd = float(np.clip(np.sqrt(2.5 * lateral * lateral * (1.0 + walls) / target), 0.05, 0.2))
+        cells = max(16, int(round(lateral / gd)))
+        half = cells * gd / 2.0
+        zlo, zhi = -depth - 1.5, 1.5
+        grid = Grid([-half, half, -half, half, zlo, zhi],
+                    [BC.PERIODIC_BOUNDARY, BC.PERIODIC_BOUNDARY, BC.INFINITE_BOUNDARY], gd)
+        r = width / 2.0
+
+        def sdf(x, y, z, hole=hole, r=r, depth=depth):
+            if hole:
+                cut = np.maximum(np.sqrt(x * x + y * y) - r, -z - depth)
+            else:
+                cut = sdf_box((x, y, z), (-r, -1e9, -depth), (r, 1e9, 1e9))
+            return np.maximum(z, -cut)
+
+        lo = [grid.min[0], grid.min[1], grid.min[2]]
+        hi = [grid.max[0] - 1, grid.max[1] - 1, grid.max[2]]
+        dom = sdf_levelset(grid, sdf, lo, hi)
+        out.append((grid, dom, constant_scalar(-rate)))
+    return out
