@@ -335,9 +335,34 @@ def _has_cuda():
         return False
 
 
-def roofline(out, peaks):
+# DRAM traffic per launch of the dominant kernel from one ncu capture of the
+# default workload (its summary sits under profiles/ with the command).
+TRAFFIC_PROFILE = {"expand": "expand_pass_dram_fp32_sphere_r40.md"}
+
+
+def default_workload(args):
+    return (args.radius == 40.0 and args.grid_delta == 0.05 and args.seed == 1234
+            and args.precision == "fp32")
+
+
+def profiled_traffic(kernel):
+    name = TRAFFIC_PROFILE.get(kernel)
+    if not name:
+        return None
+    try:
+        with open(os.path.join(ROOT, "profiles", name)) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1])
+    except OSError:
+        return None
+    return None
+
+
+def roofline(out, peaks, args=None):
     """Dominant kernel: device time share; achieved = its algorithmic bytes /
-    its average launch time."""
+    its average launch time.  traffic = ncu DRAM bytes per launch of that
+    kernel on the default workload (null for other workloads)."""
     ks = out.get("kernels") or []
     if not ks:
         return None
@@ -351,7 +376,9 @@ def roofline(out, peaks):
     total = sum(k["device_ms"] for k in ks)
     return {"bound": "hbm", "kernel": top["name"], "achieved": achieved, "peak": hbm,
             "peak_source": src, "unit": "GB/s", "frac": achieved / hbm,
-            "traffic": None, "share": top["device_ms"] / total if total else None,
+            "traffic": profiled_traffic(top["name"]) if args and default_workload(args) else None,
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, mean per launch",
+            "share": top["device_ms"] / total if total else None,
             "launch_ms": per_launch_ms}
 
 
@@ -414,7 +441,7 @@ def main():
             "dtype": "f32" if args.precision == "fp32" else "f64",
             "data": "synthetic", "config": cfg, "gpu_launches": out["launches"],
             "clocks": out["clocks"], "e2e": out.get("e2e"),
-            "roofline": roofline(out, peaks), "band_points": out["n_points"],
+            "roofline": roofline(out, peaks, args), "band_points": out["n_points"],
             "precision_report": out.get("precision_report"),
             "kernels": out.get("kernels")}
     if not args.no_cpu_baseline:

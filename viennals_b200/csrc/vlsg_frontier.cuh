@@ -104,6 +104,7 @@ struct WarpScratch {
   unsigned long long flip[8]; // cells whose definedness flips
   int nb[6];                  // face neighbours -x,+x,-y,+y,-z,+z (slot or -1-brick)
   int pad[2];
+  unsigned long long aux[8];  // a second mask of the brick (kUpdateRebuild: active cells)
   uint16_t list[BV];          // the brick's cells to evaluate, ascending
 };
 
@@ -295,7 +296,7 @@ __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
       const uint64_t dil = dilatedMask(t, v.def, slot, ws.nb, lane);
       cand = MODE == FP_EXPAND ? dil & ~own : dil;
     }
-    const int total = listCells(cand, ws.list);
+    const int total = __any_sync(0xffffffffu, cand != 0ull) ? listCells(cand, ws.list) : 0;
     for (int base = 0; base < total; base += 32) {
       const int k = base + lane;
       bool changed = false;
@@ -340,19 +341,23 @@ __global__ void __launch_bounds__(FRONTIER_THREADS)
 }
 
 // Value of a cell after Reduce(1) + update: the (updated) value of an active
-// cell, the sign sentinel of any other.
+// cell, the sign sentinel of any other.  `actHere` holds the active planes of
+// brick `slot` (shared memory); other bricks read `act`.
 template <class T>
-__device__ inline T reducedValue(const T *vals, const uint64_t *act, const int8_t *farSign,
-                                 int ref, int loc) {
+__device__ inline T reducedValue(const T *vals, const uint64_t *act, const unsigned long long *actHere,
+                                 const int8_t *farSign, int slot, int ref, int loc) {
   if (ref < 0) return sentinel<T>(farSign[-1 - ref] < 0);
   const T val = vals[(size_t)ref * BV + loc];
-  const bool a = (act[(size_t)ref * 8 + (loc >> 6)] >> (loc & 63)) & 1ull;
-  return a ? val : sentinel<T>(val < 0);
+  const uint64_t word = ref == slot ? actHere[loc >> 6] : act[(size_t)ref * 8 + (loc >> 6)];
+  return ((word >> (loc & 63)) & 1ull) ? val : sentinel<T>(val < 0);
 }
 
 // rebuildLS after updateLevelSet (the active values are already updated in
 // place): candidates are the active cells and their neighbours; every other
-// defined cell becomes undefined with its sign.
+// defined cell becomes undefined with its sign.  Those cells are neither
+// active nor candidates, so no evaluation in this pass reads more than their
+// sign, which the sentinel keeps: they are rewritten in place, and only the
+// candidates' new values go through the change log.
 template <class T>
 __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
     kUpdateRebuild(Topo t, LsView<T> v, const uint64_t *act, double cutoff, ChangeLog<T> lg,
@@ -368,6 +373,7 @@ __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
   const RebuildRule<T> rule{cutoff};
   for (int w = warp; w < n; w += nWarps) {
     const int slot = t.slotList[w];
+    if (lane < 8) ws.aux[lane] = act[(size_t)slot * 8 + lane];
     beginBrick(t, ws, slot, lane);
     const bool complex = (t.cflag[slot] & CF_STAR) != 0;
     int x0 = 0, y0 = 0, z0 = 0;
@@ -377,7 +383,7 @@ __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
     if (complex) cand = lane < 8 ? existPlane(t.g, x0, y0, z0, lane) : 0ull;
     else cand = dilatedMask(t, act, slot, ws.nb, lane);
     const uint64_t clear = own & ~cand;
-    int total = listCells(cand, ws.list);
+    const int total = listCells(cand, ws.list);
     for (int base = 0; base < total; base += 32) {
       const int k = base + lane;
       bool changed = false;
@@ -386,13 +392,13 @@ __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
       if (k < total) {
         c = ws.list[k];
         const T mem = v.vals[(size_t)slot * BV + c];
-        const T center = reducedValue<T>(v.vals, act, v.farSign, slot, c);
+        const T center = ((ws.aux[c >> 6] >> (c & 63)) & 1ull) ? mem : sentinel<T>(mem < 0);
         T nb[6];
 #pragma unroll
         for (int j = 0; j < 6; ++j) {
           int loc;
           const int ref = starRef(t, ws.nb, slot, complex, x0, y0, z0, c, j, loc);
-          nb[j] = reducedValue<T>(v.vals, act, v.farSign, ref, loc);
+          nb[j] = reducedValue<T>(v.vals, act, ws.aux, v.farSign, slot, ref, loc);
         }
         out = rule(center, nb);
         changed = out != mem || signbit(out) != signbit(mem);
@@ -400,18 +406,18 @@ __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
       }
       logChange<T>(lg, logBase, logged, changed, ((uint32_t)slot << 9) | (uint32_t)c, out);
     }
-    // defined cells away from the active ones: undefined with their sign
+    // defined cells away from the active ones: undefined with their sign,
+    // written in place (32 consecutive cells per step)
     __syncwarp();
-    total = listCells(clear, ws.list);
-    for (int base = 0; base < total; base += 32) {
-      const int k = base + lane;
-      T out = T(0);
-      int c = 0;
-      if (k < total) {
-        c = ws.list[k];
-        out = sentinel<T>(v.vals[(size_t)slot * BV + c] < 0);
-      }
-      logChange<T>(lg, logBase, logged, k < total, ((uint32_t)slot << 9) | (uint32_t)c, out);
+    if (lane < 8) ws.aux[lane] = clear;
+    __syncwarp();
+    T *bv = v.vals + (size_t)slot * BV;
+#pragma unroll 2
+    for (int i = 0; i < 16; ++i) {
+      const uint64_t word = ws.aux[i >> 1];
+      if (!word) continue;
+      const int c = i * 32 + lane;
+      if ((word >> (c & 63)) & 1ull) bv[c] = sentinel<T>(bv[c] < 0);
     }
     __syncwarp();
     if (lane < 8) ws.flip[lane] |= clear;
