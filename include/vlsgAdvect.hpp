@@ -84,9 +84,52 @@ struct VelocityFunctor {
   }
 };
 
+// viennals::VelocityField<T> (lsVelocityField.hpp:11-41) for user code: the
+// library asks it through its host callback, in batches of points and from
+// several threads at once (as the reference calls it from OpenMP threads,
+// lsAdvect.hpp:464), so overrides must be thread-safe.  The coordinate is
+// index * gridDelta, the point id the point's rank among the defined points
+// of the expanded top level set in HRLE order.
+template <class T> class VelocityField {
+public:
+  virtual ~VelocityField() = default;
+  virtual T getScalarVelocity(const std::array<T, 3> & /*coordinate*/, int /*material*/,
+                              const std::array<T, 3> & /*normalVector*/,
+                              unsigned long /*pointId*/) {
+    return 0;
+  }
+  virtual std::array<T, 3> getVectorVelocity(const std::array<T, 3> & /*coordinate*/,
+                                             int /*material*/,
+                                             const std::array<T, 3> & /*normalVector*/,
+                                             unsigned long /*pointId*/) {
+    return {0, 0, 0};
+  }
+
+  // vlsg_velocity_cb trampoline (user = the field)
+  static int callback(void *user, int64_t n, const double *coords, const int32_t *materials,
+                      const double *normals, const uint64_t *pointIds, double *scalarOut,
+                      double *vectorOut) {
+    auto *f = static_cast<VelocityField<T> *>(user);
+    try {
+      for (int64_t i = 0; i < n; ++i) {
+        const std::array<T, 3> c{T(coords[3 * i]), T(coords[3 * i + 1]), T(coords[3 * i + 2])};
+        const std::array<T, 3> nv{T(normals[3 * i]), T(normals[3 * i + 1]), T(normals[3 * i + 2])};
+        const unsigned long id = (unsigned long)pointIds[i];
+        scalarOut[i] = (double)f->getScalarVelocity(c, materials[i], nv, id);
+        const std::array<T, 3> v = f->getVectorVelocity(c, materials[i], nv, id);
+        for (int k = 0; k < 3; ++k) vectorOut[3 * i + k] = (double)v[k];
+      }
+    } catch (...) {
+      return 1;
+    }
+    return 0;
+  }
+};
+
 template <class T> class Advect {
   std::vector<std::shared_ptr<LevelSet>> levelSets;
   std::shared_ptr<VelocityFunctor> velocities;
+  std::shared_ptr<VelocityField<T>> field; // host callback mode when set
   vlsg_advect_params params{};
   vlsg_advect_result result{};
   vlsg_context *ctx = nullptr;
@@ -120,7 +163,8 @@ public:
   void setDevice(int d) { device = d; }
   void insertNextLevelSet(std::shared_ptr<LevelSet> ls) { levelSets.push_back(ls); }
   void clearLevelSets() { levelSets.clear(); }
-  void setVelocityField(std::shared_ptr<VelocityFunctor> v) { velocities = v; }
+  void setVelocityField(std::shared_ptr<VelocityFunctor> v) { velocities = v, field.reset(); }
+  void setVelocityField(std::shared_ptr<VelocityField<T>> f) { field = f, velocities.reset(); }
   void setAdvectionTime(double t) { params.advection_time = t; }
   void setSingleStep(bool b) { params.single_step = b; }
   void setTimeStepRatio(const double &cfl) { params.time_step_ratio = cfl; }
@@ -147,7 +191,8 @@ public:
   // Advect::apply, lsAdvect.hpp:1017-1043
   void apply() {
     if (levelSets.empty()) return logError("No level sets passed to Advect. Not advecting.");
-    if (!velocities) return logError("No velocity field passed to Advect. Not advecting.");
+    if (!velocities && !field)
+      return logError("No velocity field passed to Advect. Not advecting.");
     if (!ctx) {
       const int precision = sizeof(T) == 4 ? VLSG_FP32 : VLSG_FP64;
       if (!check(vlsg_create(&ctx, device, precision))) return;
@@ -163,7 +208,11 @@ public:
                                       ls.runStart.data(), ls.runSign.data(), ls.width)))
         return;
     }
-    if (!check(vlsg_set_velocity_functor(ctx, &velocities->desc))) return;
+    if (field) {
+      if (!check(vlsg_set_velocity_callback(ctx, &VelocityField<T>::callback, field.get()))) return;
+    } else if (!check(vlsg_set_velocity_functor(ctx, &velocities->desc))) {
+      return;
+    }
     if (!check(vlsg_advect(ctx, &params, &result))) return;
     for (size_t i = 0; i < levelSets.size(); ++i) {
       LevelSet &ls = *levelSets[i];

@@ -47,6 +47,55 @@ inline void vectorVelocity(const vlsg_velocity_desc &v, int material,
   for (int k = 0; k < 3; ++k) out[k] = v.vec[m][k];
 }
 
+// The velocity of one evaluation: the functor of vlsg.h, or a host callback
+// (VelocityField::getScalarVelocity and getVectorVelocity,
+// lsVelocityField.hpp:17-30) asked one point at a time with the coordinate
+// (index * gridDelta), the material, the normal and the point id the
+// reference passes.  A callback failure is recorded and reported after the
+// parallel loop that met it.
+struct VelSource {
+  vlsg_velocity_desc desc{};
+  vlsg_velocity_cb cb = nullptr;
+  void *user = nullptr;
+  mutable std::atomic<int> failed{0};
+  VelSource() = default;
+  VelSource(const VelSource &o) : desc(o.desc), cb(o.cb), user(o.user) {}
+  void query(const double coord[3], int material, const double n[3], uint64_t pointId,
+             double &scalar, double vec[3]) const {
+    if (!cb) {
+      scalar = scalarVelocity(desc, material, n);
+      vectorVelocity(desc, material, vec);
+      return;
+    }
+    const int32_t m = material;
+    if (cb(user, 1, coord, &m, n, &pointId, &scalar, vec) != 0) {
+      failed = 1;
+      scalar = 0;
+      vec[0] = vec[1] = vec[2] = 0;
+    }
+  }
+  void check() const {
+    if (failed) throw std::runtime_error("the velocity callback failed");
+  }
+};
+
+// Point id of every map entry: its rank among the defined points in HRLE
+// order (the id viennahrle's iterators report, lsAdvect.hpp:169).
+template <int D> std::vector<uint64_t> pointIds(const LS<D> &t) {
+  std::vector<uint64_t> id(t.keys.size());
+  uint64_t k = 0;
+  for (size_t i = 0; i < t.keys.size(); ++i) {
+    id[i] = k;
+    if (isDefined(t.vals[i])) ++k;
+  }
+  return id;
+}
+
+template <int D> void coordinateOf(const Grid<D> &g, uint64_t key, double c[3]) {
+  c[0] = c[1] = c[2] = 0.;
+  for (int d = 0; d < D; ++d) c[d] = double(coordOf<D>(key, d)) * g.delta;
+}
+
 struct Params {
   int spatial = VLSG_ENGQUIST_OSHER_1ST_ORDER;
   int temporal = VLSG_FORWARD_EULER;
@@ -175,7 +224,7 @@ inline double weno5(const double *x, double dx, bool plus, double eps = 1e-6) {
 template <int D> struct SchemeCtx {
   const LS<D> &top;
   const Params &P;
-  const vlsg_velocity_desc &vel;
+  const VelSource &vel;
   const double *globalAlphas; // LF: findGlobalAlphas result
 };
 
@@ -183,13 +232,15 @@ template <int D> struct SchemeCtx {
 // `alphas` accumulates finalAlphas of LLF / LLLF.
 template <int D>
 std::pair<double, double> evalScheme(const SchemeCtx<D> &S, uint64_t key,
-                                     int material, double *alphas) {
+                                     uint64_t pointId, int material, double *alphas) {
   const LS<D> &ls = S.top;
   const Grid<D> &g = ls.grid;
   const double gridDelta = g.delta;
   const int sch = S.P.spatial;
   auto V = [&](int d, int off) { return ls.at(shiftKey<D>(g, key, d, off)); };
   const double C = ls.at(key);
+  double coordinate[3];
+  coordinateOf<D>(g, key, coordinate);
 
   if (sch == VLSG_WENO_3RD_ORDER || sch == VLSG_WENO_5TH_ORDER) {
     // lsWENO.hpp:53-160
@@ -228,9 +279,8 @@ std::pair<double, double> evalScheme(const SchemeCtx<D> &S, uint64_t key,
         for (int i = 0; i < D; ++i) n[i] *= denominator;
       }
     }
-    const double scalarVel = scalarVelocity(S.vel, material, n);
-    double vv[3];
-    vectorVelocity(S.vel, material, vv);
+    double scalarVel, vv[3];
+    S.vel.query(coordinate, material, n, pointId, scalarVel, vv);
     if (scalarVel > 0)
       vel_grad += std::sqrt(gradPosTotal) * scalarVel;
     else
@@ -277,9 +327,8 @@ std::pair<double, double> evalScheme(const SchemeCtx<D> &S, uint64_t key,
       denominator = 1. / std::sqrt(denominator);
       for (int i = 0; i < D; ++i) n[i] *= denominator;
     }
-    const double sv = scalarVelocity(S.vel, material, n);
-    double vv[3];
-    vectorVelocity(S.vel, material, vv);
+    double sv, vv[3];
+    S.vel.query(coordinate, material, n, pointId, sv, vv);
     if (sv > 0)
       vel_grad += std::sqrt(gradPosTotal) * sv;
     else
@@ -319,9 +368,8 @@ std::pair<double, double> evalScheme(const SchemeCtx<D> &S, uint64_t key,
     normalModulus = 1. / std::sqrt(normalModulus);
     for (int i = 0; i < D; ++i) n[i] *= normalModulus;
   }
-  const double sv = scalarVelocity(S.vel, material, n);
-  double vv[3];
-  vectorVelocity(S.vel, material, vv);
+  double sv, vv[3];
+  S.vel.query(coordinate, material, n, pointId, sv, vv);
   double totalGrad = 0.;
   if (sv != 0.) totalGrad = sv * std::sqrt(grad);
   for (int w = 0; w < D; w++) {
@@ -373,9 +421,10 @@ std::pair<double, double> evalScheme(const SchemeCtx<D> &S, uint64_t key,
     }
     nm = 1. / std::sqrt(nm);
     for (int dir = 0; dir < D; ++dir) normal[dir] *= nm;
-    const double scaVel = scalarVelocity(S.vel, material, normal);
-    double vecVel[3];
-    vectorVelocity(S.vel, material, vecVel);
+    double coords[3] = {0, 0, 0};
+    for (int dir = 0; dir < D; ++dir) coords[dir] = coordinate[dir] + nIdx[dir] * gridDelta;
+    double scaVel, vecVel[3];
+    S.vel.query(coords, material, normal, pointId, scaVel, vecVel);
     for (int dir = 0; dir < D; ++dir) {
       const double tempAlpha = std::abs((scaVel + vecVel[dir]) * normal[dir]);
       alpha[dir] = stdMax(alpha[dir], tempAlpha);
@@ -402,7 +451,7 @@ struct RateEntry {
 template <int D> struct Advector {
   std::vector<LS<D>> &lss; // bottom .. top
   Params P;
-  vlsg_velocity_desc vel;
+  VelSource vel;
   std::vector<LS<D>> initial;
   double currentTimeStep = -1.;
   uint64_t pointUpdates = 0;
@@ -413,7 +462,7 @@ template <int D> struct Advector {
   std::vector<int64_t> rateStart;
   std::vector<RateEntry> rates;
 
-  Advector(std::vector<LS<D>> &l, const Params &p, const vlsg_velocity_desc &v)
+  Advector(std::vector<LS<D>> &l, const Params &p, const VelSource &v)
       : lss(l), P(p), vel(v) {}
 
   LS<D> &top() { return lss.back(); }
@@ -424,6 +473,7 @@ template <int D> struct Advector {
     for (int i = 0; i < D; ++i) finalAlphas[i] = 0;
     const int nt = omp_get_max_threads();
     std::vector<std::array<double, 3>> loc(nt, std::array<double, 3>{0, 0, 0});
+    const std::vector<uint64_t> ids = vel.cb ? pointIds<D>(t) : std::vector<uint64_t>();
 #pragma omp parallel for schedule(static)
     for (int64_t p = 0; p < (int64_t)t.keys.size(); ++p) {
       const double value = t.vals[p];
@@ -442,9 +492,9 @@ template <int D> struct Advector {
           }
           normalModulus = 1. / std::sqrt(normalModulus);
           for (int i = 0; i < D; ++i) normal[i] *= normalModulus;
-          const double scaVel = scalarVelocity(vel, lower, normal);
-          double vecVel[3];
-          vectorVelocity(vel, lower, vecVel);
+          double coords[3], scaVel, vecVel[3];
+          coordinateOf<D>(t.grid, key, coords);
+          vel.query(coords, lower, normal, vel.cb ? ids[p] : 0, scaVel, vecVel);
           for (int i = 0; i < D; ++i) {
             const double tempAlpha = std::abs((scaVel + vecVel[i]) * normal[i]);
             la[i] = stdMax(la[i], tempAlpha);
@@ -453,6 +503,7 @@ template <int D> struct Advector {
         }
       }
     }
+    vel.check();
     for (auto &la : loc)
       for (int i = 0; i < D; ++i) finalAlphas[i] = stdMax(finalAlphas[i], la[i]);
   }
@@ -477,6 +528,7 @@ template <int D> struct Advector {
     std::vector<double> tmin(nt, maxTimeStep);
     std::vector<std::array<double, 3>> alp(nt, std::array<double, 3>{0, 0, 0});
     const SchemeCtx<D> S{t, P, vel, globalAlphas};
+    const std::vector<uint64_t> ids = vel.cb ? pointIds<D>(t) : std::vector<uint64_t>();
     const double adaptiveFactor = 1.0 / P.adaptiveSubdivisions;
 #pragma omp parallel for schedule(static)
     for (int64_t a = 0; a < n; ++a) {
@@ -491,7 +543,7 @@ template <int D> struct Advector {
         std::pair<double, double> gd{0., 0.};
         for (int lower = 0; lower < L; ++lower) {
           if (lss[lower].at(key) <= value + Params::wrappingLayerEpsilon) {
-            gd = evalScheme<D>(S, key, lower, alp[th].data());
+            gd = evalScheme<D>(S, key, vel.cb ? ids[activePos[a]] : 0, lower, alp[th].data());
             break;
           }
         }
@@ -532,6 +584,7 @@ template <int D> struct Advector {
       chainLen[a] = len;
       if (maxStepTime < tmin[th]) tmin[th] = maxStepTime;
     }
+    vel.check();
     double tempMax = maxTimeStep;
     for (int i = 0; i < nt; ++i)
       if (tmin[i] < tempMax) tempMax = tmin[i];

@@ -64,12 +64,12 @@ vlso::Params toParams(const vlsg_advect_params *p) {
 
 template <int D>
 int advectD(Handle **hs, int n, const vlsg_advect_params *p,
-            const vlsg_velocity_desc *v, vlsg_advect_result *r) {
+            const vlso::VelSource &v, vlsg_advect_result *r) {
   if (p->ignore_voids) throw std::runtime_error("ignoreVoids is not supported");
   std::vector<vlso::LS<D>> lss;
   lss.reserve(n);
   for (int i = 0; i < n; ++i) lss.push_back(get<D>(hs[i]));
-  vlso::Advector<D> adv(lss, toParams(p), *v);
+  vlso::Advector<D> adv(lss, toParams(p), v);
   adv.apply(*r);
   for (int i = 0; i < n; ++i) get<D>(hs[i]) = lss[i];
   return 0;
@@ -240,7 +240,24 @@ int vlso_advect(void **lss, int n, const vlsg_advect_params *p,
   auto **hs = reinterpret_cast<Handle **>(lss);
   return guarded([&] {
     if (n < 1) throw std::runtime_error("no level sets");
-    return hs[0]->D == 2 ? advectD<2>(hs, n, p, v, r) : advectD<3>(hs, n, p, v, r);
+    vlso::VelSource vs;
+    vs.desc = *v;
+    return hs[0]->D == 2 ? advectD<2>(hs, n, p, vs, r) : advectD<3>(hs, n, p, vs, r);
+  });
+}
+
+// The same with a host velocity callback (called one point at a time, from
+// the OpenMP threads).
+int vlso_advect_cb(void **lss, int n, const vlsg_advect_params *p, vlsg_velocity_cb cb,
+                   void *user, vlsg_advect_result *r) {
+  auto **hs = reinterpret_cast<Handle **>(lss);
+  return guarded([&] {
+    if (n < 1) throw std::runtime_error("no level sets");
+    if (!cb) throw std::runtime_error("no velocity callback");
+    vlso::VelSource vs;
+    vs.cb = cb;
+    vs.user = user;
+    return hs[0]->D == 2 ? advectD<2>(hs, n, p, vs, r) : advectD<3>(hs, n, p, vs, r);
   });
 }
 

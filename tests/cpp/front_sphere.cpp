@@ -1,12 +1,22 @@
 // Drives libvlsgpu through the C++ front (include/vlsgAdvect.hpp) the way a
 // ViennaLS user drives viennals::Advect: a sphere (MakeGeometry::makeSphere's
 // distance rule, lsMakeGeometry.hpp:177-241) grown with a constant scalar
-// velocity.  Prints steps, advected time, point count and a checksum.
+// velocity -- the device functor, or with a second argument "callback" the
+// same velocity as a host VelocityField.  Prints steps, advected time, point
+// count and a checksum.
 #include <cmath>
 #include <cstdio>
 #include <limits>
+#include <string>
 
 #include "vlsgAdvect.hpp"
+
+struct UnitVelocity : vlsg::VelocityField<double> {
+  double getScalarVelocity(const std::array<double, 3> &, int, const std::array<double, 3> &,
+                           unsigned long) override {
+    return 1.0;
+  }
+};
 
 int main(int argc, char **argv) {
   const double gd = 0.25, radius = 5.0;
@@ -61,6 +71,8 @@ int main(int argc, char **argv) {
   auto vel = std::make_shared<vlsg::VelocityFunctor>(1);
   vel->rate(0, 1.0);
   vlsg::Advect<double> advect(ls, vel);
+  if (argc > 2 && std::string(argv[2]) == "callback")
+    advect.setVelocityField(std::make_shared<UnitVelocity>());
   advect.setSpatialScheme(vlsg::SpatialSchemeEnum::ENGQUIST_OSHER_1ST_ORDER);
   advect.setTemporalScheme(vlsg::TemporalSchemeEnum::FORWARD_EULER);
   advect.setTimeStepRatio(0.5);

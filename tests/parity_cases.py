@@ -63,7 +63,11 @@ def run_gpu(grid, level_sets, velocity, p, precision=0, profile=False):
     ctx.set_level_set_count(len(level_sets))
     for i, d in enumerate(level_sets):
         ctx.upload(i, d)
-    ctx.set_velocity(velocity.descriptor())
+    desc = velocity.descriptor()
+    if desc is None:  # a host velocity field: callback mode
+        ctx.set_velocity_callback(velocity)
+    else:
+        ctx.set_velocity(desc)
     if profile:
         ctx.set_profiling(True)
     res = ctx.advect(p)

@@ -41,3 +41,13 @@ def test_cpp_front_matches_python_front(tmp_path):
     assert int(vals["points"]) == len(val)
     assert int(vals["width"]) == w
     assert abs(float(vals["checksum"]) - s) <= 1e-9 * abs(s)
+
+
+@pytest.mark.gpu
+def test_cpp_front_host_velocity_field(tmp_path):
+    """The same run with the velocity as a C++ VelocityField (host callback)."""
+    exe = str(tmp_path / "front_sphere")
+    build_front(exe)
+    a = subprocess.check_output([exe, "2.0"], text=True)
+    b = subprocess.check_output([exe, "2.0", "callback"], text=True)
+    assert a == b

@@ -114,6 +114,11 @@ class Context:
     def set_velocity(self, desc):
         self._check(self.lib.vlsg_set_velocity_functor(self.h, ctypes.byref(desc)))
 
+    def set_velocity_callback(self, field):
+        """Host callback mode: `field` is a VelocityField (its c_callback())."""
+        self._velocity_field = field  # keeps the function pointer alive
+        self._check(self.lib.vlsg_set_velocity_callback(self.h, field.c_callback(), None))
+
     def advect(self, params):
         res = AdvectResult()
         self._check(self.lib.vlsg_advect(self.h, ctypes.byref(params), ctypes.byref(res)))
@@ -301,8 +306,6 @@ class Advect:
         if self.velocities is None:
             raise RuntimeError("No velocity field passed to Advect. Not advecting.")
         desc = self.velocities.descriptor()
-        if desc is None:
-            raise RuntimeError("the velocity field must be a FunctorVelocity on the GPU")
         if self.ctx is None:
             self.ctx = Context(self.device, self.precision)
         key = [id(d) for d in self.levelSets]
@@ -313,7 +316,10 @@ class Advect:
             self.ctx.set_level_set_count(len(self.levelSets))
             for i, d in enumerate(self.levelSets):
                 self.ctx.upload(i, d)
-        self.ctx.set_velocity(desc)
+        if desc is not None:
+            self.ctx.set_velocity(desc)
+        else:
+            self.ctx.set_velocity_callback(self.velocities)
 
     def apply(self):
         """Advect::apply, lsAdvect.hpp:1017-1043; results written back."""

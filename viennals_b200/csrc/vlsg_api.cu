@@ -27,6 +27,8 @@ struct vlsg_context {
   bool dirty = true;
   bool hasVel = false;
   vlsg_velocity_desc vel{};
+  vlsg_velocity_cb velCb = nullptr; // host callback mode when set
+  void *velUser = nullptr;
   bool profiling = false;
   std::unique_ptr<EngineBase> eng; // Engine<double> or Engine<float>
 };
@@ -429,15 +431,18 @@ int vlsg_set_velocity_functor(vlsg_context *ctx, const vlsg_velocity_desc *v) {
   if (v->n_materials < 1 || v->n_materials > VLSG_MAX_MATERIALS)
     return fail(ctx, VLSG_ERR_ARGUMENT, "n_materials out of range");
   ctx->vel = *v;
+  ctx->velCb = nullptr;
+  ctx->velUser = nullptr;
   ctx->hasVel = true;
   return VLSG_OK;
 }
 
 int vlsg_set_velocity_callback(vlsg_context *ctx, vlsg_velocity_cb cb, void *user) {
-  (void)cb;
-  (void)user;
-  return fail(ctx, VLSG_ERR_ARGUMENT,
-              "host velocity callbacks are not supported by this build; use a device functor");
+  if (!ctx || !cb) return fail(ctx, VLSG_ERR_ARGUMENT, "bad argument");
+  ctx->velCb = cb;
+  ctx->velUser = user;
+  ctx->hasVel = true;
+  return VLSG_OK;
 }
 
 int vlsg_advect(vlsg_context *ctx, const vlsg_advect_params *p, vlsg_advect_result *r) {
@@ -455,6 +460,8 @@ int vlsg_advect(vlsg_context *ctx, const vlsg_advect_params *p, vlsg_advect_resu
     ensureBuilt(ctx);
     EngineBase &e = *ctx->eng;
     e.vel = ctx->vel;
+    e.velCb = ctx->velCb;
+    e.velUser = ctx->velUser;
     e.profiling = ctx->profiling;
     if (ctx->profiling) e.timers.clear();
     e.apply(*p, *r);

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <cmath>
 #include <cstring>
@@ -15,6 +16,7 @@
 #include <limits>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "vlsg_common.cuh"
@@ -25,6 +27,7 @@
 #include "vlsg_maint.cuh"
 #include "vlsg_passes.cuh"
 #include "vlsg_rates.cuh"
+#include "vlsg_velcb.cuh"
 
 namespace vlsg {
 namespace { // internal linkage: every compilation unit has its own copy
@@ -108,7 +111,14 @@ public:
   };
   enum { X_FLAGS, X_POS, X_OB, X_BOUNDS, X_C, X_P, X_SUMS, X_BOX, X_IDX, X_VAL, X_GC, X_GE,
          X_ROWC, X_ROWG, X_PB, X_GB, X_RSTART, X_RSIGN, X_RPB, X_KEEP, X_KPOS, X_OSTART,
-         X_OSIGN, X_COUNT };
+         X_OSIGN, X_VCNT, X_VOFF, X_VSUMS, X_QC, X_QM, X_QN, X_QP, X_VS, X_VV, X_COUNT };
+  // pinned host staging of the velocity callback's queries and answers
+  struct PinScratch {
+    void *p = nullptr;
+    size_t bytes = 0;
+  };
+  enum { H_QC, H_QM, H_QN, H_QP, H_VS, H_VV, H_COUNT };
+  PinScratch hs[H_COUNT];
   Scratch xs[X_COUNT];
   uint64_t generation = 0;
   int xBuf = -1;
@@ -119,6 +129,8 @@ public:
     release();
     for (auto &x : xs)
       if (x.p) cudaFree(x.p);
+    for (auto &h : hs)
+      if (h.p) cudaFreeHost(h.p);
   }
 
   void release() {
@@ -764,9 +776,11 @@ public:
     VLSG_CUDA(cudaMemsetAsync(rateCounts, 0, 2 * sizeof(unsigned long long), stream));
     if (globalLF) {
       A.alphaMax = scal + 1;
+      if (velCb) gatherVelocities<1>(A);
       {
         Scope sc(this, "global_alphas");
-        kRates<T, 1><<<blocksRate, RATE_THREADS, 0, stream>>>(A, vel);
+        if (velCb) kRates<T, 1, true><<<blocksRate, RATE_THREADS, 0, stream>>>(A, vel);
+        else kRates<T, 1><<<blocksRate, RATE_THREADS, 0, stream>>>(A, vel);
         checkLaunch();
       }
       VLSG_CUDA(cudaMemcpyAsync(pinScal, scal, sizeof(init), cudaMemcpyDeviceToHost, stream));
@@ -783,6 +797,7 @@ public:
     } else {
       A.alphaMax = nullptr;
     }
+    if (velCb) gatherVelocities<0>(A);
     {
       // stencil input (each band value once) + output per active point
       Scope sc(this, "rates", [this] {
@@ -790,7 +805,8 @@ public:
         lastBand = (int64_t)readU64(rateCounts + 1);
         return double(sizeof(T)) * double(lastBand + lastActive);
       });
-      kRates<T, 0><<<blocksRate, RATE_THREADS, 0, stream>>>(A, vel);
+      if (velCb) kRates<T, 0, true><<<blocksRate, RATE_THREADS, 0, stream>>>(A, vel);
+      else kRates<T, 0><<<blocksRate, RATE_THREADS, 0, stream>>>(A, vel);
       checkLaunch();
     }
     VLSG_CUDA(cudaMemcpyAsync(pinScal, scal, sizeof(init), cudaMemcpyDeviceToHost, stream));
@@ -822,6 +838,79 @@ public:
     if (tempMax < maxTimeStep) maxTimeStep = tempMax;
     currentTimeStep = maxTimeStep;
     return maxTimeStep;
+  }
+
+  // Host callback mode: the queries of rate pass MODE (every active point x
+  // material x site), answered by the callback from a pool of host threads,
+  // become A's velocity table.
+  template <int MODE> void gatherVelocities(RateArgs<T> &A) {
+    Scope sc(this, "velocity_callback");
+    const int top = L - 1;
+    const int nList = readI32(nSlotsPtr());
+    uint32_t *cnt = scratch<uint32_t>(X_VCNT, nList);
+    uint32_t *off = scratch<uint32_t>(X_VOFF, nList);
+    uint32_t *sums = scratch<uint32_t>(X_VSUMS, scanScratch((size_t)nList) + 64);
+    kActiveCount<T><<<blocksRate, RATE_THREADS, 0, stream>>>(A, cnt);
+    checkLaunch();
+    scanExclusive(cnt, off, nList, sums);
+    const size_t nAct = scanTotal(sums, nList);
+    const int sites = velocitySites(A.scheme, MODE);
+    const size_t nQ = nAct * (size_t)L * sites;
+    if (nQ > ((size_t)1 << 28))
+      throw CudaError("velocity callback: more than 2^28 queries in one rate pass",
+                      VLSG_ERR_CAPACITY);
+    xBuf = -1; // the point layout below reuses the exchange's scratch
+    pointLayout(top, nList);
+    const PointRanks R{slotBrick, (const uint32_t *)xs[X_POS].p, (const int4 *)xs[X_BOUNDS].p,
+                       (const uint32_t *)xs[X_P].p, buf[top].def[buf[top].cur]};
+    double *qc = scratch<double>(X_QC, 3 * nQ);
+    int32_t *qm = scratch<int32_t>(X_QM, nQ);
+    double *qn = scratch<double>(X_QN, 3 * nQ);
+    uint64_t *qp = scratch<uint64_t>(X_QP, nQ);
+    double *vs = scratch<double>(X_VS, nQ);
+    double *vv = scratch<double>(X_VV, 3 * nQ);
+    A.actOff = off;
+    A.velS = vs;
+    A.velV = vv;
+    A.velSites = sites;
+    if (!nQ) return;
+    kVelGather<T, MODE><<<blocksRate, RATE_THREADS, 0, stream>>>(A, R, sites, qc, qm, qn, qp);
+    checkLaunch();
+    double *hc = pinned<double>(H_QC, 3 * nQ);
+    int32_t *hm = pinned<int32_t>(H_QM, nQ);
+    double *hn = pinned<double>(H_QN, 3 * nQ);
+    uint64_t *hp = pinned<uint64_t>(H_QP, nQ);
+    double *hsv = pinned<double>(H_VS, nQ);
+    double *hvv = pinned<double>(H_VV, 3 * nQ);
+    VLSG_CUDA(cudaMemcpyAsync(hc, qc, 3 * nQ * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    VLSG_CUDA(cudaMemcpyAsync(hm, qm, nQ * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+    VLSG_CUDA(cudaMemcpyAsync(hn, qn, 3 * nQ * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    VLSG_CUDA(cudaMemcpyAsync(hp, qp, nQ * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream));
+    syncErr("velocity queries");
+    const size_t chunk = 4096;
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int nt = (int)std::min<size_t>(std::max(1u, std::min(hw, 64u)), (nQ + chunk - 1) / chunk);
+    std::atomic<size_t> next{0};
+    std::atomic<int> failed{0};
+    auto worker = [&] {
+      for (size_t i = next.fetch_add(chunk); i < nQ && !failed.load(); i = next.fetch_add(chunk)) {
+        const int64_t n = (int64_t)std::min(chunk, nQ - i);
+        const int rc = velCb(velUser, n, hc + 3 * i, hm + i, hn + 3 * i, hp + i, hsv + i, hvv + 3 * i);
+        if (rc != 0) {
+          int zero = 0;
+          failed.compare_exchange_strong(zero, rc);
+        }
+      }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto &th : pool) th.join();
+    if (failed)
+      throw CudaError("the velocity callback returned " + std::to_string(failed.load()),
+                      VLSG_ERR_CALLBACK);
+    VLSG_CUDA(cudaMemcpyAsync(vs, hsv, nQ * sizeof(double), cudaMemcpyHostToDevice, stream));
+    VLSG_CUDA(cudaMemcpyAsync(vv, hvv, 3 * nQ * sizeof(double), cudaMemcpyHostToDevice, stream));
   }
 
   void adjustLowerLayers(const vlsg_advect_params &P) {
@@ -966,6 +1055,18 @@ public:
   }
 
   // ------------------------------------------------------------ exchange
+  template <class V> V *pinned(int k, size_t n) {
+    const size_t bytes = std::max<size_t>(n, 1) * sizeof(V);
+    if (hs[k].bytes < bytes) {
+      if (hs[k].p) VLSG_CUDA(cudaFreeHost(hs[k].p));
+      hs[k].p = nullptr;
+      hs[k].bytes = 0;
+      const size_t grown = bytes + bytes / 4;
+      VLSG_CUDA(cudaHostAlloc(&hs[k].p, grown, cudaHostAllocDefault));
+      hs[k].bytes = grown;
+    }
+    return (V *)hs[k].p;
+  }
   template <class V> V *scratch(int k, size_t n) {
     const size_t bytes = std::max<size_t>(n, 1) * sizeof(V);
     if (xs[k].bytes < bytes) {
@@ -1002,10 +1103,10 @@ public:
 
   // Points (HRLE order) and runs of buffer b on the device, in the scratch
   // arrays X_IDX / X_VAL / X_OSTART / X_OSIGN.
-  void buildExchange(int b) {
-    if (xBuf == b && xGen == generation) return;
-    Scope sc(this, "exchange");
-    const int nAlloc = readI32(nSlotsPtr());
+  // First half of the exchange layout of buffer b: ordered bricks, their
+  // rows and slabs, and the points before every segment (P); returns the
+  // number of points.  Also the points' bounding box (X_BOX).
+  uint32_t pointLayout(int b, int nAlloc) {
     uint32_t *flags = scratch<uint32_t>(X_FLAGS, nBricks);
     uint32_t *pos = scratch<uint32_t>(X_POS, nBricks);
     uint32_t *sums = scratch<uint32_t>(X_SUMS, scanScratch((size_t)std::max(nBricks, nAlloc * 64)) + 64);
@@ -1025,7 +1126,21 @@ public:
     const uint64_t *def = buf[b].def[buf[b].cur];
     kSegCounts<<<grid1(nSeg), 256, 0, stream>>>(g, ob, nAlloc, brickMap, bounds, def, C, box);
     scanExclusive(C, P, nSeg, sums);
-    const uint32_t nPts = scanTotal(sums, nSeg);
+    return scanTotal(sums, nSeg);
+  }
+
+  void buildExchange(int b) {
+    if (xBuf == b && xGen == generation) return;
+    Scope sc(this, "exchange");
+    const int nAlloc = readI32(nSlotsPtr());
+    const uint32_t nPts = pointLayout(b, nAlloc);
+    const size_t nSeg = (size_t)nAlloc * 64;
+    int4 *bounds = (int4 *)xs[X_BOUNDS].p;
+    uint32_t *P = (uint32_t *)xs[X_P].p;
+    uint32_t *sums = (uint32_t *)xs[X_SUMS].p;
+    int *box = (int *)xs[X_BOX].p;
+    int *ob = (int *)xs[X_OB].p;
+    const uint64_t *def = buf[b].def[buf[b].cur];
     int hbox[6];
     VLSG_CUDA(cudaMemcpyAsync(pinCounters + 16, box, sizeof(hbox), cudaMemcpyDeviceToHost, stream));
     VLSG_CUDA(cudaStreamSynchronize(stream));

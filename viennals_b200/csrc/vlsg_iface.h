@@ -107,6 +107,9 @@ class EngineBase {
 public:
   cudaStream_t stream = nullptr;
   vlsg_velocity_desc vel{};
+  // host callback mode when set (the functor `vel` is then unused)
+  vlsg_velocity_cb velCb = nullptr;
+  void *velUser = nullptr;
   bool profiling = false;
   std::vector<KernelTimer> timers;
 

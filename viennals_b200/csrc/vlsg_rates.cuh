@@ -62,6 +62,32 @@ __device__ inline void vectorVelocity(const vlsg_velocity_desc &v, int material,
   for (int k = 0; k < 3; ++k) out[k] = T(v.vec[m][k]);
 }
 
+// Velocity of one evaluation site of an active point (site 0: the point
+// itself; LocalLaxFriedrichs site 1 + q: box neighbour q, x fastest).
+// FunctorVel evaluates the device functor; TableVel reads what the host
+// callback returned for this point (entry material * sites + site).
+struct FunctorVel {
+  const vlsg_velocity_desc &d;
+  template <class T>
+  __device__ void get(int material, const T n[3], int site, T &sv, T vv[3]) const {
+    (void)site;
+    sv = scalarVelocity<T>(d, material, n);
+    vectorVelocity<T>(d, material, vv);
+  }
+};
+struct TableVel {
+  const double *s, *v;
+  size_t base;
+  int sites;
+  template <class T>
+  __device__ void get(int material, const T n[3], int site, T &sv, T vv[3]) const {
+    (void)n;
+    const size_t i = base + (size_t)material * sites + site;
+    sv = T(s[i]);
+    for (int k = 0; k < 3; ++k) vv[k] = T(v[3 * i + k]);
+  }
+};
+
 template <class T> struct RateArgs {
   GridDev g;
   MapView m;
@@ -89,6 +115,11 @@ template <class T> struct RateArgs {
   unsigned long long *alphaMax; // bits of the LLF/LLLF alphas
   unsigned long long *counts;   // out: active cells, band cells
   int *err;
+  // host callback mode: active points before list entry w, and the
+  // velocities of point p at (p * L + material) * velSites + site
+  const uint32_t *actOff;
+  const double *velS, *velV;
+  int velSites;
 };
 
 // Reader of the top level set around one active point.
@@ -219,8 +250,8 @@ __device__ inline T weno5(const T *x, T dx, bool plus) {
 }
 
 // One scheme evaluation (Hamiltonian, dissipation) for `material`.
-template <class T, class St>
-__device__ void evalScheme(const RateArgs<T> &A, const vlsg_velocity_desc &vel,
+template <class T, class St, class Vel>
+__device__ void evalScheme(const RateArgs<T> &A, const Vel &vel,
                            const St &S, T C, int material, T *alphas,
                            T &outG, T &outD) {
   const T gridDelta = T(A.g.delta);
@@ -261,9 +292,8 @@ __device__ void evalScheme(const RateArgs<T> &A, const vlsg_velocity_desc &vel,
         for (int i = 0; i < 3; ++i) n[i] *= denominator;
       }
     }
-    const T sv = scalarVelocity<T>(vel, material, n);
-    T vv[3];
-    vectorVelocity<T>(vel, material, vv);
+    T sv, vv[3];
+    vel.get(material, n, 0, sv, vv);
     if (sv > 0)
       vel_grad += sqrt(gradPosTotal) * sv;
     else
@@ -308,9 +338,8 @@ __device__ void evalScheme(const RateArgs<T> &A, const vlsg_velocity_desc &vel,
       denominator = T(1.) / sqrt(denominator);
       for (int i = 0; i < 3; ++i) n[i] *= denominator;
     }
-    const T sv = scalarVelocity<T>(vel, material, n);
-    T vv[3];
-    vectorVelocity<T>(vel, material, vv);
+    T sv, vv[3];
+    vel.get(material, n, 0, sv, vv);
     if (sv > 0)
       vel_grad += sqrt(gradPosTotal) * sv;
     else
@@ -349,9 +378,8 @@ __device__ void evalScheme(const RateArgs<T> &A, const vlsg_velocity_desc &vel,
     normalModulus = T(1.) / sqrt(normalModulus);
     for (int i = 0; i < 3; ++i) n[i] *= normalModulus;
   }
-  const T sv = scalarVelocity<T>(vel, material, n);
-  T vv[3];
-  vectorVelocity<T>(vel, material, vv);
+  T sv, vv[3];
+  vel.get(material, n, 0, sv, vv);
   T totalGrad = 0.;
   if (sv != T(0)) totalGrad = sv * sqrt(grad);
   for (int w = 0; w < 3; w++) {
@@ -398,9 +426,8 @@ __device__ void evalScheme(const RateArgs<T> &A, const vlsg_velocity_desc &vel,
     }
     nm = T(1.) / sqrt(nm);
     for (int dir = 0; dir < 3; ++dir) normal[dir] *= nm;
-    const T scaVel = scalarVelocity<T>(vel, material, normal);
-    T vecVel[3];
-    vectorVelocity<T>(vel, material, vecVel);
+    T scaVel, vecVel[3];
+    vel.get(material, normal, 1 + q, scaVel, vecVel);
     for (int dir = 0; dir < 3; ++dir) {
       const T tempAlpha = fabs((scaVel + vecVel[dir]) * normal[dir]);
       alpha[dir] = stdMax(alpha[dir], tempAlpha);
@@ -444,8 +471,8 @@ __device__ inline unsigned long long warpMaxU64(unsigned long long b) {
 // integrateTime for one active point (lsAdvect.hpp:501-592): the material
 // chain, the stored rates (velocity as updateLevelSet applies it,
 // lsAdvect.hpp:738-744, and the stop value) and the point's time budget.
-template <class T, class St>
-__device__ inline double ratePoint(const RateArgs<T> &A, const vlsg_velocity_desc &vel,
+template <class T, class St, class Vel>
+__device__ inline double ratePoint(const RateArgs<T> &A, const Vel &vel,
                                    const St &S, int slot, int c, T C, T *alphas) {
   const int L = A.L;
   const size_t q = (size_t)slot * BV + c;
@@ -541,9 +568,12 @@ __device__ inline uint64_t activePlanes(const T *vals, int slot) {
 // Resident blocks per SM: 3 for float (80 registers), 2 for double (the
 // FP64 stencils need 128 registers to stay out of local memory).
 template <class T> constexpr int rateMinBlocks() { return sizeof(T) == 4 ? 3 : 2; }
-template <class T, int MODE>
+// MODE 0: rates (integrateTime); MODE 1: the global alphas of the
+// Lax-Friedrichs schemes (findGlobalAlphas).  TABLE: velocities from the
+// host callback's table instead of the device functor.
+template <class T, int MODE, bool TABLE = false>
 __global__ void __launch_bounds__(RATE_THREADS, rateMinBlocks<T>())
-    kRates(RateArgs<T> A, const vlsg_velocity_desc vel) {
+    kRates(RateArgs<T> A, const vlsg_velocity_desc desc) {
   __shared__ uint16_t sList[RATE_THREADS / 32][BV];
   uint16_t *list = sList[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
@@ -568,6 +598,13 @@ __global__ void __launch_bounds__(RATE_THREADS, rateMinBlocks<T>())
       const int k = base + lane;
       if (k >= total) continue;
       const int c = list[k];
+      const auto vel = [&] {
+        if constexpr (TABLE)
+          return TableVel{A.velS, A.velV, ((size_t)A.actOff[w] + k) * L * A.velSites,
+                          A.velSites};
+        else
+          return FunctorVel{desc};
+      }();
       withStencil<T>(A, slot, c, [&](const auto &S, T value) {
         if constexpr (MODE == 0) {
           T alphas[3] = {0, 0, 0};
@@ -592,9 +629,8 @@ __global__ void __launch_bounds__(RATE_THREADS, rateMinBlocks<T>())
             }
             normalModulus = T(1.) / sqrt(normalModulus);
             for (int d = 0; d < 3; ++d) normal[d] *= normalModulus;
-            const T scaVel = scalarVelocity<T>(vel, lower, normal);
-            T vecVel[3];
-            vectorVelocity<T>(vel, lower, vecVel);
+            T scaVel, vecVel[3];
+            vel.get(lower, normal, 0, scaVel, vecVel);
             for (int d = 0; d < 3; ++d) {
               const unsigned long long ab =
                   alphaBits((double)fabs((scaVel + vecVel[d]) * normal[d]));

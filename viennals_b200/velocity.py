@@ -1,12 +1,17 @@
-"""Velocity fields for the device functor of vlsg.h.
+"""Velocity fields: the device functor of vlsg.h and host callbacks.
 
 `VelocityField` mirrors viennals::VelocityField<T> (lsVelocityField.hpp:11-41).
-A subclass that only sets coefficients runs entirely on the GPU
-(vlsg_set_velocity_functor); a subclass that overrides getScalarVelocity /
-getVectorVelocity is called back from the host once per stage with a batch of
-points (vlsg_set_velocity_callback).
+A `FunctorVelocity` (coefficients only) runs entirely on the GPU
+(vlsg_set_velocity_functor); any other subclass overrides getScalarVelocity /
+getVectorVelocity (one point at a time, as the reference calls them) or
+`batch` (numpy arrays of queries) and is called back from the host with
+batches of points (vlsg_set_velocity_callback).
 """
-from ._abi import MAX_MATERIALS, VelocityDesc
+import ctypes
+
+import numpy as np
+
+from ._abi import MAX_MATERIALS, VELOCITY_CALLBACK, VelocityDesc
 
 
 class VelocityField:
@@ -24,6 +29,39 @@ class VelocityField:
     def descriptor(self):
         """Return a VelocityDesc when the field is a device functor, else None."""
         return None
+
+    def batch(self, coords, materials, normals, point_ids, scalar_out, vector_out):
+        """Velocities of n queries: coords (n, 3), materials (n,), normals
+        (n, 3), point_ids (n,) in; scalar_out (n,) and vector_out (n, 3) out.
+        The default asks getScalarVelocity / getVectorVelocity per query."""
+        for i in range(len(materials)):
+            c = (float(coords[i, 0]), float(coords[i, 1]), float(coords[i, 2]))
+            n = (float(normals[i, 0]), float(normals[i, 1]), float(normals[i, 2]))
+            m, pid = int(materials[i]), int(point_ids[i])
+            scalar_out[i] = self.getScalarVelocity(c, m, n, pid)
+            vector_out[i, :] = self.getVectorVelocity(c, m, n, pid)
+
+    def c_callback(self):
+        """The vlsg_velocity_cb function pointer of this field (kept alive by
+        the field).  An exception in `batch` makes the call return 1, which
+        the library reports as VLSG_ERR_CALLBACK."""
+        cb = getattr(self, "_c_callback", None)
+        if cb is None:
+            def trampoline(user, n, coords, materials, normals, point_ids, s_out, v_out):
+                try:
+                    n = int(n)
+                    if n <= 0:
+                        return 0
+                    a = np.ctypeslib.as_array
+                    self.batch(a(coords, (n, 3)), a(materials, (n,)), a(normals, (n, 3)),
+                               a(point_ids, (n,)), a(s_out, (n,)), a(v_out, (n, 3)))
+                    return 0
+                except Exception as e:  # reported through the library's status
+                    self.last_callback_error = repr(e)
+                    return 1
+            cb = VELOCITY_CALLBACK(trampoline)
+            self._c_callback = cb
+        return cb
 
 
 class FunctorVelocity(VelocityField):
