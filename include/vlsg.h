@@ -129,6 +129,11 @@ typedef struct vlsg_velocity_desc {
   double sq_pos[VLSG_MAX_MATERIALS][3];
   double sq_neg[VLSG_MAX_MATERIALS][3];
   double vec[VLSG_MAX_MATERIALS][3];
+  /* getDissipationAlpha(direction, material, centralDifferences) =
+   * alpha[material][direction] (lsVelocityField.hpp:35-38; the scheme
+   * LOCAL_LAX_FRIEDRICHS_ANALYTICAL_1ST_ORDER asks it, e.g. the constant
+   * per-direction alphas of SquareEtch.cpp:66-83). */
+  double alpha[VLSG_MAX_MATERIALS][3];
 } vlsg_velocity_desc;
 
 /* Host velocity callback (viennals::VelocityField<T>::getScalarVelocity and
@@ -143,6 +148,17 @@ typedef int (*vlsg_velocity_cb)(void *user, int64_t n, const double *coords,
                                 const double *normals,
                                 const uint64_t *point_ids, double *scalar_out,
                                 double *vector_out);
+
+/* Host dissipation-alpha callback (VelocityField::getDissipationAlpha,
+ * lsVelocityField.hpp:35-38, batched) for LOCAL_LAX_FRIEDRICHS_ANALYTICAL
+ * with a host velocity callback: n queries of (direction, material, the
+ * three central differences of lsLocalLaxFriedrichsAnalytical.hpp:199-209);
+ * fills alpha_out[n]; returns 0 on success.  Without one, the alphas are 0
+ * (the reference's default). */
+typedef int (*vlsg_alpha_cb)(void *user, int64_t n, const int32_t *directions,
+                             const int32_t *materials,
+                             const double *central_differences,
+                             double *alpha_out);
 
 typedef struct vlsg_context vlsg_context;
 
@@ -256,6 +272,10 @@ int vlsg_compare(vlsg_context *a, int32_t slot_a, vlsg_context *b, int32_t slot_
 int vlsg_set_velocity_functor(vlsg_context *ctx, const vlsg_velocity_desc *v);
 int vlsg_set_velocity_callback(vlsg_context *ctx, vlsg_velocity_cb cb,
                                void *user);
+/* With a host velocity callback: the dissipation alphas of
+ * LOCAL_LAX_FRIEDRICHS_ANALYTICAL_1ST_ORDER (NULL clears it). */
+int vlsg_set_dissipation_alpha_callback(vlsg_context *ctx, vlsg_alpha_cb cb,
+                                        void *user);
 
 /* Advect::apply(), lsAdvect.hpp:1017-1043. */
 int vlsg_advect(vlsg_context *ctx, const vlsg_advect_params *params,

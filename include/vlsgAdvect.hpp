@@ -78,6 +78,10 @@ struct VelocityFunctor {
     desc.sq_pos[m][k] = pos, desc.sq_neg[m][k] = neg;
     return *this;
   }
+  VelocityFunctor &dissipationAlpha(int m, int dir, double a) {
+    desc.alpha[m][dir] = a;
+    return *this;
+  }
   VelocityFunctor &vector(int m, double x, double y, double z) {
     desc.vec[m][0] = x, desc.vec[m][1] = y, desc.vec[m][2] = z;
     return *this;
@@ -103,6 +107,27 @@ public:
                                              const std::array<T, 3> & /*normalVector*/,
                                              unsigned long /*pointId*/) {
     return {0, 0, 0};
+  }
+
+  // asked by LOCAL_LAX_FRIEDRICHS_ANALYTICAL_1ST_ORDER (lsVelocityField.hpp:35-38)
+  virtual T getDissipationAlpha(int /*direction*/, int /*material*/,
+                                const std::array<T, 3> & /*centralDifferences*/) {
+    return 0;
+  }
+
+  // vlsg_alpha_cb trampoline (user = the field)
+  static int alphaCallback(void *user, int64_t n, const int32_t *directions,
+                           const int32_t *materials, const double *cd, double *alphaOut) {
+    auto *f = static_cast<VelocityField<T> *>(user);
+    try {
+      for (int64_t i = 0; i < n; ++i) {
+        const std::array<T, 3> c{T(cd[3 * i]), T(cd[3 * i + 1]), T(cd[3 * i + 2])};
+        alphaOut[i] = (double)f->getDissipationAlpha(directions[i], materials[i], c);
+      }
+    } catch (...) {
+      return 1;
+    }
+    return 0;
   }
 
   // vlsg_velocity_cb trampoline (user = the field)
@@ -210,6 +235,9 @@ public:
     }
     if (field) {
       if (!check(vlsg_set_velocity_callback(ctx, &VelocityField<T>::callback, field.get()))) return;
+      if (!check(vlsg_set_dissipation_alpha_callback(ctx, &VelocityField<T>::alphaCallback,
+                                                     field.get())))
+        return;
     } else if (!check(vlsg_set_velocity_functor(ctx, &velocities->desc))) {
       return;
     }

@@ -10,7 +10,7 @@ import subprocess
 
 import numpy as np
 
-from viennals_b200._abi import VELOCITY_CALLBACK, AdvectParams, AdvectResult, VelocityDesc
+from viennals_b200._abi import ALPHA_CALLBACK, VELOCITY_CALLBACK, AdvectParams, AdvectResult, VelocityDesc
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libvlso.so")
@@ -66,7 +66,7 @@ def lib():
         L.vlso_advect.argtypes = [P(vp), i32, P(AdvectParams), P(VelocityDesc),
                                   P(AdvectResult)]
         L.vlso_advect_cb.argtypes = [P(vp), i32, P(AdvectParams), VELOCITY_CALLBACK, vp,
-                                     P(AdvectResult)]
+                                     ALPHA_CALLBACK, vp, P(AdvectResult)]
         L.vlso_last_error.restype = ctypes.c_char_p
         L.vlso_set_threads.argtypes = [i32]
         L.vlso_get_threads.restype = i32
@@ -191,7 +191,8 @@ def advect(level_sets, params, velocity):
     desc = velocity.descriptor() if hasattr(velocity, "descriptor") else velocity
     if desc is None:  # a host velocity field: one callback per point
         _check(lib().vlso_advect_cb(arr, len(level_sets), ctypes.byref(params),
-                                    velocity.c_callback(), None, ctypes.byref(res)))
+                                    velocity.c_callback(), None, velocity.c_alpha_callback(),
+                                    None, ctypes.byref(res)))
         return res
     _check(lib().vlso_advect(arr, len(level_sets), ctypes.byref(params),
                              ctypes.byref(desc), ctypes.byref(res)))

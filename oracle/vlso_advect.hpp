@@ -59,7 +59,8 @@ struct VelSource {
   void *user = nullptr;
   mutable std::atomic<int> failed{0};
   VelSource() = default;
-  VelSource(const VelSource &o) : desc(o.desc), cb(o.cb), user(o.user) {}
+  VelSource(const VelSource &o)
+      : desc(o.desc), cb(o.cb), user(o.user), alphaCb(o.alphaCb), alphaUser(o.alphaUser) {}
   void query(const double coord[3], int material, const double n[3], uint64_t pointId,
              double &scalar, double vec[3]) const {
     if (!cb) {
@@ -73,6 +74,21 @@ struct VelSource {
       scalar = 0;
       vec[0] = vec[1] = vec[2] = 0;
     }
+  }
+  vlsg_alpha_cb alphaCb = nullptr;
+  void *alphaUser = nullptr;
+  // getDissipationAlpha(direction, material, centralDifferences)
+  double alpha(int dir, int material, const double cd[3]) const {
+    if (!cb) {
+      int m = material < desc.n_materials ? material : desc.n_materials - 1;
+      if (m < 0) m = 0;
+      return desc.alpha[m][dir];
+    }
+    if (!alphaCb) return 0.;
+    const int32_t d = dir, m = material;
+    double a = 0;
+    if (alphaCb(alphaUser, 1, &d, &m, cd, &a) != 0) failed = 1;
+    return a;
   }
   void check() const {
     if (failed) throw std::runtime_error("the velocity callback failed");
@@ -123,6 +139,7 @@ inline int schemeWidth(int s) {
   case VLSG_LOCAL_LOCAL_LAX_FRIEDRICHS_2ND_ORDER: return 5;
   case VLSG_LOCAL_LAX_FRIEDRICHS_1ST_ORDER: return 7;    // lsLocalLaxFriedrichs.hpp:55
   case VLSG_LOCAL_LAX_FRIEDRICHS_2ND_ORDER: return 9;
+  case VLSG_LOCAL_LAX_FRIEDRICHS_ANALYTICAL_1ST_ORDER: return 7; // lsLocalLaxFriedrichsAnalytical.hpp:52
   case VLSG_WENO_3RD_ORDER: return 5;                    // lsWENO.hpp:44 (r=2)
   case VLSG_WENO_5TH_ORDER: return 7;                    // (r=3)
   default: return -1;
@@ -382,6 +399,47 @@ std::pair<double, double> evalScheme(const SchemeCtx<D> &S, uint64_t key,
     return {totalGrad, ((totalGrad != 0.) ? dissipation : 0)};
 
   if (totalGrad == 0.) return {0, 0}; // lsLocalLaxFriedrichs.hpp:179-181
+
+  if (sch == VLSG_LOCAL_LAX_FRIEDRICHS_ANALYTICAL_1ST_ORDER) {
+    // lsLocalLaxFriedrichsAnalytical.hpp:183-225: the user's alphas at the
+    // 3^D box (central differences, not normalised), no alphaFactor
+    double alpha[D];
+    for (int i = 0; i < D; ++i) alpha[i] = 0;
+    int nIdx[D];
+    for (int d = 0; d < D; ++d) nIdx[d] = -1;
+    int numNeighbors = 1;
+    for (int d = 0; d < D; ++d) numNeighbors *= 3;
+    auto VB = [&](const int *off) { return ls.at(offsetKey<D>(g, key, off)); };
+    for (int q = 0; q < numNeighbors; ++q) {
+      double normal[3] = {0, 0, 0};
+      const double center = VB(nIdx);
+      for (int dir = 0; dir < D; ++dir) {
+        int o[D];
+        for (int d = 0; d < D; ++d) o[d] = nIdx[d];
+        o[dir] = nIdx[dir] - 1;
+        const double neg = VB(o);
+        o[dir] = nIdx[dir] + 1;
+        const double pos = VB(o);
+        // calculateNormalComponent, :30-34
+        const double dPos = (pos - center) / gridDelta;
+        const double dNeg = (center - neg) / gridDelta;
+        normal[dir] = (dPos + dNeg) * 0.5;
+      }
+      for (int dir = 0; dir < D; ++dir) {
+        const double tempAlpha = S.vel.alpha(dir, material, normal);
+        alpha[dir] = stdMax(alpha[dir], tempAlpha);
+        alphas[dir] = stdMax(alphas[dir], tempAlpha);
+      }
+      int dim = 0;
+      for (; dim < D - 1; ++dim) {
+        if (nIdx[dim] < 1) break;
+        nIdx[dim] = -1;
+      }
+      ++nIdx[dim];
+    }
+    for (int i = 0; i < D; ++i) dissipation += alpha[i] * (gradNeg[i] - gradPos[i]) * 0.5;
+    return {totalGrad, dissipation};
+  }
 
   if (sch == VLSG_LOCAL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER ||
       sch == VLSG_LOCAL_LOCAL_LAX_FRIEDRICHS_2ND_ORDER) {

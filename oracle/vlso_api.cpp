@@ -249,7 +249,7 @@ int vlso_advect(void **lss, int n, const vlsg_advect_params *p,
 // The same with a host velocity callback (called one point at a time, from
 // the OpenMP threads).
 int vlso_advect_cb(void **lss, int n, const vlsg_advect_params *p, vlsg_velocity_cb cb,
-                   void *user, vlsg_advect_result *r) {
+                   void *user, vlsg_alpha_cb alphaCb, void *alphaUser, vlsg_advect_result *r) {
   auto **hs = reinterpret_cast<Handle **>(lss);
   return guarded([&] {
     if (n < 1) throw std::runtime_error("no level sets");
@@ -257,6 +257,8 @@ int vlso_advect_cb(void **lss, int n, const vlsg_advect_params *p, vlsg_velocity
     vlso::VelSource vs;
     vs.cb = cb;
     vs.user = user;
+    vs.alphaCb = alphaCb;
+    vs.alphaUser = alphaUser;
     return hs[0]->D == 2 ? advectD<2>(hs, n, p, vs, r) : advectD<3>(hs, n, p, vs, r);
   });
 }

@@ -118,6 +118,7 @@ class VelocityDesc(ctypes.Structure):
         ("sq_pos", _Mat3),
         ("sq_neg", _Mat3),
         ("vec", _Mat3),
+        ("alpha", _Mat3),
     ]
 
 
@@ -153,6 +154,16 @@ class CompareResult(ctypes.Structure):
         d["diff_above"] = list(self.diff_above)
         return d
 
+
+ALPHA_CALLBACK = ctypes.CFUNCTYPE(
+    ctypes.c_int,
+    ctypes.c_void_p,
+    ctypes.c_int64,
+    ctypes.POINTER(ctypes.c_int32),
+    ctypes.POINTER(ctypes.c_int32),
+    ctypes.POINTER(ctypes.c_double),
+    ctypes.POINTER(ctypes.c_double),
+)
 
 VELOCITY_CALLBACK = ctypes.CFUNCTYPE(
     ctypes.c_int,

@@ -2,7 +2,7 @@
 import ctypes
 import os
 
-from ._abi import (VELOCITY_CALLBACK, AdvectParams, AdvectResult, CompareResult, KernelStat,
+from ._abi import (ALPHA_CALLBACK, VELOCITY_CALLBACK, AdvectParams, AdvectResult, CompareResult, KernelStat,
                    VelocityDesc)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -47,6 +47,7 @@ def load(build_if_missing=True):
     L.vlsg_get_values_noalloc.argtypes = [vp, i32, i64, P(i32), P(ctypes.c_double)]
     L.vlsg_set_velocity_functor.argtypes = [vp, P(VelocityDesc)]
     L.vlsg_set_velocity_callback.argtypes = [vp, VELOCITY_CALLBACK, vp]
+    L.vlsg_set_dissipation_alpha_callback.argtypes = [vp, ALPHA_CALLBACK, vp]
     L.vlsg_advect.argtypes = [vp, P(AdvectParams), P(AdvectResult)]
     L.vlsg_set_profiling.argtypes = [vp, i32]
     L.vlsg_get_kernel_stats.argtypes = [vp, i32, P(KernelStat), P(i32)]
@@ -60,6 +61,7 @@ EXPORTED = [
     "vlsg_set_grid", "vlsg_set_level_set_count",
     "vlsg_upload_levelset", "vlsg_count_points", "vlsg_download_levelset", "vlsg_download_runs",
     "vlsg_get_values", "vlsg_get_values_noalloc",
-    "vlsg_set_velocity_functor", "vlsg_set_velocity_callback", "vlsg_advect", "vlsg_advect_batch",
+    "vlsg_set_velocity_functor", "vlsg_set_velocity_callback",
+    "vlsg_set_dissipation_alpha_callback", "vlsg_advect", "vlsg_advect_batch",
     "vlsg_set_profiling", "vlsg_get_kernel_stats", "vlsg_compare",
 ]

@@ -116,8 +116,10 @@ class Context:
 
     def set_velocity_callback(self, field):
         """Host callback mode: `field` is a VelocityField (its c_callback())."""
-        self._velocity_field = field  # keeps the function pointer alive
+        self._velocity_field = field  # keeps the function pointers alive
         self._check(self.lib.vlsg_set_velocity_callback(self.h, field.c_callback(), None))
+        self._check(self.lib.vlsg_set_dissipation_alpha_callback(self.h, field.c_alpha_callback(),
+                                                                 None))
 
     def advect(self, params):
         res = AdvectResult()

@@ -29,6 +29,8 @@ struct vlsg_context {
   vlsg_velocity_desc vel{};
   vlsg_velocity_cb velCb = nullptr; // host callback mode when set
   void *velUser = nullptr;
+  vlsg_alpha_cb alphaCb = nullptr;
+  void *alphaUser = nullptr;
   bool profiling = false;
   std::unique_ptr<EngineBase> eng; // Engine<double> or Engine<float>
 };
@@ -445,6 +447,13 @@ int vlsg_set_velocity_callback(vlsg_context *ctx, vlsg_velocity_cb cb, void *use
   return VLSG_OK;
 }
 
+int vlsg_set_dissipation_alpha_callback(vlsg_context *ctx, vlsg_alpha_cb cb, void *user) {
+  if (!ctx) return fail(nullptr, VLSG_ERR_ARGUMENT, "NULL context");
+  ctx->alphaCb = cb;
+  ctx->alphaUser = cb ? user : nullptr;
+  return VLSG_OK;
+}
+
 int vlsg_advect(vlsg_context *ctx, const vlsg_advect_params *p, vlsg_advect_result *r) {
   if (!ctx || !p || !r) return fail(ctx, VLSG_ERR_ARGUMENT, "bad argument");
   // Advect::apply validation, lsAdvect.hpp:1019-1027
@@ -462,6 +471,8 @@ int vlsg_advect(vlsg_context *ctx, const vlsg_advect_params *p, vlsg_advect_resu
     e.vel = ctx->vel;
     e.velCb = ctx->velCb;
     e.velUser = ctx->velUser;
+    e.alphaCb = ctx->velCb ? ctx->alphaCb : nullptr;
+    e.alphaUser = ctx->alphaUser;
     e.profiling = ctx->profiling;
     if (ctx->profiling) e.timers.clear();
     e.apply(*p, *r);

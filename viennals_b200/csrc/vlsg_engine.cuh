@@ -111,13 +111,14 @@ public:
   };
   enum { X_FLAGS, X_POS, X_OB, X_BOUNDS, X_C, X_P, X_SUMS, X_BOX, X_IDX, X_VAL, X_GC, X_GE,
          X_ROWC, X_ROWG, X_PB, X_GB, X_RSTART, X_RSIGN, X_RPB, X_KEEP, X_KPOS, X_OSTART,
-         X_OSIGN, X_VCNT, X_VOFF, X_VSUMS, X_QC, X_QM, X_QN, X_QP, X_VS, X_VV, X_COUNT };
+         X_OSIGN, X_VCNT, X_VOFF, X_VSUMS, X_QC, X_QM, X_QN, X_QP, X_VS, X_VV, X_AD, X_AM,
+         X_AC, X_AV, X_COUNT };
   // pinned host staging of the velocity callback's queries and answers
   struct PinScratch {
     void *p = nullptr;
     size_t bytes = 0;
   };
-  enum { H_QC, H_QM, H_QN, H_QP, H_VS, H_VV, H_COUNT };
+  enum { H_QC, H_QM, H_QN, H_QP, H_VS, H_VV, H_AD, H_AM, H_AC, H_AV, H_COUNT };
   PinScratch hs[H_COUNT];
   Scratch xs[X_COUNT];
   uint64_t generation = 0;
@@ -873,6 +874,7 @@ public:
     A.velS = vs;
     A.velV = vv;
     A.velSites = sites;
+    A.alphaTab = nullptr;
     if (!nQ) return;
     kVelGather<T, MODE><<<blocksRate, RATE_THREADS, 0, stream>>>(A, R, sites, qc, qm, qn, qp);
     checkLaunch();
@@ -887,15 +889,53 @@ public:
     VLSG_CUDA(cudaMemcpyAsync(hn, qn, 3 * nQ * sizeof(double), cudaMemcpyDeviceToHost, stream));
     VLSG_CUDA(cudaMemcpyAsync(hp, qp, nQ * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream));
     syncErr("velocity queries");
+    hostPool(nQ, [&](size_t i, int64_t n) {
+      return velCb(velUser, n, hc + 3 * i, hm + i, hn + 3 * i, hp + i, hsv + i, hvv + 3 * i);
+    }, "the velocity callback returned ");
+    VLSG_CUDA(cudaMemcpyAsync(vs, hsv, nQ * sizeof(double), cudaMemcpyHostToDevice, stream));
+    VLSG_CUDA(cudaMemcpyAsync(vv, hvv, 3 * nQ * sizeof(double), cudaMemcpyHostToDevice, stream));
+    if (MODE == 0 && A.scheme == VLSG_LOCAL_LAX_FRIEDRICHS_ANALYTICAL_1ST_ORDER && alphaCb)
+      gatherAlphas(A, nAct);
+  }
+
+  // LocalLaxFriedrichsAnalytical with host callbacks: every active point x
+  // material x box neighbour x direction asked through the alpha callback.
+  void gatherAlphas(RateArgs<T> &A, size_t nAct) {
+    const size_t nA = nAct * (size_t)L * 81;
+    if (nA > ((size_t)1 << 28))
+      throw CudaError("alpha callback: more than 2^28 queries in one rate pass", VLSG_ERR_CAPACITY);
+    int32_t *ad = scratch<int32_t>(X_AD, nA);
+    int32_t *am = scratch<int32_t>(X_AM, nA);
+    double *ac = scratch<double>(X_AC, 3 * nA);
+    double *av = scratch<double>(X_AV, nA);
+    kAlphaGather<T><<<blocksRate, RATE_THREADS, 0, stream>>>(A, ad, am, ac);
+    checkLaunch();
+    int32_t *hd = pinned<int32_t>(H_AD, nA);
+    int32_t *hm = pinned<int32_t>(H_AM, nA);
+    double *hc = pinned<double>(H_AC, 3 * nA);
+    double *hv = pinned<double>(H_AV, nA);
+    VLSG_CUDA(cudaMemcpyAsync(hd, ad, nA * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+    VLSG_CUDA(cudaMemcpyAsync(hm, am, nA * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+    VLSG_CUDA(cudaMemcpyAsync(hc, ac, 3 * nA * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    syncErr("alpha queries");
+    hostPool(nA, [&](size_t i, int64_t n) {
+      return alphaCb(alphaUser, n, hd + i, hm + i, hc + 3 * i, hv + i);
+    }, "the dissipation alpha callback returned ");
+    VLSG_CUDA(cudaMemcpyAsync(av, hv, nA * sizeof(double), cudaMemcpyHostToDevice, stream));
+    A.alphaTab = av;
+  }
+
+  // Runs fn(first, count) over [0, n) in chunks of 4096 from a pool of host
+  // threads; a non-zero return ends the work with VLSG_ERR_CALLBACK.
+  template <class Fn> void hostPool(size_t n, Fn fn, const char *what) {
     const size_t chunk = 4096;
     const unsigned hw = std::thread::hardware_concurrency();
-    const int nt = (int)std::min<size_t>(std::max(1u, std::min(hw, 64u)), (nQ + chunk - 1) / chunk);
+    const int nt = (int)std::min<size_t>(std::max(1u, std::min(hw, 64u)), (n + chunk - 1) / chunk);
     std::atomic<size_t> next{0};
     std::atomic<int> failed{0};
     auto worker = [&] {
-      for (size_t i = next.fetch_add(chunk); i < nQ && !failed.load(); i = next.fetch_add(chunk)) {
-        const int64_t n = (int64_t)std::min(chunk, nQ - i);
-        const int rc = velCb(velUser, n, hc + 3 * i, hm + i, hn + 3 * i, hp + i, hsv + i, hvv + 3 * i);
+      for (size_t i = next.fetch_add(chunk); i < n && !failed.load(); i = next.fetch_add(chunk)) {
+        const int rc = fn(i, (int64_t)std::min(chunk, n - i));
         if (rc != 0) {
           int zero = 0;
           failed.compare_exchange_strong(zero, rc);
@@ -906,11 +946,7 @@ public:
     for (int t = 1; t < nt; ++t) pool.emplace_back(worker);
     worker();
     for (auto &th : pool) th.join();
-    if (failed)
-      throw CudaError("the velocity callback returned " + std::to_string(failed.load()),
-                      VLSG_ERR_CALLBACK);
-    VLSG_CUDA(cudaMemcpyAsync(vs, hsv, nQ * sizeof(double), cudaMemcpyHostToDevice, stream));
-    VLSG_CUDA(cudaMemcpyAsync(vv, hvv, 3 * nQ * sizeof(double), cudaMemcpyHostToDevice, stream));
+    if (failed) throw CudaError(std::string(what) + std::to_string(failed.load()), VLSG_ERR_CALLBACK);
   }
 
   void adjustLowerLayers(const vlsg_advect_params &P) {

@@ -95,6 +95,7 @@ inline int schemeWidth(int s) {
   case VLSG_LOCAL_LOCAL_LAX_FRIEDRICHS_2ND_ORDER: return 5;
   case VLSG_LOCAL_LAX_FRIEDRICHS_1ST_ORDER: return 7;
   case VLSG_LOCAL_LAX_FRIEDRICHS_2ND_ORDER: return 9;
+  case VLSG_LOCAL_LAX_FRIEDRICHS_ANALYTICAL_1ST_ORDER: return 7;
   case VLSG_WENO_3RD_ORDER: return 5;
   case VLSG_WENO_5TH_ORDER: return 7;
   default: return -1;
@@ -110,6 +111,8 @@ public:
   // host callback mode when set (the functor `vel` is then unused)
   vlsg_velocity_cb velCb = nullptr;
   void *velUser = nullptr;
+  vlsg_alpha_cb alphaCb = nullptr; // dissipation alphas with a callback
+  void *alphaUser = nullptr;
   bool profiling = false;
   std::vector<KernelTimer> timers;
 

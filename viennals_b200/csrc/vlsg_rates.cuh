@@ -66,6 +66,8 @@ __device__ inline void vectorVelocity(const vlsg_velocity_desc &v, int material,
 // itself; LocalLaxFriedrichs site 1 + q: box neighbour q, x fastest).
 // FunctorVel evaluates the device functor; TableVel reads what the host
 // callback returned for this point (entry material * sites + site).
+// alpha(dir, material, cd, q): getDissipationAlpha at box neighbour q
+// (LocalLaxFriedrichsAnalytical).
 struct FunctorVel {
   const vlsg_velocity_desc &d;
   template <class T>
@@ -74,17 +76,29 @@ struct FunctorVel {
     sv = scalarVelocity<T>(d, material, n);
     vectorVelocity<T>(d, material, vv);
   }
+  template <class T> __device__ T alpha(int dir, int material, const T cd[3], int q) const {
+    (void)cd, (void)q;
+    int m = material < d.n_materials ? material : d.n_materials - 1;
+    if (m < 0) m = 0;
+    return T(d.alpha[m][dir]);
+  }
 };
 struct TableVel {
   const double *s, *v;
   size_t base;
   int sites;
+  const double *a; // alphas: ((p * L + material) * 27 + q) * 3 + dir, or none
+  size_t alphaBase;
   template <class T>
   __device__ void get(int material, const T n[3], int site, T &sv, T vv[3]) const {
     (void)n;
     const size_t i = base + (size_t)material * sites + site;
     sv = T(s[i]);
     for (int k = 0; k < 3; ++k) vv[k] = T(v[3 * i + k]);
+  }
+  template <class T> __device__ T alpha(int dir, int material, const T cd[3], int q) const {
+    (void)cd;
+    return a ? T(a[alphaBase + ((size_t)material * 27 + q) * 3 + dir]) : T(0);
   }
 };
 
@@ -120,6 +134,7 @@ template <class T> struct RateArgs {
   const uint32_t *actOff;
   const double *velS, *velV;
   int velSites;
+  const double *alphaTab; // LocalLaxFriedrichsAnalytical: the alpha callback's answers
 };
 
 // Reader of the top level set around one active point.
@@ -247,6 +262,21 @@ __device__ inline T weno5(const T *x, T dx, bool plus) {
   const T p2 = c16 * (-d[1] + 5 * d[2] + 2 * d[3]);
   const T p3 = c16 * (2 * d[2] + 5 * d[3] - d[4]);
   return (al1 * p1 + al2 * p2 + al3 * p3) / (alsum * dx);
+}
+
+// Central differences at box neighbour q (x fastest):
+// calculateNormalComponent of lsLocalLaxFriedrichsAnalytical.hpp:30-34.
+template <class T, class St>
+__device__ inline void boxDifferences(const St &S, T gridDelta, int q, T cd[3]) {
+  const int ox = q % 3 - 1, oy = (q / 3) % 3 - 1, oz = q / 9 - 1;
+  const T center = S.at(ox, oy, oz);
+  for (int dir = 0; dir < 3; ++dir) {
+    const T neg = S.at(ox - (dir == 0), oy - (dir == 1), oz - (dir == 2));
+    const T pos = S.at(ox + (dir == 0), oy + (dir == 1), oz + (dir == 2));
+    const T diffPos = (pos - center) / gridDelta;
+    const T diffNeg = (center - neg) / gridDelta;
+    cd[dir] = (diffPos + diffNeg) * T(0.5);
+  }
 }
 
 // One scheme evaluation (Hamiltonian, dissipation) for `material`.
@@ -396,6 +426,24 @@ __device__ void evalScheme(const RateArgs<T> &A, const Vel &vel,
   if (totalGrad == T(0)) {
     outG = 0;
     outD = 0;
+    return;
+  }
+  if (sch == VLSG_LOCAL_LAX_FRIEDRICHS_ANALYTICAL_1ST_ORDER) {
+    // the user's alphas over the 3x3x3 box at the central differences
+    // (calculateNormalComponent, not normalised), no alphaFactor
+    T alpha[3] = {0, 0, 0};
+    for (int q = 0; q < 27; ++q) {
+      T cd[3];
+      boxDifferences<T>(S, gridDelta, q, cd);
+      for (int dir = 0; dir < 3; ++dir) {
+        const T tempAlpha = vel.alpha(dir, material, cd, q);
+        alpha[dir] = stdMax(alpha[dir], tempAlpha);
+        alphas[dir] = stdMax(alphas[dir], tempAlpha);
+      }
+    }
+    for (int i = 0; i < 3; ++i) dissipation += alpha[i] * (gradNeg[i] - gradPos[i]) * T(0.5);
+    outG = totalGrad;
+    outD = dissipation;
     return;
   }
   if (sch == VLSG_LOCAL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER ||
@@ -601,7 +649,7 @@ __global__ void __launch_bounds__(RATE_THREADS, rateMinBlocks<T>())
       const auto vel = [&] {
         if constexpr (TABLE)
           return TableVel{A.velS, A.velV, ((size_t)A.actOff[w] + k) * L * A.velSites,
-                          A.velSites};
+                          A.velSites, A.alphaTab, ((size_t)A.actOff[w] + k) * L * 81};
         else
           return FunctorVel{desc};
       }();

@@ -220,5 +220,46 @@ __global__ void __launch_bounds__(RATE_THREADS)
   }
 }
 
+// LocalLaxFriedrichsAnalytical: the alpha queries of every active point p,
+// material, box neighbour q and direction, at
+// ((p * L + material) * 27 + q) * 3 + dir.
+template <class T>
+__global__ void __launch_bounds__(RATE_THREADS)
+    kAlphaGather(RateArgs<T> A, int32_t *direction, int32_t *material, double *cd) {
+  __shared__ uint16_t sList[RATE_THREADS / 32][BV];
+  uint16_t *list = sList[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nWarps = (gridDim.x * blockDim.x) >> 5;
+  const int n = *A.nSlots;
+  const int L = A.L;
+  const Buf<T> &top = A.ls[L - 1];
+  const T gridDelta = T(A.g.delta);
+  for (int w = warp; w < n; w += nWarps) {
+    const int slot = A.slotList[w];
+    const uint64_t own = lane < 8 ? A.def[(size_t)slot * 8 + lane] : 0ull;
+    uint64_t a = 0ull;
+    if (__any_sync(0xffffffffu, own != 0ull)) a = activePlanes<T>(top.vals, slot);
+    const int total = listCells(a, list);
+    for (int k = lane; k < total; k += 32) {
+      const int c = list[k];
+      const size_t p = (size_t)A.actOff[w] + k;
+      withStencil<T>(A, slot, c, [&](const auto &S, T) {
+        for (int q = 0; q < 27; ++q) {
+          T d3[3];
+          boxDifferences<T>(S, gridDelta, q, d3);
+          for (int m = 0; m < L; ++m)
+            for (int dir = 0; dir < 3; ++dir) {
+              const size_t e = ((p * L + m) * 27 + q) * 3 + dir;
+              direction[e] = dir;
+              material[e] = m;
+              for (int k3 = 0; k3 < 3; ++k3) cd[3 * e + k3] = (double)d3[k3];
+            }
+        }
+      });
+    }
+  }
+}
+
 } // namespace
 } // namespace vlsg

@@ -11,7 +11,7 @@ import ctypes
 
 import numpy as np
 
-from ._abi import MAX_MATERIALS, VELOCITY_CALLBACK, VelocityDesc
+from ._abi import ALPHA_CALLBACK, MAX_MATERIALS, VELOCITY_CALLBACK, VelocityDesc
 
 
 class VelocityField:
@@ -63,6 +63,34 @@ class VelocityField:
             self._c_callback = cb
         return cb
 
+    def alpha_batch(self, directions, materials, central_differences, alpha_out):
+        """getDissipationAlpha of n queries: directions (n,), materials (n,),
+        central_differences (n, 3) in; alpha_out (n,) out."""
+        for i in range(len(materials)):
+            cd = (float(central_differences[i, 0]), float(central_differences[i, 1]),
+                  float(central_differences[i, 2]))
+            alpha_out[i] = self.getDissipationAlpha(int(directions[i]), int(materials[i]), cd)
+
+    def c_alpha_callback(self):
+        """The vlsg_alpha_cb function pointer of this field."""
+        cb = getattr(self, "_c_alpha_callback", None)
+        if cb is None:
+            def trampoline(user, n, directions, materials, cd, out):
+                try:
+                    n = int(n)
+                    if n <= 0:
+                        return 0
+                    a = np.ctypeslib.as_array
+                    self.alpha_batch(a(directions, (n,)), a(materials, (n,)), a(cd, (n, 3)),
+                                     a(out, (n,)))
+                    return 0
+                except Exception as e:  # reported through the library's status
+                    self.last_callback_error = repr(e)
+                    return 1
+            cb = ALPHA_CALLBACK(trampoline)
+            self._c_alpha_callback = cb
+        return cb
+
 
 class FunctorVelocity(VelocityField):
     """Per-material polynomial in the unit normal, evaluated on the device.
@@ -85,6 +113,7 @@ class FunctorVelocity(VelocityField):
         self.abs_pos, self.abs_neg = z3(), z3()
         self.sq_pos, self.sq_neg = z3(), z3()
         self.vec = z3()
+        self.alpha = z3()
 
     # convenience builders -------------------------------------------------
     def set_rate(self, material, rate):
@@ -104,6 +133,11 @@ class FunctorVelocity(VelocityField):
     def set_square(self, material, axis, coeff_pos, coeff_neg=None):
         self.sq_pos[material][axis] = float(coeff_pos)
         self.sq_neg[material][axis] = float(coeff_pos if coeff_neg is None else coeff_neg)
+        return self
+
+    def set_dissipation_alpha(self, material, direction, alpha):
+        """getDissipationAlpha(direction, material, .) = alpha (constant)."""
+        self.alpha[material][direction] = float(alpha)
         return self
 
     def set_vector(self, material, v):
@@ -131,6 +165,9 @@ class FunctorVelocity(VelocityField):
     def getVectorVelocity(self, coordinate, material, normalVector, pointId):
         return tuple(self.vec[self._m(material)])
 
+    def getDissipationAlpha(self, direction, material, centralDifferences):
+        return self.alpha[self._m(material)][direction]
+
     def descriptor(self):
         d = VelocityDesc()
         d.n_materials = self.n
@@ -144,6 +181,7 @@ class FunctorVelocity(VelocityField):
                 d.sq_pos[m][k] = self.sq_pos[m][k]
                 d.sq_neg[m][k] = self.sq_neg[m][k]
                 d.vec[m][k] = self.vec[m][k]
+                d.alpha[m][k] = self.alpha[m][k]
         return d
 
 
