@@ -95,6 +95,10 @@ typedef struct vlsg_advect_params {
   int32_t save_advection_velocities; /* setSaveAdvectionVelocities :916 */
   int32_t update_point_data;       /* setUpdatePointData (1)      :962 */
   uint32_t max_steps;              /* guard against dt == 0 loops (0 = 1e7) */
+  double max_dissipation;          /* StencilLocalLaxFriedrichsScalar::
+                                      setMaxDissipation (lsStencilLocalLax
+                                      FriedrichsScalar.hpp:215); <= 0 means
+                                      no limit (the reference's default) */
 } vlsg_advect_params;
 
 /* Getters of viennals::Advect (lsAdvect.hpp:920-932) plus work counters. */

@@ -205,6 +205,8 @@ public:
   void setDissipationAlpha(const double &a) { params.dissipation_alpha = a; }
   void setCheckDissipation(bool b) { params.check_dissipation = b; }
   void setUpdatePointData(bool b) { params.update_point_data = b; }
+  // StencilLocalLaxFriedrichsScalar<T,D,1>::setMaxDissipation, per Advect here
+  void setMaxDissipation(double d) { params.max_dissipation = d; }
 
   double getAdvectedTime() const { return result.advected_time; }
   double getCurrentTimeStep() const { return result.current_time_step; }

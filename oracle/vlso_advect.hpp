@@ -124,6 +124,10 @@ struct Params {
   unsigned adaptiveSubdivisions = 20;
   bool checkDissipation = true;
   uint32_t maxSteps = 10000000;
+  // StencilLocalLaxFriedrichsScalar::setMaxDissipation (static, default max)
+  double maxDissipation = std::numeric_limits<double>::max();
+  // baseNormalEpsilon of StencilLocalLaxFriedrichsScalar (:44-45)
+  double baseNormalEpsilon = std::cbrt(std::numeric_limits<double>::epsilon());
   static constexpr double integrationCutoff = 0.5;    // lsAdvect.hpp:77
   static constexpr double wrappingLayerEpsilon = 1e-4; // lsAdvect.hpp:80
 };
@@ -140,6 +144,7 @@ inline int schemeWidth(int s) {
   case VLSG_LOCAL_LAX_FRIEDRICHS_1ST_ORDER: return 7;    // lsLocalLaxFriedrichs.hpp:55
   case VLSG_LOCAL_LAX_FRIEDRICHS_2ND_ORDER: return 9;
   case VLSG_LOCAL_LAX_FRIEDRICHS_ANALYTICAL_1ST_ORDER: return 7; // lsLocalLaxFriedrichsAnalytical.hpp:52
+  case VLSG_STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER: return 8; // lsStencilLocalLaxFriedrichsScalar.hpp:207
   case VLSG_WENO_3RD_ORDER: return 5;                    // lsWENO.hpp:44 (r=2)
   case VLSG_WENO_5TH_ORDER: return 7;                    // (r=3)
   default: return -1;
@@ -258,6 +263,134 @@ std::pair<double, double> evalScheme(const SchemeCtx<D> &S, uint64_t key,
   const double C = ls.at(key);
   double coordinate[3];
   coordinateOf<D>(g, key, coordinate);
+
+  if (sch == VLSG_STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER) {
+    // StencilLocalLaxFriedrichsScalar<T,D,1> with FIRST_ORDER differences and
+    // ADAPTIVE_EPSILON_STRATEGY 1 (lsStencilLocalLaxFriedrichsScalar.hpp:219-400).
+    // `alphas` receives this call's finalAlphas and alphas[3] = 1 when the
+    // call gets past the zero-velocity return (they bound the time step).
+    auto VI = [&](const int *off) { return ls.at(offsetKey<D>(g, key, off)); };
+    // component i of calculateGradient / calculateNormal at `off`: the three
+    // values along i are taken with coordinate i set to -1, 0, 1 (:342-352,
+    // :360-372), whatever off[i] is
+    auto grad1 = [&](const int *off, int i) {
+      int o[D];
+      for (int d = 0; d < D; ++d) o[d] = off[d];
+      double v[3];
+      for (int j = 0; j < 3; ++j) {
+        o[i] = j - 1;
+        v[j] = VI(o);
+      }
+      const double dNeg = (v[1] - v[0]) / gridDelta; // lsFiniteDifferences.hpp:132-134
+      const double dPos = (v[2] - v[1]) / gridDelta; // :155-157
+      return (dPos + dNeg) * 0.5;                    // :177-181
+    };
+    auto normalAt = [&](const int *off, double *n) {
+      n[0] = n[1] = n[2] = 0.;
+      double modulus = 0.;
+      for (int i = 0; i < D; ++i) {
+        n[i] = grad1(off, i);
+        modulus += n[i] * n[i];
+      }
+      modulus = 1. / std::sqrt(modulus);
+      for (int i = 0; i < D; ++i) n[i] *= modulus;
+    };
+    int zero[D];
+    for (int d = 0; d < D; ++d) zero[d] = 0;
+    double normalVector[3];
+    normalAt(zero, normalVector);
+    double scalarVelocity, vectorVelocity[3];
+    S.vel.query(coordinate, material, normalVector, pointId, scalarVelocity, vectorVelocity);
+    for (int i = 0; i < D; ++i) scalarVelocity += vectorVelocity[i] * normalVector[i];
+    if (scalarVelocity == 0.) return {0, 0};
+    double gradSq = 0.; // Norm(calculateGradient(0))
+    for (int i = 0; i < D; ++i) {
+      const double gi = grad1(zero, i);
+      gradSq += gi * gi;
+    }
+    const double hamiltonian = std::sqrt(gradSq) * scalarVelocity;
+    constexpr int numStencil = D == 3 ? 27 : 9;
+    double sa[27][3] = {};
+    int cur[D];
+    for (int d = 0; d < D; ++d) cur[d] = -1;
+    for (int st = 0; st < numStencil; ++st) {
+      double localNormal[3];
+      normalAt(cur, localNormal);
+      // a corrupted normal leaves the stencil index where it is (:288-293)
+      if (std::abs(localNormal[0]) < 1e-6 && std::abs(localNormal[1]) < 1e-6 &&
+          std::abs(localNormal[2]) < 1e-6)
+        continue;
+      double localCoord[3] = {coordinate[0], coordinate[1], coordinate[2]};
+      for (int dir = 0; dir < D; ++dir) localCoord[dir] += cur[dir] * gridDelta;
+      double lsv, lvv[3];
+      S.vel.query(localCoord, material, localNormal, pointId, lsv, lvv);
+      for (int dir = 0; dir < D; ++dir) lsv += lvv[dir] * localNormal[dir];
+      // calculateSimpleAdaptiveEpsilon, :60-75
+      const double absVel = std::abs(lsv);
+      const double baseEps = S.P.baseNormalEpsilon * gridDelta;
+      double DN = baseEps;
+      if (absVel > 1e-10) {
+        const double scale = stdMax(0.1, stdMin(10.0, absVel));
+        DN = baseEps * scale;
+      }
+      double np[3] = {localNormal[0], localNormal[1], localNormal[2]};
+      double nn[3] = {localNormal[0], localNormal[1], localNormal[2]};
+      double velocityDelta[3] = {0, 0, 0};
+      for (int k = 0; k < D; ++k) {
+        np[k] -= DN;
+        nn[k] += DN;
+        double vp, vn, unused[3];
+        S.vel.query(localCoord, material, np, pointId, vp, unused);
+        S.vel.query(localCoord, material, nn, pointId, vn, unused);
+        velocityDelta[k] = (vn - vp) / (2.0 * DN);
+        np[k] += DN;
+        nn[k] -= DN;
+      }
+      for (int k = 0; k < D; ++k) {
+        double gradient[3];
+        for (int i = 0; i < D; ++i) gradient[i] = grad1(cur, i);
+        double monti = 0, toifl = 0;
+        for (int j = 0; j < D - 1; ++j) {
+          const int idx = (k + 1 + j) % D;
+          monti += gradient[idx] * gradient[idx];
+          toifl += gradient[idx] * velocityDelta[idx];
+        }
+        double denom = 0;
+        for (int i = 0; i < D; ++i) denom += gradient[i] * gradient[i];
+        monti *= velocityDelta[k] / denom;
+        toifl *= -gradient[k] / denom;
+        const double osher = lsv * localNormal[k];
+        sa[st][k] = std::fabs(monti + toifl + osher);
+      }
+      // incrementIndex, :196-204
+      int dim = 0;
+      for (; dim < D - 1; ++dim) {
+        if (cur[dim] < 1) break;
+        cur[dim] = -1;
+      }
+      ++cur[dim];
+    }
+    double dissipation = 0.;
+    for (int d = 0; d < D; ++d) {
+      int o[D];
+      for (int e = 0; e < D; ++e) o[e] = 0;
+      double v[3];
+      for (int j = 0; j < 3; ++j) {
+        o[d] = j - 1;
+        v[j] = VI(o);
+      }
+      const double dNeg = (v[1] - v[0]) / gridDelta;
+      const double dPos = (v[2] - v[1]) / gridDelta;
+      const double gradientDiff = (dPos - dNeg) * 0.5; // :183-187
+      double maxAlpha = 0;
+      for (int i = 0; i < numStencil; ++i) maxAlpha = stdMax(maxAlpha, sa[i][d]);
+      const double finalAlpha = stdMin(maxAlpha, S.P.maxDissipation);
+      alphas[d] = finalAlpha;
+      dissipation += finalAlpha * gradientDiff;
+    }
+    alphas[3] = 1.;
+    return {hamiltonian, dissipation};
+  }
 
   if (sch == VLSG_WENO_3RD_ORDER || sch == VLSG_WENO_5TH_ORDER) {
     // lsWENO.hpp:53-160
@@ -586,6 +719,11 @@ template <int D> struct Advector {
     std::vector<double> tmin(nt, maxTimeStep);
     std::vector<std::array<double, 3>> alp(nt, std::array<double, 3>{0, 0, 0});
     const SchemeCtx<D> S{t, P, vel, globalAlphas};
+    // StencilLocalLaxFriedrichs bounds dt with the finalAlphas of its last
+    // call that got past the zero-velocity return; with one thread that is
+    // the last such call in HRLE order (lsAdvect.hpp:599-606)
+    const bool sllf = P.spatial == VLSG_STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER;
+    std::vector<std::array<double, 4>> sllfLast(sllf ? n : 0, std::array<double, 4>{0, 0, 0, 0});
     const std::vector<uint64_t> ids = vel.cb ? pointIds<D>(t) : std::vector<uint64_t>();
     const double adaptiveFactor = 1.0 / P.adaptiveSubdivisions;
 #pragma omp parallel for schedule(static)
@@ -601,7 +739,8 @@ template <int D> struct Advector {
         std::pair<double, double> gd{0., 0.};
         for (int lower = 0; lower < L; ++lower) {
           if (lss[lower].at(key) <= value + Params::wrappingLayerEpsilon) {
-            gd = evalScheme<D>(S, key, vel.cb ? ids[activePos[a]] : 0, lower, alp[th].data());
+            gd = evalScheme<D>(S, key, vel.cb ? ids[activePos[a]] : 0, lower,
+                               sllf ? sllfLast[a].data() : alp[th].data());
             break;
           }
         }
@@ -655,6 +794,12 @@ template <int D> struct Advector {
       double fa[3] = {0, 0, 0};
       if (s == VLSG_LAX_FRIEDRICHS_1ST_ORDER || s == VLSG_LAX_FRIEDRICHS_2ND_ORDER) {
         for (int i = 0; i < D; ++i) fa[i] = globalAlphas[i];
+      } else if (sllf) {
+        for (int64_t a = n - 1; a >= 0; --a)
+          if (sllfLast[a][3] != 0.) {
+            for (int i = 0; i < D; ++i) fa[i] = sllfLast[a][i];
+            break;
+          }
       } else {
         for (int th = 0; th < nt; ++th)
           for (int i = 0; i < D; ++i) fa[i] = stdMax(fa[i], alp[th][i]);
@@ -724,9 +869,13 @@ template <int D> struct Advector {
     t.finalizeMap();
   }
 
-  void rebuildLS() { rebuild<D>(top(), 1.0, 2); } // :250-256 (SLLF: 1.5, 3)
+  void rebuildLS() { // :250-256
+    if (P.spatial == VLSG_STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER) rebuild<D>(top(), 1.5, 3);
+    else rebuild<D>(top(), 1.0, 2);
+  }
 
-  void adjustLowerLayers() { // :802-813
+  void adjustLowerLayers() { // :802-813 (not with StencilLocalLaxFriedrichs)
+    if (P.spatial == VLSG_STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER) return;
     for (size_t i = 0; i + 1 < lss.size(); ++i)
       booleanOp<D>(lss[i], top(), maxComp);
   }

@@ -59,6 +59,7 @@ vlso::Params toParams(const vlsg_advect_params *p) {
   P.adaptiveSubdivisions = p->adaptive_subdivisions < 1 ? 1 : p->adaptive_subdivisions;
   P.checkDissipation = p->check_dissipation != 0;
   P.maxSteps = p->max_steps ? p->max_steps : 10000000u;
+  if (p->max_dissipation > 0) P.maxDissipation = p->max_dissipation;
   return P;
 }
 

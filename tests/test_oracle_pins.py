@@ -4,6 +4,9 @@
   analytic result, for EO1 / WENO3 / WENO5 x FE / RK2 / RK3.
 - BooleanOperationExactZero (result.hpp): the golden run list of Box u Plane
   after the boolean operation's Prune passes (2D, reflective x).
+- StencilLocalLaxFriedrichs.cpp:33-84: a sphere of radius 1 grown at v = 1
+  for t = 0.5 with STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER, Chamfer distance
+  to the radius-1.5 sphere < 0.035.
 - LSTEST_ASSERT_VALID_LS (lsTestAsserts.hpp:11-23) after every advection.
 """
 import json
@@ -49,6 +52,22 @@ def test_time_integration_chamfer(ti_setup, spatial, temporal, threshold):
     assert ls.check() == 0
     c = O.chamfer(ref, ls)
     assert c["chamfer"] < threshold
+
+
+def test_stencil_llf_sphere_chamfer():
+    from viennals_b200.velocity import constant_scalar
+
+    g = Grid([-3, 3, -3, 3, -3, 3], [BC.INFINITE_BOUNDARY] * 3, 0.1)
+    ls = O.OracleLS(g, make_sphere(g, [0, 0, 0], 1.0))
+    ref = O.OracleLS(g, make_sphere(g, [0, 0, 0], 1.5))
+    p = AdvectParams.defaults()
+    p.spatial_scheme = 9  # STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER
+    p.advection_time = 0.5
+    res = O.advect([ls], p, constant_scalar(1.0))
+    assert res.advected_time == pytest.approx(0.5)
+    assert ls.check() == 0
+    c = O.chamfer(ref, ls)
+    assert c["chamfer"] < 0.035
 
 
 def test_boolean_exact_zero_golden():

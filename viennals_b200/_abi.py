@@ -70,6 +70,7 @@ class AdvectParams(ctypes.Structure):
         ("save_advection_velocities", ctypes.c_int32),
         ("update_point_data", ctypes.c_int32),
         ("max_steps", ctypes.c_uint32),
+        ("max_dissipation", ctypes.c_double),
     ]
 
     @classmethod
@@ -90,6 +91,7 @@ class AdvectParams(ctypes.Structure):
         p.save_advection_velocities = 0
         p.update_point_data = 1
         p.max_steps = 0
+        p.max_dissipation = 0.0  # no limit
         return p
 
 

@@ -278,6 +278,11 @@ class Advect:
     def setUpdatePointData(self, b):
         self.params.update_point_data = int(bool(b))
 
+    def setMaxDissipation(self, d):
+        """StencilLocalLaxFriedrichsScalar.setMaxDissipation (a class-wide
+        static in the reference, per Advect object here)."""
+        self.params.max_dissipation = float(d)
+
     def setVelocityUpdateCallback(self, cb):
         raise RuntimeError("setVelocityUpdateCallback is not supported by the GPU front")
 

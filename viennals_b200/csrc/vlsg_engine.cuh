@@ -112,7 +112,7 @@ public:
   enum { X_FLAGS, X_POS, X_OB, X_BOUNDS, X_C, X_P, X_SUMS, X_BOX, X_IDX, X_VAL, X_GC, X_GE,
          X_ROWC, X_ROWG, X_PB, X_GB, X_RSTART, X_RSIGN, X_RPB, X_KEEP, X_KPOS, X_OSTART,
          X_OSIGN, X_VCNT, X_VOFF, X_VSUMS, X_QC, X_QM, X_QN, X_QP, X_VS, X_VV, X_AD, X_AM,
-         X_AC, X_AV, X_COUNT };
+         X_AC, X_AV, X_SKEY, X_SALPHA, X_QC2, X_QN2, X_QM2, X_QP2, X_VS2, X_COUNT };
   // pinned host staging of the velocity callback's queries and answers
   struct PinScratch {
     void *p = nullptr;
@@ -647,9 +647,13 @@ public:
     frontierPass<FP_PRUNE>(b, PruneRule<T>{rsz}, "prune");
     buf[b].width = 2;
   }
+  // rebuildLS: cutoff 1 and width 2, or 1.5 and 3 for StencilLocalLaxFriedrichs
+  // (lsAdvect.hpp:250-256)
+  double rebuildCutoff = 1.0;
+  int rebuildWidth = 2;
   void rebuild(int b) {
-    frontierPass<FP_ALL>(b, RebuildRule<T>{1.0}, "rebuild");
-    buf[b].width = 2;
+    frontierPass<FP_ALL>(b, RebuildRule<T>{T(rebuildCutoff)}, "rebuild");
+    buf[b].width = rebuildWidth;
     buf[b].bound = 1.0;
   }
   // updateLevelSet (value update + Reduce(1)) followed by rebuildLS
@@ -673,15 +677,15 @@ public:
       });
       uint8_t *visitOut = visit[1 - vcur];
       VLSG_CUDA(cudaMemsetAsync(visitOut, 0, cap, stream));
-      kUpdateRebuild<T><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(topo(), lsView(top), act, 1.0,
-                                                                     changeLog(), visitOut);
+      kUpdateRebuild<T><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(
+          topo(), lsView(top), act, rebuildCutoff, changeLog(), visitOut);
       vcur ^= 1;
       visitBuf = top;
       checkLaunch();
     }
     applyChanges(top);
     buf[top].cur ^= 1;
-    buf[top].width = 2;
+    buf[top].width = rebuildWidth;
     buf[top].bound = 1.0;
     ++stages;
   }
@@ -798,6 +802,16 @@ public:
     } else {
       A.alphaMax = nullptr;
     }
+    const bool stencil = s == VLSG_STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER;
+    const int rateWarps = blocksRate * (RATE_THREADS / 32);
+    if (stencil) {
+      // the time-step alphas come from the last passing call (kSllfPick)
+      A.alphaMax = nullptr;
+      A.sllfEps = std::cbrt(std::numeric_limits<double>::epsilon());
+      A.maxDissipation = P.max_dissipation > 0 ? P.max_dissipation : DBL_MAX;
+      A.sllfKey = scratch<unsigned long long>(X_SKEY, rateWarps);
+      A.sllfAlpha = scratch<double>(X_SALPHA, 3 * (size_t)rateWarps);
+    }
     if (velCb) gatherVelocities<0>(A);
     {
       // stencil input (each band value once) + output per active point
@@ -806,8 +820,20 @@ public:
         lastBand = (int64_t)readU64(rateCounts + 1);
         return double(sizeof(T)) * double(lastBand + lastActive);
       });
-      if (velCb) kRates<T, 0, true><<<blocksRate, RATE_THREADS, 0, stream>>>(A, vel);
-      else kRates<T, 0><<<blocksRate, RATE_THREADS, 0, stream>>>(A, vel);
+      const bool weno = s == VLSG_WENO_3RD_ORDER || s == VLSG_WENO_5TH_ORDER;
+      if (stencil) {
+        if (velCb) kRates<T, 0, true, FAM_STENCIL><<<blocksRate, RATE_THREADS, 0, stream>>>(A, vel);
+        else kRates<T, 0, false, FAM_STENCIL><<<blocksRate, RATE_THREADS, 0, stream>>>(A, vel);
+        checkLaunch();
+        kSllfPick<<<1, 1024, 0, stream>>>(A.sllfKey, A.sllfAlpha, rateWarps, scal + 1);
+      } else if (weno) {
+        if (velCb) kRates<T, 0, true, FAM_WENO><<<blocksRate, RATE_THREADS, 0, stream>>>(A, vel);
+        else kRates<T, 0, false, FAM_WENO><<<blocksRate, RATE_THREADS, 0, stream>>>(A, vel);
+      } else if (velCb) {
+        kRates<T, 0, true><<<blocksRate, RATE_THREADS, 0, stream>>>(A, vel);
+      } else {
+        kRates<T, 0><<<blocksRate, RATE_THREADS, 0, stream>>>(A, vel);
+      }
       checkLaunch();
     }
     VLSG_CUDA(cudaMemcpyAsync(pinScal, scal, sizeof(init), cudaMemcpyDeviceToHost, stream));
@@ -875,27 +901,54 @@ public:
     A.velV = vv;
     A.velSites = sites;
     A.alphaTab = nullptr;
+    A.velS2 = nullptr;
     if (!nQ) return;
     kVelGather<T, MODE><<<blocksRate, RATE_THREADS, 0, stream>>>(A, R, sites, qc, qm, qn, qp);
     checkLaunch();
-    double *hc = pinned<double>(H_QC, 3 * nQ);
-    int32_t *hm = pinned<int32_t>(H_QM, nQ);
-    double *hn = pinned<double>(H_QN, 3 * nQ);
-    uint64_t *hp = pinned<uint64_t>(H_QP, nQ);
-    double *hsv = pinned<double>(H_VS, nQ);
-    double *hvv = pinned<double>(H_VV, 3 * nQ);
-    VLSG_CUDA(cudaMemcpyAsync(hc, qc, 3 * nQ * sizeof(double), cudaMemcpyDeviceToHost, stream));
-    VLSG_CUDA(cudaMemcpyAsync(hm, qm, nQ * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
-    VLSG_CUDA(cudaMemcpyAsync(hn, qn, 3 * nQ * sizeof(double), cudaMemcpyDeviceToHost, stream));
-    VLSG_CUDA(cudaMemcpyAsync(hp, qp, nQ * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream));
-    syncErr("velocity queries");
-    hostPool(nQ, [&](size_t i, int64_t n) {
-      return velCb(velUser, n, hc + 3 * i, hm + i, hn + 3 * i, hp + i, hsv + i, hvv + 3 * i);
-    }, "the velocity callback returned ");
-    VLSG_CUDA(cudaMemcpyAsync(vs, hsv, nQ * sizeof(double), cudaMemcpyHostToDevice, stream));
-    VLSG_CUDA(cudaMemcpyAsync(vv, hvv, 3 * nQ * sizeof(double), cudaMemcpyHostToDevice, stream));
+    askVelocity(nQ, qc, qm, qn, qp, vs, vv);
     if (MODE == 0 && A.scheme == VLSG_LOCAL_LAX_FRIEDRICHS_ANALYTICAL_1ST_ORDER && alphaCb)
       gatherAlphas(A, nAct);
+    if (MODE == 0 && A.scheme == VLSG_STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER) {
+      // second round: the nudged normals, which depend on the first answers
+      const size_t n2 = nAct * (size_t)L * 162;
+      if (n2 > ((size_t)1 << 28))
+        throw CudaError("velocity callback: more than 2^28 queries in one rate pass",
+                        VLSG_ERR_CAPACITY);
+      double *qc2 = scratch<double>(X_QC2, 3 * n2);
+      double *qn2 = scratch<double>(X_QN2, 3 * n2);
+      int32_t *qm2 = scratch<int32_t>(X_QM2, n2);
+      uint64_t *qp2 = scratch<uint64_t>(X_QP2, n2);
+      double *vs2 = scratch<double>(X_VS2, n2);
+      kStencilGather<T><<<blocksRate, RATE_THREADS, 0, stream>>>(A, R, qc2, qm2, qn2, qp2);
+      checkLaunch();
+      askVelocity(n2, qc2, qm2, qn2, qp2, vs2, nullptr);
+      A.velS2 = vs2;
+    }
+  }
+
+  // The velocity callback on n queries staged on the device; the scalar (and,
+  // with vOut, the vector) answers land in device arrays, stream-ordered.
+  void askVelocity(size_t n, const double *qc, const int32_t *qm, const double *qn,
+                   const uint64_t *qp, double *sOut, double *vOut) {
+    // earlier copies out of the pinned staging buffers are complete
+    VLSG_CUDA(cudaStreamSynchronize(stream));
+    double *hc = pinned<double>(H_QC, 3 * n);
+    int32_t *hm = pinned<int32_t>(H_QM, n);
+    double *hn = pinned<double>(H_QN, 3 * n);
+    uint64_t *hp = pinned<uint64_t>(H_QP, n);
+    double *hsv = pinned<double>(H_VS, n);
+    double *hvv = pinned<double>(H_VV, 3 * n);
+    VLSG_CUDA(cudaMemcpyAsync(hc, qc, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    VLSG_CUDA(cudaMemcpyAsync(hm, qm, n * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+    VLSG_CUDA(cudaMemcpyAsync(hn, qn, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    VLSG_CUDA(cudaMemcpyAsync(hp, qp, n * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream));
+    syncErr("velocity queries");
+    hostPool(n, [&](size_t i, int64_t m) {
+      return velCb(velUser, m, hc + 3 * i, hm + i, hn + 3 * i, hp + i, hsv + i, hvv + 3 * i);
+    }, "the velocity callback returned ");
+    VLSG_CUDA(cudaMemcpyAsync(sOut, hsv, n * sizeof(double), cudaMemcpyHostToDevice, stream));
+    if (vOut)
+      VLSG_CUDA(cudaMemcpyAsync(vOut, hvv, 3 * n * sizeof(double), cudaMemcpyHostToDevice, stream));
   }
 
   // LocalLaxFriedrichsAnalytical with host callbacks: every active point x
@@ -910,6 +963,7 @@ public:
     double *av = scratch<double>(X_AV, nA);
     kAlphaGather<T><<<blocksRate, RATE_THREADS, 0, stream>>>(A, ad, am, ac);
     checkLaunch();
+    VLSG_CUDA(cudaStreamSynchronize(stream));
     int32_t *hd = pinned<int32_t>(H_AD, nA);
     int32_t *hm = pinned<int32_t>(H_AM, nA);
     double *hc = pinned<double>(H_AC, 3 * nA);
@@ -1040,6 +1094,9 @@ public:
 
   void apply(const vlsg_advect_params &P, vlsg_advect_result &r) override {
     ++generation;
+    const bool sllf = P.spatial_scheme == VLSG_STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER;
+    rebuildCutoff = sllf ? 1.5 : 1.0;
+    rebuildWidth = sllf ? 3 : 2;
     pointUpdates = 0;
     stages = 0;
     const uint64_t l0 = launches;

@@ -96,6 +96,7 @@ inline int schemeWidth(int s) {
   case VLSG_LOCAL_LAX_FRIEDRICHS_1ST_ORDER: return 7;
   case VLSG_LOCAL_LAX_FRIEDRICHS_2ND_ORDER: return 9;
   case VLSG_LOCAL_LAX_FRIEDRICHS_ANALYTICAL_1ST_ORDER: return 7;
+  case VLSG_STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER: return 8;
   case VLSG_WENO_3RD_ORDER: return 5;
   case VLSG_WENO_5TH_ORDER: return 7;
   default: return -1;

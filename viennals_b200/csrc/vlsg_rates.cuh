@@ -20,6 +20,8 @@
 // j * poolCells + q).
 #pragma once
 
+#include <type_traits>
+
 #include "vlsg_common.cuh"
 #include "vlsg_frontier.cuh"
 #include "vlsg_passes.cuh"
@@ -89,9 +91,18 @@ struct TableVel {
   int sites;
   const double *a; // alphas: ((p * L + material) * 27 + q) * 3 + dir, or none
   size_t alphaBase;
+  // StencilLocalLaxFriedrichs: sites 28.. (nudged normals, scalar only) at
+  // (p * L + material) * 162 + site - 28
+  const double *s2;
+  size_t base2;
   template <class T>
   __device__ void get(int material, const T n[3], int site, T &sv, T vv[3]) const {
     (void)n;
+    if (site >= 28) {
+      sv = T(s2[base2 + (size_t)material * 162 + (site - 28)]);
+      vv[0] = vv[1] = vv[2] = T(0);
+      return;
+    }
     const size_t i = base + (size_t)material * sites + site;
     sv = T(s[i]);
     for (int k = 0; k < 3; ++k) vv[k] = T(v[3 * i + k]);
@@ -135,6 +146,13 @@ template <class T> struct RateArgs {
   const double *velS, *velV;
   int velSites;
   const double *alphaTab; // LocalLaxFriedrichsAnalytical: the alpha callback's answers
+  const double *velS2;    // StencilLocalLaxFriedrichs: the nudged-normal answers
+  // StencilLocalLaxFriedrichs: baseNormalEpsilon, the dissipation limit, and
+  // per warp the last (HRLE order) call's finalAlphas: key, alphas
+  double sllfEps;
+  double maxDissipation;
+  unsigned long long *sllfKey;
+  double *sllfAlpha;
 };
 
 // Reader of the top level set around one active point.
@@ -279,14 +297,152 @@ __device__ inline void boxDifferences(const St &S, T gridDelta, int q, T cd[3]) 
   }
 }
 
-// One scheme evaluation (Hamiltonian, dissipation) for `material`.
+// StencilLocalLaxFriedrichsScalar's FIRST_ORDER gradient component i at
+// box offset (ox, oy, oz): the three values along i are taken with
+// coordinate i set to -1, 0, 1 whatever the offset's (calculateGradient /
+// calculateNormal, lsStencilLocalLaxFriedrichsScalar.hpp:336-378;
+// FiniteDifferences, lsFiniteDifferences.hpp:132-181).
+template <class T, class St>
+__device__ inline T sllfGrad(const St &S, double delta, int ox, int oy, int oz, int i) {
+  T v[3];
+  for (int j = 0; j < 3; ++j)
+    v[j] = S.at(i == 0 ? j - 1 : ox, i == 1 ? j - 1 : oy, i == 2 ? j - 1 : oz);
+  const T dNeg = T((v[1] - v[0]) / delta);
+  const T dPos = T((v[2] - v[1]) / delta);
+  return T((dPos + dNeg) * 0.5);
+}
+template <class T, class St>
+__device__ inline void sllfNormal(const St &S, double delta, int ox, int oy, int oz, T n[3]) {
+  T modulus = 0.;
+  for (int i = 0; i < 3; ++i) {
+    n[i] = sllfGrad<T>(S, delta, ox, oy, oz, i);
+    modulus += n[i] * n[i];
+  }
+  modulus = T(1) / sqrt(modulus);
+  for (int i = 0; i < 3; ++i) n[i] *= modulus;
+}
+// calculateSimpleAdaptiveEpsilon (ADAPTIVE_EPSILON_STRATEGY 1, :60-75)
+template <class T> __device__ inline T sllfEpsilon(T velocity, double baseNormalEpsilon, double delta) {
+  const T absVel = fabs(velocity);
+  const T baseEps = T(baseNormalEpsilon * delta);
+  if (absVel > T(1e-10)) {
+    const T scale = stdMax(T(0.1), stdMin(T(10.0), absVel));
+    return baseEps * scale;
+  }
+  return baseEps;
+}
+
+// StencilLocalLaxFriedrichsScalar<T,3,1>::operator() (:219-400).  Velocity
+// sites: 0 the point, 1 + q the stencil point q (x fastest), 28 + 6q + 2k
+// (+1) the normal of q nudged by -DN (+DN) along k.  alphas[0..2] receive
+// this call's finalAlphas and alphas[3] = 1 when the call gets past the
+// zero-velocity return.
 template <class T, class St, class Vel>
+__device__ void evalStencilLLF(const RateArgs<T> &A, const Vel &vel, const St &S, int material,
+                               T *alphas, T &outG, T &outD) {
+  const double delta = A.g.delta;
+  T normalVector[3];
+  sllfNormal<T>(S, delta, 0, 0, 0, normalVector);
+  T sv0, vv0[3];
+  vel.get(material, normalVector, 0, sv0, vv0);
+  double scalarVelocity = (double)sv0;
+  for (int i = 0; i < 3; ++i) scalarVelocity += (double)(vv0[i] * normalVector[i]);
+  if (scalarVelocity == 0.) {
+    outG = 0;
+    outD = 0;
+    return;
+  }
+  T gradSq = 0;
+  for (int i = 0; i < 3; ++i) {
+    const T gi = sllfGrad<T>(S, delta, 0, 0, 0, i);
+    gradSq += gi * gi;
+  }
+  const T hamiltonian = T((double)sqrt(gradSq) * scalarVelocity);
+  T maxAlpha[3] = {0, 0, 0};
+  int cx = -1, cy = -1, cz = -1;
+  for (int st = 0; st < 27; ++st) {
+    T ln[3];
+    sllfNormal<T>(S, delta, cx, cy, cz, ln);
+    // a corrupted normal leaves the stencil index where it is (:288-293)
+    if (fabs(ln[0]) < T(1e-6) && fabs(ln[1]) < T(1e-6) && fabs(ln[2]) < T(1e-6)) continue;
+    const int q = (cz + 1) * 9 + (cy + 1) * 3 + (cx + 1);
+    T lsv, lvv[3];
+    vel.get(material, ln, 1 + q, lsv, lvv);
+    for (int dir = 0; dir < 3; ++dir) lsv += lvv[dir] * ln[dir];
+    const T DN = sllfEpsilon<T>(lsv, A.sllfEps, delta);
+    T np[3] = {ln[0], ln[1], ln[2]}, nn[3] = {ln[0], ln[1], ln[2]}, vd[3];
+    for (int k = 0; k < 3; ++k) {
+      np[k] -= DN;
+      nn[k] += DN;
+      T vp, vn, unused[3];
+      vel.get(material, np, 28 + 6 * q + 2 * k, vp, unused);
+      vel.get(material, nn, 28 + 6 * q + 2 * k + 1, vn, unused);
+      vd[k] = T((double)(vn - vp) / (2.0 * (double)DN));
+      np[k] += DN;
+      nn[k] -= DN;
+    }
+    T gr[3];
+    for (int i = 0; i < 3; ++i) gr[i] = sllfGrad<T>(S, delta, cx, cy, cz, i);
+    T denom = 0;
+    for (int i = 0; i < 3; ++i) denom += gr[i] * gr[i];
+    for (int k = 0; k < 3; ++k) {
+      T monti = 0, toifl = 0;
+      for (int j = 0; j < 2; ++j) {
+        const int idx = (k + 1 + j) % 3;
+        monti += gr[idx] * gr[idx];
+        toifl += gr[idx] * vd[idx];
+      }
+      monti *= vd[k] / denom;
+      toifl *= -gr[k] / denom;
+      const T osher = lsv * ln[k];
+      maxAlpha[k] = stdMax(maxAlpha[k], T(fabs(monti + toifl + osher)));
+    }
+    // incrementIndex, x fastest (:196-204)
+    if (cx < 1) {
+      ++cx;
+    } else {
+      cx = -1;
+      if (cy < 1) {
+        ++cy;
+      } else {
+        cy = -1;
+        ++cz;
+      }
+    }
+  }
+  T dissipation = 0.;
+  for (int d = 0; d < 3; ++d) {
+    T v[3];
+    for (int j = 0; j < 3; ++j) v[j] = S.at(d == 0 ? j - 1 : 0, d == 1 ? j - 1 : 0, d == 2 ? j - 1 : 0);
+    const T dNeg = T((v[1] - v[0]) / delta);
+    const T dPos = T((v[2] - v[1]) / delta);
+    const T gradientDiff = T((dPos - dNeg) * 0.5);
+    const T finalAlpha = stdMin(maxAlpha[d], T(A.maxDissipation));
+    alphas[d] = finalAlpha;
+    dissipation += finalAlpha * gradientDiff;
+  }
+  alphas[3] = T(1);
+  outG = hamiltonian;
+  outD = dissipation;
+}
+
+// One scheme evaluation (Hamiltonian, dissipation) for `material`.
+// Scheme families a rate kernel is compiled for: every scheme but the
+// stencil one (chosen at run time), WENO only, StencilLocalLaxFriedrichs only.
+enum : int { FAM_ANY = 0, FAM_WENO = 1, FAM_STENCIL = 2 };
+
+template <class T, class St, class Vel, int FAM = FAM_ANY>
 __device__ void evalScheme(const RateArgs<T> &A, const Vel &vel,
                            const St &S, T C, int material, T *alphas,
                            T &outG, T &outD) {
+  if constexpr (FAM == FAM_STENCIL) {
+    (void)C;
+    evalStencilLLF<T>(A, vel, S, material, alphas, outG, outD);
+    return;
+  }
   const T gridDelta = T(A.g.delta);
   const int sch = A.scheme;
-  if (sch == VLSG_WENO_3RD_ORDER || sch == VLSG_WENO_5TH_ORDER) {
+  if (FAM == FAM_WENO || sch == VLSG_WENO_3RD_ORDER || sch == VLSG_WENO_5TH_ORDER) {
     const int r = sch == VLSG_WENO_3RD_ORDER ? 2 : 3;
     T gradPosTotal = 0, gradNegTotal = 0;
     T wMinus[3], wPlus[3], st[7];
@@ -338,6 +494,9 @@ __device__ void evalScheme(const RateArgs<T> &A, const Vel &vel,
     outD = 0;
     return;
   }
+  if constexpr (FAM == FAM_WENO) {
+    return;
+  } else {
   const int order = (sch == VLSG_ENGQUIST_OSHER_2ND_ORDER ||
                      sch == VLSG_LAX_FRIEDRICHS_2ND_ORDER ||
                      sch == VLSG_LOCAL_LOCAL_LAX_FRIEDRICHS_2ND_ORDER ||
@@ -486,6 +645,7 @@ __device__ void evalScheme(const RateArgs<T> &A, const Vel &vel,
     dissipation += alphaFactor * alpha[i] * (gradNeg[i] - gradPos[i]) * T(0.5);
   outG = totalGrad;
   outD = dissipation;
+  }
 }
 
 template <class T>
@@ -519,7 +679,7 @@ __device__ inline unsigned long long warpMaxU64(unsigned long long b) {
 // integrateTime for one active point (lsAdvect.hpp:501-592): the material
 // chain, the stored rates (velocity as updateLevelSet applies it,
 // lsAdvect.hpp:738-744, and the stop value) and the point's time budget.
-template <class T, class St, class Vel>
+template <class T, class St, class Vel, int FAM = FAM_ANY>
 __device__ inline double ratePoint(const RateArgs<T> &A, const Vel &vel,
                                    const St &S, int slot, int c, T C, T *alphas) {
   const int L = A.L;
@@ -533,7 +693,7 @@ __device__ inline double ratePoint(const RateArgs<T> &A, const Vel &vel,
     for (int lower = 0; lower < L; ++lower) {
       const T lv = lower == L - 1 ? C : lsValueAt<T>(A.ls[lower], slot, c);
       if ((double)lv <= (double)value + 1e-4) {
-        evalScheme<T>(A, vel, S, C, lower, alphas, g, d);
+        evalScheme<T, St, Vel, FAM>(A, vel, S, C, lower, alphas, g, d);
         break;
       }
     }
@@ -619,7 +779,7 @@ template <class T> constexpr int rateMinBlocks() { return sizeof(T) == 4 ? 3 : 2
 // MODE 0: rates (integrateTime); MODE 1: the global alphas of the
 // Lax-Friedrichs schemes (findGlobalAlphas).  TABLE: velocities from the
 // host callback's table instead of the device functor.
-template <class T, int MODE, bool TABLE = false>
+template <class T, int MODE, bool TABLE = false, int FAM = FAM_ANY>
 __global__ void __launch_bounds__(RATE_THREADS, rateMinBlocks<T>())
     kRates(RateArgs<T> A, const vlsg_velocity_desc desc) {
   __shared__ uint16_t sList[RATE_THREADS / 32][BV];
@@ -631,6 +791,9 @@ __global__ void __launch_bounds__(RATE_THREADS, rateMinBlocks<T>())
   const int L = A.L;
   const Buf<T> &top = A.ls[L - 1];
   unsigned long long minBits = ~0ull, alphaMax[3] = {0, 0, 0}, nAct = 0, nBand = 0;
+  // StencilLLF: HRLE key and finalAlphas of this thread's last passing call
+  unsigned long long lastKey = 0;
+  T lastAlpha[3] = {0, 0, 0};
   for (int w = warp; w < n; w += nWarps) {
     const int slot = A.slotList[w];
     const uint64_t own = lane < 8 ? A.def[(size_t)slot * 8 + lane] : 0ull;
@@ -649,19 +812,38 @@ __global__ void __launch_bounds__(RATE_THREADS, rateMinBlocks<T>())
       const auto vel = [&] {
         if constexpr (TABLE)
           return TableVel{A.velS, A.velV, ((size_t)A.actOff[w] + k) * L * A.velSites,
-                          A.velSites, A.alphaTab, ((size_t)A.actOff[w] + k) * L * 81};
+                          A.velSites, A.alphaTab, ((size_t)A.actOff[w] + k) * L * 81,
+                          A.velS2, ((size_t)A.actOff[w] + k) * L * 162};
         else
           return FunctorVel{desc};
       }();
       withStencil<T>(A, slot, c, [&](const auto &S, T value) {
         if constexpr (MODE == 0) {
-          T alphas[3] = {0, 0, 0};
-          const double step = ratePoint<T>(A, vel, S, slot, c, value, alphas);
+          constexpr bool STENCIL = FAM == FAM_STENCIL;
+          T alphas[STENCIL ? 4 : 3] = {};
+          const double step =
+              ratePoint<T, std::decay_t<decltype(S)>, std::decay_t<decltype(vel)>, FAM>(
+                  A, vel, S, slot, c, value, alphas);
           const unsigned long long sb = stepBits(step);
           minBits = sb < minBits ? sb : minBits;
-          for (int d = 0; d < 3; ++d) {
-            const unsigned long long ab = alphaBits((double)alphas[d]);
-            alphaMax[d] = ab > alphaMax[d] ? ab : alphaMax[d];
+          if constexpr (STENCIL) {
+            if (alphas[3] != T(0)) {
+              int bx, by, bz;
+              brickCoords(A.g, A.m.slotBrick[slot], bx, by, bz);
+              const unsigned long long x = A.g.org[0] + bx * BS + (c & 7) + (1 << 20),
+                                       y = A.g.org[1] + by * BS + ((c >> 3) & 7) + (1 << 20),
+                                       z = A.g.org[2] + bz * BS + (c >> 6) + (1 << 20);
+              const unsigned long long key = (z << 42) | (y << 21) | x;
+              if (key > lastKey) {
+                lastKey = key;
+                for (int d = 0; d < 3; ++d) lastAlpha[d] = alphas[d];
+              }
+            }
+          } else {
+            for (int d = 0; d < 3; ++d) {
+              const unsigned long long ab = alphaBits((double)alphas[d]);
+              alphaMax[d] = ab > alphaMax[d] ? ab : alphaMax[d];
+            }
           }
         } else {
         for (int lower = 0; lower < L; ++lower) {
@@ -691,6 +873,14 @@ __global__ void __launch_bounds__(RATE_THREADS, rateMinBlocks<T>())
       });
     }
   }
+  if constexpr (FAM == FAM_STENCIL && MODE == 0) {
+    const unsigned long long best = warpMaxU64(lastKey);
+    const unsigned owner = __ballot_sync(0xffffffffu, best != 0ull && lastKey == best);
+    if (best == 0ull ? lane == 0 : (owner >> lane) & 1u) {
+      A.sllfKey[warp] = best;
+      for (int d = 0; d < 3; ++d) A.sllfAlpha[3 * warp + d] = (double)lastAlpha[d];
+    }
+  }
   minBits = warpMinU64(minBits);
   for (int d = 0; d < 3; ++d) alphaMax[d] = warpMaxU64(alphaMax[d]);
   for (int o = 16; o > 0; o >>= 1) {
@@ -706,6 +896,34 @@ __global__ void __launch_bounds__(RATE_THREADS, rateMinBlocks<T>())
       if (nAct) atomicAdd(&A.counts[0], nAct);
       if (nBand) atomicAdd(&A.counts[1], nBand);
     }
+  }
+}
+
+// StencilLocalLaxFriedrichs time-step alphas: the finalAlphas of the warp
+// entry with the largest HRLE key (the last passing call in HRLE order) go to
+// alphaOut[0..2] as double bits; nothing is written when no call passed.
+__global__ void __launch_bounds__(1024)
+    kSllfPick(const unsigned long long *key, const double *alpha, int n,
+              unsigned long long *alphaOut) {
+  __shared__ unsigned long long sk[32];
+  __shared__ int si[32];
+  unsigned long long best = 0;
+  int bi = -1;
+  for (int i = threadIdx.x; i < n; i += blockDim.x)
+    if (key[i] > best) best = key[i], bi = i;
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long k2 = __shfl_xor_sync(0xffffffffu, best, o);
+    const int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
+    if (k2 > best) best = k2, bi = i2;
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) sk[wid] = best, si[wid] = bi;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
+      if (sk[w] > best) best = sk[w], bi = si[w];
+    if (best != 0ull && bi >= 0)
+      for (int d = 0; d < 3; ++d) alphaOut[d] = (unsigned long long)__double_as_longlong(alpha[3 * bi + d]);
   }
 }
 

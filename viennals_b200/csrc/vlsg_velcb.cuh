@@ -30,9 +30,12 @@ namespace { // internal linkage: every compilation unit has its own copy
 
 // Evaluation sites per point: LocalLaxFriedrichs also asks its 27 box
 // neighbours (site 1 + q, x fastest) in the rate pass.
+// StencilLocalLaxFriedrichs asks its 27 stencil points (site 1 + q) in a
+// first round and the nudged normals (kStencilGather) in a second.
 inline int velocitySites(int scheme, int mode) {
   return (mode == 0 && (scheme == VLSG_LOCAL_LAX_FRIEDRICHS_1ST_ORDER ||
-                        scheme == VLSG_LOCAL_LAX_FRIEDRICHS_2ND_ORDER))
+                        scheme == VLSG_LOCAL_LAX_FRIEDRICHS_2ND_ORDER ||
+                        scheme == VLSG_STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER))
              ? 28
              : 1;
 }
@@ -42,6 +45,10 @@ template <class T, class St>
 __device__ inline void centreNormal(const RateArgs<T> &A, const St &S, T C, T n[3]) {
   const int sch = A.scheme;
   n[0] = n[1] = n[2] = T(0);
+  if (sch == VLSG_STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER) {
+    sllfNormal<T>(S, A.g.delta, 0, 0, 0, n);
+    return;
+  }
   if (sch == VLSG_WENO_3RD_ORDER || sch == VLSG_WENO_5TH_ORDER) {
     if (A.dissipationAlpha != 0.0) {
       T denominator = 0;
@@ -197,6 +204,9 @@ __global__ void __launch_bounds__(RATE_THREADS)
             alphaNormal<T>(S, nrm);
           } else if (s == 0) {
             centreNormal<T>(A, S, C, nrm);
+          } else if (A.scheme == VLSG_STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER) {
+            const int q = s - 1;
+            sllfNormal<T>(S, delta, q % 3 - 1, (q / 3) % 3 - 1, q / 9 - 1, nrm);
           } else {
             boxNormal<T>(S, T(delta), s - 1, nrm);
           }
@@ -213,6 +223,76 @@ __global__ void __launch_bounds__(RATE_THREADS)
             }
             material[q] = m;
             pid[q] = id;
+          }
+        }
+      });
+    }
+  }
+}
+
+// StencilLocalLaxFriedrichs, second round: the nudged normals of every
+// active point p, material and stencil point q, built from the first
+// round's answers (sites 1 + q) exactly as evalStencilLLF builds them, at
+// (p * L + material) * 162 + 6q + 2k (+1 for +DN).
+template <class T>
+__global__ void __launch_bounds__(RATE_THREADS)
+    kStencilGather(RateArgs<T> A, PointRanks R, double *coord, int32_t *material,
+                   double *normal, uint64_t *pid) {
+  __shared__ uint16_t sList[RATE_THREADS / 32][BV];
+  uint16_t *list = sList[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nWarps = (gridDim.x * blockDim.x) >> 5;
+  const int n = *A.nSlots;
+  const int L = A.L;
+  const Buf<T> &top = A.ls[L - 1];
+  const double delta = A.g.delta;
+  for (int w = warp; w < n; w += nWarps) {
+    const int slot = A.slotList[w];
+    const uint64_t own = lane < 8 ? A.def[(size_t)slot * 8 + lane] : 0ull;
+    uint64_t a = 0ull;
+    if (__any_sync(0xffffffffu, own != 0ull)) a = activePlanes<T>(top.vals, slot);
+    const int total = listCells(a, list);
+    int bx, by, bz;
+    brickCoords(A.g, A.m.slotBrick[slot], bx, by, bz);
+    for (int k = lane; k < total; k += 32) {
+      const int c = list[k];
+      const size_t p = (size_t)A.actOff[w] + k;
+      const uint64_t id = R.of(slot, c);
+      const int idx[3] = {A.g.org[0] + bx * BS + (c & 7), A.g.org[1] + by * BS + ((c >> 3) & 7),
+                          A.g.org[2] + bz * BS + (c >> 6)};
+      T coordinate[3];
+      for (int d = 0; d < 3; ++d) coordinate[d] = T(idx[d] * delta);
+      withStencil<T>(A, slot, c, [&](const auto &S, T) {
+        for (int q = 0; q < 27; ++q) {
+          const int off[3] = {q % 3 - 1, (q / 3) % 3 - 1, q / 9 - 1};
+          T ln[3], crd[3];
+          sllfNormal<T>(S, delta, off[0], off[1], off[2], ln);
+          for (int d = 0; d < 3; ++d) crd[d] = T(coordinate[d] + off[d] * delta);
+          for (int m = 0; m < L; ++m) {
+            const size_t r1 = (p * L + m) * 28 + 1 + q;
+            T lsv = T(A.velS[r1]);
+            T lvv[3];
+            for (int d = 0; d < 3; ++d) lvv[d] = T(A.velV[3 * r1 + d]);
+            for (int dir = 0; dir < 3; ++dir) lsv += lvv[dir] * ln[dir];
+            const T DN = sllfEpsilon<T>(lsv, A.sllfEps, delta);
+            T np[3] = {ln[0], ln[1], ln[2]}, nn[3] = {ln[0], ln[1], ln[2]};
+            for (int kk = 0; kk < 3; ++kk) {
+              np[kk] -= DN;
+              nn[kk] += DN;
+              for (int side = 0; side < 2; ++side) {
+                const size_t e = (p * L + m) * 162 + 6 * q + 2 * kk + side;
+                const T *nv = side ? nn : np;
+                for (int d = 0; d < 3; ++d) {
+                  coord[3 * e + d] = (double)crd[d];
+                  normal[3 * e + d] = (double)nv[d];
+                }
+                material[e] = m;
+                pid[e] = id;
+              }
+              np[kk] += DN;
+              nn[kk] -= DN;
+            }
           }
         }
       });
