@@ -272,6 +272,15 @@ typedef struct vlsg_compare_result {
 int vlsg_compare(vlsg_context *a, int32_t slot_a, vlsg_context *b, int32_t slot_b,
                  vlsg_compare_result *out);
 
+/* PrepareStencilLocalLaxFriedrichs (lsStencilLocalLaxFriedrichsScalar.hpp:
+ * 423-477) on the context's level sets: is_depo[i] tells whether level set i
+ * is deposited on (n entries, missing ones false); the top level set becomes
+ * the layer wrapping STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER advects. */
+int vlsg_prepare_stencil_llf(vlsg_context *ctx, const int32_t *is_depo, int32_t n);
+/* FinalizeStencilLocalLaxFriedrichs (:480-492): restores the usual wrapping
+ * (top = inverted top united with the level set below; needs two). */
+int vlsg_finalize_stencil_llf(vlsg_context *ctx);
+
 /* Velocity plugin: either a device functor or a host callback. */
 int vlsg_set_velocity_functor(vlsg_context *ctx, const vlsg_velocity_desc *v);
 int vlsg_set_velocity_callback(vlsg_context *ctx, vlsg_velocity_cb cb,

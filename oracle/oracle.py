@@ -67,6 +67,8 @@ def lib():
                                   P(AdvectResult)]
         L.vlso_advect_cb.argtypes = [P(vp), i32, P(AdvectParams), VELOCITY_CALLBACK, vp,
                                      ALPHA_CALLBACK, vp, P(AdvectResult)]
+        L.vlso_prepare_stencil_llf.argtypes = [P(vp), i32, P(ctypes.c_int32), i32]
+        L.vlso_finalize_stencil_llf.argtypes = [P(vp), i32]
         L.vlso_last_error.restype = ctypes.c_char_p
         L.vlso_set_threads.argtypes = [i32]
         L.vlso_get_threads.restype = i32
@@ -197,3 +199,16 @@ def advect(level_sets, params, velocity):
     _check(lib().vlso_advect(arr, len(level_sets), ctypes.byref(params),
                              ctypes.byref(desc), ctypes.byref(res)))
     return res
+
+
+def prepare_stencil_llf(level_sets, is_depo):
+    """PrepareStencilLocalLaxFriedrichs on the oracle (top level set replaced)."""
+    arr = (ctypes.c_void_p * len(level_sets))(*[ls.h for ls in level_sets])
+    d = np.asarray([1 if x else 0 for x in is_depo], dtype=np.int32)
+    _check(lib().vlso_prepare_stencil_llf(arr, len(level_sets), _ptr(d, ctypes.c_int32), len(d)))
+
+
+def finalize_stencil_llf(level_sets):
+    """FinalizeStencilLocalLaxFriedrichs on the oracle."""
+    arr = (ctypes.c_void_p * len(level_sets))(*[ls.h for ls in level_sets])
+    _check(lib().vlso_finalize_stencil_llf(arr, len(level_sets)))

@@ -5,6 +5,8 @@
 #include <memory>
 #include <mutex>
 
+#include <type_traits>
+
 #include "vlso_advect.hpp"
 #include "vlso_metrics.hpp"
 
@@ -261,6 +263,42 @@ int vlso_advect_cb(void **lss, int n, const vlsg_advect_params *p, vlsg_velocity
     vs.alphaCb = alphaCb;
     vs.alphaUser = alphaUser;
     return hs[0]->D == 2 ? advectD<2>(hs, n, p, vs, r) : advectD<3>(hs, n, p, vs, r);
+  });
+}
+
+// Prepare / FinalizeStencilLocalLaxFriedrichs on level sets bottom..top.
+int vlso_prepare_stencil_llf(void **lss, int n, const int32_t *isDepo, int nd) {
+  auto **hs = reinterpret_cast<Handle **>(lss);
+  return guarded([&] {
+    if (n < 1) throw std::runtime_error("no level sets");
+    std::vector<bool> depo(nd);
+    for (int i = 0; i < nd; ++i) depo[i] = isDepo[i] != 0;
+    auto run = [&](auto dim) {
+      constexpr int D = decltype(dim)::value;
+      std::vector<vlso::LS<D>> v;
+      for (int i = 0; i < n; ++i) v.push_back(get<D>(hs[i]));
+      vlso::prepareStencilLLF<D>(v, depo);
+      get<D>(hs[n - 1]) = v.back();
+    };
+    if (hs[0]->D == 2) run(std::integral_constant<int, 2>());
+    else run(std::integral_constant<int, 3>());
+    return 0;
+  });
+}
+int vlso_finalize_stencil_llf(void **lss, int n) {
+  auto **hs = reinterpret_cast<Handle **>(lss);
+  return guarded([&] {
+    if (n < 2) throw std::runtime_error("FinalizeStencilLocalLaxFriedrichs needs two level sets");
+    auto run = [&](auto dim) {
+      constexpr int D = decltype(dim)::value;
+      std::vector<vlso::LS<D>> v;
+      for (int i = 0; i < n; ++i) v.push_back(get<D>(hs[i]));
+      vlso::finalizeStencilLLF<D>(v);
+      get<D>(hs[n - 1]) = v.back();
+    };
+    if (hs[0]->D == 2) run(std::integral_constant<int, 2>());
+    else run(std::integral_constant<int, 3>());
+    return 0;
   });
 }
 

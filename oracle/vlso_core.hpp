@@ -174,13 +174,14 @@ template <int D> struct LS {
   std::vector<uint64_t> keys; // sorted, HRLE order
   std::vector<double> vals;   // defined value or +-max (shell)
   int width = 1;              // Domain::levelSetWidth, lsDomain.hpp:42
+  double emptyValue = POS;    // the value everywhere when the map is empty
   HashIndex index;
   int64_t nDefined = 0;
   mutable std::atomic<int64_t> farQueries{0};
 
   LS() = default;
   LS(const LS &o)
-      : grid(o.grid), keys(o.keys), vals(o.vals), width(o.width),
+      : grid(o.grid), keys(o.keys), vals(o.vals), width(o.width), emptyValue(o.emptyValue),
         nDefined(o.nDefined) {
     index.build(keys);
   }
@@ -189,6 +190,7 @@ template <int D> struct LS {
     keys = o.keys;
     vals = o.vals;
     width = o.width;
+    emptyValue = o.emptyValue;
     nDefined = o.nDefined;
     index.build(keys);
     return *this;
@@ -216,7 +218,7 @@ template <int D> struct LS {
   // (a new Domain is filled with POS_VALUE, lsDomain.hpp:64-65).
   double farValue(uint64_t k) const {
     farQueries.fetch_add(1, std::memory_order_relaxed);
-    if (keys.empty()) return POS;
+    if (keys.empty()) return emptyValue;
     // 1. same x-row (keys of a row are contiguous)
     const uint64_t row = k >> KB;
     auto it = std::lower_bound(keys.begin(), keys.end(), k);
@@ -592,6 +594,58 @@ template <int D> void rebuild(LS<D> &ls, double cutoff, int finalWidth) {
     return distance >= -cutoff ? distance : NEG;
   });
   ls.width = finalWidth; // :428
+}
+
+// BooleanOperation INVERT, lsBooleanOperation.hpp:215-255: every value
+// negated, undefined signs swapped; the width is kept.
+template <int D> void invert(LS<D> &ls) {
+  for (auto &v : ls.vals) v = -v;
+  ls.emptyValue = -ls.emptyValue;
+  ls.finalizeMap();
+}
+
+// PrepareStencilLocalLaxFriedrichs, lsStencilLocalLaxFriedrichsScalar.hpp:
+// 423-477.  The reference tests a layer with isDepo[isDepo[i]] (:448: it
+// indexes the vector with the element); kept, with an index past the end
+// read as false.
+template <int D> void prepareStencilLLF(std::vector<LS<D>> &lss, std::vector<bool> isDepo) {
+  const int L = (int)lss.size();
+  isDepo.resize(L, false);
+  LS<D> finalTop;
+  finalTop.grid = lss[0].grid;
+  finalTop.width = 1;
+  finalTop.finalizeMap();
+  auto relComp = [](double a, double b) { return maxComp(a, -b); };
+  bool layerAboveIsDepo = false;
+  int layer = L - 1;
+  for (int i = L - 1; i >= 0; --i) {
+    const size_t e = isDepo[i] ? 1 : 0;
+    const bool depo = e < isDepo.size() && isDepo[e];
+    if (depo) {
+      if (!layerAboveIsDepo) {
+        layer = i;
+        layerAboveIsDepo = true;
+      }
+    } else {
+      if (layerAboveIsDepo) {
+        LS<D> layerAbove = lss[layer];
+        booleanOp<D>(layerAbove, lss[i], relComp);
+        booleanOp<D>(finalTop, layerAbove, minComp);
+        prune<D>(finalTop, false);
+      }
+      layerAboveIsDepo = false;
+    }
+  }
+  if (layerAboveIsDepo) booleanOp<D>(finalTop, lss[layer], minComp);
+  invert<D>(finalTop);
+  lss.back() = finalTop;
+}
+
+// FinalizeStencilLocalLaxFriedrichs, :480-492.
+template <int D> void finalizeStencilLLF(std::vector<LS<D>> &lss) {
+  LS<D> &top = lss.back();
+  invert<D>(top);
+  booleanOp<D>(top, lss[lss.size() - 2], minComp);
 }
 
 } // namespace vlso

@@ -117,3 +117,66 @@ def test_gpu_sllf_callbacks():
     ctx, gres = run_gpu(g, ls, vel, p)
     compare(ols, ctx)
     assert gres.current_time_step == ores.current_time_step
+
+
+DEPO_PATTERNS = [[False, True], [True, True], [True, False], [False, False]]
+
+
+@pytest.mark.parametrize("depo", DEPO_PATTERNS)
+def test_oracle_prepare_finalize_valid(depo):
+    from oracle import oracle as O
+
+    g, ls, _, _ = trench_case()
+    ols = [O.OracleLS(g, d) for d in ls]
+    O.prepare_stencil_llf(ols, depo)
+    assert ols[-1].check() == 0
+    O.finalize_stencil_llf(ols)
+    assert ols[-1].check() == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("depo", DEPO_PATTERNS)
+def test_gpu_prepare_finalize(depo):
+    """PrepareStencilLocalLaxFriedrichs, then FinalizeStencilLocalLaxFriedrichs,
+    on the GPU equal the oracle's."""
+    from oracle import oracle as O
+    from viennals_b200.advect import Context
+
+    g, ls, _, _ = trench_case()
+    ols = [O.OracleLS(g, d) for d in ls]
+    ctx = Context(0, 0)
+    ctx.set_grid(g)
+    ctx.set_level_set_count(len(ls))
+    for i, d in enumerate(ls):
+        ctx.upload(i, d)
+    O.prepare_stencil_llf(ols, depo)
+    ctx.prepare_stencil_llf(depo)
+    compare(ols, ctx)
+    O.finalize_stencil_llf(ols)
+    ctx.finalize_stencil_llf()
+    compare(ols, ctx)
+
+
+@pytest.mark.gpu
+def test_gpu_stencil_workflow():
+    """Prepare, advect with Stencil LLF (SquareEtch velocity), finalize."""
+    from oracle import oracle as O
+    from viennals_b200.advect import Context
+
+    g, ls, _, p = trench_case(SLLF, TS.FORWARD_EULER, 0.2)
+    depo = [False, True]
+    ols = [O.OracleLS(g, d) for d in ls]
+    O.prepare_stencil_llf(ols, depo)
+    ores = O.advect(ols, p, square_etch())
+    O.finalize_stencil_llf(ols)
+    ctx = Context(0, 0)
+    ctx.set_grid(g)
+    ctx.set_level_set_count(len(ls))
+    for i, d in enumerate(ls):
+        ctx.upload(i, d)
+    ctx.set_velocity(square_etch().descriptor())
+    ctx.prepare_stencil_llf(depo)
+    gres = ctx.advect(p)
+    ctx.finalize_stencil_llf()
+    compare(ols, ctx)
+    assert gres.number_of_time_steps == ores.number_of_time_steps

@@ -111,6 +111,15 @@ class Context:
         self._check(self.lib.vlsg_compare(self.h, int(slot), other.h, int(other_slot), ctypes.byref(r)))
         return r.as_dict()
 
+    def prepare_stencil_llf(self, is_depo):
+        """vlsg_prepare_stencil_llf: the top level set becomes the wrapping
+        STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER advects."""
+        d = (ctypes.c_int32 * max(1, len(is_depo)))(*[1 if x else 0 for x in is_depo])
+        self._check(self.lib.vlsg_prepare_stencil_llf(self.h, d, len(is_depo)))
+
+    def finalize_stencil_llf(self):
+        self._check(self.lib.vlsg_finalize_stencil_llf(self.h))
+
     def set_velocity(self, desc):
         self._check(self.lib.vlsg_set_velocity_functor(self.h, ctypes.byref(desc)))
 
@@ -339,3 +348,31 @@ class Advect:
         self._resident = ([id(d) for d in self.levelSets],
                           [self._fingerprint(d) for d in self.levelSets])
         return self.result
+
+
+def _stencil_helper(levelSets, fn, device, precision):
+    ctx = Context(device, precision)
+    try:
+        ctx.set_grid(levelSets[-1].grid)
+        ctx.set_level_set_count(len(levelSets))
+        for i, d in enumerate(levelSets):
+            ctx.upload(i, d)
+        fn(ctx)
+        nd = ctx.download_domain(len(levelSets) - 1, levelSets[-1].grid)
+        top = levelSets[-1]
+        top.idx, top.values, top.run_start, top.run_sign, top.width = (
+            nd.idx, nd.values, nd.run_start, nd.run_sign, nd.width)
+    finally:
+        ctx.close()
+
+
+def PrepareStencilLocalLaxFriedrichs(levelSets, isDepo, device=0, precision=Precision.FP64):
+    """viennals::PrepareStencilLocalLaxFriedrichs
+    (lsStencilLocalLaxFriedrichsScalar.hpp:423-477) on the GPU: the last
+    Domain is replaced by the layer wrapping the Stencil LLF scheme advects."""
+    _stencil_helper(levelSets, lambda c: c.prepare_stencil_llf(list(isDepo)), device, precision)
+
+
+def FinalizeStencilLocalLaxFriedrichs(levelSets, device=0, precision=Precision.FP64):
+    """viennals::FinalizeStencilLocalLaxFriedrichs (:480-492) on the GPU."""
+    _stencil_helper(levelSets, lambda c: c.finalize_stencil_llf(), device, precision)

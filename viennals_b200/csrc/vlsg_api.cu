@@ -428,6 +428,29 @@ int vlsg_compare(vlsg_context *a, int32_t slotA, vlsg_context *b, int32_t slotB,
   });
 }
 
+int vlsg_prepare_stencil_llf(vlsg_context *ctx, const int32_t *is_depo, int32_t n) {
+  if (!ctx || n < 0 || (n > 0 && !is_depo)) return fail(ctx, VLSG_ERR_ARGUMENT, "bad argument");
+  if (ctx->staged.empty()) return fail(ctx, VLSG_ERR_STATE, "no level set uploaded");
+  return guarded(ctx, [&] {
+    ensureBuilt(ctx);
+    std::vector<bool> depo(n);
+    for (int32_t i = 0; i < n; ++i) depo[i] = is_depo[i] != 0;
+    ctx->eng->prepareStencilLLF(depo);
+    return VLSG_OK;
+  });
+}
+
+int vlsg_finalize_stencil_llf(vlsg_context *ctx) {
+  if (!ctx) return fail(ctx, VLSG_ERR_ARGUMENT, "bad argument");
+  if (ctx->staged.size() < 2)
+    return fail(ctx, VLSG_ERR_STATE, "FinalizeStencilLocalLaxFriedrichs needs two level sets");
+  return guarded(ctx, [&] {
+    ensureBuilt(ctx);
+    ctx->eng->finalizeStencilLLF();
+    return VLSG_OK;
+  });
+}
+
 int vlsg_set_velocity_functor(vlsg_context *ctx, const vlsg_velocity_desc *v) {
   if (!ctx || !v) return fail(ctx, VLSG_ERR_ARGUMENT, "bad argument");
   if (v->n_materials < 1 || v->n_materials > VLSG_MAX_MATERIALS)

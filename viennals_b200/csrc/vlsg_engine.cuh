@@ -721,6 +721,78 @@ public:
     prune(a, false);
   }
 
+  // An empty level set in buffer b (Domain(grid): positive everywhere, width 1).
+  void clearBuffer(int b) {
+    allocBuffers(b + 1);
+    if (visitBuf == b) visitBuf = -1;
+    auto &B = buf[b];
+    kFillSlots<T><<<blocksPass, 256, 0, stream>>>(slotList, nSlotsPtr(), B.vals, B.def[B.cur],
+                                                  Lim<T>::max());
+    checkLaunch();
+    VLSG_CUDA(cudaMemsetAsync(B.farSign, 1, nBricks, stream));
+    B.width = 1;
+    B.bound = 0;
+    B.nDef = 0;
+    B.live = true;
+  }
+  // BooleanOperation INVERT on buffer b
+  void invertBuffer(int b) {
+    auto &B = buf[b];
+    kNegateSlots<T><<<blocksPass, 256, 0, stream>>>(slotList, nSlotsPtr(), B.vals, B.farSign,
+                                                    nBricks);
+    checkLaunch();
+  }
+
+  // PrepareStencilLocalLaxFriedrichs (lsStencilLocalLaxFriedrichsScalar.hpp:
+  // 423-477): the top level set becomes the inverted union of every depo
+  // layer minus the first non-depo layer below it.  The reference tests a
+  // layer with isDepo[isDepo[i]] (:448, it indexes the vector with the
+  // element), which is kept.
+  void prepareStencil(std::vector<bool> isDepo) {
+    ++generation;
+    isDepo.resize(L, false);
+    const int fin = L, above = L + 1;
+    clearBuffer(fin);
+    bool layerAboveIsDepo = false;
+    int layer = L - 1;
+    for (int i = L - 1; i >= 0; --i) {
+      const size_t e = isDepo[i] ? 1 : 0;
+      const bool depo = e < isDepo.size() && isDepo[e];
+      if (depo) {
+        if (!layerAboveIsDepo) {
+          layer = i;
+          layerAboveIsDepo = true;
+        }
+      } else {
+        if (layerAboveIsDepo) {
+          copyBuffer(layer, above);
+          booleanOp(above, i, RelComplementComp<T>{});
+          booleanOp(fin, above, MinComp<T>{});
+          prune(fin, false);
+        }
+        layerAboveIsDepo = false;
+      }
+    }
+    if (layerAboveIsDepo) booleanOp(fin, layer, MinComp<T>{});
+    invertBuffer(fin);
+    copyBuffer(fin, L - 1);
+    buf[fin].live = false;
+    if (above < 2 * L) buf[above].live = false;
+    visitBuf = -1;
+    maintain();
+    syncErr("PrepareStencilLocalLaxFriedrichs");
+  }
+  // FinalizeStencilLocalLaxFriedrichs (:480-492): top = INVERT(top) u the
+  // level set below it.
+  void finalizeStencil() {
+    ++generation;
+    visitBuf = -1;
+    invertBuffer(L - 1);
+    booleanOp(L - 1, L - 2, MinComp<T>{});
+    maintain();
+    syncErr("FinalizeStencilLocalLaxFriedrichs");
+  }
+
   void copyBuffer(int src, int dst) {
     if (visitBuf == dst) visitBuf = -1;
     allocBuffers(dst + 1);
@@ -1331,6 +1403,9 @@ public:
     *val = (const double *)xs[X_VAL].p;
     *n = xPoints;
   }
+  void prepareStencilLLF(const std::vector<bool> &isDepo) override { prepareStencil(isDepo); }
+  void finalizeStencilLLF() override { finalizeStencil(); }
+
   uint64_t insideCells(int b) override {
     VLSG_CUDA(cudaMemsetAsync(small + 15, 0, sizeof(unsigned long long), stream));
     kInsideCells<T><<<blocksPass, 256, 0, stream>>>(g, mapView(), view(b), nBricks, small + 15);

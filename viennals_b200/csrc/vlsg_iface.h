@@ -135,6 +135,9 @@ public:
   // releases with cudaFree; sorted by cell key)
   virtual void exchange(int b, const int32_t **idx, const double **val, int64_t *n) = 0;
   virtual uint64_t insideCells(int b) = 0;
+  // PrepareStencilLocalLaxFriedrichs / FinalizeStencilLocalLaxFriedrichs
+  virtual void prepareStencilLLF(const std::vector<bool> &isDepo) = 0;
+  virtual void finalizeStencilLLF() = 0;
   virtual int64_t surfaceNodes(int b, double **nodes, uint64_t **keys) = 0;
 };
 

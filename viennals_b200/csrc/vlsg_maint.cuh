@@ -501,5 +501,32 @@ __global__ void kCopySlots(const int *slotList, const int *nSlots, const T *sv,
   }
 }
 
+// Every cell of the listed slots set to v (undefined: v is a sentinel).
+template <class T>
+__global__ void kFillSlots(const int *slotList, const int *nSlots, T *vals, uint64_t *def, T v) {
+  const size_t n = (size_t)*nSlots * BV;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const size_t slot = slotList[i / BV];
+    vals[slot * BV + i % BV] = v;
+    if (i % BV < 8) def[slot * 8 + i % BV] = 0ull;
+  }
+}
+
+// BooleanOperation INVERT (lsBooleanOperation.hpp:215-255): every value of
+// the listed slots negated (sentinels swap sign), and every far sign.
+template <class T>
+__global__ void kNegateSlots(const int *slotList, const int *nSlots, T *vals, int8_t *farSign,
+                             int nBricks) {
+  const size_t n = (size_t)*nSlots * BV;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const size_t slot = slotList[i / BV];
+    vals[slot * BV + i % BV] = -vals[slot * BV + i % BV];
+  }
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nBricks; b += gridDim.x * blockDim.x)
+    farSign[b] = (int8_t)-farSign[b];
+}
+
 } // namespace
 } // namespace vlsg
