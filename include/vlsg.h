@@ -164,6 +164,25 @@ typedef int (*vlsg_alpha_cb)(void *user, int64_t n, const int32_t *directions,
                              const double *central_differences,
                              double *alpha_out);
 
+/* A level set as the velocity-update callback sees it: defined points and
+ * undefined runs in HRLE order (valid during the call only). */
+typedef struct vlsg_levelset_view {
+  int64_t n_points;
+  const int32_t *indices; /* 3 per point */
+  const double *values;
+  int64_t n_runs;
+  const int32_t *run_start; /* 3 per run */
+  const int8_t *run_sign;
+  int32_t width;
+} vlsg_levelset_view;
+
+/* setVelocityUpdateCallback (lsAdvect.hpp:966-969): called by the RK2/RK3
+ * schemes between stages with the top level set (lsAdvectIntegrationSchemes
+ * .hpp:88-89, :129-130, :147-149), e.g. to recompute the velocity field it
+ * feeds.  Returning non-zero ends apply() with VLSG_ERR_CALLBACK (the
+ * reference ignores the callback's bool). */
+typedef int (*vlsg_update_cb)(void *user, const vlsg_levelset_view *top);
+
 typedef struct vlsg_context vlsg_context;
 
 /* Library / context lifetime ---------------------------------------------- */
@@ -271,6 +290,9 @@ typedef struct vlsg_compare_result {
 } vlsg_compare_result;
 int vlsg_compare(vlsg_context *a, int32_t slot_a, vlsg_context *b, int32_t slot_b,
                  vlsg_compare_result *out);
+
+/* setVelocityUpdateCallback (lsAdvect.hpp:966-969); NULL clears it. */
+int vlsg_set_velocity_update_callback(vlsg_context *ctx, vlsg_update_cb cb, void *user);
 
 /* PrepareStencilLocalLaxFriedrichs (lsStencilLocalLaxFriedrichsScalar.hpp:
  * 423-477) on the context's level sets: is_depo[i] tells whether level set i

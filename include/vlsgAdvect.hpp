@@ -15,6 +15,7 @@
 #include <array>
 #include <cstdint>
 #include <cstdio>
+#include <functional>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -155,6 +156,23 @@ template <class T> class Advect {
   std::vector<std::shared_ptr<LevelSet>> levelSets;
   std::shared_ptr<VelocityFunctor> velocities;
   std::shared_ptr<VelocityField<T>> field; // host callback mode when set
+  std::function<bool(std::shared_ptr<LevelSet>)> velocityUpdateCallback;
+  static int updateTrampoline(void *user, const vlsg_levelset_view *v) {
+    auto *self = static_cast<Advect<T> *>(user);
+    auto ls = std::make_shared<LevelSet>();
+    ls->grid = self->levelSets.back()->grid;
+    ls->indices.assign(v->indices, v->indices + 3 * v->n_points);
+    ls->values.assign(v->values, v->values + v->n_points);
+    ls->runStart.assign(v->run_start, v->run_start + 3 * v->n_runs);
+    ls->runSign.assign(v->run_sign, v->run_sign + v->n_runs);
+    ls->width = v->width;
+    try {
+      self->velocityUpdateCallback(ls); // the reference ignores the bool
+    } catch (...) {
+      return 1;
+    }
+    return 0;
+  }
   vlsg_advect_params params{};
   vlsg_advect_result result{};
   vlsg_context *ctx = nullptr;
@@ -207,6 +225,11 @@ public:
   void setUpdatePointData(bool b) { params.update_point_data = b; }
   // StencilLocalLaxFriedrichsScalar<T,D,1>::setMaxDissipation, per Advect here
   void setMaxDissipation(double d) { params.max_dissipation = d; }
+  // lsAdvect.hpp:966-969: called between RK2/RK3 stages with a copy of the
+  // top level set
+  void setVelocityUpdateCallback(std::function<bool(std::shared_ptr<LevelSet>)> cb) {
+    velocityUpdateCallback = std::move(cb);
+  }
 
   double getAdvectedTime() const { return result.advected_time; }
   double getCurrentTimeStep() const { return result.current_time_step; }
@@ -243,6 +266,9 @@ public:
     } else if (!check(vlsg_set_velocity_functor(ctx, &velocities->desc))) {
       return;
     }
+    if (!check(vlsg_set_velocity_update_callback(
+            ctx, velocityUpdateCallback ? &Advect<T>::updateTrampoline : nullptr, this)))
+      return;
     if (!check(vlsg_advect(ctx, &params, &result))) return;
     for (size_t i = 0; i < levelSets.size(); ++i) {
       LevelSet &ls = *levelSets[i];

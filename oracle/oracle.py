@@ -10,7 +10,7 @@ import subprocess
 
 import numpy as np
 
-from viennals_b200._abi import ALPHA_CALLBACK, VELOCITY_CALLBACK, AdvectParams, AdvectResult, VelocityDesc
+from viennals_b200._abi import ALPHA_CALLBACK, UPDATE_CALLBACK, VELOCITY_CALLBACK, AdvectParams, AdvectResult, VelocityDesc
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libvlso.so")
@@ -67,6 +67,8 @@ def lib():
                                   P(AdvectResult)]
         L.vlso_advect_cb.argtypes = [P(vp), i32, P(AdvectParams), VELOCITY_CALLBACK, vp,
                                      ALPHA_CALLBACK, vp, P(AdvectResult)]
+        L.vlso_advect_ex.argtypes = [P(vp), i32, P(AdvectParams), P(VelocityDesc), VELOCITY_CALLBACK,
+                                     vp, ALPHA_CALLBACK, vp, UPDATE_CALLBACK, vp, P(AdvectResult)]
         L.vlso_prepare_stencil_llf.argtypes = [P(vp), i32, P(ctypes.c_int32), i32]
         L.vlso_finalize_stencil_llf.argtypes = [P(vp), i32]
         L.vlso_last_error.restype = ctypes.c_char_p
@@ -186,11 +188,22 @@ def chamfer(target, sample):
                 max=out[4], n_target=int(cnt[0]), n_sample=int(cnt[1]))
 
 
-def advect(level_sets, params, velocity):
-    """Advect::apply on the oracle; level_sets bottom..top (modified)."""
+def advect(level_sets, params, velocity, update=None):
+    """Advect::apply on the oracle; level_sets bottom..top (modified).
+    `update`: a velocity-update callback fn(Domain) (points only)."""
     arr = (ctypes.c_void_p * len(level_sets))(*[ls.h for ls in level_sets])
     res = AdvectResult()
     desc = velocity.descriptor() if hasattr(velocity, "descriptor") else velocity
+    if update is not None:
+        from viennals_b200.advect import update_callback
+        ucb = update_callback(update)
+        if desc is None:
+            vcb, acb, dptr = velocity.c_callback(), velocity.c_alpha_callback(), None
+        else:
+            vcb, acb, dptr = VELOCITY_CALLBACK(), ALPHA_CALLBACK(), ctypes.byref(desc)
+        _check(lib().vlso_advect_ex(arr, len(level_sets), ctypes.byref(params), dptr, vcb, None,
+                                    acb, None, ucb, None, ctypes.byref(res)))
+        return res
     if desc is None:  # a host velocity field: one callback per point
         _check(lib().vlso_advect_cb(arr, len(level_sets), ctypes.byref(params),
                                     velocity.c_callback(), None, velocity.c_alpha_callback(),

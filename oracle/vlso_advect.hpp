@@ -923,22 +923,50 @@ template <int D> struct Advector {
   void restoreLower() {
     for (size_t i = 0; i + 1 < lss.size(); ++i) lss[i] = initial[i];
   }
+  // velocityUpdateCallback (lsAdvect.hpp:82, :966-969) with the top level
+  // set's defined points in HRLE order (no runs)
+  vlsg_update_cb updateCb = nullptr;
+  void *updateUser = nullptr;
+  void callUpdate() {
+    LS<D> &t = top();
+    std::vector<int32_t> idx;
+    std::vector<double> val;
+    for (size_t i = 0; i < t.keys.size(); ++i) {
+      if (!isDefined(t.vals[i])) continue;
+      int64_t c[D];
+      decode<D>(t.keys[i], c);
+      for (int d = 0; d < 3; ++d) idx.push_back(d < D ? (int32_t)c[d] : 0);
+      val.push_back(t.vals[i]);
+    }
+    const vlsg_levelset_view v{(int64_t)val.size(), idx.data(), val.data(), 0, nullptr, nullptr,
+                               t.width};
+    if (updateCb(updateUser, &v) != 0) throw std::runtime_error("the velocity update callback failed");
+  }
+  // lsAdvectIntegrationSchemes.hpp:59-108
   double evolveRungeKutta2(double maxTimeStep) {
-    saveInitial(false); // no velocity-update callback in the oracle
-    const double dt1 = evolveForwardEuler(maxTimeStep, false);
+    const bool cb = updateCb != nullptr;
+    saveInitial(cb);
+    const double dt1 = evolveForwardEuler(maxTimeStep, cb);
     if (dt1 <= 0.) return 0.;
+    if (cb) callUpdate();
     const double dt2 = evolveForwardEuler(dt1, false);
-    combineLevelSets(0.5, 0.5);
+    const bool etched = combineLevelSets(0.5, 0.5);
+    if (etched && cb) restoreLower();
     adjustLowerLayers();
     return 0.5 * dt1 + 0.5 * dt2;
   }
+  // :110-168
   double evolveRungeKutta3(double maxTimeStep) {
+    const bool cb = updateCb != nullptr;
     saveInitial(true);
-    const double dt1 = evolveForwardEuler(maxTimeStep, false);
+    const double dt1 = evolveForwardEuler(maxTimeStep, cb);
     if (dt1 <= 0.) return 0.;
+    if (cb) callUpdate();
     const double dt2 = evolveForwardEuler(dt1, false);
-    combineLevelSets(0.75, 0.25);
+    const bool etched1 = combineLevelSets(0.75, 0.25);
+    if (etched1 && cb) restoreLower();
     adjustLowerLayers();
+    if (cb) callUpdate();
     const double dt3 = evolveForwardEuler(dt1, false);
     const bool etched2 = combineLevelSets(1.0 / 3.0, 2.0 / 3.0);
     if (etched2) restoreLower();

@@ -67,12 +67,15 @@ vlso::Params toParams(const vlsg_advect_params *p) {
 
 template <int D>
 int advectD(Handle **hs, int n, const vlsg_advect_params *p,
-            const vlso::VelSource &v, vlsg_advect_result *r) {
+            const vlso::VelSource &v, vlsg_advect_result *r,
+            vlsg_update_cb upd = nullptr, void *updUser = nullptr) {
   if (p->ignore_voids) throw std::runtime_error("ignoreVoids is not supported");
   std::vector<vlso::LS<D>> lss;
   lss.reserve(n);
   for (int i = 0; i < n; ++i) lss.push_back(get<D>(hs[i]));
   vlso::Advector<D> adv(lss, toParams(p), v);
+  adv.updateCb = upd;
+  adv.updateUser = updUser;
   adv.apply(*r);
   for (int i = 0; i < n; ++i) get<D>(hs[i]) = lss[i];
   return 0;
@@ -263,6 +266,28 @@ int vlso_advect_cb(void **lss, int n, const vlsg_advect_params *p, vlsg_velocity
     vs.alphaCb = alphaCb;
     vs.alphaUser = alphaUser;
     return hs[0]->D == 2 ? advectD<2>(hs, n, p, vs, r) : advectD<3>(hs, n, p, vs, r);
+  });
+}
+
+// Either velocity form (desc when cb is NULL) with a velocity-update callback.
+int vlso_advect_ex(void **lss, int n, const vlsg_advect_params *p, const vlsg_velocity_desc *desc,
+                   vlsg_velocity_cb cb, void *user, vlsg_alpha_cb alphaCb, void *alphaUser,
+                   vlsg_update_cb upd, void *updUser, vlsg_advect_result *r) {
+  auto **hs = reinterpret_cast<Handle **>(lss);
+  return guarded([&] {
+    if (n < 1) throw std::runtime_error("no level sets");
+    vlso::VelSource vs;
+    if (cb) {
+      vs.cb = cb;
+      vs.user = user;
+      vs.alphaCb = alphaCb;
+      vs.alphaUser = alphaUser;
+    } else {
+      if (!desc) throw std::runtime_error("no velocity");
+      vs.desc = *desc;
+    }
+    return hs[0]->D == 2 ? advectD<2>(hs, n, p, vs, r, upd, updUser)
+                         : advectD<3>(hs, n, p, vs, r, upd, updUser);
   });
 }
 

@@ -167,6 +167,21 @@ ALPHA_CALLBACK = ctypes.CFUNCTYPE(
     ctypes.POINTER(ctypes.c_double),
 )
 
+class LevelSetView(ctypes.Structure):
+    """vlsg_levelset_view: a level set as the velocity-update callback sees it."""
+    _fields_ = [
+        ("n_points", ctypes.c_int64),
+        ("indices", ctypes.POINTER(ctypes.c_int32)),
+        ("values", ctypes.POINTER(ctypes.c_double)),
+        ("n_runs", ctypes.c_int64),
+        ("run_start", ctypes.POINTER(ctypes.c_int32)),
+        ("run_sign", ctypes.POINTER(ctypes.c_int8)),
+        ("width", ctypes.c_int32),
+    ]
+
+
+UPDATE_CALLBACK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(LevelSetView))
+
 VELOCITY_CALLBACK = ctypes.CFUNCTYPE(
     ctypes.c_int,
     ctypes.c_void_p,

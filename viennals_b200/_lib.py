@@ -2,7 +2,7 @@
 import ctypes
 import os
 
-from ._abi import (ALPHA_CALLBACK, VELOCITY_CALLBACK, AdvectParams, AdvectResult, CompareResult, KernelStat,
+from ._abi import (ALPHA_CALLBACK, UPDATE_CALLBACK, VELOCITY_CALLBACK, AdvectParams, AdvectResult, CompareResult, KernelStat,
                    VelocityDesc)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -48,6 +48,7 @@ def load(build_if_missing=True):
     L.vlsg_set_velocity_functor.argtypes = [vp, P(VelocityDesc)]
     L.vlsg_set_velocity_callback.argtypes = [vp, VELOCITY_CALLBACK, vp]
     L.vlsg_set_dissipation_alpha_callback.argtypes = [vp, ALPHA_CALLBACK, vp]
+    L.vlsg_set_velocity_update_callback.argtypes = [vp, UPDATE_CALLBACK, vp]
     L.vlsg_prepare_stencil_llf.argtypes = [vp, ctypes.POINTER(ctypes.c_int32), ctypes.c_int32]
     L.vlsg_finalize_stencil_llf.argtypes = [vp]
     L.vlsg_advect.argtypes = [vp, P(AdvectParams), P(AdvectResult)]
@@ -64,6 +65,7 @@ EXPORTED = [
     "vlsg_upload_levelset", "vlsg_count_points", "vlsg_download_levelset", "vlsg_download_runs",
     "vlsg_get_values", "vlsg_get_values_noalloc",
     "vlsg_set_velocity_functor", "vlsg_set_velocity_callback",
-    "vlsg_set_dissipation_alpha_callback", "vlsg_prepare_stencil_llf", "vlsg_finalize_stencil_llf", "vlsg_advect", "vlsg_advect_batch",
+    "vlsg_set_dissipation_alpha_callback", "vlsg_prepare_stencil_llf", "vlsg_finalize_stencil_llf",
+    "vlsg_set_velocity_update_callback", "vlsg_advect", "vlsg_advect_batch",
     "vlsg_set_profiling", "vlsg_get_kernel_stats", "vlsg_compare",
 ]

@@ -56,6 +56,7 @@ class Context:
         return s.value
 
     def set_grid(self, grid):
+        self._grid = grid
         gmin = np.array(grid.min[:3], np.int64)
         gmax = np.array(grid.max[:3], np.int64)
         bc = np.array(grid.bc[:3], np.int32)
@@ -122,6 +123,13 @@ class Context:
 
     def set_velocity(self, desc):
         self._check(self.lib.vlsg_set_velocity_functor(self.h, ctypes.byref(desc)))
+
+    def set_velocity_update_callback(self, fn):
+        """setVelocityUpdateCallback: fn(Domain) between RK stages (None clears)."""
+        from ._abi import UPDATE_CALLBACK
+        self._update_cb = update_callback(fn, getattr(self, "_grid", None)) if fn is not None else None
+        self._check(self.lib.vlsg_set_velocity_update_callback(
+            self.h, self._update_cb if fn is not None else UPDATE_CALLBACK(), None))
 
     def set_velocity_callback(self, field):
         """Host callback mode: `field` is a VelocityField (its c_callback())."""
@@ -287,6 +295,11 @@ class Advect:
     def setUpdatePointData(self, b):
         self.params.update_point_data = int(bool(b))
 
+    def setVelocityUpdateCallback(self, callback):
+        """setVelocityUpdateCallback (lsAdvect.hpp:966-969): callback(Domain)
+        with the top level set between the RK2/RK3 stages."""
+        self.velocityUpdateCallback = callback
+
     def setMaxDissipation(self, d):
         """StencilLocalLaxFriedrichsScalar.setMaxDissipation (a class-wide
         static in the reference, per Advect object here)."""
@@ -336,6 +349,7 @@ class Advect:
             self.ctx.set_velocity(desc)
         else:
             self.ctx.set_velocity_callback(self.velocities)
+        self.ctx.set_velocity_update_callback(getattr(self, "velocityUpdateCallback", None))
 
     def apply(self):
         """Advect::apply, lsAdvect.hpp:1017-1043; results written back."""
@@ -348,6 +362,31 @@ class Advect:
         self._resident = ([id(d) for d in self.levelSets],
                           [self._fingerprint(d) for d in self.levelSets])
         return self.result
+
+
+def update_callback(fn, grid=None):
+    """vlsg_update_cb around fn(Domain): the Domain holds copies of the top
+    level set's points and runs (HRLE order); an exception in fn makes the
+    call return 1 (VLSG_ERR_CALLBACK)."""
+    from ._abi import UPDATE_CALLBACK
+
+    def trampoline(user, view):
+        try:
+            v = view.contents
+            n, m = int(v.n_points), int(v.n_runs)
+            a = np.ctypeslib.as_array
+            d = Domain.__new__(Domain)
+            d.grid = grid
+            d.idx = a(v.indices, (n, 3)).copy() if n else np.zeros((0, 3), np.int32)
+            d.values = a(v.values, (n,)).copy() if n else np.zeros(0)
+            d.run_start = a(v.run_start, (m, 3)).copy() if m else np.zeros((0, 3), np.int32)
+            d.run_sign = a(v.run_sign, (m,)).copy() if m else np.zeros(0, np.int8)
+            d.width = int(v.width)
+            fn(d)
+            return 0
+        except Exception:  # reported through the library's status
+            return 1
+    return UPDATE_CALLBACK(trampoline)
 
 
 def _stencil_helper(levelSets, fn, device, precision):

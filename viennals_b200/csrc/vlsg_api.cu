@@ -31,6 +31,8 @@ struct vlsg_context {
   void *velUser = nullptr;
   vlsg_alpha_cb alphaCb = nullptr;
   void *alphaUser = nullptr;
+  vlsg_update_cb updCb = nullptr;
+  void *updUser = nullptr;
   bool profiling = false;
   std::unique_ptr<EngineBase> eng; // Engine<double> or Engine<float>
 };
@@ -428,6 +430,13 @@ int vlsg_compare(vlsg_context *a, int32_t slotA, vlsg_context *b, int32_t slotB,
   });
 }
 
+int vlsg_set_velocity_update_callback(vlsg_context *ctx, vlsg_update_cb cb, void *user) {
+  if (!ctx) return fail(nullptr, VLSG_ERR_ARGUMENT, "NULL context");
+  ctx->updCb = cb;
+  ctx->updUser = cb ? user : nullptr;
+  return VLSG_OK;
+}
+
 int vlsg_prepare_stencil_llf(vlsg_context *ctx, const int32_t *is_depo, int32_t n) {
   if (!ctx || n < 0 || (n > 0 && !is_depo)) return fail(ctx, VLSG_ERR_ARGUMENT, "bad argument");
   if (ctx->staged.empty()) return fail(ctx, VLSG_ERR_STATE, "no level set uploaded");
@@ -496,6 +505,8 @@ int vlsg_advect(vlsg_context *ctx, const vlsg_advect_params *p, vlsg_advect_resu
     e.velUser = ctx->velUser;
     e.alphaCb = ctx->velCb ? ctx->alphaCb : nullptr;
     e.alphaUser = ctx->alphaUser;
+    e.updCb = ctx->updCb;
+    e.updUser = ctx->updUser;
     e.profiling = ctx->profiling;
     if (ctx->profiling) e.timers.clear();
     e.apply(*p, *r);

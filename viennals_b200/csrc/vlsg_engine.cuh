@@ -1134,22 +1134,52 @@ public:
     }
   }
 
+  // velocityUpdateCallback with the top level set in the exchange format
+  void callUpdate() {
+    ++generation; // the level sets changed since the last exchange
+    const int top = L - 1;
+    const int64_t n = compact(top, nullptr, nullptr, 0);
+    std::vector<int32_t> idx(3 * (size_t)n);
+    std::vector<double> val((size_t)n);
+    compact(top, idx.data(), val.data(), n);
+    const int64_t m = runs(top, nullptr, nullptr, 0);
+    std::vector<int32_t> rs(3 * (size_t)m);
+    std::vector<int8_t> sg((size_t)m);
+    runs(top, rs.data(), sg.data(), m);
+    const vlsg_levelset_view v{n, idx.data(), val.data(), m, rs.data(), sg.data(), buf[top].width};
+    const int rc = updCb(updUser, &v);
+    if (rc != 0)
+      throw CudaError("the velocity update callback returned " + std::to_string(rc),
+                      VLSG_ERR_CALLBACK);
+  }
+
+  // Heun RK2 (lsAdvectIntegrationSchemes.hpp:59-108): with a velocity-update
+  // callback, stage 1 adjusts the lower layers, the callback runs after it,
+  // and the lower layers are restored when the combination etched.
   double evolveRungeKutta2(const vlsg_advect_params &P, double maxTimeStep) {
-    saveInitial(false);
-    const double dt1 = evolveForwardEuler(P, maxTimeStep, false);
+    const bool cb = updCb != nullptr;
+    saveInitial(cb);
+    const double dt1 = evolveForwardEuler(P, maxTimeStep, cb);
     if (dt1 <= 0.) return 0.;
+    if (cb) callUpdate();
     const double dt2 = evolveForwardEuler(P, dt1, false);
-    combineLevelSets(P, 0.5, 0.5);
+    const bool etched = combineLevelSets(P, 0.5, 0.5);
+    if (etched && cb) restoreLower();
     adjustLowerLayers(P);
     return 0.5 * dt1 + 0.5 * dt2;
   }
+  // SSP RK3 (:110-168)
   double evolveRungeKutta3(const vlsg_advect_params &P, double maxTimeStep) {
+    const bool cb = updCb != nullptr;
     saveInitial(true);
-    const double dt1 = evolveForwardEuler(P, maxTimeStep, false);
+    const double dt1 = evolveForwardEuler(P, maxTimeStep, cb);
     if (dt1 <= 0.) return 0.;
+    if (cb) callUpdate();
     const double dt2 = evolveForwardEuler(P, dt1, false);
-    combineLevelSets(P, 0.75, 0.25);
+    const bool etched1 = combineLevelSets(P, 0.75, 0.25);
+    if (etched1 && cb) restoreLower();
     adjustLowerLayers(P);
+    if (cb) callUpdate();
     const double dt3 = evolveForwardEuler(P, dt1, false);
     const bool etched2 = combineLevelSets(P, 1.0 / 3.0, 2.0 / 3.0);
     if (etched2) restoreLower();

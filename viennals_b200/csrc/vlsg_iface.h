@@ -114,6 +114,8 @@ public:
   void *velUser = nullptr;
   vlsg_alpha_cb alphaCb = nullptr; // dissipation alphas with a callback
   void *alphaUser = nullptr;
+  vlsg_update_cb updCb = nullptr; // setVelocityUpdateCallback
+  void *updUser = nullptr;
   bool profiling = false;
   std::vector<KernelTimer> timers;
 
