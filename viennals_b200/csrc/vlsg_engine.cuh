@@ -598,8 +598,8 @@ public:
   // --------------------------------------------------------------- passes
   void applyChanges(int b) {
     Scope sc(this, "apply_changes");
-    kApplyChanges<T><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(buf[b].vals, changeLog(),
-                                                                   logSegments);
+    kApplyChanges<T><<<logSegments, FRONTIER_THREADS, 0, stream>>>(buf[b].vals, changeLog(),
+                                                                    logSegments);
     checkLaunch();
   }
 

@@ -327,13 +327,24 @@ __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
 template <class T>
 __global__ void __launch_bounds__(FRONTIER_THREADS)
     kApplyChanges(T *vals, ChangeLog<T> lg, int segments) {
-  const int lane = threadIdx.x & 31;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nWarps = (gridDim.x * blockDim.x) >> 5;
-  for (int w = warp; w < segments; w += nWarps) {
+  // block b takes segments b, b + gridDim.x, ...; its 256 threads stride the
+  // entries, four loads in flight per thread
+  for (int w = blockIdx.x; w < segments; w += gridDim.x) {
     const int n = lg.count[w];
     const size_t base = (size_t)w * lg.per;
-    for (int i = lane; i < n; i += 32) {
+    int i = threadIdx.x;
+    for (; i + 3 * blockDim.x < n; i += 4 * blockDim.x) {
+      uint32_t q[4];
+      T val[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        q[k] = lg.cell[base + i + k * blockDim.x];
+        val[k] = lg.val[base + i + k * blockDim.x];
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) vals[(size_t)(q[k] >> 9) * BV + (q[k] & 511)] = val[k];
+    }
+    for (; i < n; i += blockDim.x) {
       const uint32_t q = lg.cell[base + i];
       vals[(size_t)(q >> 9) * BV + (q & 511)] = lg.val[base + i];
     }
