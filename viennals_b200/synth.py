@@ -190,3 +190,112 @@ def batch_domains(n=256, seed=7, points_range=(1e4, 2e6), device=None):
         dom = sdf_levelset(grid, sdf, lo, hi)
         out.append((grid, dom, constant_scalar(-rate)))
     return out
+
+
+def _sdf_band_torch(grid, sdf, lo, hi, device, chunk_cells=1 << 24):
+    """Width-2 band (|sdf| <= gridDelta) of an SDF with Lipschitz constant 1
+    over the index box [lo, hi], evaluated with torch on `device`: bricks of
+    8^3 cells whose centre is further than half a diagonal plus 1.5 cells
+    from the surface are skipped.  Returns (idx int32 (N,3), values)."""
+    import torch
+
+    gd = grid.delta
+    dev = torch.device(device)
+    B = 8
+    nb = [(hi[d] - lo[d]) // B + 1 for d in range(3)]
+    reach = (math.sqrt(3.0) * 4.0 + 1.5) * gd
+    off = torch.arange(B, device=dev, dtype=torch.int64)
+    OZ, OY, OX = torch.meshgrid(off, off, off, indexing="ij")
+    offs = torch.stack([OX.reshape(-1), OY.reshape(-1), OZ.reshape(-1)], 1)
+    by_, bx_ = torch.meshgrid(torch.arange(nb[1], device=dev), torch.arange(nb[0], device=dev),
+                              indexing="ij")
+    bx_, by_ = bx_.reshape(-1), by_.reshape(-1)
+    idx_parts, val_parts = [], []
+    for bz in range(nb[2]):
+        cx = (lo[0] + bx_ * B + 3.5) * gd
+        cy = (lo[1] + by_ * B + 3.5) * gd
+        cz = torch.full_like(cx, (lo[2] + bz * B + 3.5) * gd, dtype=torch.float64)
+        near = torch.abs(sdf(cx.double(), cy.double(), cz)) <= reach
+        if not bool(near.any()):
+            continue
+        corner = torch.stack([lo[0] + bx_[near] * B, lo[1] + by_[near] * B,
+                              torch.full_like(bx_[near], lo[2] + bz * B)], 1)
+        per = max(1, chunk_cells // (B ** 3))
+        for s in range(0, len(corner), per):
+            cells = (corner[s:s + per, None, :] + offs[None, :, :]).reshape(-1, 3)
+            inside = (cells[:, 0] <= hi[0]) & (cells[:, 1] <= hi[1]) & (cells[:, 2] <= hi[2])
+            cells = cells[inside]
+            v = sdf(cells[:, 0].double() * gd, cells[:, 1].double() * gd,
+                    cells[:, 2].double() * gd) / gd
+            keep = torch.abs(v) <= 1.0
+            idx_parts.append(cells[keep].cpu().numpy())
+            val_parts.append(v[keep].cpu().numpy())
+    idx = np.concatenate(idx_parts) if idx_parts else np.zeros((0, 3), np.int64)
+    vals = np.concatenate(val_parts) if val_parts else np.zeros(0)
+    for d in range(3):
+        if grid.is_periodic(d):
+            idx[:, d] = grid.map_index(d, idx[:, d])
+    return idx.astype(np.int32), vals
+
+
+def hole_stack(lateral_cells=4096, grid_delta=0.02, pitch=1.28, radius=0.5, depth=2.0,
+               layers=(0.1, 0.3), shift=(0.31, 0.17), device="cpu"):
+    """The stacked-layer hole array: a substrate (material 0) with a square
+    array of cylindrical holes (radius, depth, pitch; periodic in x/y) under
+    two slabs on the flat top between the holes, of thickness layers[0]
+    (material 1) and layers[1] (material 2, the top level set); every level
+    set wraps the ones below.  Velocity per material 1.0 / 0.6 / 0.0 plus
+    0.2 |n_z|.  The hole axes sit `shift` cells off the grid points: with
+    axes on grid points, cells at exactly the radius carry values of order
+    1e-9 whose sign FP32 and FP64 Prune judge differently (it compares with
+    the precision's epsilon), which moves the lower bands by a cell.
+    Returns (grid, [three Domains], velocity)."""
+    import torch
+
+    from .velocity import FunctorVelocity
+
+    half = lateral_cells * grid_delta / 2.0
+    zlo, zhi = -depth - 0.5, layers[-1] + 0.5
+    grid = Grid([-half, half, -half, half, zlo, zhi],
+                [BC.PERIODIC_BOUNDARY, BC.PERIODIC_BOUNDARY, BC.INFINITE_BOUNDARY], grid_delta)
+
+    sx, sy = shift[0] * grid_delta, shift[1] * grid_delta
+
+    def rho(x, y):
+        px = torch.remainder(x + half - sx, pitch) - pitch / 2.0
+        py = torch.remainder(y + half - sy, pitch) - pitch / 2.0
+        return torch.sqrt(px * px + py * py)
+
+    def substrate(x, y, z):
+        return torch.maximum(z, -torch.maximum(rho(x, y) - radius, -z - depth))
+
+    def stacked(h):
+        def f(x, y, z):
+            slab = torch.maximum(torch.maximum(z - h, -z), radius - rho(x, y))
+            return torch.minimum(substrate(x, y, z), slab)
+        return f
+
+    lo = [grid.min[0], grid.min[1], grid.min[2]]
+    hi = [grid.max[0] - 1, grid.max[1] - 1, grid.max[2]]
+    doms = []
+    for sdf in (substrate, stacked(layers[0]), stacked(layers[1])):
+        idx, vals = _sdf_band_torch(grid, sdf, lo, hi, device)
+        gd = grid.delta
+
+        def sign_fn(x, y, z, sdf=sdf):
+            out = np.empty(len(x), np.int64)
+            step = 1 << 22
+            for s in range(0, len(x), step):
+                t = [torch.as_tensor(np.asarray(a[s:s + step], np.float64) * gd, device=device)
+                     for a in (x, y, z)]
+                out[s:s + step] = np.where(sdf(*t).cpu().numpy() < 0, -1, 1)
+            return out
+
+        rs, sg = make_runs(idx, sign_fn, [lo[0] - 1, lo[1] - 1, lo[2] - 1],
+                           [hi[0] + 1, hi[1] + 1, hi[2] + 1])
+        doms.append(Domain(grid, idx, vals, rs, sg, width=2))
+    vel = FunctorVelocity(3)
+    for m, rate in enumerate((1.0, 0.6, 0.0)):
+        vel.set_rate(m, rate)
+        vel.set_abs(m, 2, 0.2)
+    return grid, doms, vel
