@@ -121,6 +121,7 @@ struct Params {
   bool singleStep = false;
   bool calculateNormalVectors = true;
   bool adaptiveTimeStepping = false;
+  bool ignoreVoids = false; // setIgnoreVoids, lsAdvect.hpp:899
   unsigned adaptiveSubdivisions = 20;
   bool checkDissipation = true;
   uint32_t maxSteps = 10000000;
@@ -634,6 +635,104 @@ std::pair<double, double> evalScheme(const SchemeCtx<D> &S, uint64_t key,
   return {totalGrad, dissipation};
 }
 
+// MarkVoidPoints with its default options (lsMarkVoidPoints.hpp:157-300),
+// restated on grid cells: the sign field (value >= 0 or < 0, :37-39) splits
+// into star-connected components over a box around the map (its bounding box
+// plus 2 cells; bounded directions: the whole extent); the top component
+// holds the box's last cell in HRLE order.  A defined point >= 0 is void when
+// it lies outside the top component; a negative one when no neighbour of the
+// other sign lies in it (:268-287).  Returns a marker per map entry.  When
+// the last cell is negative nothing is marked.
+template <int D> std::vector<uint8_t> voidMarkers(const LS<D> &t) {
+  const Grid<D> &g = t.grid;
+  std::vector<uint8_t> mark(t.keys.size(), 0);
+  if (t.keys.empty()) return mark;
+  int64_t lo[D], hi[D], n[D];
+  for (int d = 0; d < D; ++d) lo[d] = INT64_MAX, hi[d] = INT64_MIN;
+  for (uint64_t k : t.keys)
+    for (int d = 0; d < D; ++d) {
+      const int64_t c = coordOf<D>(k, d);
+      lo[d] = std::min(lo[d], c), hi[d] = std::max(hi[d], c);
+    }
+  size_t N = 1;
+  for (int d = 0; d < D; ++d) {
+    if (g.bounded(d)) {
+      lo[d] = g.minI[d];
+      hi[d] = g.bc[d] == VLSG_PERIODIC_BOUNDARY ? g.maxI[d] - 1 : g.maxI[d];
+    } else {
+      lo[d] -= 2, hi[d] += 2;
+    }
+    n[d] = hi[d] - lo[d] + 1;
+    N *= (size_t)n[d];
+  }
+  auto boxIndex = [&](const int64_t *c) {
+    size_t i = 0;
+    for (int d = D - 1; d >= 0; --d) i = i * n[d] + (size_t)(c[d] - lo[d]);
+    return i;
+  };
+  std::vector<double> v(N);
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < (int64_t)N; ++i) {
+    int64_t c[D];
+    size_t r = (size_t)i;
+    for (int d = 0; d < D; ++d) c[d] = lo[d] + (int64_t)(r % n[d]), r /= n[d];
+    v[i] = t.at(encode<D>(c));
+  }
+  std::vector<size_t> parent(N);
+  for (size_t i = 0; i < N; ++i) parent[i] = i;
+  auto find = [&](size_t x) {
+    while (parent[x] != x) x = parent[x] = parent[parent[x]];
+    return x;
+  };
+  // a neighbour inside the box (through the boundary conditions), or none
+  auto neighbour = [&](const int64_t *c, int d, int s, size_t &out) {
+    int64_t q[D];
+    for (int e = 0; e < D; ++e) q[e] = c[e];
+    q[d] = g.mapCoord(d, c[d] + s);
+    if (q[d] < lo[d] || q[d] > hi[d]) return false;
+    out = boxIndex(q);
+    return true;
+  };
+  for (size_t i = 0; i < N; ++i) {
+    int64_t c[D];
+    size_t r = i;
+    for (int d = 0; d < D; ++d) c[d] = lo[d] + (int64_t)(r % n[d]), r /= n[d];
+    for (int d = 0; d < D; ++d)
+      for (int s = -1; s <= 1; s += 2) {
+        size_t j;
+        if (!neighbour(c, d, s, j)) continue;
+        if ((v[i] >= 0) != (v[j] >= 0)) continue;
+        const size_t a = find(i), b = find(j);
+        if (a != b) parent[std::max(a, b)] = std::min(a, b);
+      }
+  }
+  if (v[N - 1] < 0) return mark;
+  const size_t top = find(N - 1);
+  for (size_t p = 0; p < t.keys.size(); ++p) {
+    if (!isDefined(t.vals[p])) continue;
+    int64_t c[D];
+    decode<D>(t.keys[p], c);
+    bool inBox = true;
+    for (int d = 0; d < D; ++d) inBox = inBox && c[d] >= lo[d] && c[d] <= hi[d];
+    if (!inBox) continue;
+    const size_t i = boxIndex(c);
+    if (t.vals[p] >= 0) {
+      mark[p] = find(i) != top;
+    } else {
+      bool reached = false;
+      for (int d = 0; d < D && !reached; ++d)
+        for (int s = -1; s <= 1 && !reached; s += 2) {
+          size_t j;
+          if (!neighbour(c, d, s, j)) continue;
+          if (std::signbit(v[j]) == std::signbit(t.vals[p])) continue;
+          reached = find(j) == top;
+        }
+      mark[p] = !reached;
+    }
+  }
+  return mark;
+}
+
 // Per-point rate chain of integrateTime (lsAdvect.hpp:530-588).
 struct RateEntry {
   double gradient, dissipation, stop;
@@ -719,6 +818,8 @@ template <int D> struct Advector {
     std::vector<double> tmin(nt, maxTimeStep);
     std::vector<std::array<double, 3>> alp(nt, std::array<double, 3>{0, 0, 0});
     const SchemeCtx<D> S{t, P, vel, globalAlphas};
+    // setIgnoreVoids: void points get no rates (lsAdvect.hpp:443-454, :510)
+    const std::vector<uint8_t> voids = P.ignoreVoids ? voidMarkers<D>(t) : std::vector<uint8_t>();
     // StencilLocalLaxFriedrichs bounds dt with the finalAlphas of its last
     // call that got past the zero-velocity return; with one thread that is
     // the last such call in HRLE order (lsAdvect.hpp:599-606)
@@ -737,11 +838,13 @@ template <int D> struct Advector {
       RateEntry *chain = &chainStore[size_t(a) * L];
       for (int cur = L - 1; cur >= 0; --cur) {
         std::pair<double, double> gd{0., 0.};
-        for (int lower = 0; lower < L; ++lower) {
-          if (lss[lower].at(key) <= value + Params::wrappingLayerEpsilon) {
-            gd = evalScheme<D>(S, key, vel.cb ? ids[activePos[a]] : 0, lower,
-                               sllf ? sllfLast[a].data() : alp[th].data());
-            break;
+        if (!(P.ignoreVoids && voids[activePos[a]])) {
+          for (int lower = 0; lower < L; ++lower) {
+            if (lss[lower].at(key) <= value + Params::wrappingLayerEpsilon) {
+              gd = evalScheme<D>(S, key, vel.cb ? ids[activePos[a]] : 0, lower,
+                                 sllf ? sllfLast[a].data() : alp[th].data());
+              break;
+            }
           }
         }
         const double velocity = gd.first - gd.second;

@@ -58,6 +58,7 @@ vlso::Params toParams(const vlsg_advect_params *p) {
   P.singleStep = p->single_step != 0;
   P.calculateNormalVectors = p->calculate_normal_vectors != 0;
   P.adaptiveTimeStepping = p->adaptive_time_stepping != 0;
+  P.ignoreVoids = p->ignore_voids != 0;
   P.adaptiveSubdivisions = p->adaptive_subdivisions < 1 ? 1 : p->adaptive_subdivisions;
   P.checkDissipation = p->check_dissipation != 0;
   P.maxSteps = p->max_steps ? p->max_steps : 10000000u;
@@ -69,7 +70,6 @@ template <int D>
 int advectD(Handle **hs, int n, const vlsg_advect_params *p,
             const vlso::VelSource &v, vlsg_advect_result *r,
             vlsg_update_cb upd = nullptr, void *updUser = nullptr) {
-  if (p->ignore_voids) throw std::runtime_error("ignoreVoids is not supported");
   std::vector<vlso::LS<D>> lss;
   lss.reserve(n);
   for (int i = 0; i < n; ++i) lss.push_back(get<D>(hs[i]));

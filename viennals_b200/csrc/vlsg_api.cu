@@ -492,7 +492,6 @@ int vlsg_advect(vlsg_context *ctx, const vlsg_advect_params *p, vlsg_advect_resu
   if (ctx->staged.empty()) return fail(ctx, VLSG_ERR_STATE, "No level sets passed to Advect. Not advecting.");
   if (!ctx->hasVel)
     return fail(ctx, VLSG_ERR_STATE, "No velocity field passed to Advect. Not advecting.");
-  if (p->ignore_voids) return fail(ctx, VLSG_ERR_ARGUMENT, "setIgnoreVoids(true) is not supported");
   if (schemeWidth(p->spatial_scheme) < 0)
     return fail(ctx, VLSG_ERR_ARGUMENT, "Advect: Discretization scheme not found.");
   if (p->temporal_scheme < 0 || p->temporal_scheme > 2)

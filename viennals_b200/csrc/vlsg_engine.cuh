@@ -28,6 +28,7 @@
 #include "vlsg_passes.cuh"
 #include "vlsg_rates.cuh"
 #include "vlsg_velcb.cuh"
+#include "vlsg_voids.cuh"
 
 namespace vlsg {
 namespace { // internal linkage: every compilation unit has its own copy
@@ -112,7 +113,8 @@ public:
   enum { X_FLAGS, X_POS, X_OB, X_BOUNDS, X_C, X_P, X_SUMS, X_BOX, X_IDX, X_VAL, X_GC, X_GE,
          X_ROWC, X_ROWG, X_PB, X_GB, X_RSTART, X_RSIGN, X_RPB, X_KEEP, X_KPOS, X_OSTART,
          X_OSIGN, X_VCNT, X_VOFF, X_VSUMS, X_QC, X_QM, X_QN, X_QP, X_VS, X_VV, X_AD, X_AM,
-         X_AC, X_AV, X_SKEY, X_SALPHA, X_QC2, X_QN2, X_QM2, X_QP2, X_VS2, X_COUNT };
+         X_AC, X_AV, X_SKEY, X_SALPHA, X_QC2, X_QN2, X_QM2, X_QP2, X_VS2, X_VPARENT, X_VMASK,
+         X_VTOP, X_COUNT };
   // pinned host staging of the velocity callback's queries and answers
   struct PinScratch {
     void *p = nullptr;
@@ -541,6 +543,7 @@ public:
       if (e & 8) m += " freed brick held a defined point;";
       if (e & 64) m += " band reached an unallocated brick;";
       if (e & 128) m += " a point index lies outside the supported range (+-2^19);";
+      if (e & 256) m += " the void search did not settle within its bound;";
       int z = 0;
       cudaMemcpy(errPtr(), &z, sizeof(int), cudaMemcpyHostToDevice);
       throw CudaError(m, (e & 4) ? VLSG_ERR_CAPACITY : VLSG_ERR_DEVICE_CHECK);
@@ -884,6 +887,7 @@ public:
       A.sllfKey = scratch<unsigned long long>(X_SKEY, rateWarps);
       A.sllfAlpha = scratch<double>(X_SALPHA, 3 * (size_t)rateWarps);
     }
+    A.voidMask = P.ignore_voids ? markVoids() : nullptr;
     if (velCb) gatherVelocities<0>(A);
     {
       // stencil input (each band value once) + output per active point
@@ -937,6 +941,33 @@ public:
     if (tempMax < maxTimeStep) maxTimeStep = tempMax;
     currentTimeStep = maxTimeStep;
     return maxTimeStep;
+  }
+
+  // setIgnoreVoids: MarkVoidPoints on the top level set (vlsg_voids.cuh);
+  // returns the void bits per slot.
+  const uint64_t *markVoids() {
+    Scope sc(this, "mark_voids");
+    const int top = L - 1;
+    const size_t nodes = poolCells + (size_t)nBricks;
+    if (nodes >= (size_t)UINT32_MAX)
+      throw CudaError("setIgnoreVoids: too many cells for the void search", VLSG_ERR_CAPACITY);
+    uint32_t *parent = scratch<uint32_t>(X_VPARENT, nodes);
+    uint64_t *mask = scratch<uint64_t>(X_VMASK, (size_t)capSlots * 8);
+    uint32_t *topNode = scratch<uint32_t>(X_VTOP, 2);
+    const Buf<T> b = view(top);
+    kVoidInit<<<grid1(nodes), 256, 0, stream>>>(parent, nodes);
+    kVoidUnionCells<T><<<blocksPass, 256, 0, stream>>>(g, mapView(), b, slotList, nSlotsPtr(),
+                                                       poolCells, parent, errPtr());
+    kVoidUnionBricks<T><<<grid1(nBricks), 256, 0, stream>>>(g, mapView(), b, nBricks, poolCells,
+                                                            parent, errPtr());
+    kVoidTop<T><<<1, 32, 0, stream>>>(g, mapView(), b, poolCells, parent, topNode, errPtr());
+    VLSG_CUDA(cudaMemsetAsync(mask, 0, (size_t)capSlots * 8 * sizeof(uint64_t), stream));
+    kVoidMark<T><<<blocksPass, 256, 0, stream>>>(g, mapView(), b, slotList, nSlotsPtr(),
+                                                 buf[top].def[buf[top].cur], poolCells, parent,
+                                                 topNode, mask, errPtr());
+    checkLaunch();
+    syncErr("MarkVoidPoints");
+    return mask;
   }
 
   // Host callback mode: the queries of rate pass MODE (every active point x

@@ -153,6 +153,8 @@ template <class T> struct RateArgs {
   double maxDissipation;
   unsigned long long *sllfKey;
   double *sllfAlpha;
+  // setIgnoreVoids: void bits of the top level set (no rates there), or none
+  const uint64_t *voidMask;
 };
 
 // Reader of the top level set around one active point.
@@ -688,9 +690,10 @@ __device__ inline double ratePoint(const RateArgs<T> &A, const Vel &vel,
   double maxStepTime = 0;
   double cfl = A.cfl;
   int len = 0;
+  const bool isVoid = A.voidMask && ((A.voidMask[(size_t)slot * 8 + (c >> 6)] >> (c & 63)) & 1ull);
   for (int cur = L - 1; cur >= 0; --cur) {
     T g = 0, d = 0;
-    for (int lower = 0; lower < L; ++lower) {
+    for (int lower = 0; lower < L && !isVoid; ++lower) {
       const T lv = lower == L - 1 ? C : lsValueAt<T>(A.ls[lower], slot, c);
       if ((double)lv <= (double)value + 1e-4) {
         evalScheme<T, St, Vel, FAM>(A, vel, S, C, lower, alphas, g, d);
