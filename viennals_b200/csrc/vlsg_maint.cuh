@@ -238,25 +238,6 @@ __global__ void kMarkPointBricks(GridDev g, int n, const int *idx, uint8_t *core
   }
 }
 
-template <class T>
-__global__ void kFillFromRuns(GridDev g, const int *slotList, const int *nSlots,
-                              const int *slotBrick, const uint64_t *runKeys,
-                              const int8_t *runSign, int nRuns, T *vals) {
-  const int n = *nSlots;
-  for (int it = blockIdx.x; it < n; it += gridDim.x) {
-    const int slot = slotList[it];
-    int bx, by, bz;
-    brickCoords(g, slotBrick[slot], bx, by, bz);
-    for (int c = threadIdx.x; c < BV; c += blockDim.x) {
-      int x = g.org[0] + bx * BS + (c & 7), y = g.org[1] + by * BS + ((c >> 3) & 7),
-          z = g.org[2] + bz * BS + (c >> 6);
-      x = mapCoord(g, 0, x), y = mapCoord(g, 1, y), z = mapCoord(g, 2, z);
-      const int8_t s = runSignAt(runKeys, runSign, nRuns, cellKey(x, y, z));
-      vals[(size_t)slot * BV + c] = s < 0 ? Lim<T>::lowest() : Lim<T>::max();
-    }
-  }
-}
-
 // Undefined cells of every allocated brick from the runs' signs (before the
 // points are scattered): one thread per x-row of a brick, one binary search
 // per row and a walk along it; bricks next to a boundary that remaps cells
@@ -422,45 +403,6 @@ __global__ void kMasksFromValues(GridDev g, const int *slotBrick, const int *slo
   }
 }
 
-// Defined cells of a buffer as (HRLE key, value) pairs (one warp per slot,
-// walking the set bits of its mask).
-template <class T>
-__global__ void kCompactDefined(GridDev g, const int *slotList, const int *nSlots,
-                                const int *slotBrick, const T *vals, const uint64_t *def,
-                                uint64_t *keys, double *out, int *nOut, int room) {
-  const int lane = threadIdx.x & 31;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nWarps = (gridDim.x * blockDim.x) >> 5;
-  const int n = *nSlots;
-  for (int w = warp; w < n; w += nWarps) {
-    const int slot = slotList[w];
-    int bx, by, bz;
-    brickCoords(g, slotBrick[slot], bx, by, bz);
-    for (int z = 0; z < 8; ++z) {
-      const uint64_t m = def[(size_t)slot * 8 + z];
-      if (!m) continue;
-      const unsigned lo = (unsigned)m, hi = (unsigned)(m >> 32);
-      const int nlo = __popc(lo), cnt = nlo + __popc(hi);
-      for (int base = 0; base < cnt; base += 32) {
-        const int k = base + lane;
-        const bool has = k < cnt;
-        int c = 0;
-        if (has) c = z * 64 + (k < nlo ? __fns(lo, 0, k + 1) : 32 + __fns(hi, 0, k - nlo + 1));
-        const unsigned mask = __ballot_sync(0xffffffffu, has);
-        int off = 0;
-        if (lane == 0) off = atomicAdd(nOut, __popc(mask));
-        off = __shfl_sync(0xffffffffu, off, 0);
-        const int p = off + lane;
-        if (has && p < room) {
-          keys[p] = cellKey(g.org[0] + bx * BS + (c & 7), g.org[1] + by * BS + ((c >> 3) & 7),
-                            g.org[2] + bz * BS + (c >> 6));
-          out[p] = (double)vals[(size_t)slot * BV + c];
-        }
-      }
-    }
-  }
-}
-
 template <class T>
 __global__ void kQueryValues(GridDev g, MapView m, Buf<T> b, int n, const int *idx,
                              double *out) {
@@ -484,20 +426,6 @@ __global__ void kCountDefined(const int *slotList, const int *nSlots, const uint
     }
     for (int o = 16; o > 0; o >>= 1) nd += __shfl_xor_sync(0xffffffffu, nd, o);
     if ((threadIdx.x & 31) == 0 && nd) atomicAdd(cnt, (unsigned long long)nd);
-  }
-}
-
-// Copy the listed slots of one buffer (values and masks) into another.
-template <class T>
-__global__ void kCopySlots(const int *slotList, const int *nSlots, const T *sv,
-                           const uint64_t *sd, T *dv, uint64_t *dd) {
-  const size_t n = (size_t)*nSlots * BV;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x) {
-    const size_t slot = slotList[i >> 9];
-    const int c = i & (BV - 1);
-    dv[slot * BV + c] = sv[slot * BV + c];
-    if (c < 8) dd[slot * 8 + c] = sd[slot * 8 + c];
   }
 }
 
