@@ -678,10 +678,11 @@ public:
         // in: the active band; out: the new band
         return bandPassBytes(lastActive, buf[top].nDef);
       });
+      const uint8_t *visitIn = visitBuf == top ? visit[vcur] : nullptr;
       uint8_t *visitOut = visit[1 - vcur];
       VLSG_CUDA(cudaMemsetAsync(visitOut, 0, cap, stream));
       kUpdateRebuild<T><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(
-          topo(), lsView(top), act, rebuildCutoff, changeLog(), visitOut);
+          topo(), lsView(top), act, rebuildCutoff, changeLog(), visitIn, visitOut);
       vcur ^= 1;
       visitBuf = top;
       checkLaunch();

@@ -372,7 +372,7 @@ __device__ inline T reducedValue(const T *vals, const uint64_t *act, const unsig
 template <class T>
 __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
     kUpdateRebuild(Topo t, LsView<T> v, const uint64_t *act, double cutoff, ChangeLog<T> lg,
-                   uint8_t *visitOut) {
+                   const uint8_t *visitIn, uint8_t *visitOut) {
   __shared__ WarpScratch sm[FRONTIER_THREADS / 32];
   WarpScratch &ws = sm[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
@@ -384,9 +384,15 @@ __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
   const RebuildRule<T> rule{cutoff};
   for (int w = warp; w < n; w += nWarps) {
     const int slot = t.slotList[w];
+    const bool complex = (t.cflag[slot] & CF_STAR) != 0;
+    // a brick the previous pass of this buffer did not mark has no defined
+    // cell (so no active one) and no defined face neighbour cell
+    if (visitIn && !complex && !visitIn[slot]) {
+      if (lane < 8) v.defNext[(size_t)slot * 8 + lane] = 0ull;
+      continue;
+    }
     if (lane < 8) ws.aux[lane] = act[(size_t)slot * 8 + lane];
     beginBrick(t, ws, slot, lane);
-    const bool complex = (t.cflag[slot] & CF_STAR) != 0;
     int x0 = 0, y0 = 0, z0 = 0;
     if (complex) brickOrigin(t, slot, x0, y0, z0);
     const uint64_t own = lane < 8 ? v.def[(size_t)slot * 8 + lane] : 0ull;
