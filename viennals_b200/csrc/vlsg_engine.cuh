@@ -567,7 +567,8 @@ public:
 
   // Bring the allocated bricks back to dilate(core) of the live buffers.
   void maintain() {
-    visitBuf = -1; // slots come and go
+    // the visit flags stay valid: freed slots leave the list, new ones are
+    // marked (kVisitNewSlots), the defined masks do not change
     VLSG_CUDA(cudaMemsetAsync(needed, 0, nBricks, stream));
     {
       Scope sc(this, "maint_mark");
@@ -594,6 +595,10 @@ public:
       Scope sc(this, "maint_init");
       kInitNewSlots<T><<<blocksPass, 128, 0, stream>>>(g, newList, nNewPtr(), slotBrick, bufSet());
       checkLaunch();
+      if (visitBuf >= 0) {
+        kVisitNewSlots<<<blocksPass, 256, 0, stream>>>(newList, nNewPtr(), visit[vcur]);
+        checkLaunch();
+      }
     }
     rebuildSlotList();
   }

@@ -126,6 +126,14 @@ __global__ void kAllocNeeded(int nBricks, int *brickMap, int *slotBrick, const u
   }
 }
 
+// New slots are visited by the next pass: the face cells of their
+// neighbours were not marked for them while they were unallocated.
+__global__ void kVisitNewSlots(const int *newList, const int *nNew, uint8_t *visit) {
+  const int n = *nNew;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    visit[newList[i]] = 1;
+}
+
 // New slots: every cell undefined with the brick's far sign, no defined cell.
 // Cells past the end of a bounded direction hold +max.
 template <class T>
