@@ -1121,10 +1121,17 @@ public:
                             bool updateLowerLayers) {
     const double dt = computeRates(P, maxTimeStep);
     updateRebuild(dt);
-    maintain();
+    if (!deferMaintain) maintain();
     if (updateLowerLayers) adjustLowerLayers(P);
     return dt;
   }
+  // Within an RK step with time_step_ratio <= 0.5 a stage moves the surface
+  // by at most half a cell, and no band is wider than 4.5 cells on either
+  // side (LocalLaxFriedrichs 2nd order): every cell the step defines lies
+  // within 7 cells of a cell defined at the step's start, inside the brick
+  // margin the last maintenance left.  Such steps maintain once, at the end;
+  // the device check (band reached an unallocated brick) stays armed.
+  bool deferMaintain = false;
 
   bool combineLevelSets(const vlsg_advect_params &P, double wTarget, double wSource) {
     int steps = 1;
@@ -1140,7 +1147,7 @@ public:
     prune(top, true);
     prune(top, false);
     rebuild(top);
-    maintain();
+    if (!deferMaintain) maintain();
     if (L > 1) {
       VLSG_CUDA(cudaMemcpyAsync(pinCounters, counters, 16 * sizeof(int), cudaMemcpyDeviceToHost, stream));
       VLSG_CUDA(cudaStreamSynchronize(stream));
@@ -1193,24 +1200,41 @@ public:
   // Heun RK2 (lsAdvectIntegrationSchemes.hpp:59-108): with a velocity-update
   // callback, stage 1 adjusts the lower layers, the callback runs after it,
   // and the lower layers are restored when the combination etched.
+  // the deferred maintenance at the end of an RK step
+  void endStep() {
+    if (deferMaintain) {
+      deferMaintain = false;
+      maintain();
+    }
+  }
+
   double evolveRungeKutta2(const vlsg_advect_params &P, double maxTimeStep) {
     const bool cb = updCb != nullptr;
+    deferMaintain = P.time_step_ratio <= 0.5;
     saveInitial(cb);
     const double dt1 = evolveForwardEuler(P, maxTimeStep, cb);
-    if (dt1 <= 0.) return 0.;
+    if (dt1 <= 0.) {
+      endStep();
+      return 0.;
+    }
     if (cb) callUpdate();
     const double dt2 = evolveForwardEuler(P, dt1, false);
     const bool etched = combineLevelSets(P, 0.5, 0.5);
     if (etched && cb) restoreLower();
     adjustLowerLayers(P);
+    endStep();
     return 0.5 * dt1 + 0.5 * dt2;
   }
   // SSP RK3 (:110-168)
   double evolveRungeKutta3(const vlsg_advect_params &P, double maxTimeStep) {
     const bool cb = updCb != nullptr;
+    deferMaintain = P.time_step_ratio <= 0.5;
     saveInitial(true);
     const double dt1 = evolveForwardEuler(P, maxTimeStep, cb);
-    if (dt1 <= 0.) return 0.;
+    if (dt1 <= 0.) {
+      endStep();
+      return 0.;
+    }
     if (cb) callUpdate();
     const double dt2 = evolveForwardEuler(P, dt1, false);
     const bool etched1 = combineLevelSets(P, 0.75, 0.25);
@@ -1221,6 +1245,7 @@ public:
     const bool etched2 = combineLevelSets(P, 1.0 / 3.0, 2.0 / 3.0);
     if (etched2) restoreLower();
     adjustLowerLayers(P);
+    endStep();
     return (dt1 + dt2 + 4.0 * dt3) / 6.0;
   }
   double advect(const vlsg_advect_params &P, double maxTimeStep) {
@@ -1233,6 +1258,7 @@ public:
 
   void apply(const vlsg_advect_params &P, vlsg_advect_result &r) override {
     ++generation;
+    deferMaintain = false; // an earlier apply may have ended in an error mid-step
     const bool sllf = P.spatial_scheme == VLSG_STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER;
     rebuildCutoff = sllf ? 1.5 : 1.0;
     rebuildWidth = sllf ? 3 : 2;
