@@ -84,10 +84,30 @@ public:
   int *logCount = nullptr;
   size_t logPer = 0;
   int logSegments = 0;
-  // bricks the next frontier pass of buffer visitBuf must visit (written by
-  // the previous pass of that buffer; visitBuf < 0: visit every brick)
-  uint8_t *visit[2] = {nullptr, nullptr};
-  int vcur = 0, visitBuf = -1;
+  // per buffer: the bricks its next frontier pass must visit, written by the
+  // previous pass over it (visitOk false: visit every brick).  A pass writes
+  // visitSpare, which then takes the buffer's place.  Flags stay valid while
+  // the defined cells only shrink (they over-approximate).
+  uint8_t *visit[MAXB] = {};
+  uint8_t *visitSpare = nullptr;
+  bool visitOk[MAXB] = {};
+  void dropVisits() {
+    for (bool &v : visitOk) v = false;
+  }
+  const uint8_t *visitIn(int b) const { return visitOk[b] ? visit[b] : nullptr; }
+  uint8_t *visitOut() {
+    VLSG_CUDA(cudaMemsetAsync(visitSpare, 0, cap, stream));
+    return visitSpare;
+  }
+  void visitDone(int b) {
+    std::swap(visit[b], visitSpare);
+    visitOk[b] = true;
+  }
+  void copyVisits(int src, int dst) {
+    visitOk[dst] = visitOk[src];
+    if (visitOk[src])
+      VLSG_CUDA(cudaMemcpyAsync(visit[dst], visit[src], cap, cudaMemcpyDeviceToDevice, stream));
+  }
   // host mirrors
   int hCounters[16];
   unsigned long long hScal[4];
@@ -140,9 +160,13 @@ public:
     auto f = [](void *p) { if (p) cudaFree(p); };
     f(brickMap); f(slotBrick); f(slotList); f(freeStack); f(newList); f(counters); f(needed);
     f(scal); f(defCnt); f(rateCounts); f(nbr); f(cflag); f(core); f(small); f(rateV);
-    f(rateStop); f(rateLen); f(act); f(logCell); f(logVal); f(logCount); f(visit[0]); f(visit[1]);
-    visit[0] = visit[1] = nullptr;
-    visitBuf = -1;
+    f(rateStop); f(rateLen); f(act); f(logCell); f(logVal); f(logCount); f(visitSpare);
+    for (auto &v : visit) {
+      f(v);
+      v = nullptr;
+    }
+    visitSpare = nullptr;
+    dropVisits();
     for (auto &k : runKeys) f(k);
     for (auto &b : buf) {
       f(b.vals); f(b.def[0]); f(b.def[1]); f(b.farSign);
@@ -304,8 +328,12 @@ public:
       for (void *p : {(void *)slotBrick, (void *)slotList, (void *)freeStack, (void *)newList,
                       (void *)nbr, (void *)cflag, (void *)act, (void *)logCell, (void *)logVal,
                       (void *)logCount, (void *)rateV, (void *)rateStop, (void *)rateLen,
-                      (void *)visit[0], (void *)visit[1]})
+                      (void *)visitSpare})
         if (p) VLSG_CUDA(cudaFree(p));
+      for (auto &v : visit) {
+        if (v) VLSG_CUDA(cudaFree(v));
+        v = nullptr;
+      }
       slotBrick = slotList = freeStack = newList = nbr = logCount = nullptr;
       cflag = rateLen = nullptr, act = nullptr, logCell = nullptr;
       logVal = rateV = rateStop = nullptr;
@@ -325,9 +353,9 @@ public:
       VLSG_CUDA(cudaMalloc(&logCell, logPer * logSegments * sizeof(uint32_t)));
       VLSG_CUDA(cudaMalloc(&logVal, logPer * logSegments * sizeof(T)));
       VLSG_CUDA(cudaMalloc(&logCount, logSegments * sizeof(int)));
-      VLSG_CUDA(cudaMalloc(&visit[0], n));
-      VLSG_CUDA(cudaMalloc(&visit[1], n));
-      visitBuf = -1;
+      for (auto &v : visit) VLSG_CUDA(cudaMalloc(&v, n));
+      VLSG_CUDA(cudaMalloc(&visitSpare, n));
+      dropVisits();
       VLSG_CUDA(cudaMalloc(&rateV, n * BV * sizeof(T) * l));
       VLSG_CUDA(cudaMalloc(&rateStop, n * BV * sizeof(T) * l));
       VLSG_CUDA(cudaMalloc(&rateLen, n * BV));
@@ -361,7 +389,7 @@ public:
   // are large enough.
   void build(const GridDev &grid, std::vector<StagedLS> &ls, int margin) override {
     ++generation;
-    visitBuf = -1;
+    dropVisits();
     ensureSmall();
     g = grid;
     L = (int)ls.size();
@@ -595,8 +623,11 @@ public:
       Scope sc(this, "maint_init");
       kInitNewSlots<T><<<blocksPass, 128, 0, stream>>>(g, newList, nNewPtr(), slotBrick, bufSet());
       checkLaunch();
-      if (visitBuf >= 0) {
-        kVisitNewSlots<<<blocksPass, 256, 0, stream>>>(newList, nNewPtr(), visit[vcur]);
+      VisitSet vs{};
+      for (int b = 0; b < MAXB; ++b)
+        if (visitOk[b]) vs.p[vs.n++] = visit[b];
+      if (vs.n) {
+        kVisitNewSlots<<<blocksPass, 256, 0, stream>>>(newList, nNewPtr(), vs);
         checkLaunch();
       }
     }
@@ -622,13 +653,9 @@ public:
         buf[b].cur ^= 1;
         return bandPassBytes(nIn, buf[b].nDef);
       });
-      const uint8_t *visitIn = visitBuf == b ? visit[vcur] : nullptr;
-      uint8_t *visitOut = visit[1 - vcur];
-      VLSG_CUDA(cudaMemsetAsync(visitOut, 0, cap, stream));
       kFrontierPass<T, MODE, Rule><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(
-          topo(), lsView(b), rule, changeLog(), visitIn, visitOut);
-      vcur ^= 1;
-      visitBuf = b;
+          topo(), lsView(b), rule, changeLog(), visitIn(b), visitOut());
+      visitDone(b);
       checkLaunch();
     }
     applyChanges(b);
@@ -683,13 +710,9 @@ public:
         // in: the active band; out: the new band
         return bandPassBytes(lastActive, buf[top].nDef);
       });
-      const uint8_t *visitIn = visitBuf == top ? visit[vcur] : nullptr;
-      uint8_t *visitOut = visit[1 - vcur];
-      VLSG_CUDA(cudaMemsetAsync(visitOut, 0, cap, stream));
       kUpdateRebuild<T><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(
-          topo(), lsView(top), act, rebuildCutoff, changeLog(), visitIn, visitOut);
-      vcur ^= 1;
-      visitBuf = top;
+          topo(), lsView(top), act, rebuildCutoff, changeLog(), visitIn(top), visitOut());
+      visitDone(top);
       checkLaunch();
     }
     applyChanges(top);
@@ -699,7 +722,8 @@ public:
     ++stages;
   }
   template <class Comp> void pointwise(int a, int bb, Comp comp, int *flag) {
-    visitBuf = -1;
+    // a combination that only undefines cells keeps a's flags valid
+    if (!Comp::keepsUndefinedA) visitOk[a] = false;
     {
       const int64_t nA = profiling ? defined(a) : 0, nB = profiling ? defined(bb) : 0;
       Scope sc(this, "boolean", [this, a, nA, nB] {
@@ -733,7 +757,7 @@ public:
   // An empty level set in buffer b (Domain(grid): positive everywhere, width 1).
   void clearBuffer(int b) {
     allocBuffers(b + 1);
-    if (visitBuf == b) visitBuf = -1;
+    visitOk[b] = false;
     auto &B = buf[b];
     kFillSlots<T><<<blocksPass, 256, 0, stream>>>(slotList, nSlotsPtr(), B.vals, B.def[B.cur],
                                                   Lim<T>::max());
@@ -787,7 +811,7 @@ public:
     copyBuffer(fin, L - 1);
     buf[fin].live = false;
     if (above < 2 * L) buf[above].live = false;
-    visitBuf = -1;
+    dropVisits();
     maintain();
     syncErr("PrepareStencilLocalLaxFriedrichs");
   }
@@ -795,7 +819,7 @@ public:
   // level set below it.
   void finalizeStencil() {
     ++generation;
-    visitBuf = -1;
+    dropVisits();
     invertBuffer(L - 1);
     booleanOp(L - 1, L - 2, MinComp<T>{});
     maintain();
@@ -803,8 +827,8 @@ public:
   }
 
   void copyBuffer(int src, int dst) {
-    if (visitBuf == dst) visitBuf = -1;
     allocBuffers(dst + 1);
+    copyVisits(src, dst);
     auto &S = buf[src];
     auto &D = buf[dst];
     {
@@ -1160,8 +1184,8 @@ public:
     for (int l = all ? 0 : L - 1; l < L; ++l) copyBuffer(l, L + l);
   }
   void restoreLower() {
-    visitBuf = -1;
     for (int l = 0; l + 1 < L; ++l) {
+      copyVisits(L + l, l);
       // copy initial back into the current buffer
       auto &S = buf[L + l];
       auto &D = buf[l];

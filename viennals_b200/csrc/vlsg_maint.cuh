@@ -128,10 +128,16 @@ __global__ void kAllocNeeded(int nBricks, int *brickMap, int *slotBrick, const u
 
 // New slots are visited by the next pass: the face cells of their
 // neighbours were not marked for them while they were unallocated.
-__global__ void kVisitNewSlots(const int *newList, const int *nNew, uint8_t *visit) {
+struct VisitSet {
+  uint8_t *p[MAXB];
+  int n;
+};
+__global__ void kVisitNewSlots(const int *newList, const int *nNew, VisitSet v) {
   const int n = *nNew;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    visit[newList[i]] = 1;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int slot = newList[i];
+    for (int k = 0; k < v.n; ++k) v.p[k][slot] = 1;
+  }
 }
 
 // New slots: every cell undefined with the brick's far sign, no defined cell.
