@@ -674,6 +674,13 @@ public:
       ExpandRule<T> r{totalLimit, T((startWidth + c + 1) * T(0.5))};
       if (onlyUndefined) frontierPass<FP_EXPAND>(b, r, "expand");
       else frontierPass<FP_ALL>(b, r, "expand");
+      if (b == L - 1 && startWidth + c + 1 == saveTopAt) {
+        // the RK copy of the top level set, taken at this width (saveTop)
+        saveTopAt = 0;
+        copyBuffer(b, 2 * L - 1);
+        buf[2 * L - 1].width = startWidth + c + 1;
+        buf[2 * L - 1].bound = 0.5 * (startWidth + c + 1);
+      }
     }
     buf[b].width = width;
     buf[b].bound = (double)totalLimit;
@@ -1180,8 +1187,23 @@ public:
     return false;
   }
 
-  void saveInitial(bool all) {
-    for (int l = all ? 0 : L - 1; l < L; ++l) copyBuffer(l, L + l);
+  // The RK copy of the top level set is first read by the stage combination,
+  // after Expand to E = ceil(2 steps ratio + 1) (combineLevelSets).  When the
+  // first stage's Expand to the scheme's width S and the copy's Expand to E
+  // both only define new cells (|value| <= min(E, S) / 2 on the defined
+  // cells), each of their cycles depends only on the width it starts from,
+  // so the first stage's band at width min(E, S) is the copy expanded to that
+  // width, value for value.  The copy is taken there (expand()), which saves
+  // the copy's own Expand cycles.  Otherwise it is taken now.
+  int saveTopAt = 0;
+  void saveTop(const vlsg_advect_params &P, int steps) {
+    const int top = L - 1;
+    const int E = (int)std::ceil(2.0 * steps * P.time_step_ratio + 1);
+    const int S = schemeWidth(P.spatial_scheme);
+    const int at = std::min(E, S);
+    saveTopAt = 0;
+    if (S < 0 || buf[top].width >= at || buf[top].bound > 0.5 * at) copyBuffer(top, L + top);
+    else saveTopAt = at;
   }
   void restoreLower() {
     for (int l = 0; l + 1 < L; ++l) {
@@ -1235,7 +1257,9 @@ public:
   double evolveRungeKutta2(const vlsg_advect_params &P, double maxTimeStep) {
     const bool cb = updCb != nullptr;
     deferMaintain = P.time_step_ratio <= 0.5;
-    saveInitial(cb);
+    if (cb)
+      for (int l = 0; l + 1 < L; ++l) copyBuffer(l, L + l);
+    saveTop(P, 2);
     const double dt1 = evolveForwardEuler(P, maxTimeStep, cb);
     if (dt1 <= 0.) {
       endStep();
@@ -1253,7 +1277,8 @@ public:
   double evolveRungeKutta3(const vlsg_advect_params &P, double maxTimeStep) {
     const bool cb = updCb != nullptr;
     deferMaintain = P.time_step_ratio <= 0.5;
-    saveInitial(true);
+    for (int l = 0; l + 1 < L; ++l) copyBuffer(l, L + l);
+    saveTop(P, 3);
     const double dt1 = evolveForwardEuler(P, maxTimeStep, cb);
     if (dt1 <= 0.) {
       endStep();
@@ -1283,6 +1308,7 @@ public:
   void apply(const vlsg_advect_params &P, vlsg_advect_result &r) override {
     ++generation;
     deferMaintain = false; // an earlier apply may have ended in an error mid-step
+    saveTopAt = 0;
     const bool sllf = P.spatial_scheme == VLSG_STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER;
     rebuildCutoff = sllf ? 1.5 : 1.0;
     rebuildWidth = sllf ? 3 : 2;
