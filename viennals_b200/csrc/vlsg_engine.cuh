@@ -124,6 +124,7 @@ public:
   int numSMs = 148;
   int blocksPass = 148 * VLSG_PASS_MIN_BLOCKS;
   int blocksRate = 148 * rateMinBlocks<T>();
+  int blocksRateWeno = 148 * rateMinBlocks<T, FAM_WENO>();
   // exchange format (points and runs in HRLE order), cached per buffer until
   // the level sets change
   struct Scratch {
@@ -373,6 +374,7 @@ public:
     VLSG_CUDA(cudaDeviceGetAttribute(&numSMs, cudaDevAttrMultiProcessorCount, dev));
     blocksPass = numSMs * VLSG_PASS_MIN_BLOCKS;
     blocksRate = numSMs * rateMinBlocks<T>();
+    blocksRateWeno = numSMs * rateMinBlocks<T, FAM_WENO>();
     VLSG_CUDA(cudaHostAlloc(&pinCounters, 32 * sizeof(int), cudaHostAllocDefault));
     VLSG_CUDA(cudaHostAlloc(&pinScal, 32 * sizeof(unsigned long long), cudaHostAllocDefault));
     VLSG_CUDA(cudaMalloc(&counters, 16 * sizeof(int)));
@@ -940,8 +942,8 @@ public:
         checkLaunch();
         kSllfPick<<<1, 1024, 0, stream>>>(A.sllfKey, A.sllfAlpha, rateWarps, scal + 1);
       } else if (weno) {
-        if (velCb) kRates<T, 0, true, FAM_WENO><<<blocksRate, RATE_THREADS, 0, stream>>>(A, vel);
-        else kRates<T, 0, false, FAM_WENO><<<blocksRate, RATE_THREADS, 0, stream>>>(A, vel);
+        if (velCb) kRates<T, 0, true, FAM_WENO><<<blocksRateWeno, RATE_THREADS, 0, stream>>>(A, vel);
+        else kRates<T, 0, false, FAM_WENO><<<blocksRateWeno, RATE_THREADS, 0, stream>>>(A, vel);
       } else if (velCb) {
         kRates<T, 0, true><<<blocksRate, RATE_THREADS, 0, stream>>>(A, vel);
       } else {

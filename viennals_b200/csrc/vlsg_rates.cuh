@@ -776,14 +776,18 @@ __device__ inline uint64_t activePlanes(const T *vals, int slot) {
   return mine;
 }
 
-// Resident blocks per SM: 3 for float (80 registers), 2 for double (the
-// FP64 stencils need 128 registers to stay out of local memory).
-template <class T> constexpr int rateMinBlocks() { return sizeof(T) == 4 ? 3 : 2; }
+// Resident blocks per SM: 3 for float (80 registers), 4 for the float WENO
+// kernels (64 registers: a few spilled values, 8% faster than 3 blocks), 2
+// for double (the FP64 stencils need 128 registers to stay out of local
+// memory).
+template <class T, int FAM = FAM_ANY> constexpr int rateMinBlocks() {
+  return sizeof(T) == 4 ? (FAM == FAM_WENO ? 4 : 3) : 2;
+}
 // MODE 0: rates (integrateTime); MODE 1: the global alphas of the
 // Lax-Friedrichs schemes (findGlobalAlphas).  TABLE: velocities from the
 // host callback's table instead of the device functor.
 template <class T, int MODE, bool TABLE = false, int FAM = FAM_ANY>
-__global__ void __launch_bounds__(RATE_THREADS, rateMinBlocks<T>())
+__global__ void __launch_bounds__(RATE_THREADS, rateMinBlocks<T, FAM>())
     kRates(RateArgs<T> A, const vlsg_velocity_desc desc) {
   __shared__ uint16_t sList[RATE_THREADS / 32][BV];
   uint16_t *list = sList[threadIdx.x >> 5];
