@@ -192,6 +192,7 @@ public:
   int *flagPtr() { return counters + 4; }
   int *nOutPtr() { return counters + 5; }
   int *nNewPtr() { return counters + 10; }
+  int *zeroPtr() { return counters + 14; } // a Prune pass met a defined +-0
 
   MapView mapView() const { return MapView{brickMap, slotBrick}; }
   Buf<T> view(int b) const { return Buf<T>{buf[b].vals, buf[b].farSign}; }
@@ -645,7 +646,8 @@ public:
   }
 
   // One star pass of `rule` over buffer b: candidates, changes, write-back.
-  template <int MODE, class Rule> void frontierPass(int b, Rule rule, const char *name) {
+  template <int MODE, class Rule>
+  void frontierPass(int b, Rule rule, const char *name, int zeroMode = 0) {
     const int64_t nIn = profiling ? defined(b) : 0;
     {
       Scope sc(this, name, [this, b, nIn] {
@@ -656,7 +658,7 @@ public:
         return bandPassBytes(nIn, buf[b].nDef);
       });
       kFrontierPass<T, MODE, Rule><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(
-          topo(), lsView(b), rule, changeLog(), visitIn(b), visitOut());
+          topo(), lsView(b), rule, changeLog(), visitIn(b), visitOut(), zeroPtr(), zeroMode, cap);
       visitDone(b);
       checkLaunch();
     }
@@ -686,6 +688,18 @@ public:
     }
     buf[b].width = width;
     buf[b].bound = (double)totalLimit;
+  }
+  // Prune with stray-zero removal, then without (lsBooleanOperation.hpp:
+  // 203-210).  When the first pass meets no defined value +-0 it only turns
+  // cells undefined with their sign class, and every cell it keeps keeps a
+  // star neighbour of the other sign class (that neighbour is kept as well,
+  // or is undefined and keeps its class): the second pass then changes
+  // nothing, and its kernel only carries the masks and visit flags over.
+  void prunePair(int b) {
+    VLSG_CUDA(cudaMemsetAsync(zeroPtr(), 0, sizeof(int), stream));
+    frontierPass<FP_PRUNE>(b, PruneRule<T>{true}, "prune", 1);
+    frontierPass<FP_PRUNE>(b, PruneRule<T>{false}, "prune", 2);
+    buf[b].width = 2;
   }
   void prune(int b, bool rsz) {
     frontierPass<FP_PRUNE>(b, PruneRule<T>{rsz}, "prune");
@@ -759,8 +773,7 @@ public:
   // BooleanOperation + Prune x2 (lsBooleanOperation.hpp:199-212)
   template <class Comp> void booleanOp(int a, int bb, Comp comp, int *flag = nullptr) {
     pointwise(a, bb, comp, flag);
-    prune(a, true);
-    prune(a, false);
+    prunePair(a);
   }
 
   // An empty level set in buffer b (Domain(grid): positive everywhere, width 1).
@@ -1177,8 +1190,7 @@ public:
     VLSG_CUDA(cudaMemsetAsync(flagPtr(), 0, sizeof(int), stream));
     CombineComp<T> comp{wTarget, wSource};
     pointwise(top, init, comp, flagPtr());
-    prune(top, true);
-    prune(top, false);
+    prunePair(top);
     rebuild(top);
     if (!deferMaintain) maintain();
     if (L > 1) {

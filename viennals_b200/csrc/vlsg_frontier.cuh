@@ -260,7 +260,7 @@ enum : int { FP_EXPAND = 0, FP_PRUNE = 1, FP_ALL = 2 };
 template <class T, int MODE, class Rule>
 __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
     kFrontierPass(Topo t, LsView<T> v, Rule rule, ChangeLog<T> lg, const uint8_t *visitIn,
-                  uint8_t *visitOut) {
+                  uint8_t *visitOut, int *zeros, int zeroMode, int poolSlots) {
   __shared__ WarpScratch sm[FRONTIER_THREADS / 32];
   WarpScratch &ws = sm[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
@@ -269,6 +269,23 @@ __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
   const int n = *t.nSlots;
   const size_t logBase = (size_t)warp * lg.per;
   int logged = 0;
+  // zeroMode 1: record a defined candidate +-0 in *zeros; zeroMode 2: when
+  // *zeros is 0 the pass is known to change nothing (the second Prune of a
+  // pair): copy the masks and the visit flags of the whole pool (free slots
+  // included, whose contents no one reads), log nothing
+  if (MODE == FP_PRUNE && zeroMode == 2 && *zeros == 0) {
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t nThreads = (size_t)gridDim.x * blockDim.x;
+    const uint4 *src = reinterpret_cast<const uint4 *>(v.def); // 4 x 16 bytes per slot
+    uint4 *dst = reinterpret_cast<uint4 *>(v.defNext);
+    for (size_t i = tid; i < (size_t)poolSlots * 4; i += nThreads) dst[i] = src[i];
+    if (visitOut)
+      for (size_t i = tid; i < (size_t)poolSlots; i += nThreads)
+        visitOut[i] = visitIn ? visitIn[i] : 1;
+    if (lane == 0) lg.count[warp] = 0;
+    return;
+  }
+  bool zeroHit = false;
   for (int w = warp; w < n; w += nWarps) {
     const int slot = t.slotList[w];
     const bool complex = (t.cflag[slot] & CF_STAR) != 0;
@@ -305,6 +322,7 @@ __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
       if (k < total) {
         c = ws.list[k];
         const T center = v.vals[(size_t)slot * BV + c];
+        if (MODE == FP_PRUNE && center == T(0)) zeroHit = true;
         T nb[6];
 #pragma unroll
         for (int j = 0; j < 6; ++j) {
@@ -321,6 +339,8 @@ __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
     finishBrick(ws, v.defNext, slot, lane, own, visitOut);
   }
   if (lane == 0) lg.count[warp] = logged;
+  if (MODE == FP_PRUNE && zeroMode == 1 && __any_sync(0xffffffffu, zeroHit) && lane == 0)
+    atomicOr(zeros, 1);
 }
 
 // Write a change log back: warp w copies segment w.
