@@ -58,10 +58,16 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "20"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # the timed region is short (~0.1 s): start it once nvidia-smi
+            # reports, and count only the samples taken from then on
+            t0 = time.time()
+            while not self.samples and time.time() - t0 < 5.0 and self.proc.poll() is None:
+                time.sleep(0.005)
+            self.samples = []
         except Exception:
             self.proc = None
         return self
