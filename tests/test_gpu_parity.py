@@ -53,6 +53,21 @@ def test_time_integration_cases(spatial, temporal):
     _parity(g, lss, constant_vector([1.0, 0.0, 0.0]), params(spatial, temporal, 0.5))
 
 
+@pytest.mark.parametrize("half,spatial,temporal", [(3.0, 11, 2), (1.5, 11, 1), (1.5, 0, 2),
+                                                   (2.5, 8, 2), (1.0, 0, 2), (1.0, 5, 1)])
+def test_band_width_and_saved_copy(half, spatial, temporal):
+    # Uploaded bands of width 2 * half.  The RK copy of the top level set is
+    # taken during the first stage's Expand when the band is narrower than the
+    # stage combination's Expand width and its values stay within half of it,
+    # otherwise at the step's start; both must match the reference's deep copy
+    # at the step's start.
+    g = Grid([-5, 5, -5, 5, -5, 5], [BC.INFINITE_BOUNDARY] * 3, 0.15)
+    ls = sdf_levelset(g, lambda x, y, z: np.sqrt(x * x + y * y + z * z) - 1.5,
+                      [-22] * 3, [22] * 3, half_width=half)
+    assert ls.width == int(round(2 * half))
+    _parity(g, [ls], constant_vector([1.0, 0.0, 0.0]), params(spatial, temporal, 0.3))
+
+
 @pytest.mark.parametrize("spatial", [0, 1, 2, 3, 5, 6, 7, 8, 10, 11])
 def test_all_schemes_egg_velocity(spatial):
     g = Grid(None, [BC.INFINITE_BOUNDARY] * 3, 0.6999999)

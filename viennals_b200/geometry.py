@@ -67,14 +67,15 @@ def make_sphere(grid, origin, radius):
     return Domain(grid, idx.astype(np.int32), vals, rs, sg, width=2)
 
 
-def sdf_levelset(grid, sdf, lo, hi, lipschitz=1.0):
-    """Width-2 band of a signed distance function (physical units).
+def sdf_levelset(grid, sdf, lo, hi, lipschitz=1.0, half_width=1.0):
+    """Band of a signed distance function (physical units), width 2 by default.
 
-    Every cell of the index box [lo, hi] with |sdf| <= gridDelta is defined
-    with value sdf / gridDelta; undefined runs carry the sign of sdf.  Bricks
-    of 8^3 cells whose centre is further than their half diagonal (times
-    `lipschitz`) plus one cell from the surface are skipped unevaluated.
-    sdf(x, y, z) takes float arrays of coordinates.
+    Every cell of the index box [lo, hi] with |sdf| <= half_width * gridDelta
+    is defined with value sdf / gridDelta (the level set's width is
+    2 * half_width); undefined runs carry the sign of sdf.  Bricks of 8^3
+    cells whose centre is further than their half diagonal (times
+    `lipschitz`) plus half_width + 0.5 cells from the surface are skipped
+    unevaluated.  sdf(x, y, z) takes float arrays of coordinates.
     """
     gd = grid.delta
     lo = [int(v) for v in lo]
@@ -86,7 +87,7 @@ def sdf_levelset(grid, sdf, lo, hi, lipschitz=1.0):
     cy = (lo[1] + by * B + 3.5) * gd
     cz = (lo[2] + bz * B + 3.5) * gd
     dc = sdf(cx.ravel(), cy.ravel(), cz.ravel())
-    reach = (np.sqrt(3.0) * 4.0 * lipschitz + 1.5) * gd
+    reach = (np.sqrt(3.0) * 4.0 * lipschitz + half_width + 0.5) * gd
     near = np.nonzero(np.abs(dc) <= reach)[0]
     off = np.arange(B)
     oz, oy, ox = np.meshgrid(off, off, off, indexing="ij")
@@ -101,7 +102,7 @@ def sdf_levelset(grid, sdf, lo, hi, lipschitz=1.0):
         inside = (X <= hi[0]) & (Y <= hi[1]) & (Z <= hi[2])
         X, Y, Z = X[inside], Y[inside], Z[inside]
         v = sdf(X * gd, Y * gd, Z * gd) / gd
-        keep = np.abs(v) <= 1.0
+        keep = np.abs(v) <= half_width
         idx_parts.append(np.stack([X[keep], Y[keep], Z[keep]], 1))
         val_parts.append(v[keep])
     idx = np.concatenate(idx_parts) if idx_parts else np.zeros((0, 3), np.int64)
@@ -118,7 +119,7 @@ def sdf_levelset(grid, sdf, lo, hi, lipschitz=1.0):
         return np.where(sdf(np.asarray(x) * gd, np.asarray(y) * gd, np.asarray(z) * gd) < 0, -1, 1)
 
     rs, sg = make_runs(idx, sign_fn, [lo[0] - 1, lo[1] - 1, lo[2] - 1], [hi[0] + 1, hi[1] + 1, hi[2] + 1])
-    return Domain(grid, idx.astype(np.int32), vals, rs, sg, width=2)
+    return Domain(grid, idx.astype(np.int32), vals, rs, sg, width=int(round(2 * half_width)))
 
 
 # signed distance helpers (physical units) ----------------------------------
