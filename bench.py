@@ -99,6 +99,18 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.samples)}
 
 
+def reduce_over_ranks(ms, updates, device):
+    """Timed-region milliseconds (max over ranks) and point updates (sum over
+    ranks) through the initialised process group."""
+    import torch
+
+    t = torch.tensor([float(ms)], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    u = torch.tensor([float(updates)], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(u)
+    return float(t.item()), float(u.item())
+
+
 def build_workload(args, device):
     from viennals_b200.synth import perturbed_sphere, precision_velocity
 
@@ -160,12 +172,11 @@ def run_ours(args, rank, world):
     ms = ev0.elapsed_time(ev1)
     if dist:
         torch.distributed.barrier()
-        t = torch.tensor([ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-        u = torch.tensor([float(updates)], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(u)
-        total_updates = float(u.item())
+        ms, total_updates = reduce_over_ranks(ms, updates, dev)
+        # what follows (profiling step, e2e, precision report, CPU baseline)
+        # runs on rank 0 alone and needs no collective: the other ranks leave
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
     else:
         total_updates = float(updates)
     value = total_updates / (ms / 1e3)
@@ -430,13 +441,10 @@ def main():
     if world > 1:
         import torch
         torch.cuda.set_device(args.local_rank)
+        # collectives: barriers and reductions around the timed region only
         torch.distributed.init_process_group(
-            "nccl", timeout=__import__("datetime").timedelta(seconds=600))
+            "nccl", timeout=__import__("datetime").timedelta(seconds=120))
     out = run_ours(args, rank, world)
-    if world > 1:
-        import torch
-        torch.distributed.barrier()
-        torch.distributed.destroy_process_group()
     if rank != 0:
         return
     peaks = measured_peaks()
