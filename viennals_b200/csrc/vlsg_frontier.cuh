@@ -236,7 +236,8 @@ __device__ inline int listCells(uint64_t plane, uint16_t *list) {
 }
 
 __device__ inline void markCell(unsigned long long *words, int c) {
-  atomicOr(&words[c >> 6], 1ull << (c & 63));
+  // the 32-bit half of the plane word that holds the cell (little endian)
+  atomicOr(reinterpret_cast<unsigned *>(words) + (c >> 5), 1u << (c & 31));
 }
 
 // Append the lanes with `has` to the warp's log segment (warp-uniform call).
