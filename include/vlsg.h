@@ -303,6 +303,11 @@ int vlsg_prepare_stencil_llf(vlsg_context *ctx, const int32_t *is_depo, int32_t 
  * (top = inverted top united with the level set below; needs two). */
 int vlsg_finalize_stencil_llf(vlsg_context *ctx);
 
+/* Advect::prepareLS (lsAdvect.hpp:972-1015): Expand the top level set to the
+ * width the spatial scheme reads (vlsg_spatial_scheme); VLSG_ERR_ARGUMENT for
+ * an unknown scheme ("Advect: Discretization scheme not found."). */
+int vlsg_prepare_ls(vlsg_context *ctx, int32_t spatial_scheme);
+
 /* Velocity plugin: either a device functor or a host callback. */
 int vlsg_set_velocity_functor(vlsg_context *ctx, const vlsg_velocity_desc *v);
 int vlsg_set_velocity_callback(vlsg_context *ctx, vlsg_velocity_cb cb,

@@ -239,25 +239,20 @@ public:
   const vlsg_advect_result &getResult() const { return result; }
 
   // Advect::apply, lsAdvect.hpp:1017-1043
+  // Advect::prepareLS (lsAdvect.hpp:972-1015): the top level set expanded to
+  // the width the spatial scheme reads, written back.
+  void prepareLS() {
+    if (levelSets.empty()) return logError("No level sets passed to Advect.");
+    if (!uploadLevelSets()) return;
+    if (!check(vlsg_prepare_ls(ctx, params.spatial_scheme))) return;
+    downloadLevelSet(levelSets.size() - 1);
+  }
+
   void apply() {
     if (levelSets.empty()) return logError("No level sets passed to Advect. Not advecting.");
     if (!velocities && !field)
       return logError("No velocity field passed to Advect. Not advecting.");
-    if (!ctx) {
-      const int precision = sizeof(T) == 4 ? VLSG_FP32 : VLSG_FP64;
-      if (!check(vlsg_create(&ctx, device, precision))) return;
-    }
-    const Grid &g = levelSets.back()->grid;
-    if (!check(vlsg_set_grid(ctx, 3, g.min.data(), g.max.data(), g.boundary.data(), g.gridDelta)))
-      return;
-    if (!check(vlsg_set_level_set_count(ctx, (int32_t)levelSets.size()))) return;
-    for (size_t i = 0; i < levelSets.size(); ++i) {
-      const LevelSet &ls = *levelSets[i];
-      if (!check(vlsg_upload_levelset(ctx, (int32_t)i, ls.numberOfPoints(), ls.indices.data(),
-                                      ls.values.data(), (int64_t)ls.runSign.size(),
-                                      ls.runStart.data(), ls.runSign.data(), ls.width)))
-        return;
-    }
+    if (!uploadLevelSets()) return;
     if (field) {
       if (!check(vlsg_set_velocity_callback(ctx, &VelocityField<T>::callback, field.get()))) return;
       if (!check(vlsg_set_dissipation_alpha_callback(ctx, &VelocityField<T>::alphaCallback,
@@ -270,27 +265,49 @@ public:
             ctx, velocityUpdateCallback ? &Advect<T>::updateTrampoline : nullptr, this)))
       return;
     if (!check(vlsg_advect(ctx, &params, &result))) return;
-    for (size_t i = 0; i < levelSets.size(); ++i) {
-      LevelSet &ls = *levelSets[i];
-      int64_t n = 0;
-      if (!check(vlsg_count_points(ctx, (int32_t)i, &n))) return;
-      ls.indices.resize(3 * n);
-      ls.values.resize(n);
-      int32_t w = 0;
-      if (!check(vlsg_download_levelset(ctx, (int32_t)i, n, ls.indices.data(), ls.values.data(), &w)))
-        return;
-      ls.width = w;
-      // undefined runs in HRLE order, built on the device
-      int64_t m = 0;
-      const int rc = vlsg_download_runs(ctx, (int32_t)i, 0, nullptr, nullptr, &m);
-      if (rc != VLSG_OK && rc != VLSG_ERR_CAPACITY && !check(rc)) return;
-      ls.runStart.resize(3 * m);
-      ls.runSign.resize(m);
-      if (!check(vlsg_download_runs(ctx, (int32_t)i, m, ls.runStart.data(), ls.runSign.data(), &m)))
-        return;
-    }
+    for (size_t i = 0; i < levelSets.size(); ++i)
+      if (!downloadLevelSet(i)) return;
   }
 
+private:
+  // the context (created on first use) holding the grid and all level sets
+  bool uploadLevelSets() {
+    if (!ctx) {
+      const int precision = sizeof(T) == 4 ? VLSG_FP32 : VLSG_FP64;
+      if (!check(vlsg_create(&ctx, device, precision))) return false;
+    }
+    const Grid &g = levelSets.back()->grid;
+    if (!check(vlsg_set_grid(ctx, 3, g.min.data(), g.max.data(), g.boundary.data(), g.gridDelta)))
+      return false;
+    if (!check(vlsg_set_level_set_count(ctx, (int32_t)levelSets.size()))) return false;
+    for (size_t i = 0; i < levelSets.size(); ++i) {
+      const LevelSet &ls = *levelSets[i];
+      if (!check(vlsg_upload_levelset(ctx, (int32_t)i, ls.numberOfPoints(), ls.indices.data(),
+                                      ls.values.data(), (int64_t)ls.runSign.size(),
+                                      ls.runStart.data(), ls.runSign.data(), ls.width)))
+        return false;
+    }
+    return true;
+  }
+  // level set i written back: defined points and undefined runs in HRLE
+  // order, both built on the device
+  bool downloadLevelSet(size_t i) {
+    LevelSet &ls = *levelSets[i];
+    int64_t n = 0;
+    if (!check(vlsg_count_points(ctx, (int32_t)i, &n))) return false;
+    ls.indices.resize(3 * n);
+    ls.values.resize(n);
+    int32_t w = 0;
+    if (!check(vlsg_download_levelset(ctx, (int32_t)i, n, ls.indices.data(), ls.values.data(), &w)))
+      return false;
+    ls.width = w;
+    int64_t m = 0;
+    const int rc = vlsg_download_runs(ctx, (int32_t)i, 0, nullptr, nullptr, &m);
+    if (rc != VLSG_OK && rc != VLSG_ERR_CAPACITY && !check(rc)) return false;
+    ls.runStart.resize(3 * m);
+    ls.runSign.resize(m);
+    return check(vlsg_download_runs(ctx, (int32_t)i, m, ls.runStart.data(), ls.runSign.data(), &m));
+  }
 };
 
 } // namespace vlsg

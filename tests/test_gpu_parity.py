@@ -150,3 +150,38 @@ def test_empty_level_set():
     d = Domain(g, np.zeros((0, 3), np.int32), np.zeros(0),
                np.array([[-100, -100, -100]], np.int32), np.array([1], np.int8), 2)
     _parity(g, [d], constant_scalar(1.0), params(0, 0, 0.5))
+
+
+# Expand width per spatial scheme (the schemes' prepareLS)
+SCHEME_WIDTH = {0: 3, 1: 5, 2: 3, 3: 5, 4: 7, 5: 3, 6: 5, 7: 7, 8: 9, 9: 8, 10: 5, 11: 7}
+
+
+@pytest.mark.parametrize("spatial", [0, 3, 8, 9, 11])
+def test_prepare_ls_matches_oracle_expand(spatial):
+    # Advect::prepareLS (lsAdvect.hpp:972-1015) through vlsg_prepare_ls: the
+    # top level set expanded to the scheme's width
+    from oracle import oracle as O
+    from viennals_b200.advect import Context
+
+    g, lss = sphere_case(5.0, 0.25)
+    ols = O.OracleLS(g, lss[0])
+    ols.expand(SCHEME_WIDTH[spatial])
+    ctx = Context()
+    ctx.set_grid(g)
+    ctx.set_level_set_count(1)
+    ctx.upload(0, lss[0])
+    ctx.prepare_ls(spatial)
+    assert ctx.download(0)[2] == ols.width == SCHEME_WIDTH[spatial]
+    compare([ols], ctx)
+
+
+def test_prepare_ls_unknown_scheme_is_an_error():
+    from viennals_b200.advect import Context
+
+    g, lss = sphere_case(5.0, 0.25)
+    ctx = Context()
+    ctx.set_grid(g)
+    ctx.set_level_set_count(1)
+    ctx.upload(0, lss[0])
+    with pytest.raises(RuntimeError, match="Discretization scheme not found"):
+        ctx.prepare_ls(99)

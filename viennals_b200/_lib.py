@@ -51,6 +51,7 @@ def load(build_if_missing=True):
     L.vlsg_set_velocity_update_callback.argtypes = [vp, UPDATE_CALLBACK, vp]
     L.vlsg_prepare_stencil_llf.argtypes = [vp, ctypes.POINTER(ctypes.c_int32), ctypes.c_int32]
     L.vlsg_finalize_stencil_llf.argtypes = [vp]
+    L.vlsg_prepare_ls.argtypes = [vp, i32]
     L.vlsg_advect.argtypes = [vp, P(AdvectParams), P(AdvectResult)]
     L.vlsg_set_profiling.argtypes = [vp, i32]
     L.vlsg_get_kernel_stats.argtypes = [vp, i32, P(KernelStat), P(i32)]
@@ -66,6 +67,7 @@ EXPORTED = [
     "vlsg_get_values", "vlsg_get_values_noalloc",
     "vlsg_set_velocity_functor", "vlsg_set_velocity_callback",
     "vlsg_set_dissipation_alpha_callback", "vlsg_prepare_stencil_llf", "vlsg_finalize_stencil_llf",
+    "vlsg_prepare_ls",
     "vlsg_set_velocity_update_callback", "vlsg_advect", "vlsg_advect_batch",
     "vlsg_set_profiling", "vlsg_get_kernel_stats", "vlsg_compare",
 ]

@@ -121,6 +121,10 @@ class Context:
     def finalize_stencil_llf(self):
         self._check(self.lib.vlsg_finalize_stencil_llf(self.h))
 
+    def prepare_ls(self, spatial_scheme):
+        """vlsg_prepare_ls: Expand the top level set to the scheme's width."""
+        self._check(self.lib.vlsg_prepare_ls(self.h, int(spatial_scheme)))
+
     def set_velocity(self, desc):
         self._check(self.lib.vlsg_set_velocity_functor(self.h, ctypes.byref(desc)))
 
@@ -305,9 +309,6 @@ class Advect:
         static in the reference, per Advect object here)."""
         self.params.max_dissipation = float(d)
 
-    def setVelocityUpdateCallback(self, cb):
-        raise RuntimeError("setVelocityUpdateCallback is not supported by the GPU front")
-
     # getters, lsAdvect.hpp:920-932 ---------------------------------------
     def getAdvectedTime(self):
         return self.result.advected_time
@@ -329,12 +330,11 @@ class Advect:
     def _fingerprint(d):
         return (d.n_points, d.width, hash(d.idx.tobytes()), hash(d.values.tobytes()))
 
-    def _sync_to_device(self):
+    def _sync_to_device(self, need_velocity=True):
         if not self.levelSets:
             raise RuntimeError("No level sets passed to Advect. Not advecting.")
-        if self.velocities is None:
+        if self.velocities is None and need_velocity:
             raise RuntimeError("No velocity field passed to Advect. Not advecting.")
-        desc = self.velocities.descriptor()
         if self.ctx is None:
             self.ctx = Context(self.device, self.precision)
         key = [id(d) for d in self.levelSets]
@@ -345,22 +345,37 @@ class Advect:
             self.ctx.set_level_set_count(len(self.levelSets))
             for i, d in enumerate(self.levelSets):
                 self.ctx.upload(i, d)
-        if desc is not None:
-            self.ctx.set_velocity(desc)
-        else:
-            self.ctx.set_velocity_callback(self.velocities)
+        if self.velocities is not None:
+            desc = self.velocities.descriptor()
+            if desc is not None:
+                self.ctx.set_velocity(desc)
+            else:
+                self.ctx.set_velocity_callback(self.velocities)
         self.ctx.set_velocity_update_callback(getattr(self, "velocityUpdateCallback", None))
 
-    def apply(self):
-        """Advect::apply, lsAdvect.hpp:1017-1043; results written back."""
-        self._sync_to_device()
-        self.result = self.ctx.advect(self.params)
-        for i, d in enumerate(self.levelSets):
+    def _write_back(self, which):
+        for i in which:
+            d = self.levelSets[i]
             nd = self.ctx.download_domain(i, d.grid)
             d.idx, d.values, d.run_start, d.run_sign, d.width = (
                 nd.idx, nd.values, nd.run_start, nd.run_sign, nd.width)
         self._resident = ([id(d) for d in self.levelSets],
                           [self._fingerprint(d) for d in self.levelSets])
+
+    def prepareLS(self):
+        """Advect::prepareLS, lsAdvect.hpp:972-1015: the top level set expanded
+        to the width the spatial scheme reads, written back."""
+        if not self.levelSets:
+            raise RuntimeError("No level sets passed to Advect.")
+        self._sync_to_device(need_velocity=False)
+        self.ctx.prepare_ls(self.params.spatial_scheme)
+        self._write_back([len(self.levelSets) - 1])
+
+    def apply(self):
+        """Advect::apply, lsAdvect.hpp:1017-1043; results written back."""
+        self._sync_to_device()
+        self.result = self.ctx.advect(self.params)
+        self._write_back(range(len(self.levelSets)))
         return self.result
 
 

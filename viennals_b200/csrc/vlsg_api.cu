@@ -460,6 +460,16 @@ int vlsg_finalize_stencil_llf(vlsg_context *ctx) {
   });
 }
 
+int vlsg_prepare_ls(vlsg_context *ctx, int32_t spatial_scheme) {
+  if (!ctx) return fail(ctx, VLSG_ERR_ARGUMENT, "bad argument");
+  if (ctx->staged.empty()) return fail(ctx, VLSG_ERR_STATE, "No level sets passed to Advect.");
+  return guarded(ctx, [&] {
+    ensureBuilt(ctx);
+    ctx->eng->prepareLS(spatial_scheme);
+    return VLSG_OK;
+  });
+}
+
 int vlsg_set_velocity_functor(vlsg_context *ctx, const vlsg_velocity_desc *v) {
   if (!ctx || !v) return fail(ctx, VLSG_ERR_ARGUMENT, "bad argument");
   if (v->n_materials < 1 || v->n_materials > VLSG_MAX_MATERIALS)

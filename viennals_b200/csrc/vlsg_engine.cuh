@@ -1562,6 +1562,14 @@ public:
   }
   void prepareStencilLLF(const std::vector<bool> &isDepo) override { prepareStencil(isDepo); }
   void finalizeStencilLLF() override { finalizeStencil(); }
+  // Advect::prepareLS (lsAdvect.hpp:972-1015): Expand to the scheme's width
+  void prepareLS(int s) override {
+    const int w = schemeWidth(s);
+    if (w < 0) throw CudaError("Advect: Discretization scheme not found.", VLSG_ERR_ARGUMENT);
+    ++generation; // the exchange format is rebuilt on the next download
+    expand(L - 1, w);
+    syncErr("prepareLS");
+  }
 
   uint64_t insideCells(int b) override {
     VLSG_CUDA(cudaMemsetAsync(small + 15, 0, sizeof(unsigned long long), stream));

@@ -140,6 +140,7 @@ public:
   // PrepareStencilLocalLaxFriedrichs / FinalizeStencilLocalLaxFriedrichs
   virtual void prepareStencilLLF(const std::vector<bool> &isDepo) = 0;
   virtual void finalizeStencilLLF() = 0;
+  virtual void prepareLS(int spatialScheme) = 0;
   virtual int64_t surfaceNodes(int b, double **nodes, uint64_t **keys) = 0;
 };
 
