@@ -1567,6 +1567,7 @@ public:
     const int w = schemeWidth(s);
     if (w < 0) throw CudaError("Advect: Discretization scheme not found.", VLSG_ERR_ARGUMENT);
     ++generation; // the exchange format is rebuilt on the next download
+    saveTopAt = 0;
     expand(L - 1, w);
     syncErr("prepareLS");
   }
