@@ -219,6 +219,8 @@ public:
   }
   void setSaveAdvectionVelocities(bool b) { params.save_advection_velocities = b; }
   void setSpatialScheme(SpatialSchemeEnum s) { params.spatial_scheme = (int32_t)s; }
+  // the deprecated name of setSpatialScheme (lsAdvect.hpp:940-946)
+  void setIntegrationScheme(SpatialSchemeEnum s) { setSpatialScheme(s); }
   void setTemporalScheme(TemporalSchemeEnum s) { params.temporal_scheme = (int32_t)s; }
   void setDissipationAlpha(const double &a) { params.dissipation_alpha = a; }
   void setCheckDissipation(bool b) { params.check_dissipation = b; }
