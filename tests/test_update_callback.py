@@ -96,3 +96,31 @@ def test_gpu_update_callback_failure():
     with pytest.raises(RuntimeError, match="callback"):
         run_gpu_upd(g, ls, Bad(), params(S.ENGQUIST_OSHER_1ST_ORDER, TS.RUNGE_KUTTA_2ND_ORDER,
                                          0.0, single_step=1))
+
+
+@pytest.mark.gpu
+def test_python_front_apply_with_update_callback():
+    # the same run through viennals_b200.advect.Advect (the reference's Python
+    # binding names): setters, the update callback, apply() and the written-back
+    # Domain
+    from oracle import oracle as O
+    from viennals_b200.advect import Advect
+
+    g, ls = sphere_case(4.0, 0.25)
+    p = params(S.WENO_5TH_ORDER, TS.RUNGE_KUTTA_3RD_ORDER, 0.3)
+    vo, vg = Stateful(), Stateful()
+    ols = [O.OracleLS(g, d) for d in ls]
+    ores = O.advect(ols, p, vo, update=vo.update)
+    a = Advect(ls[0], vg)
+    a.setSpatialScheme(S.WENO_5TH_ORDER)
+    a.setTemporalScheme(TS.RUNGE_KUTTA_3RD_ORDER)
+    a.setAdvectionTime(0.3)
+    a.setVelocityUpdateCallback(vg.update)
+    a.apply()
+    assert vg.seen == vo.seen
+    assert a.getNumberOfTimeSteps() == ores.number_of_time_steps
+    assert a.getAdvectedTime() == ores.advected_time
+    compare(ols, a.ctx)
+    oi, ov = ols[0].points(0)
+    assert np.array_equal(ls[0].idx, oi)
+    assert np.array_equal(np.asarray(ls[0].values).view(np.int64), ov.view(np.int64))
