@@ -422,7 +422,7 @@ def main():
     cfg = {"workload": f"perturbed sphere R={args.radius} gridDelta={args.grid_delta} "
                        f"(seed {args.seed}), WENO5+RK3, CFL 0.4, v=1+0.3 n_z",
            "precision": args.precision, "step": "one RK3 time step (3 FE stages + 2 combines)",
-           "l2": "inputs larger than L2 (band ~10M points)", "parallelism": f"replicas x{world}"}
+           "l2": "inputs larger than L2 (band ~17M points, ~1.3 GB of values per buffer at R 40)", "parallelism": f"replicas x{world}"}
 
     if args.impl == "reference":
         if rank != 0:
