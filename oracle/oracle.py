@@ -49,6 +49,8 @@ def lib():
         L.vlso_ls_get.restype = i64
         L.vlso_ls_get.argtypes = [vp, i32, P(ctypes.c_int32), P(dbl)]
         L.vlso_ls_width.argtypes = [vp]
+        L.vlso_void_markers.restype = i64
+        L.vlso_void_markers.argtypes = [vp, P(ctypes.c_uint8)]
         L.vlso_ls_set_width.argtypes = [vp, i32]
         L.vlso_ls_far_queries.restype = i64
         L.vlso_ls_far_queries.argtypes = [vp]
@@ -144,6 +146,15 @@ class OracleLS:
         _check(lib().vlso_ls_values_at(self.h, len(idx), _ptr(idx, ctypes.c_int32),
                                        _ptr(out, ctypes.c_double)))
         return out
+
+    def void_markers(self):
+        """MarkVoidPoints (default options) markers of the defined points, in
+        the order of points(0)."""
+        L = lib()
+        n = L.vlso_void_markers(self.h, None)
+        out = np.zeros(n, np.uint8)
+        L.vlso_void_markers(self.h, _ptr(out, ctypes.c_uint8))
+        return out.astype(bool)
 
     @property
     def width(self):

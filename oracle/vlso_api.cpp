@@ -48,6 +48,19 @@ int64_t listPoints(vlso::LS<D> &ls, int which, int32_t *idx, double *vals) {
   return n;
 }
 
+// MarkVoidPoints markers (default options) of the defined points, in the
+// order of vlso_ls_get(which = 0).
+template <int D> int64_t listVoidMarkers(vlso::LS<D> &ls, uint8_t *out) {
+  const std::vector<uint8_t> m = vlso::voidMarkers<D>(ls);
+  int64_t n = 0;
+  for (size_t i = 0; i < ls.keys.size(); ++i) {
+    if (!vlso::isDefined(ls.vals[i])) continue;
+    if (out) out[n] = m[i];
+    ++n;
+  }
+  return n;
+}
+
 vlso::Params toParams(const vlsg_advect_params *p) {
   vlso::Params P;
   P.spatial = p->spatial_scheme;
@@ -137,6 +150,10 @@ int64_t vlso_ls_get(void *p, int which, int32_t *idx, double *vals) {
   auto *h = static_cast<Handle *>(p);
   return h->D == 2 ? listPoints<2>(*h->l2, which, idx, vals)
                    : listPoints<3>(*h->l3, which, idx, vals);
+}
+int64_t vlso_void_markers(void *p, uint8_t *out) {
+  auto *h = static_cast<Handle *>(p);
+  return h->D == 2 ? listVoidMarkers<2>(*h->l2, out) : listVoidMarkers<3>(*h->l3, out);
 }
 int vlso_ls_width(void *p) {
   auto *h = static_cast<Handle *>(p);

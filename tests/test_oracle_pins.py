@@ -8,6 +8,9 @@
   for t = 0.5 with STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER, Chamfer distance
   to the radius-1.5 sphere < 0.035.
 - LSTEST_ASSERT_VALID_LS (lsTestAsserts.hpp:11-23) after every advection.
+- MarkVoidPoints.cpp:57-108: a plane at y = 0.35 with two circular holes of
+  radius 5.1 centred at (+-8, -9.5) below it (2D, gridDelta 1, reflective x):
+  exactly the defined points with y < -2 are voids.
 """
 import json
 import os
@@ -105,3 +108,29 @@ def test_boolean_exact_zero_golden():
     for r, v in zip(und, got):
         assert abs(v) > 1e300
         assert (v < 0) == (r["value"] < 0), r
+
+
+def test_mark_void_points_known_answer():
+    # MarkVoidPoints.cpp:57-108 (default options; the geometry as a width-2
+    # band of its signed distance: material below the plane minus the holes)
+    g = Grid([-15, 15, -15, 15], [BC.REFLECTIVE_BOUNDARY, BC.INFINITE_BOUNDARY], 1.0, dim=2)
+
+    def sdf(x, y):
+        holes = [5.1 - np.hypot(x - cx, y + 9.5) for cx in (-8.0, 8.0)]
+        return np.maximum(np.maximum(y - 0.35, holes[0]), holes[1])
+
+    X, Y = np.meshgrid(np.arange(-15, 16), np.arange(-20, 6), indexing="xy")
+    X, Y = X.ravel(), Y.ravel()
+    v = sdf(X.astype(float), Y.astype(float))
+    keep = np.abs(v) <= 1.0
+    idx = np.stack([X[keep], Y[keep]], 1).astype(np.int32)  # y slowest, x fastest
+    vals = v[keep]
+    idx3 = np.concatenate([idx, np.zeros((len(idx), 1), np.int32)], 1)
+    rs, sg = make_runs(idx3, lambda x, y, z: np.where(sdf(np.asarray(x, float),
+                                                          np.asarray(y, float)) < 0, -1, 1),
+                       [-15, -22, 0], [15, 8, 0])
+    ls = O.OracleLS(g, Domain(g, idx, vals, rs[:, :2], sg, width=2))
+    pi, _ = ls.points(0)
+    marks = ls.void_markers()
+    assert len(marks) == len(pi) and marks.any() and not marks.all()
+    assert np.array_equal(marks, pi[:, 1] < -2)
