@@ -1,4 +1,4 @@
-"""Config 5's kind of workload: three stacked level sets over a periodic
+"""The stacked-deposition workload: three stacked level sets over a periodic
 hole array (substrate with holes of radius 0.5 and depth 2.0 at pitch 1.28,
 two slabs on the flat top; gridDelta 0.02), velocities 1.0 / 0.6 / 0.0 plus
 0.2 |n_z| per material, WENO5 + RK3, 20 time steps, FP32 against the FP64
@@ -30,7 +30,7 @@ def advect_steps(grid, doms, vel, p, precision, steps):
 
 
 @pytest.mark.gpu
-def test_config5_hole_stack_fp32_vs_fp64():
+def test_deposition_hole_stack_fp32_vs_fp64():
     from parity_cases import params
     from viennals_b200 import SpatialSchemeEnum as S, TemporalSchemeEnum as TS
     from viennals_b200.synth import hole_stack
@@ -39,7 +39,7 @@ def test_config5_hole_stack_fp32_vs_fp64():
     p = params(S.WENO_5TH_ORDER, TS.RUNGE_KUTTA_3RD_ORDER, 1.0, cfl=0.4, single_step=1)
     c64, t64, u64 = advect_steps(grid, doms, vel, p, 0, 20)
     c32, t32, u32 = advect_steps(grid, doms, vel, p, 1, 20)
-    print(f"\nconfig 5 (1024^2): points {[d.n_points for d in doms]}, time fp64 {t64:.6f} "
+    print(f"\ndeposition (1024^2): points {[d.n_points for d in doms]}, time fp64 {t64:.6f} "
           f"fp32 {t32:.6f}, point updates {u64} / {u32}")
     assert abs(t32 - t64) <= 1e-4 * t64
     for i in range(3):

@@ -1,11 +1,11 @@
-"""The BASELINE configurations other than the bench's, at their full sizes,
+"""The benchmark workloads other than the bench's, at their full sizes,
 as parity cases:
-  * config 2: square-trench etch, two materials, 128 x 128 x 64 cells at
+  * the square-trench etch: two materials, 128 x 128 x 64 cells at
     gridDelta 0.1, periodic in x/y, v = -1 on the substrate and 0 on the mask
     plus -0.3 n_z, local Lax-Friedrichs 2nd order, RK3, double: the FP64 GPU
     path against the oracle, bit for bit (defined points, values, signs,
     time steps);
-  * config 3 at a reduced radius (the full 10M-point band is the bench's
+  * the perturbed sphere at a reduced radius (the full band is the bench's
     workload, compared there FP32 against FP64 on the device): FP64 against
     the oracle.
 """
@@ -20,7 +20,7 @@ from viennals_b200.velocity import FunctorVelocity
 pytestmark = pytest.mark.gpu
 
 
-def config2(time=0.0):
+def trench_etch(time=0.0):
     g = Grid([-6.4, 6.4, -6.4, 6.4, -3.2, 3.2],
              [BC.PERIODIC_BOUNDARY, BC.PERIODIC_BOUNDARY, BC.INFINITE_BOUNDARY], 0.1)
     mask, top = trench_etch_level_sets(g, 0.5, 4.0)
@@ -43,18 +43,18 @@ def _parity(grid, lss, vel, p):
     return ctx
 
 
-def test_config2_trench_full_size_one_step():
-    g, lss, v, p = config2(0.0)
+def test_trench_etch_full_size_one_step():
+    g, lss, v, p = trench_etch(0.0)
     ctx = _parity(g, lss, v, p)
     n = [ctx.count(i) for i in range(2)]
     # measured at this size: 78k defined points after the step (mask and
-    # substrate bands of width 2 over 128 x 128 columns), not the 1.5M the
-    # configuration text estimates
+    # substrate bands of width 2 over 128 x 128 columns), not the 1.5M first
+    # estimated for this workload
     assert sum(n) > 50_000, n
-    print("config 2 defined points after one step:", n)
+    print("trench etch defined points after one step:", n)
 
 
-def test_config3_precision_form_reduced_radius_fp64():
+def test_perturbed_sphere_reduced_radius_fp64():
     import torch
     from viennals_b200.synth import perturbed_sphere, precision_velocity
 
@@ -63,7 +63,7 @@ def test_config3_precision_form_reduced_radius_fp64():
     _parity(grid, [dom], precision_velocity(), p)
 
 
-def test_config4_batching_form_matches_loop():
+def test_batching_form_matches_loop():
     """Batching form (FP32, LLF1, RK2): a batch of independent trench / hole
     domains advanced together equals advancing each alone, bit for bit."""
     import time

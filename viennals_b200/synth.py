@@ -247,7 +247,7 @@ def hole_stack(lateral_cells=4096, grid_delta=0.02, pitch=1.28, radius=0.5, dept
     set wraps the ones below.  Velocity per material 1.0 / 0.6 / 0.0 plus
     0.2 |n_z|.  The hole axes sit `shift` cells off the grid points: with
     axes on grid points, cells at exactly the radius carry values of order
-    1e-9 whose sign FP32 and FP64 Prune judge differently (it compares with
+    1e-9 whose sign FP32 and FP64 Prune decide differently (it compares with
     the precision's epsilon), which moves the lower bands by a cell.
     Returns (grid, [three Domains], velocity)."""
     import torch
