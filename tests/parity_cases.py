@@ -31,7 +31,7 @@ def params(spatial=0, temporal=0, time=0.0, cfl=0.4999, **kw):
     return p
 
 
-def config1():
+def sphere_growth_eo1():
     """Sphere R 5 at gridDelta 0.25, v = +1, EO1, FE, CFL 0.5, t = 2."""
     g, ls = sphere_case(5.0, 0.25)
     return g, ls, constant_scalar(1.0), params(0, 0, 2.0, cfl=0.5)

@@ -30,9 +30,9 @@ def test_cpp_front_matches_python_front(tmp_path):
     build_front(exe)
     out = subprocess.check_output([exe, "2.0"], text=True).split()
     vals = dict(zip(out[0::2], out[1::2]))
-    from parity_cases import config1, run_gpu
+    from parity_cases import sphere_growth_eo1, run_gpu
 
-    g, lss, v, p = config1()
+    g, lss, v, p = sphere_growth_eo1()
     ctx, res = run_gpu(g, lss, v, p)
     idx, val, w = ctx.download(0)
     s = float(np.sum(val * (1.0 + 1e-3 * (idx[:, 0] + 7 * idx[:, 1] + 13 * idx[:, 2]))))

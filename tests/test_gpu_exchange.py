@@ -5,7 +5,7 @@ upload -> download round trip through it."""
 import numpy as np
 import pytest
 
-from parity_cases import config1, egg_velocity, params, run_gpu, sphere_case, trench_case
+from parity_cases import sphere_growth_eo1, egg_velocity, params, run_gpu, sphere_case, trench_case
 from viennals_b200 import BoundaryConditionEnum as BC, Grid
 
 pytestmark = pytest.mark.gpu
@@ -22,7 +22,7 @@ def _check_runs(ctx, grid, slot=0):
 
 
 def test_runs_sphere_after_advect():
-    g, lss, v, p = config1()
+    g, lss, v, p = sphere_growth_eo1()
     ctx, _ = run_gpu(g, lss, v, p)
     dev = _check_runs(ctx, g)
     assert len(dev.run_sign) > 0 and len(dev.values) > 0

@@ -4,7 +4,7 @@ bit-exact; FP64 phi within 0 ulp, which implies the 1e-9*gridDelta bound)."""
 import numpy as np
 import pytest
 
-from parity_cases import (compare, config1, egg_velocity, params, run_gpu,
+from parity_cases import (compare, sphere_growth_eo1, egg_velocity, params, run_gpu,
                           run_oracle, sphere_case, trench_case)
 from viennals_b200 import BoundaryConditionEnum as BC, Grid
 from viennals_b200.geometry import make_sphere, sdf_levelset
@@ -40,8 +40,8 @@ def test_roundtrip_upload_download():
     assert np.array_equal(val, ref_v)
 
 
-def test_config1_sphere_eo1_fe():
-    g, lss, v, p = config1()
+def test_sphere_growth_eo1_fe():
+    g, lss, v, p = sphere_growth_eo1()
     _parity(g, lss, v, p)
 
 
