@@ -319,29 +319,42 @@ def precision_report(args, grid, dom, vel, p, stream):
     }
 
 
-def cpu_baseline(args, sample_radius, steps=1):
-    """The oracle (FP64 restatement, OpenMP on all host cores) on a bounded
-    sample: the same workload at a smaller radius."""
+def cpu_baseline(args, sample_radius, steps=1, threads=None):
+    """The oracle (FP64 restatement, OpenMP) on a bounded sample: the same
+    workload at a smaller radius, `steps` RK3 steps each timed on its own.
+    value = the median of the per-step point-updates/s."""
     from oracle import oracle as O
     from viennals_b200.synth import perturbed_sphere, precision_velocity
 
-    cores = os.cpu_count() or 1
+    cores = threads or os.cpu_count() or 1
     O.set_threads(cores)
     grid, dom = perturbed_sphere(radius=sample_radius, grid_delta=args.grid_delta,
                                  seed=args.seed, device="cuda" if _has_cuda() else "cpu")
     ls = O.OracleLS(grid, dom)
     p = params_for(args)
-    updates = 0
-    t0 = time.perf_counter()
+    runs = []
     for _ in range(steps):
+        t0 = time.perf_counter()
         r = O.advect([ls], p, precision_velocity())
-        updates += r.point_updates
-    dt = time.perf_counter() - t0
-    return {"value": updates / dt, "unit": UNIT, "cores": cores, "kind": "port",
+        runs.append(r.point_updates / (time.perf_counter() - t0))
+    runs_sorted = sorted(runs)
+    return {"value": runs_sorted[len(runs) // 2], "unit": UNIT, "cores": cores, "kind": "port",
+            "runs": runs, "band_points": int(dom.n_points), "radius": sample_radius,
             "sample": (f"perturbed sphere R={sample_radius} at gridDelta {args.grid_delta} "
-                       f"({dom.n_points} band points), WENO5+RK3 CFL 0.4, {steps} step(s), "
-                       f"FP64 oracle restatement (the reference cannot be built here)"),
-            "seconds": dt}
+                       f"({dom.n_points} band points), WENO5+RK3 CFL 0.4, v=1+0.3 n_z, "
+                       f"median of {steps} single-step run(s) on {cores} host thread(s), FP64 "
+                       f"oracle restatement (the reference cannot be built here)")}
+
+
+def cpu_baseline_line(args, steps):
+    """All host threads on the R `cpu_sample_radius` sample (median of
+    `steps` runs) and one thread on the smaller R `cpu_single_radius` sample."""
+    cb = cpu_baseline(args, args.cpu_sample_radius, steps=steps)
+    one = cpu_baseline(args, args.cpu_single_radius, steps=1, threads=1)
+    out = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    out["runs"] = cb["runs"]
+    out["single_thread"] = {k: one[k] for k in ("value", "unit", "cores", "sample")}
+    return out, cb
 
 
 def _has_cuda():
@@ -411,6 +424,10 @@ def main():
     ap.add_argument("--seed", type=int, default=1234)
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-sample-radius", type=float, default=8.0)
+    ap.add_argument("--cpu-single-radius", type=float, default=4.0,
+                    help="sample radius of the single-thread CPU figure")
+    ap.add_argument("--cpu-runs", type=int, default=5,
+                    help="single-step oracle runs behind the cpu_baseline median")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--err-steps", type=int, default=50,
                     help="RK3 steps of the FP32-vs-FP64 precision report (0: skip)")
@@ -427,12 +444,22 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        cb = cpu_baseline(args, args.cpu_sample_radius, steps=max(1, args.steps))
+        # K single-step runs of the oracle on all host threads (median), plus
+        # one single-thread run on a smaller sample
+        cbl, cb = cpu_baseline_line(args, max(1, args.steps))
+        ref_cfg = dict(cfg)
+        ref_cfg["workload"] = (f"perturbed sphere R={cb['radius']} gridDelta={args.grid_delta} "
+                               f"(seed {args.seed}, {cb['band_points']} band points), WENO5+RK3, "
+                               f"CFL 0.4, v=1+0.3 n_z")
+        ref_cfg["sample_of"] = cfg["workload"]
+        ref_cfg["precision"] = "fp64"
+        ref_cfg["l2"] = "CPU run (no GPU)"
+        ref_cfg["timing"] = f"median of {max(1, args.steps)} single-step runs"
         line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "impl": "reference",
                 "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f64", "data": "synthetic", "config": cfg,
-                "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "dtype": "f64", "data": "synthetic", "config": ref_cfg,
+                "cpu_baseline": cbl,
                 "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
@@ -459,8 +486,7 @@ def main():
             "precision_report": out.get("precision_report"),
             "kernels": out.get("kernels")}
     if not args.no_cpu_baseline:
-        cb = cpu_baseline(args, args.cpu_sample_radius)
-        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        line["cpu_baseline"], _ = cpu_baseline_line(args, args.cpu_runs)
     print(json.dumps(line))
 
 

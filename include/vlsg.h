@@ -246,15 +246,18 @@ int vlsg_get_values(vlsg_context *ctx, int32_t slot, int64_t n,
  * stages the query indices and the returned values in device buffers it
  * allocates and frees on every call; this entry point stages them instead in
  * one static device array of the library, sized for VLSG_NOALLOC_MAX_QUERIES
- * queries (1.25 MiB, held on every GPU that loads the library until the
- * process exits).
+ * queries (1.25 MiB per GPU, held until the process exits).
  *   - n > VLSG_NOALLOC_MAX_QUERIES is rejected with VLSG_ERR_CAPACITY.
  *   - The level sets must already be on the device (after vlsg_advect,
  *     vlsg_count_points, vlsg_download_levelset or vlsg_get_values), because
  *     moving them there allocates; otherwise VLSG_ERR_STATE.
- *   - The first call on a device looks up the array's device address (once
- *     per device, with the context's device current); make that first call
- *     before any stream capture on that device.
+ *   - The array is taken at set-up: the first time a context on a device
+ *     moves its level sets there, the library looks up the array's device
+ *     address with that device current (once per device).  Under lazy module
+ *     loading (the CUDA default) that lookup is what places the array in
+ *     device memory, so it happens while the set-up allocates anyway, not in
+ *     a later no-allocation call.  Do that set-up before any stream capture
+ *     on the device.
  *   - All calls share the array.  Calls that overlap on the GPU (contexts on
  *     the same device driven from several host threads at once) race on it.
  *     Each call writes every byte it reads, so nothing needs clearing between

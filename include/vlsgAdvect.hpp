@@ -6,10 +6,8 @@
 //
 // `vlsg::LevelSet` holds what crosses the C ABI for one level set: the grid,
 // the defined points with their values (grid units) and the undefined runs,
-// all in HRLE order.  With ViennaLS available, define VLSG_WITH_VIENNALS
-// before including this header to get conversions from and to
-// viennals::Domain<T,3> (they iterate the HRLE domain the way
-// lsReduce.hpp:281-296 does).
+// all in HRLE order (what a viennahrle::ConstSparseIterator over a
+// viennals::Domain<T,3> visits: defined points and undefined runs).
 #pragma once
 
 #include <array>

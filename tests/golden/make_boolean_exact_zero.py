@@ -3,16 +3,19 @@
 Reads tests/BooleanOperationExactZero/result.hpp of ViennaLS 5.8.3 (the only
 golden fixture of the reference) and writes boolean_exact_zero.json: the HRLE
 run list (start index, value) of Union(Plane, Box) after the boolean
-operation's two Prune passes.  Run once in a container that has the
-reference checked out; the JSON is committed.
+operation's two Prune passes.  Run once where the reference is checked
+out, with its root directory as the only argument; the JSON is committed.
+
+    python make_boolean_exact_zero.py <path of the ViennaLS checkout>
 """
 import json
 import os
 import re
 import sys
 
-SRC = os.path.join(sys.argv[1] if len(sys.argv) > 1 else "/root/reference",
-                   "tests", "BooleanOperationExactZero", "result.hpp")
+if len(sys.argv) != 2:
+    sys.exit("usage: make_boolean_exact_zero.py <path of the ViennaLS checkout>")
+SRC = os.path.join(sys.argv[1], "tests", "BooleanOperationExactZero", "result.hpp")
 text = open(SRC).read()
 idx = re.findall(r"VectorType<double, 2>\{(-?\d+), (-?\d+)\}", text)
 vals = [v.strip() for v in text.split("resultValues[] = {")[1].split("}")[0].split(",") if v.strip()]

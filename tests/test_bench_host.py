@@ -49,7 +49,8 @@ def test_reference_arm_line():
     for k in ("RANK", "WORLD_SIZE", "LOCAL_RANK"):
         env.pop(k, None)
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
-                        "--steps", "1", "--warmup", "0", "--cpu-sample-radius", "2.0"],
+                        "--steps", "3", "--warmup", "0", "--cpu-sample-radius", "2.0",
+                        "--cpu-single-radius", "1.5"],
                        env=env, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     line = json.loads(r.stdout.strip().splitlines()[-1])
@@ -59,3 +60,10 @@ def test_reference_arm_line():
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"] == {"value": line["value"], "unit": bench.UNIT,
                            "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    # the labels name what ran: the sample's radius and band, FP64, a median
+    cfg, cb = line["config"], line["cpu_baseline"]
+    assert "R=2.0" in cfg["workload"] and "band points" in cfg["workload"]
+    assert "R=40.0" in cfg["sample_of"] and cfg["precision"] == "fp64"
+    assert line["dtype"] == "f64" and "median of 3" in cfg["timing"]
+    assert len(cb["runs"]) == 3 and cb["value"] == sorted(cb["runs"])[1]
+    assert cb["single_thread"]["cores"] == 1 and cb["single_thread"]["value"] > 0

@@ -23,6 +23,13 @@ def _query(ctx, fn, idx):
     return rc, out
 
 
+def _free_bytes():
+    import torch
+
+    torch.cuda.synchronize()
+    return torch.cuda.mem_get_info(0)[0]
+
+
 def _queries(ctx, n, seed):
     """Half defined points of the band, half random indices around it and far
     outside it (undefined regions of both signs, outside the brick box)."""
@@ -54,8 +61,11 @@ def test_noalloc_matches_get_values_twice(precision):
         q = _queries(ctx, n, seed)
         rc_ref, ref = _query(ctx, L.vlsg_get_values, q)
         assert rc_ref == 0, L.vlsg_last_error(ctx.h)
+        free_before = _free_bytes()
         rc, got = _query(ctx, L.vlsg_get_values_noalloc, q)
         assert rc == 0, L.vlsg_last_error(ctx.h)
+        # the staging array was placed at set-up: the call takes no memory
+        assert _free_bytes() == free_before
         assert np.array_equal(got, ref)
         assert np.array_equal(np.signbit(got), np.signbit(ref))
         assert np.isfinite(got).all()

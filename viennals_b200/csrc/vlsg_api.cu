@@ -178,8 +178,17 @@ void ensureBuilt(vlsg_context *ctx) {
   if (ctx->staged.empty()) throw CudaError("no level set uploaded", VLSG_ERR_STATE);
   if (!ctx->dirty) return;
   const int margin = 4;
-  if (!ctx->eng)
+  if (!ctx->eng) {
+    // Set-up of vlsg_get_values_noalloc on this device: with lazy module
+    // loading (the CUDA default) the static staging array is only placed in
+    // device memory when this file's module loads, which the address lookup
+    // forces.  Doing it here, while the context sets up and may allocate,
+    // keeps the later no-allocation calls from loading the module.
+    unsigned char *scratch = nullptr;
+    const int rc = noallocScratch(ctx, ctx->device, &scratch);
+    if (rc != VLSG_OK) throw CudaError(ctx->err, rc);
     ctx->eng.reset(ctx->precision == VLSG_FP64 ? makeEngineF64() : makeEngineF32());
+  }
   ctx->eng->stream = ctx->stream;
   ctx->eng->build(ctx->grid, ctx->staged, margin);
   ctx->dirty = false;

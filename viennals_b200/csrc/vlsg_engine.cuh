@@ -1549,8 +1549,11 @@ public:
   void queryStaged(int b, int64_t n, const int32_t *idx, double *out, int32_t *di,
                    double *dv) override {
     VLSG_CUDA(cudaMemcpyAsync(di, idx, n * 3 * sizeof(int32_t), cudaMemcpyHostToDevice, stream));
-    kQueryValues<T><<<grid1(n), 256, 0, stream>>>(g, mapView(), view(b), (int)n, di, dv);
-    checkLaunch();
+    {
+      Scope sc(this, "query");
+      kQueryValues<T><<<grid1(n), 256, 0, stream>>>(g, mapView(), view(b), (int)n, di, dv);
+      checkLaunch();
+    }
     VLSG_CUDA(cudaMemcpyAsync(out, dv, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
     VLSG_CUDA(cudaStreamSynchronize(stream));
   }
