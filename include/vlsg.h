@@ -99,6 +99,11 @@ typedef struct vlsg_advect_params {
                                       setMaxDissipation (lsStencilLocalLax
                                       FriedrichsScalar.hpp:215); <= 0 means
                                       no limit (the reference's default) */
+  int32_t track_point_data;        /* carry the top level set's point data
+                                      through the advection (the source ids
+                                      of translateFromMultiData); read it with
+                                      vlsg_download_point_data.  Implied by
+                                      save_advection_velocities. */
 } vlsg_advect_params;
 
 /* Getters of viennals::Advect (lsAdvect.hpp:920-932) plus work counters. */
@@ -229,6 +234,29 @@ int vlsg_download_levelset(vlsg_context *ctx, int32_t slot, int64_t capacity,
 int vlsg_download_runs(vlsg_context *ctx, int32_t slot, int64_t capacity,
                        int32_t *run_start, int8_t *run_sign, int64_t *n_runs);
 
+/* Point data of the top level set after vlsg_advect with track_point_data
+ * or save_advection_velocities (replaces reading Domain::getPointData()
+ * after Advect::apply).  Per defined point, in the order of
+ * vlsg_download_levelset:
+ *   source[i]      the index (in the download order of the top level set as
+ *                  it was when that vlsg_advect started) of the point whose
+ *                  data point i now carries -- the source ids the reference's
+ *                  Expand, Reduce, Prune, BooleanOperation and rebuildLS pass
+ *                  to translateFromMultiData (lsExpand.hpp:110-150,
+ *                  lsAdvect.hpp:318-410, lsBooleanOperation.hpp:104-114);
+ *                  -1 where the reference records none;
+ *   velocity[i]    "AdvectionVelocities": the rate of the last value update
+ *                  (lsAdvect.hpp:764-767, 794), with save_advection_velocities;
+ *   dissipation[i] "Dissipation" (lsAdvect.hpp:795); 0 without it.
+ * *has_point_data = 0 (and nothing else written) when the top level set
+ * carries none: no tracking was asked for, or update_point_data was 0, in
+ * which case rebuildLS drops all point data (lsAdvect.hpp:418-423).
+ * Only the top level set (slot = count - 1); VLSG_ERR_CAPACITY when capacity
+ * is below the number of points (vlsg_count_points). */
+int vlsg_download_point_data(vlsg_context *ctx, int32_t slot, int64_t capacity,
+                             int64_t *source, double *velocity, double *dissipation,
+                             int32_t *has_point_data);
+
 /* Values of arbitrary grid points of a level set (indices are mapped through
  * the boundary conditions): the defined value, or +-DBL_MAX carrying the sign
  * of the undefined region -- what viennahrle's iterators return for them
@@ -296,6 +324,33 @@ int vlsg_compare(vlsg_context *a, int32_t slot_a, vlsg_context *b, int32_t slot_
 
 /* setVelocityUpdateCallback (lsAdvect.hpp:966-969); NULL clears it. */
 int vlsg_set_velocity_update_callback(vlsg_context *ctx, vlsg_update_cb cb, void *user);
+
+/* Spatial sharding of one level-set domain over several contexts (one per
+ * GPU), each holding a slab of the band plus ghost layers.  No counterpart in
+ * Advect: the reference's only decomposition is its OpenMP segments, whose
+ * per-thread time-step minima and alpha maxima it reduces in critical
+ * sections (lsAdvect.hpp:595-606, :186-191); these two calls are that
+ * reduction across contexts.
+ *
+ * vlsg_set_owned_region: only active points with index[axis] in [lo, hi)
+ * contribute to the time step, the Lax-Friedrichs alphas and the point-update
+ * count; the other (ghost) points are advanced all the same.  axis = -1 (the
+ * default) owns everything; only axis 2 (the slowest index of the HRLE order)
+ * is supported, and not with STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER.
+ *
+ * vlsg_set_reduction_callback: called from vlsg_advect with this context's
+ * partial values before they are used -- the smallest per-point time step of
+ * a rate pass (n = 1, op VLSG_REDUCE_MIN; DBL_MAX when it has none), the
+ * alphas of the Lax-Friedrichs schemes (n = 3, VLSG_REDUCE_MAX) and the
+ * "moved down" flag of a stage combination with lower layers (n = 1,
+ * VLSG_REDUCE_MAX).  The callback replaces values[] by the reduction over all
+ * shards (e.g. an all-reduce) and returns 0; every shard must call vlsg_advect
+ * with the same parameters so that the calls line up.  NULL clears it. */
+#define VLSG_REDUCE_MIN 0
+#define VLSG_REDUCE_MAX 1
+typedef int (*vlsg_reduce_cb)(void *user, double *values, int32_t n, int32_t op);
+int vlsg_set_owned_region(vlsg_context *ctx, int32_t axis, int64_t lo, int64_t hi);
+int vlsg_set_reduction_callback(vlsg_context *ctx, vlsg_reduce_cb cb, void *user);
 
 /* PrepareStencilLocalLaxFriedrichs (lsStencilLocalLaxFriedrichsScalar.hpp:
  * 423-477) on the context's level sets: is_depo[i] tells whether level set i

@@ -11,9 +11,11 @@
 #pragma once
 
 #include <array>
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <functional>
+#include <map>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -57,6 +59,19 @@ struct LevelSet {
   std::vector<int32_t> runStart; // 3 per undefined run
   std::vector<int8_t> runSign;
   int width = 2;
+  // Version stamp: Advect::apply writes its results back with a fresh stamp
+  // and keeps the device copy; a later apply on the same, unchanged objects
+  // skips the upload.  Code that changes a level set in place afterwards
+  // calls touch() (a new object, or one whose array sizes changed, is always
+  // uploaded).
+  uint64_t version = 0;
+  void touch() { version = 0; }
+  // Domain::getPointData(): scalar arrays per defined point, by label.  The
+  // top level set's arrays are carried through Advect::apply the way the
+  // reference's passes translate them (setSaveAdvectionVelocities adds
+  // "AdvectionVelocities" and "Dissipation"; setUpdatePointData(false)
+  // drops them all).
+  std::map<std::string, std::vector<double>> pointData;
   int64_t numberOfPoints() const { return (int64_t)values.size(); }
 };
 
@@ -174,6 +189,7 @@ template <class T> class Advect {
   vlsg_advect_params params{};
   vlsg_advect_result result{};
   vlsg_context *ctx = nullptr;
+  uint64_t skippedUploads = 0;
   int device = 0;
 
   static void logError(const std::string &m) { std::fprintf(stderr, "[vlsg] %s\n", m.c_str()); }
@@ -184,6 +200,10 @@ template <class T> class Advect {
   }
 
 public:
+  // labels of the saved arrays (lsAdvect.hpp:833-834)
+  static constexpr const char *velocityLabel = "AdvectionVelocities";
+  static constexpr const char *dissipationLabel = "Dissipation";
+
   Advect() { vlsg_default_params(&params), result.current_time_step = -1.; }
   explicit Advect(std::shared_ptr<LevelSet> ls) : Advect() { levelSets.push_back(ls); }
   Advect(std::shared_ptr<LevelSet> ls, std::shared_ptr<VelocityFunctor> v) : Advect() {
@@ -245,13 +265,16 @@ public:
     if (levelSets.empty()) return logError("No level sets passed to Advect.");
     if (!uploadLevelSets()) return;
     if (!check(vlsg_prepare_ls(ctx, params.spatial_scheme))) return;
-    downloadLevelSet(levelSets.size() - 1);
+    if (downloadLevelSet(levelSets.size() - 1)) markResident();
   }
 
   void apply() {
     if (levelSets.empty()) return logError("No level sets passed to Advect. Not advecting.");
     if (!velocities && !field)
       return logError("No velocity field passed to Advect. Not advecting.");
+    const bool save = params.save_advection_velocities != 0;
+    const bool track = save || !levelSets.back()->pointData.empty();
+    params.track_point_data = track;
     if (!uploadLevelSets()) return;
     if (field) {
       if (!check(vlsg_set_velocity_callback(ctx, &VelocityField<T>::callback, field.get()))) return;
@@ -267,11 +290,54 @@ public:
     if (!check(vlsg_advect(ctx, &params, &result))) return;
     for (size_t i = 0; i < levelSets.size(); ++i)
       if (!downloadLevelSet(i)) return;
+    if (track && !translatePointData(save)) return;
+    markResident();
   }
 
+  // applies (and prepareLS calls) that found the device copy current
+  uint64_t getSkippedUploads() const { return skippedUploads; }
+
 private:
-  // the context (created on first use) holding the grid and all level sets
+  // What the device holds since the last write-back: the level-set objects,
+  // their stamps and array sizes (B2 of the drop-in contract: device state is
+  // reused only while the host objects are unchanged).
+  struct Resident {
+    const LevelSet *ls;
+    uint64_t version;
+    size_t points, runs;
+  };
+  std::vector<Resident> resident;
+  static uint64_t freshStamp() {
+    static std::atomic<uint64_t> next{1};
+    return next.fetch_add(1);
+  }
+  bool residentUnchanged() const {
+    if (!ctx || resident.size() != levelSets.size()) return false;
+    for (size_t i = 0; i < levelSets.size(); ++i) {
+      const LevelSet &ls = *levelSets[i];
+      const Resident &r = resident[i];
+      if (r.ls != &ls || ls.version == 0 || r.version != ls.version ||
+          r.points != ls.values.size() || r.runs != ls.runSign.size())
+        return false;
+    }
+    return true;
+  }
+  void markResident() {
+    resident.clear();
+    for (auto &p : levelSets) {
+      p->version = freshStamp();
+      resident.push_back({p.get(), p->version, p->values.size(), p->runSign.size()});
+    }
+  }
+
+  // the context (created on first use) holding the grid and all level sets;
+  // nothing crosses PCIe when the device copy is still current
   bool uploadLevelSets() {
+    if (residentUnchanged()) {
+      ++skippedUploads;
+      return true;
+    }
+    resident.clear();
     if (!ctx) {
       const int precision = sizeof(T) == 4 ? VLSG_FP32 : VLSG_FP64;
       if (!check(vlsg_create(&ctx, device, precision))) return false;
@@ -289,6 +355,36 @@ private:
     }
     return true;
   }
+  // The top level set's point data after an advection: every array gathered
+  // by the source ids (0 where there is none); the saved velocity arrays
+  // replace earlier ones.
+  bool translatePointData(bool save) {
+    LevelSet &ls = *levelSets.back();
+    const int64_t n = ls.numberOfPoints();
+    std::vector<int64_t> src(n);
+    std::vector<double> vel(n), diss(n);
+    int32_t has = 0;
+    if (!check(vlsg_download_point_data(ctx, (int32_t)levelSets.size() - 1, n, src.data(),
+                                        vel.data(), diss.data(), &has)))
+      return false;
+    std::map<std::string, std::vector<double>> out;
+    if (has) {
+      for (auto &kv : ls.pointData) {
+        if (save && (kv.first == velocityLabel || kv.first == dissipationLabel)) continue;
+        std::vector<double> a(n, 0.0);
+        for (int64_t i = 0; i < n; ++i)
+          if (src[i] >= 0 && src[i] < (int64_t)kv.second.size()) a[i] = kv.second[src[i]];
+        out[kv.first] = std::move(a);
+      }
+      if (save) {
+        out[velocityLabel] = std::move(vel);
+        out[dissipationLabel] = std::move(diss);
+      }
+    }
+    ls.pointData = std::move(out);
+    return true;
+  }
+
   // level set i written back: defined points and undefined runs in HRLE
   // order, both built on the device
   bool downloadLevelSet(size_t i) {

@@ -10,7 +10,8 @@ import subprocess
 
 import numpy as np
 
-from viennals_b200._abi import ALPHA_CALLBACK, UPDATE_CALLBACK, VELOCITY_CALLBACK, AdvectParams, AdvectResult, VelocityDesc
+from viennals_b200._abi import (ALPHA_CALLBACK, REDUCE_CALLBACK, UPDATE_CALLBACK, VELOCITY_CALLBACK,
+                                AdvectParams, AdvectResult, VelocityDesc)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libvlso.so")
@@ -49,6 +50,10 @@ def lib():
         L.vlso_ls_get.restype = i64
         L.vlso_ls_get.argtypes = [vp, i32, P(ctypes.c_int32), P(dbl)]
         L.vlso_ls_width.argtypes = [vp]
+        L.vlso_set_shard.argtypes = [i32, i64, i64, REDUCE_CALLBACK, vp]
+        L.vlso_set_shard.restype = None
+        L.vlso_point_data.restype = i64
+        L.vlso_point_data.argtypes = [vp, P(i64), P(dbl), P(dbl)]
         L.vlso_void_markers.restype = i64
         L.vlso_void_markers.argtypes = [vp, P(ctypes.c_uint8)]
         L.vlso_ls_set_width.argtypes = [vp, i32]
@@ -87,6 +92,28 @@ def _ptr(a, t):
 def _check(rc):
     if rc != 0:
         raise RuntimeError("oracle: " + lib().vlso_last_error().decode())
+
+
+_shard_cb = None
+
+
+def set_shard(axis=-1, lo=0, hi=0, reduce=None):
+    """Owned z-slab and cross-shard reduction of the following advections:
+    reduce(values (numpy array, changed in place), op) with op 0 = min,
+    1 = max."""
+    global _shard_cb
+    if reduce is None:
+        _shard_cb = REDUCE_CALLBACK()
+    else:
+        def cb(user, values, n, op):
+            try:
+                arr = np.ctypeslib.as_array(values, shape=(n,))
+                reduce(arr, int(op))
+                return 0
+            except Exception:  # noqa: BLE001 -- reported to the C side as a failure
+                return 1
+        _shard_cb = REDUCE_CALLBACK(cb)
+    lib().vlso_set_shard(int(axis), int(lo), int(hi), _shard_cb, None)
 
 
 def set_threads(n):
@@ -146,6 +173,20 @@ class OracleLS:
         _check(lib().vlso_ls_values_at(self.h, len(idx), _ptr(idx, ctypes.c_int32),
                                        _ptr(out, ctypes.c_double)))
         return out
+
+    def point_data(self):
+        """(source, velocity, dissipation) of the defined points in the order
+        of points(0), or None when the level set carries no point data."""
+        L = lib()
+        n = L.vlso_point_data(self.h, None, None, None)
+        if n < 0:
+            return None
+        src = np.zeros(n, np.int64)
+        vel = np.zeros(n)
+        diss = np.zeros(n)
+        L.vlso_point_data(self.h, _ptr(src, ctypes.c_int64), _ptr(vel, ctypes.c_double),
+                          _ptr(diss, ctypes.c_double))
+        return src, vel, diss
 
     def void_markers(self):
         """MarkVoidPoints (default options) markers of the defined points, in

@@ -12,6 +12,8 @@
 // taken over all points, i.e. the reference run with one thread.
 #pragma once
 
+#include <cfloat>
+
 #include "vlso_core.hpp"
 
 namespace vlso {
@@ -124,6 +126,9 @@ struct Params {
   bool ignoreVoids = false; // setIgnoreVoids, lsAdvect.hpp:899
   unsigned adaptiveSubdivisions = 20;
   bool checkDissipation = true;
+  bool saveAdvectionVelocities = false; // lsAdvect.hpp:916
+  bool updatePointData = true;          // lsAdvect.hpp:962
+  bool trackPointData = false;          // carry point data through apply
   uint32_t maxSteps = 10000000;
   // StencilLocalLaxFriedrichsScalar::setMaxDissipation (static, default max)
   double maxDissipation = std::numeric_limits<double>::max();
@@ -757,6 +762,24 @@ template <int D> struct Advector {
 
   LS<D> &top() { return lss.back(); }
 
+  // Sharding: only points with z in [ownLo, ownHi) count towards the time
+  // step, the alphas and the point updates; reduceCb combines the partial
+  // values over all shards (the contract of vlsg_set_owned_region and
+  // vlsg_set_reduction_callback).
+  bool ownZ = false;
+  int64_t ownLo = 0, ownHi = 0;
+  vlsg_reduce_cb reduceCb = nullptr;
+  void *reduceUser = nullptr;
+  bool owned(uint64_t key) const {
+    if (!ownZ) return true;
+    const int64_t z = coordOf<D>(key, D - 1);
+    return z >= ownLo && z < ownHi;
+  }
+  void reduceAcross(double *v, int n, int op) {
+    if (reduceCb && reduceCb(reduceUser, v, n, op) != 0)
+      throw std::runtime_error("the reduction callback failed");
+  }
+
   // findGlobalAlphas, lsAdvect.hpp:90-195
   void findGlobalAlphas(double *finalAlphas) {
     const LS<D> &t = top();
@@ -769,6 +792,7 @@ template <int D> struct Advector {
       const double value = t.vals[p];
       if (!isDefined(value) || std::abs(value) > Params::integrationCutoff) continue;
       const uint64_t key = t.keys[p];
+      if (!owned(key)) continue;
       auto &la = loc[omp_get_thread_num()];
       for (int lower = 0; lower < (int)lss.size(); ++lower) {
         if (lss[lower].at(key) <= value + Params::wrappingLayerEpsilon) {
@@ -796,6 +820,7 @@ template <int D> struct Advector {
     vel.check();
     for (auto &la : loc)
       for (int i = 0; i < D; ++i) finalAlphas[i] = stdMax(finalAlphas[i], la[i]);
+    reduceAcross(finalAlphas, D, VLSG_REDUCE_MAX);
   }
 
   // integrateTime, lsAdvect.hpp:435-612
@@ -841,8 +866,10 @@ template <int D> struct Advector {
         if (!(P.ignoreVoids && voids[activePos[a]])) {
           for (int lower = 0; lower < L; ++lower) {
             if (lss[lower].at(key) <= value + Params::wrappingLayerEpsilon) {
+              double ghostAlphas[4] = {0, 0, 0, 0};
               gd = evalScheme<D>(S, key, vel.cb ? ids[activePos[a]] : 0, lower,
-                                 sllf ? sllfLast[a].data() : alp[th].data());
+                                 sllf ? sllfLast[a].data()
+                                      : (owned(key) ? alp[th].data() : ghostAlphas));
               break;
             }
           }
@@ -882,12 +909,19 @@ template <int D> struct Advector {
         }
       }
       chainLen[a] = len;
-      if (maxStepTime < tmin[th]) tmin[th] = maxStepTime;
+      if (owned(key) && maxStepTime < tmin[th]) tmin[th] = maxStepTime;
     }
     vel.check();
     double tempMax = maxTimeStep;
     for (int i = 0; i < nt; ++i)
       if (tmin[i] < tempMax) tempMax = tmin[i];
+    if (reduceCb) {
+      double m = DBL_MAX;
+      for (int i = 0; i < nt; ++i)
+        if (tmin[i] < m) m = tmin[i];
+      reduceAcross(&m, 1, VLSG_REDUCE_MIN);
+      if (m < tempMax) tempMax = m;
+    }
     // reduceTimeStepHamiltonJacobi of the LF family (e.g. lsLaxFriedrichs.hpp:350-362)
     const int s = P.spatial;
     const bool lfFamily = !(s == VLSG_ENGQUIST_OSHER_1ST_ORDER ||
@@ -906,6 +940,7 @@ template <int D> struct Advector {
       } else {
         for (int th = 0; th < nt; ++th)
           for (int i = 0; i < D; ++i) fa[i] = stdMax(fa[i], alp[th][i]);
+        reduceAcross(fa, D, VLSG_REDUCE_MAX);
       }
       double timeStep = 0;
       for (int i = 0; i < D; ++i) timeStep += fa[i] / t.grid.delta;
@@ -965,16 +1000,30 @@ template <int D> struct Advector {
         rate = time * velocity;
       }
       value -= rate;
+      // setSaveAdvectionVelocities: the last leg's rate and the dissipation
+      // of the chain entry it ended on (lsAdvect.hpp:764-767)
+      if (P.saveAdvectionVelocities && !t.pd.empty()) {
+        t.pd[p].vel = rate;
+        t.pd[p].diss = it->dissipation;
+      }
       ++a;
     }
-    pointUpdates += a;
+    if (ownZ) {
+      int64_t ownedActive = 0;
+      for (const uint64_t k : activeKeys) ownedActive += owned(k) ? 1 : 0;
+      pointUpdates += ownedActive;
+    } else {
+      pointUpdates += a;
+    }
     ++stages;
     t.finalizeMap();
   }
 
   void rebuildLS() { // :250-256
-    if (P.spatial == VLSG_STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER) rebuild<D>(top(), 1.5, 3);
-    else rebuild<D>(top(), 1.0, 2);
+    if (P.spatial == VLSG_STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER)
+      rebuild<D>(top(), 1.5, 3, P.updatePointData);
+    else
+      rebuild<D>(top(), 1.0, 2, P.updatePointData);
   }
 
   void adjustLowerLayers() { // :802-813 (not with StencilLocalLaxFriedrichs)
@@ -1001,9 +1050,16 @@ template <int D> struct Advector {
       }
       if (a == POS || a == NEG) return a;
       return b;
+    }, true, [](double a, double b) { // defined results come from A (:221-226)
+      return a != POS && a != NEG && b != POS && b != NEG;
     });
     movedDown = md.load();
     rebuildLS();
+    if (lss.size() > 1) {
+      double m = movedDown ? 1.0 : 0.0;
+      reduceAcross(&m, 1, VLSG_REDUCE_MAX);
+      movedDown = m != 0.0;
+    }
     return movedDown;
   }
 
@@ -1085,6 +1141,17 @@ template <int D> struct Advector {
   }
   // apply, lsAdvect.hpp:1017-1043
   void apply(vlsg_advect_result &res) {
+    // point data of the top level set: every defined point carries its own
+    // index (HRLE order) into the data the caller holds
+    if (P.trackPointData || P.saveAdvectionVelocities) {
+      LS<D> &t = top();
+      t.pd.assign(t.keys.size(), PointData{});
+      int64_t r = 0;
+      for (size_t i = 0; i < t.keys.size(); ++i)
+        if (isDefined(t.vals[i])) t.pd[i].src = r++;
+    } else {
+      top().pd.clear();
+    }
     double advectedTime = 0.;
     unsigned steps = 0;
     if (P.advectionTime == 0.) {

@@ -61,6 +61,26 @@ template <int D> int64_t listVoidMarkers(vlso::LS<D> &ls, uint8_t *out) {
   return n;
 }
 
+// Point data of the defined points (vlso_ls_get order); -1 when the level
+// set carries none.
+template <int D>
+int64_t listPointData(vlso::LS<D> &ls, int64_t *src, double *vel, double *diss) {
+  if (ls.pd.empty()) return -1;
+  int64_t n = 0;
+  for (size_t i = 0; i < ls.keys.size(); ++i) {
+    if (!vlso::isDefined(ls.vals[i])) continue;
+    if (src) src[n] = ls.pd[i].src, vel[n] = ls.pd[i].vel, diss[n] = ls.pd[i].diss;
+    ++n;
+  }
+  return n;
+}
+
+// Sharding settings of the next advections (vlso_set_shard).
+bool g_ownZ = false;
+int64_t g_ownLo = 0, g_ownHi = 0;
+vlsg_reduce_cb g_reduceCb = nullptr;
+void *g_reduceUser = nullptr;
+
 vlso::Params toParams(const vlsg_advect_params *p) {
   vlso::Params P;
   P.spatial = p->spatial_scheme;
@@ -74,6 +94,9 @@ vlso::Params toParams(const vlsg_advect_params *p) {
   P.ignoreVoids = p->ignore_voids != 0;
   P.adaptiveSubdivisions = p->adaptive_subdivisions < 1 ? 1 : p->adaptive_subdivisions;
   P.checkDissipation = p->check_dissipation != 0;
+  P.saveAdvectionVelocities = p->save_advection_velocities != 0;
+  P.updatePointData = p->update_point_data != 0;
+  P.trackPointData = p->track_point_data != 0;
   P.maxSteps = p->max_steps ? p->max_steps : 10000000u;
   if (p->max_dissipation > 0) P.maxDissipation = p->max_dissipation;
   return P;
@@ -89,6 +112,11 @@ int advectD(Handle **hs, int n, const vlsg_advect_params *p,
   vlso::Advector<D> adv(lss, toParams(p), v);
   adv.updateCb = upd;
   adv.updateUser = updUser;
+  adv.ownZ = g_ownZ;
+  adv.ownLo = g_ownLo;
+  adv.ownHi = g_ownHi;
+  adv.reduceCb = g_reduceCb;
+  adv.reduceUser = g_reduceUser;
   adv.apply(*r);
   for (int i = 0; i < n; ++i) get<D>(hs[i]) = lss[i];
   return 0;
@@ -150,6 +178,22 @@ int64_t vlso_ls_get(void *p, int which, int32_t *idx, double *vals) {
   auto *h = static_cast<Handle *>(p);
   return h->D == 2 ? listPoints<2>(*h->l2, which, idx, vals)
                    : listPoints<3>(*h->l3, which, idx, vals);
+}
+// Owned z-slab (axis 2; axis -1 owns everything) and reduction callback of
+// the following advections, as vlsg_set_owned_region /
+// vlsg_set_reduction_callback set them for a context.
+void vlso_set_shard(int axis, int64_t lo, int64_t hi, vlsg_reduce_cb cb, void *user) {
+  g_ownZ = axis == 2;
+  g_ownLo = lo;
+  g_ownHi = hi;
+  g_reduceCb = cb;
+  g_reduceUser = user;
+}
+
+int64_t vlso_point_data(void *p, int64_t *src, double *vel, double *diss) {
+  auto *h = static_cast<Handle *>(p);
+  return h->D == 2 ? listPointData<2>(*h->l2, src, vel, diss)
+                   : listPointData<3>(*h->l3, src, vel, diss);
 }
 int64_t vlso_void_markers(void *p, uint8_t *out) {
   auto *h = static_cast<Handle *>(p);

@@ -169,6 +169,18 @@ struct HashIndex {
   }
 };
 
+// Point data of one defined point while it is carried through the passes
+// (translateFromMultiData with the source point ids the reference's Expand,
+// Reduce, Prune, BooleanOperation and rebuildLS record: lsExpand.hpp:110-150,
+// lsReduce.hpp:108-112, lsPrune.hpp:164-168, lsBooleanOperation.hpp:104-114,
+// lsAdvect.hpp:318-410): the index of the point, at the start of the
+// advection, whose data it carries (-1: none), and the AdvectionVelocities /
+// Dissipation values of the last value update (lsAdvect.hpp:780-796).
+struct PointData {
+  int64_t src = -1;
+  double vel = 0., diss = 0.;
+};
+
 template <int D> struct LS {
   Grid<D> grid;
   std::vector<uint64_t> keys; // sorted, HRLE order
@@ -178,11 +190,13 @@ template <int D> struct LS {
   HashIndex index;
   int64_t nDefined = 0;
   mutable std::atomic<int64_t> farQueries{0};
+  // point data per map entry (empty: not tracked)
+  std::vector<PointData> pd;
 
   LS() = default;
   LS(const LS &o)
       : grid(o.grid), keys(o.keys), vals(o.vals), width(o.width), emptyValue(o.emptyValue),
-        nDefined(o.nDefined) {
+        nDefined(o.nDefined), pd(o.pd) {
     index.build(keys);
   }
   LS &operator=(const LS &o) {
@@ -192,6 +206,7 @@ template <int D> struct LS {
     width = o.width;
     emptyValue = o.emptyValue;
     nDefined = o.nDefined;
+    pd = o.pd;
     index.build(keys);
     return *this;
   }
@@ -278,12 +293,19 @@ struct RunSigns {
 // Collect (defined points) + (star shell) into a fresh sorted map.  `shellVal`
 // gives the value of a shell point, given the key of the shell point and the
 // index (into defKeys) of the defined point it was reached from.
+// With `defPd` (point data of the defined points) the map carries point data.
 template <int D, class ShellFn>
 void assembleMap(LS<D> &out, const std::vector<uint64_t> &defKeys,
-                 const std::vector<double> &defVals, ShellFn shellVal) {
+                 const std::vector<double> &defVals, ShellFn shellVal,
+                 const std::vector<PointData> *defPd = nullptr) {
+  struct Entry {
+    uint64_t key;
+    double val;
+    int64_t def; // index into defKeys, -1 for a shell point
+  };
   const int64_t n = defKeys.size();
   const int nt = omp_get_max_threads();
-  std::vector<std::vector<std::pair<uint64_t, double>>> shell(nt);
+  std::vector<std::vector<Entry>> shell(nt);
 #pragma omp parallel
   {
     auto &loc = shell[omp_get_thread_num()];
@@ -293,29 +315,39 @@ void assembleMap(LS<D> &out, const std::vector<uint64_t> &defKeys,
         for (int s = -1; s <= 1; s += 2) {
           const uint64_t nk = shiftKey<D>(out.grid, defKeys[i], d, s);
           if (std::binary_search(defKeys.begin(), defKeys.end(), nk)) continue;
-          loc.emplace_back(nk, shellVal(nk, i));
+          loc.push_back({nk, shellVal(nk, i), -1});
         }
     }
   }
-  std::vector<std::pair<uint64_t, double>> all;
+  std::vector<Entry> all;
   all.reserve(n + n);
-  for (int64_t i = 0; i < n; ++i) all.emplace_back(defKeys[i], defVals[i]);
+  for (int64_t i = 0; i < n; ++i) all.push_back({defKeys[i], defVals[i], i});
   for (auto &v : shell) all.insert(all.end(), v.begin(), v.end());
-  std::sort(all.begin(), all.end(),
-            [](const auto &a, const auto &b) { return a.first < b.first; });
+  std::sort(all.begin(), all.end(), [](const Entry &a, const Entry &b) { return a.key < b.key; });
   out.keys.clear();
   out.vals.clear();
+  out.pd.clear();
   out.keys.reserve(all.size());
   out.vals.reserve(all.size());
+  std::vector<int64_t> from;
+  from.reserve(all.size());
   for (size_t i = 0; i < all.size(); ++i) {
-    if (i > 0 && all[i].first == all[i - 1].first) {
+    if (i > 0 && all[i].key == all[i - 1].key) {
       // a defined point always wins over a shell copy of itself
-      if (isDefined(all[i].second) && !isDefined(out.vals.back()))
-        out.vals.back() = all[i].second;
+      if (isDefined(all[i].val) && !isDefined(out.vals.back())) {
+        out.vals.back() = all[i].val;
+        from.back() = all[i].def;
+      }
       continue;
     }
-    out.keys.push_back(all[i].first);
-    out.vals.push_back(all[i].second);
+    out.keys.push_back(all[i].key);
+    out.vals.push_back(all[i].val);
+    from.push_back(all[i].def);
+  }
+  if (defPd) {
+    out.pd.assign(out.keys.size(), PointData{});
+    for (size_t i = 0; i < out.keys.size(); ++i)
+      if (from[i] >= 0) out.pd[i] = (*defPd)[from[i]];
   }
   out.finalizeMap();
 }
@@ -360,9 +392,12 @@ void fromPoints(LS<D> &ls, const Grid<D> &g, int64_t n, const int32_t *idx,
 // ConstSparseStarIterator<.,1> numbers them (lsWENO.hpp:252-256).  Every rule
 // used with it maps an all-undefined neighbourhood to the centre's own
 // undefined value, which makes points outside the map invariant.
+// `rule(center, nb, src)` also names the point whose data the result
+// carries: src = -1 the centre, 0..2D-1 neighbour src, -2 none.
 template <int D, class Rule> void starPass(LS<D> &ls, Rule rule) {
   const int64_t n = ls.keys.size();
   std::vector<double> out(n);
+  std::vector<int> srcOf(n, -1);
 #pragma omp parallel for schedule(static)
   for (int64_t i = 0; i < n; ++i) {
     double nb[2 * D];
@@ -377,13 +412,29 @@ template <int D, class Rule> void starPass(LS<D> &ls, Rule rule) {
         nb[s * D + d] = v;
       }
     }
-    out[i] = rule(ls.vals[i], nb);
+    out[i] = rule(ls.vals[i], nb, srcOf[i]);
   }
   std::vector<uint64_t> dk;
   std::vector<double> dv;
   std::vector<int64_t> from;
   for (int64_t i = 0; i < n; ++i)
     if (isDefined(out[i])) dk.push_back(ls.keys[i]), dv.push_back(out[i]), from.push_back(i);
+  std::vector<PointData> dpd;
+  const bool track = !ls.pd.empty();
+  if (track) {
+    dpd.resize(dk.size());
+    for (size_t j = 0; j < dk.size(); ++j) {
+      const int64_t i = from[j];
+      const int src = srcOf[i];
+      if (src == -1) {
+        dpd[j] = ls.pd[i];
+      } else if (src >= 0) {
+        const int d = src % D, sgn = src < D ? 1 : -1;
+        const int64_t p = ls.index.find(shiftKey<D>(ls.grid, ls.keys[i], d, sgn));
+        dpd[j] = p >= 0 ? ls.pd[p] : PointData{};
+      }
+    }
+  }
   LS<D> res;
   res.grid = ls.grid;
   res.width = ls.width;
@@ -394,9 +445,10 @@ template <int D, class Rule> void starPass(LS<D> &ls, Rule rule) {
     // (then undefined) point it is adjacent to
     const double old = ls.vals[from[j]];
     return isDefined(old) ? ls.farValue(nk) : old;
-  });
+  }, track ? &dpd : nullptr);
   ls.keys.swap(res.keys);
   ls.vals.swap(res.vals);
+  ls.pd.swap(res.pd);
   ls.finalizeMap();
 }
 
@@ -409,20 +461,20 @@ template <int D> void expand(LS<D> &ls, int width) {
   const int cycles = width - startWidth;
   for (int c = 0; c < cycles; ++c) {
     const double limit = (startWidth + c + 1) * double(0.5); // :67
-    starPass<D>(ls, [&](double center, const double *nb) {
+    starPass<D>(ls, [&](double center, const double *nb, int &src) {
       if (std::abs(center) <= totalLimit) return center; // :108-112
       if (center > -EPS) {                                // :114
         double distance = POS;
         for (int i = 0; i < 2 * D; ++i) {
           const double nv = nb[i] + double(1);
-          if (distance > nv) distance = nv;
+          if (distance > nv) distance = nv, src = i;
         }
         return distance <= limit ? distance : POS; // :124-134
       }
       double distance = NEG;
       for (int i = 0; i < 2 * D; ++i) {
         const double nv = nb[i] - double(1);
-        if (distance < nv) distance = nv;
+        if (distance < nv) distance = nv, src = i;
       }
       return distance >= -limit ? distance : NEG; // :145-155
     });
@@ -437,12 +489,15 @@ template <int D> void reduce(LS<D> &ls, int width) {
   const double valueLimit = width * 0.5;
   std::vector<uint64_t> dk;
   std::vector<double> dv;
+  std::vector<PointData> dpd;
   std::vector<double> newVal(ls.vals.size());
+  const bool track = !ls.pd.empty();
   for (size_t i = 0; i < ls.vals.size(); ++i) {
     const double v = ls.vals[i];
     if (isDefined(v) && std::abs(v) <= valueLimit) {
       dk.push_back(ls.keys[i]);
       dv.push_back(v);
+      if (track) dpd.push_back(ls.pd[i]);
       newVal[i] = v;
     } else {
       newVal[i] = v < 0 ? NEG : POS; // :292-295
@@ -453,9 +508,10 @@ template <int D> void reduce(LS<D> &ls, int width) {
   assembleMap<D>(res, dk, dv, [&](uint64_t nk, int64_t) {
     const int64_t p = ls.index.find(nk);
     return p >= 0 ? newVal[p] : ls.farValue(nk);
-  });
+  }, track ? &dpd : nullptr);
   ls.keys.swap(res.keys);
   ls.vals.swap(res.vals);
+  ls.pd.swap(res.pd);
   ls.finalizeMap();
   ls.width = width; // :311
 }
@@ -474,7 +530,7 @@ template <int D> void prune(LS<D> &ls, bool removeStrayZeros) {
   auto isMonotone = [&](double a, double c) -> bool {                           // :50-52
     return a == 0. || c == 0. || isSignDifferent(a, c);
   };
-  starPass<D>(ls, [&](double center, const double *nb) {
+  starPass<D>(ls, [&](double center, const double *nb, int &src) {
     const bool centerSign = isNegative(center);
     if (!isDefined(center)) return centerSign ? NEG : POS; // :175-179
     bool keepPoint = true;
@@ -490,8 +546,12 @@ template <int D> void prune(LS<D> &ls, bool removeStrayZeros) {
       for (int i = 0; i < D; ++i) {
         const double negVal = nb[i];     // getNeighbor(i)   = +e_i
         const double posVal = nb[D + i]; // getNeighbor(D+i) = -e_i
-        if (!isMonotone(negVal, posVal))
+        // the reference records no source for this point (lsPrune.hpp:
+        // 150-155 inserts it without a data id)
+        if (!isMonotone(negVal, posVal)) {
+          src = -2;
           return std::abs(negVal) < std::abs(posVal) ? negVal : posVal;
+        }
       }
     }
     if (keepPoint) return center;
@@ -504,8 +564,13 @@ template <int D> void prune(LS<D> &ls, bool removeStrayZeros) {
 // the comparator over (A value, B value) -> (value, fromA).  Points of A's
 // and B's maps are visited; everything else is undefined in both and the
 // comparator of two sentinels is again a sentinel.
-template <int D, class Comp>
-void booleanOp(LS<D> &A, const LS<D> &B, Comp comp, bool pruneResult = true) {
+// `fromA(a, b)`: whether a defined result takes A's point data (the
+// comparator's second value); results from B take B's, or none when B
+// carries no point data (lsBooleanOperation.hpp:160-196).
+inline bool neverFromA(double, double) { return false; }
+template <int D, class Comp, class FromA = bool (*)(double, double)>
+void booleanOp(LS<D> &A, const LS<D> &B, Comp comp, bool pruneResult = true,
+               FromA fromA = neverFromA) {
   std::vector<uint64_t> cand;
   cand.reserve(A.keys.size() + B.keys.size());
   std::merge(A.keys.begin(), A.keys.end(), B.keys.begin(), B.keys.end(),
@@ -524,6 +589,21 @@ void booleanOp(LS<D> &A, const LS<D> &B, Comp comp, bool pruneResult = true) {
   std::vector<int64_t> from;
   for (int64_t i = 0; i < n; ++i)
     if (isDefined(out[i])) dk.push_back(cand[i]), dv.push_back(out[i]), from.push_back(i);
+  const bool track = !A.pd.empty();
+  std::vector<PointData> dpd;
+  if (track) {
+    dpd.resize(dk.size());
+    for (size_t j = 0; j < dk.size(); ++j) {
+      const int64_t i = from[j];
+      if (fromA(va[i], vb[i])) {
+        const int64_t p = A.index.find(cand[i]);
+        if (p >= 0) dpd[j] = A.pd[p];
+      } else if (!B.pd.empty()) {
+        const int64_t p = B.index.find(cand[i]);
+        if (p >= 0) dpd[j] = B.pd[p];
+      }
+    }
+  }
   LS<D> res;
   res.grid = A.grid;
   assembleMap<D>(res, dk, dv, [&](uint64_t nk, int64_t j) {
@@ -536,10 +616,11 @@ void booleanOp(LS<D> &A, const LS<D> &B, Comp comp, bool pruneResult = true) {
     const double a = isDefined(va[f]) ? A.farValue(nk) : va[f];
     const double b = isDefined(vb[f]) ? B.farValue(nk) : vb[f];
     return comp(a, b);
-  });
+  }, track ? &dpd : nullptr);
   const int widthA = A.width;
   A.keys.swap(res.keys);
   A.vals.swap(res.vals);
+  A.pd.swap(res.pd);
   A.finalizeMap();
   A.width = widthA; // :201
   if (pruneResult) { // :203-210
@@ -550,10 +631,15 @@ void booleanOp(LS<D> &A, const LS<D> &B, Comp comp, bool pruneResult = true) {
 
 inline double minComp(double a, double b) { return a < b ? a : b; } // :262-268
 inline double maxComp(double a, double b) { return a > b ? a : b; } // :270-276
+inline bool minFromA(double a, double b) { return a < b; }
+inline bool maxFromA(double a, double b) { return a > b; }
 
 // lsAdvect.hpp:238-429, rebuildLS.
-template <int D> void rebuild(LS<D> &ls, double cutoff, int finalWidth) {
-  starPass<D>(ls, [&](double c, const double *nb) {
+// With updateData false the new level set carries no point data
+// (lsAdvect.hpp:418-423 translates it only when updatePointData is set).
+template <int D>
+void rebuild(LS<D> &ls, double cutoff, int finalWidth, bool updateData = true) {
+  starPass<D>(ls, [&](double c, const double *nb, int &src) {
     if (std::abs(c) <= 1.0) { // :306
       int k = 0;
       for (; k < 2 * D; k++)
@@ -564,12 +650,14 @@ template <int D> void rebuild(LS<D> &ls, double cutoff, int finalWidth) {
           for (; j < 2 * D; j++)
             if (std::abs(nb[j]) <= 1.0)
               if (nb[j] < -0.5) break;
+          if (j != 2 * D) src = j;
           return j == 2 * D ? c : 0.5;
         } else if (c < -0.5) {
           int j = 0;
           for (; j < 2 * D; j++)
             if (std::abs(nb[j]) <= 1.0)
               if (nb[j] > 0.5) break;
+          if (j != 2 * D) src = j;
           return j == 2 * D ? c : -0.5;
         }
         return c;
@@ -581,7 +669,7 @@ template <int D> void rebuild(LS<D> &ls, double cutoff, int finalWidth) {
       for (int i = 0; i < 2 * D; i++) {
         const double value = nb[i];
         if (std::abs(value) <= 1.0 && (value < 0.))
-          if (distance > value + 1.0) distance = value + 1.0;
+          if (distance > value + 1.0) distance = value + 1.0, src = i;
       }
       return distance <= cutoff ? distance : POS;
     }
@@ -589,10 +677,11 @@ template <int D> void rebuild(LS<D> &ls, double cutoff, int finalWidth) {
     for (int i = 0; i < 2 * D; i++) {
       const double value = nb[i];
       if (std::abs(value) <= 1.0 && (value > 0))
-        if (distance < value - 1.0) distance = value - 1.0;
+        if (distance < value - 1.0) distance = value - 1.0, src = i;
     }
     return distance >= -cutoff ? distance : NEG;
   });
+  if (!updateData) ls.pd.clear();
   ls.width = finalWidth; // :428
 }
 

@@ -4,6 +4,7 @@
 // velocity -- the device functor, or with a second argument "callback" the
 // same velocity as a host VelocityField.  Prints steps, advected time, point
 // count and a checksum.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <limits>
@@ -76,8 +77,23 @@ int main(int argc, char **argv) {
   advect.setSpatialScheme(vlsg::SpatialSchemeEnum::ENGQUIST_OSHER_1ST_ORDER);
   advect.setTemporalScheme(vlsg::TemporalSchemeEnum::FORWARD_EULER);
   advect.setTimeStepRatio(0.5);
-  advect.setAdvectionTime(argc > 1 ? std::atof(argv[1]) : 2.0);
-  advect.apply();
+  if (argc > 2 && std::string(argv[2]) == "loop") {
+    // a caller that loops single steps (as the reference's examples loop
+    // Advect::apply): argv[1] steps of advectionTime 0; the level set stays
+    // on the device between them.  After the loop the object is changed in
+    // place and touch()ed, so the next apply uploads it again.
+    advect.setAdvectionTime(0.0);
+    const int steps = argc > 1 ? std::atoi(argv[1]) : 5;
+    for (int k = 0; k < steps; ++k) advect.apply();
+    std::printf("skipped %llu ", (unsigned long long)advect.getSkippedUploads());
+    for (auto &v : ls->values) v = std::min(v, 0.25) ; // change in place ...
+    ls->touch();                                        // ... and say so
+    advect.apply();
+    std::printf("after_touch %llu ", (unsigned long long)advect.getSkippedUploads());
+  } else {
+    advect.setAdvectionTime(argc > 1 ? std::atof(argv[1]) : 2.0);
+    advect.apply();
+  }
   double sum = 0;
   for (size_t i = 0; i < ls->values.size(); ++i)
     sum += ls->values[i] * (1.0 + 1e-3 * (ls->indices[3 * i] + 7 * ls->indices[3 * i + 1] +

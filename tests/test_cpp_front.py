@@ -51,3 +51,17 @@ def test_cpp_front_host_velocity_field(tmp_path):
     a = subprocess.check_output([exe, "2.0"], text=True)
     b = subprocess.check_output([exe, "2.0", "callback"], text=True)
     assert a == b
+
+
+@pytest.mark.gpu
+def test_cpp_front_keeps_level_sets_resident(tmp_path):
+    """Five single-step applies through the C++ front: the first uploads, the
+    next four find the device copy current (version stamps) and skip the
+    upload; the results equal five single steps of a context.  A touch()ed
+    level set is uploaded again."""
+    exe = str(tmp_path / "front_sphere")
+    build_front(exe)
+    out = subprocess.check_output([exe, "5", "loop"], text=True).split()
+    vals = dict(zip(out[0::2], out[1::2]))
+    assert int(vals["skipped"]) == 4
+    assert int(vals["after_touch"]) == 4  # the touched object was uploaded

@@ -71,6 +71,7 @@ class AdvectParams(ctypes.Structure):
         ("update_point_data", ctypes.c_int32),
         ("max_steps", ctypes.c_uint32),
         ("max_dissipation", ctypes.c_double),
+        ("track_point_data", ctypes.c_int32),
     ]
 
     @classmethod
@@ -92,6 +93,7 @@ class AdvectParams(ctypes.Structure):
         p.update_point_data = 1
         p.max_steps = 0
         p.max_dissipation = 0.0  # no limit
+        p.track_point_data = 0
         return p
 
 
@@ -181,6 +183,11 @@ class LevelSetView(ctypes.Structure):
 
 
 UPDATE_CALLBACK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(LevelSetView))
+# vlsg_reduce_cb: (user, double *values, n, op) -> int
+REDUCE_CALLBACK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                   ctypes.c_int32, ctypes.c_int32)
+REDUCE_MIN = 0
+REDUCE_MAX = 1
 
 VELOCITY_CALLBACK = ctypes.CFUNCTYPE(
     ctypes.c_int,

@@ -2,7 +2,7 @@
 import ctypes
 import os
 
-from ._abi import (ALPHA_CALLBACK, UPDATE_CALLBACK, VELOCITY_CALLBACK, AdvectParams, AdvectResult, CompareResult, KernelStat,
+from ._abi import (ALPHA_CALLBACK, REDUCE_CALLBACK, UPDATE_CALLBACK, VELOCITY_CALLBACK, AdvectParams, AdvectResult, CompareResult, KernelStat,
                    VelocityDesc)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -41,6 +41,10 @@ def load(build_if_missing=True):
     L.vlsg_count_points.argtypes = [vp, i32, P(i64)]
     L.vlsg_download_levelset.argtypes = [vp, i32, i64, P(i32), P(ctypes.c_double), P(i32)]
     L.vlsg_get_values.argtypes = [vp, i32, i64, P(i32), P(ctypes.c_double)]
+    L.vlsg_set_owned_region.argtypes = [vp, i32, i64, i64]
+    L.vlsg_set_reduction_callback.argtypes = [vp, REDUCE_CALLBACK, vp]
+    L.vlsg_download_point_data.argtypes = [vp, i32, i64, P(i64), P(ctypes.c_double),
+                                           P(ctypes.c_double), P(i32)]
     L.vlsg_download_runs.argtypes = [vp, i32, i64, P(i32), P(ctypes.c_int8), P(i64)]
     L.vlsg_compare.argtypes = [vp, i32, vp, i32, P(CompareResult)]
     L.vlsg_advect_batch.argtypes = [P(vp), i32, P(AdvectParams), P(AdvectResult), i32]
@@ -64,10 +68,11 @@ EXPORTED = [
     "vlsg_default_params", "vlsg_set_stream", "vlsg_get_stream",
     "vlsg_set_grid", "vlsg_set_level_set_count",
     "vlsg_upload_levelset", "vlsg_count_points", "vlsg_download_levelset", "vlsg_download_runs",
-    "vlsg_get_values", "vlsg_get_values_noalloc",
+    "vlsg_get_values", "vlsg_get_values_noalloc", "vlsg_download_point_data",
     "vlsg_set_velocity_functor", "vlsg_set_velocity_callback",
     "vlsg_set_dissipation_alpha_callback", "vlsg_prepare_stencil_llf", "vlsg_finalize_stencil_llf",
     "vlsg_prepare_ls",
     "vlsg_set_velocity_update_callback", "vlsg_advect", "vlsg_advect_batch",
     "vlsg_set_profiling", "vlsg_get_kernel_stats", "vlsg_compare",
+    "vlsg_set_owned_region", "vlsg_set_reduction_callback",
 ]

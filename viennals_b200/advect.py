@@ -97,6 +97,45 @@ class Context:
                                                     _p(val, ctypes.c_double), ctypes.byref(w)))
         return idx, val, w.value
 
+    def set_owned_region(self, axis, lo=0, hi=0):
+        """vlsg_set_owned_region: only points with index[axis] in [lo, hi)
+        count towards the time step, the alphas and the point updates (axis 2;
+        -1 owns everything)."""
+        self._check(self.lib.vlsg_set_owned_region(self.h, int(axis), int(lo), int(hi)))
+
+    def set_reduction_callback(self, fn):
+        """vlsg_set_reduction_callback: fn(values, op) replaces the numpy array
+        `values` by its reduction over all shards (op 0 = min, 1 = max).  None
+        clears it."""
+        from ._abi import REDUCE_CALLBACK
+
+        if fn is None:
+            self._reduce_cb = REDUCE_CALLBACK()
+        else:
+            def cb(user, values, n, op):
+                try:
+                    arr = np.ctypeslib.as_array(values, shape=(n,))
+                    fn(arr, int(op))
+                    return 0
+                except Exception:  # noqa: BLE001 -- reported as VLSG_ERR_CALLBACK
+                    return 1
+            self._reduce_cb = REDUCE_CALLBACK(cb)
+        self._check(self.lib.vlsg_set_reduction_callback(self.h, self._reduce_cb, None))
+
+    def download_point_data(self, slot):
+        """vlsg_download_point_data: (source, velocity, dissipation) of the
+        defined points in download order, or None when the level set carries
+        no point data."""
+        n = self.count(slot)
+        src = np.empty(n, np.int64)
+        vel = np.empty(n)
+        diss = np.empty(n)
+        has = ctypes.c_int32()
+        self._check(self.lib.vlsg_download_point_data(
+            self.h, int(slot), n, _p(src, ctypes.c_int64), _p(vel, ctypes.c_double),
+            _p(diss, ctypes.c_double), ctypes.byref(has)))
+        return (src, vel, diss) if has.value else None
+
     def values_at(self, slot, idx):
         idx = np.ascontiguousarray(idx, np.int32)
         out = np.zeros(len(idx))
@@ -372,11 +411,42 @@ class Advect:
         self._write_back([len(self.levelSets) - 1])
 
     def apply(self):
-        """Advect::apply, lsAdvect.hpp:1017-1043; results written back."""
+        """Advect::apply, lsAdvect.hpp:1017-1043; results written back.  The top
+        level set's point data (Domain.point_data) is carried along as the
+        reference's passes translate it; with setSaveAdvectionVelocities it
+        gains the "AdvectionVelocities" and "Dissipation" arrays of the last
+        value update (lsAdvect.hpp:780-796); with setUpdatePointData(False) it
+        is dropped (rebuildLS keeps none, lsAdvect.hpp:418-423)."""
+        top = self.levelSets[-1] if self.levelSets else None
+        save = bool(self.params.save_advection_velocities)
+        track = save or bool(top is not None and top.point_data)
+        self.params.track_point_data = int(track)
         self._sync_to_device()
         self.result = self.ctx.advect(self.params)
+        old = dict(top.point_data) if top is not None else {}
         self._write_back(range(len(self.levelSets)))
+        if track:
+            top.point_data = self._translate_point_data(old, save)
         return self.result
+
+    def _translate_point_data(self, old, save):
+        pd = self.ctx.download_point_data(len(self.levelSets) - 1)
+        if pd is None:
+            return {}
+        src, vel, diss = pd
+        ok = src >= 0
+        new = {}
+        for label, arr in old.items():
+            if save and label in (self.velocityLabel, self.dissipationLabel):
+                continue  # replaced by this advection's values
+            arr = np.asarray(arr)
+            out = np.zeros((len(src),) + arr.shape[1:], arr.dtype)
+            out[ok] = arr[src[ok]]
+            new[label] = out
+        if save:
+            new[self.velocityLabel] = vel
+            new[self.dissipationLabel] = diss
+        return new
 
 
 def update_callback(fn, grid=None):

@@ -33,6 +33,10 @@ struct vlsg_context {
   void *alphaUser = nullptr;
   vlsg_update_cb updCb = nullptr;
   void *updUser = nullptr;
+  vlsg_reduce_cb reduceCb = nullptr; // sharding
+  void *reduceUser = nullptr;
+  int ownAxis = -1;
+  int64_t ownLo = 0, ownHi = 0;
   bool profiling = false;
   std::unique_ptr<EngineBase> eng; // Engine<double> or Engine<float>
 };
@@ -383,6 +387,27 @@ int vlsg_download_runs(vlsg_context *ctx, int32_t slot, int64_t capacity, int32_
   });
 }
 
+int vlsg_download_point_data(vlsg_context *ctx, int32_t slot, int64_t capacity,
+                             int64_t *source, double *velocity, double *dissipation,
+                             int32_t *has_point_data) {
+  if (!ctx || !has_point_data || capacity < 0 ||
+      (capacity > 0 && (!source || !velocity || !dissipation)))
+    return fail(ctx, VLSG_ERR_ARGUMENT, "bad argument");
+  return guarded(ctx, [&] {
+    ensureBuilt(ctx);
+    if (slot < 0 || slot >= (int)ctx->staged.size())
+      return fail(ctx, VLSG_ERR_ARGUMENT, "level set slot out of range");
+    if (slot != (int)ctx->staged.size() - 1)
+      return fail(ctx, VLSG_ERR_ARGUMENT, "point data is kept for the top level set only");
+    const int64_t n = ctx->eng->pointData(slot, nullptr, nullptr, nullptr, 0);
+    *has_point_data = n >= 0 ? 1 : 0;
+    if (n < 0) return VLSG_OK;
+    if (n > capacity) return fail(ctx, VLSG_ERR_CAPACITY, "point data capacity too small");
+    ctx->eng->pointData(slot, source, velocity, dissipation, capacity);
+    return VLSG_OK;
+  });
+}
+
 int vlsg_get_values(vlsg_context *ctx, int32_t slot, int64_t n, const int32_t *idx,
                     double *values) {
   if (!ctx || n < 0 || (n > 0 && (!idx || !values)))
@@ -515,6 +540,9 @@ int vlsg_advect(vlsg_context *ctx, const vlsg_advect_params *p, vlsg_advect_resu
     return fail(ctx, VLSG_ERR_ARGUMENT, "Advect: Discretization scheme not found.");
   if (p->temporal_scheme < 0 || p->temporal_scheme > 2)
     return fail(ctx, VLSG_ERR_ARGUMENT, "unknown temporal scheme");
+  if (ctx->ownAxis >= 0 && p->spatial_scheme == VLSG_STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER)
+    return fail(ctx, VLSG_ERR_ARGUMENT,
+                "an owned region (sharding) is not supported with STENCIL_LOCAL_LAX_FRIEDRICHS");
   return guarded(ctx, [&] {
     ensureBuilt(ctx);
     EngineBase &e = *ctx->eng;
@@ -525,11 +553,34 @@ int vlsg_advect(vlsg_context *ctx, const vlsg_advect_params *p, vlsg_advect_resu
     e.alphaUser = ctx->alphaUser;
     e.updCb = ctx->updCb;
     e.updUser = ctx->updUser;
+    e.reduceCb = ctx->reduceCb;
+    e.reduceUser = ctx->reduceUser;
+    e.ownAxis = ctx->ownAxis;
+    e.ownLo = ctx->ownLo;
+    e.ownHi = ctx->ownHi;
     e.profiling = ctx->profiling;
     if (ctx->profiling) e.timers.clear();
     e.apply(*p, *r);
     return VLSG_OK;
   });
+}
+
+int vlsg_set_owned_region(vlsg_context *ctx, int32_t axis, int64_t lo, int64_t hi) {
+  if (!ctx) return fail(nullptr, VLSG_ERR_ARGUMENT, "NULL context");
+  if (axis != -1 && axis != 2)
+    return fail(ctx, VLSG_ERR_ARGUMENT, "vlsg_set_owned_region: axis must be 2 (or -1: all)");
+  if (axis == 2 && !(lo < hi)) return fail(ctx, VLSG_ERR_ARGUMENT, "vlsg_set_owned_region: empty");
+  ctx->ownAxis = axis;
+  ctx->ownLo = lo;
+  ctx->ownHi = hi;
+  return VLSG_OK;
+}
+
+int vlsg_set_reduction_callback(vlsg_context *ctx, vlsg_reduce_cb cb, void *user) {
+  if (!ctx) return fail(nullptr, VLSG_ERR_ARGUMENT, "NULL context");
+  ctx->reduceCb = cb;
+  ctx->reduceUser = user;
+  return VLSG_OK;
 }
 
 int vlsg_advect_batch(vlsg_context **ctxs, int32_t n, const vlsg_advect_params *params,

@@ -111,11 +111,41 @@ __device__ inline T cellValue(const GridDev &g, const MapView &m, const Buf<T> &
   return b.vals[(size_t)slot * BV + ((rz & 7) * 64 + (ry & 7) * 8 + (rx & 7))];
 }
 
+// Pool index (slot * 512 + cell) of mapped cell (x,y,z), with cellValue's
+// clamping; only for a cell whose value is defined (its brick has a slot).
+__device__ inline size_t cellIndex(const GridDev &g, const MapView &m, int x, int y, int z) {
+  int rx = x - g.org[0], ry = y - g.org[1], rz = z - g.org[2];
+  const int ex = g.nb[0] * BS - 1, ey = g.nb[1] * BS - 1, ez = g.nb[2] * BS - 1;
+  rx = rx < 0 ? 0 : (rx > ex ? ex : rx);
+  ry = ry < 0 ? 0 : (ry > ey ? ey : ry);
+  rz = rz < 0 ? 0 : (rz > ez ? ez : rz);
+  const int slot = m.brickMap[brickIndex(g, rx >> 3, ry >> 3, rz >> 3)];
+  return (size_t)slot * BV + ((rz & 7) * 64 + (ry & 7) * 8 + (rx & 7));
+}
+
 template <class T>
 __device__ inline T cellValueRaw(const GridDev &g, const MapView &m,
                                  const Buf<T> &b, int x, int y, int z) {
   return cellValue<T>(g, m, b, mapCoord(g, 0, x), mapCoord(g, 1, y),
                       mapCoord(g, 2, z));
+}
+
+// hi + lo of a value with a compensation term; a zero term leaves hi as it is
+// (keeping the sign of a zero).
+__host__ __device__ inline double withLo(double hi, float lo) {
+  return lo != 0.f ? hi + (double)lo : hi;
+}
+
+// cellValueRaw as a double, plus the compensation term `lo` of a defined
+// value when the buffer carries one (lo non-null).
+template <class T>
+__device__ inline double cellValueFull(const GridDev &g, const MapView &m, const Buf<T> &b,
+                                       const float *lo, int x, int y, int z) {
+  x = mapCoord(g, 0, x), y = mapCoord(g, 1, y), z = mapCoord(g, 2, z);
+  const T v = cellValue<T>(g, m, b, x, y, z);
+  double r = (double)v;
+  if (lo && isDef(v)) r = withLo(r, lo[cellIndex(g, m, x, y, z)]);
+  return r;
 }
 
 __device__ inline void brickCoords(const GridDev &g, int bi, int &bx, int &by,

@@ -27,6 +27,7 @@
 #include "vlsg_maint.cuh"
 #include "vlsg_passes.cuh"
 #include "vlsg_rates.cuh"
+#include "vlsg_rows.cuh"
 #include "vlsg_velcb.cuh"
 #include "vlsg_voids.cuh"
 
@@ -73,6 +74,8 @@ public:
     bool live = false;
     double bound = 0;  // upper bound of |value| over the defined cells
     int64_t nDef = 0;  // defined cells (profiling mode)
+    float *lo = nullptr; // compensation terms (FP32 top level set and its RK copy)
+    size_t capLo = 0;
   };
   DBuf buf[MAXB];
   T *rateV = nullptr, *rateStop = nullptr; // pool shaped, L chain entries
@@ -135,7 +138,7 @@ public:
          X_ROWC, X_ROWG, X_PB, X_GB, X_RSTART, X_RSIGN, X_RPB, X_KEEP, X_KPOS, X_OSTART,
          X_OSIGN, X_VCNT, X_VOFF, X_VSUMS, X_QC, X_QM, X_QN, X_QP, X_VS, X_VV, X_AD, X_AM,
          X_AC, X_AV, X_SKEY, X_SALPHA, X_QC2, X_QN2, X_QM2, X_QP2, X_VS2, X_VPARENT, X_VMASK,
-         X_VTOP, X_COUNT };
+         X_VTOP, X_PSRC, X_PVEL, X_PDISS, X_COUNT };
   // pinned host staging of the velocity callback's queries and answers
   struct PinScratch {
     void *p = nullptr;
@@ -159,9 +162,15 @@ public:
 
   void release() {
     auto f = [](void *p) { if (p) cudaFree(p); };
+    for (auto &b : buf) f(b.lo);
     f(brickMap); f(slotBrick); f(slotList); f(freeStack); f(newList); f(counters); f(needed);
     f(scal); f(defCnt); f(rateCounts); f(nbr); f(cflag); f(core); f(small); f(rateV);
     f(rateStop); f(rateLen); f(act); f(logCell); f(logVal); f(logCount); f(visitSpare);
+    freePayload(pdCells);
+    freePayload(pdLog);
+    f(rateD);
+    rateD = nullptr;
+    capPdCells = capPdLog = capRateD = 0;
     for (auto &v : visit) {
       f(v);
       v = nullptr;
@@ -199,9 +208,60 @@ public:
   Topo topo() { return Topo{g, brickMap, slotBrick, slotList, nSlotsPtr(), nbr, cflag, errPtr()}; }
   LsView<T> lsView(int b) {
     auto &B = buf[b];
-    return LsView<T>{B.vals, B.def[B.cur], B.def[1 - B.cur], B.farSign};
+    return LsView<T>{B.vals, B.def[B.cur], B.def[1 - B.cur], B.farSign, payloadOf(b)};
   }
-  ChangeLog<T> changeLog() { return ChangeLog<T>{logCell, logVal, logCount, logPer}; }
+  ChangeLog<T> changeLog(int b) {
+    return ChangeLog<T>{logCell, logVal, logCount, logPer,
+                        pdTracked(b) ? pdLog : Payload<T>{nullptr, nullptr, nullptr}};
+  }
+
+  // --------------------------------------------------------- point data
+  // The top level set's point data through an advection: per cell of its
+  // buffer the source id and the saved velocity / dissipation, carried by
+  // every pass through its change log (pdLog), set at the start of
+  // vlsg_advect from the points' ranks and by the value update.
+  Payload<T> pdCells{}, pdLog{};
+  size_t capPdCells = 0, capPdLog = 0;
+  T *rateD = nullptr;
+  size_t capRateD = 0;
+  bool pdTrack = false; // carried through this advection
+  bool pdSave = false;  // saved velocities (setSaveAdvectionVelocities)
+  bool pdHas = false;   // the top level set carries point data now
+  bool pdTracked(int b) const { return pdTrack && b == L - 1; }
+  Payload<T> payloadOf(int b) const {
+    return pdTracked(b) ? pdCells : Payload<T>{nullptr, nullptr, nullptr};
+  }
+  static void freePayload(Payload<T> &p) {
+    if (p.src) cudaFree(p.src);
+    if (p.vel) cudaFree(p.vel);
+    if (p.diss) cudaFree(p.diss);
+    p = Payload<T>{nullptr, nullptr, nullptr};
+  }
+  static void allocPayload(Payload<T> &p, size_t &cap, size_t n) {
+    if (cap >= n && p.src) return;
+    freePayload(p);
+    VLSG_CUDA(cudaMalloc(&p.src, n * sizeof(int32_t)));
+    VLSG_CUDA(cudaMalloc(&p.vel, n * sizeof(T)));
+    VLSG_CUDA(cudaMalloc(&p.diss, n * sizeof(T)));
+    cap = n;
+  }
+  // Start of an advection with point data: every defined cell of the top
+  // level set carries its own rank (the order of vlsg_download_levelset).
+  void initPointData() {
+    const int top = L - 1;
+    allocPayload(pdCells, capPdCells, poolCells);
+    allocPayload(pdLog, capPdLog, logPer * (size_t)logSegments);
+    if (pdSave) growDevice(rateD, capRateD, poolCells * (size_t)L);
+    const int nList = readI32(nSlotsPtr());
+    xBuf = -1; // the point layout below reuses the exchange's scratch
+    pointLayout(top, nList);
+    const PointRanks R{slotBrick, (const uint32_t *)xs[X_POS].p, (const int4 *)xs[X_BOUNDS].p,
+                       (const uint32_t *)xs[X_P].p, buf[top].def[buf[top].cur]};
+    Scope sc(this, "point_data");
+    kInitPointData<T><<<blocksPass, 256, 0, stream>>>(slotList, nSlotsPtr(),
+                                                      buf[top].def[buf[top].cur], R, pdCells);
+    checkLaunch();
+  }
 
   // ---------------------------------------------------------------- timing
   // One kernel launch.  With profiling on it is bracketed by CUDA events on
@@ -295,8 +355,25 @@ public:
         VLSG_CUDA(cudaMalloc(&B.farSign, capBricks));
         B.capBricks = capBricks;
       }
+      if (hasLo(b) && (B.capLo < capSlots || !B.lo)) {
+        if (B.lo) VLSG_CUDA(cudaFree(B.lo));
+        B.lo = nullptr;
+        VLSG_CUDA(cudaMalloc(&B.lo, capSlots * BV * sizeof(float)));
+        B.capLo = capSlots;
+      }
     }
   }
+  // The precision form (T = float) keeps, for the top level set and its RK
+  // copy, a second FP32 array per cell: the compensation term `lo` of the
+  // value, whose exact value is hi + lo.  Only the value update and the RK
+  // stage combination (both in double) produce a non-zero term; every other
+  // write of a value (a pass's change, a boolean, a copy without terms) sets
+  // it to zero, so that hi + lo is always the value the FP64 arithmetic of
+  // those two steps produced or the stored value itself.  Stencils and pass
+  // rules read hi only; downloads and queries return hi + lo.
+  static constexpr bool kComp = sizeof(T) == 4;
+  bool hasLo(int b) const { return kComp && (b == L - 1 || b == 2 * L - 1); }
+  float *loOf(int b) { return hasLo(b) ? buf[b].lo : nullptr; }
 
   // The live buffers (current level sets and the RK copies in use).
   BufSet bufSet() {
@@ -393,6 +470,7 @@ public:
   void build(const GridDev &grid, std::vector<StagedLS> &ls, int margin) override {
     ++generation;
     dropVisits();
+    pdTrack = pdSave = pdHas = false;
     ensureSmall();
     g = grid;
     L = (int)ls.size();
@@ -510,7 +588,7 @@ public:
       if (s.n) {
         Scope sc(this, "upload_scatter");
         kScatterPoints<T><<<grid1(s.n), 256, 0, stream>>>(g, (int)s.n, s.idx, s.vals, brickMap,
-                                                          buf[l].vals, errPtr());
+                                                          buf[l].vals, errPtr(), loOf(l));
         checkLaunch();
       }
       {
@@ -640,8 +718,9 @@ public:
   // --------------------------------------------------------------- passes
   void applyChanges(int b) {
     Scope sc(this, "apply_changes");
-    kApplyChanges<T><<<logSegments, FRONTIER_THREADS, 0, stream>>>(buf[b].vals, changeLog(),
-                                                                    logSegments);
+    kApplyChanges<T><<<logSegments, FRONTIER_THREADS, 0, stream>>>(buf[b].vals, changeLog(b),
+                                                                    logSegments, loOf(b),
+                                                                    payloadOf(b));
     checkLaunch();
   }
 
@@ -658,7 +737,28 @@ public:
         return bandPassBytes(nIn, buf[b].nDef);
       });
       kFrontierPass<T, MODE, Rule><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(
-          topo(), lsView(b), rule, changeLog(), visitIn(b), visitOut(), zeroPtr(), zeroMode, cap);
+          topo(), lsView(b), rule, changeLog(b), visitIn(b), visitOut(), zeroPtr(), zeroMode, cap);
+      visitDone(b);
+      checkLaunch();
+    }
+    applyChanges(b);
+    buf[b].cur ^= 1;
+  }
+
+  // One Expand cycle that only defines new cells (every defined |value| is
+  // within the total limit): the row pass.
+  void expandRows(int b, const ExpandRule<T> &rule) {
+    const int64_t nIn = profiling ? defined(b) : 0;
+    {
+      Scope sc(this, "expand", [this, b, nIn] {
+        buf[b].cur ^= 1;
+        buf[b].nDef = defined(b);
+        buf[b].cur ^= 1;
+        return bandPassBytes(nIn, buf[b].nDef);
+      });
+      kExpandRows<T><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(topo(), lsView(b), rule,
+                                                                  changeLog(b), visitIn(b),
+                                                                  visitOut());
       visitDone(b);
       checkLaunch();
     }
@@ -676,7 +776,7 @@ public:
     const bool onlyUndefined = buf[b].bound <= (double)totalLimit;
     for (int c = 0; c < cycles; ++c) {
       ExpandRule<T> r{totalLimit, T((startWidth + c + 1) * T(0.5))};
-      if (onlyUndefined) frontierPass<FP_EXPAND>(b, r, "expand");
+      if (onlyUndefined) expandRows(b, r);
       else frontierPass<FP_ALL>(b, r, "expand");
       if (b == L - 1 && startWidth + c + 1 == saveTopAt) {
         // the RK copy of the top level set, taken at this width (saveTop)
@@ -722,7 +822,10 @@ public:
       Scope sc(this, "update", [this] { return 3.0 * double(sizeof(T)) * double(lastActive); });
       kUpdate<T><<<blocksPass, RATE_THREADS, 0, stream>>>(slotList, nSlotsPtr(), act, buf[top].vals,
                                                           rateV, rateStop, rateLen, poolCells, L,
-                                                          dt, errPtr());
+                                                          dt, errPtr(), loOf(top),
+                                                          pdSave ? pdCells.vel : nullptr,
+                                                          pdSave ? pdCells.diss : nullptr,
+                                                          pdSave ? rateD : nullptr);
       checkLaunch();
     }
     {
@@ -734,7 +837,7 @@ public:
         return bandPassBytes(lastActive, buf[top].nDef);
       });
       kUpdateRebuild<T><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(
-          topo(), lsView(top), act, rebuildCutoff, changeLog(), visitIn(top), visitOut());
+          topo(), lsView(top), act, rebuildCutoff, changeLog(top), visitIn(top), visitOut());
       visitDone(top);
       checkLaunch();
     }
@@ -755,10 +858,11 @@ public:
       });
       if constexpr (Comp::keepsUndefinedA) {
         kPointwiseDefined<T, Comp><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(
-            topo(), buf[a].vals, buf[a].def[buf[a].cur], buf[bb].vals, comp, flag);
+            topo(), buf[a].vals, buf[a].def[buf[a].cur], buf[bb].vals, comp, flag, loOf(a),
+            loOf(bb));
       } else {
         kPointwise<T, Comp><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(
-            topo(), buf[a].vals, buf[a].def[buf[a].cur], buf[bb].vals, comp, flag);
+            topo(), buf[a].vals, buf[a].def[buf[a].cur], buf[bb].vals, comp, flag, loOf(a));
       }
       checkLaunch();
     }
@@ -794,7 +898,7 @@ public:
   void invertBuffer(int b) {
     auto &B = buf[b];
     kNegateSlots<T><<<blocksPass, 256, 0, stream>>>(slotList, nSlotsPtr(), B.vals, B.farSign,
-                                                    nBricks);
+                                                    nBricks, loOf(b));
     checkLaunch();
   }
 
@@ -805,6 +909,7 @@ public:
   // element), which is kept.
   void prepareStencil(std::vector<bool> isDepo) {
     ++generation;
+    pdTrack = pdSave = pdHas = false; // these operations carry no point data
     isDepo.resize(L, false);
     const int fin = L, above = L + 1;
     clearBuffer(fin);
@@ -841,6 +946,7 @@ public:
   // level set below it.
   void finalizeStencil() {
     ++generation;
+    pdTrack = pdSave = pdHas = false;
     dropVisits();
     invertBuffer(L - 1);
     booleanOp(L - 1, L - 2, MinComp<T>{});
@@ -856,7 +962,7 @@ public:
     {
       Scope sc(this, "copy");
       kCopySlots16<T><<<blocksPass, 256, 0, stream>>>(slotList, nSlotsPtr(), S.vals, S.def[S.cur],
-                                                      D.vals, D.def[D.cur]);
+                                                      D.vals, D.def[D.cur], loOf(src), loOf(dst));
       checkLaunch();
     }
     VLSG_CUDA(cudaMemcpyAsync(D.farSign, S.farSign, nBricks, cudaMemcpyDeviceToDevice, stream));
@@ -898,11 +1004,15 @@ public:
     A.checkDiss = P.check_dissipation;
     A.rateV = rateV;
     A.rateStop = rateStop;
+    A.rateD = pdSave ? rateD : nullptr;
     A.rateLen = rateLen;
     A.poolCells = poolCells;
     A.minStep = scal;
     A.counts = rateCounts;
     A.err = errPtr();
+    A.ownZ = ownAxis == 2;
+    A.ownLo = (int)std::max<int64_t>(ownLo, INT_MIN / 2);
+    A.ownHi = (int)std::min<int64_t>(ownHi, INT_MAX / 2);
     unsigned long long init[4] = {~0ull, 0, 0, 0};
     VLSG_CUDA(cudaMemcpyAsync(scal, init, sizeof(init), cudaMemcpyHostToDevice, stream));
     VLSG_CUDA(cudaMemsetAsync(rateCounts, 0, 2 * sizeof(unsigned long long), stream));
@@ -921,8 +1031,9 @@ public:
         double a;
         std::memcpy(&a, &pinScal[1 + k], 8);
         alphas[k] = a;
-        A.globalAlpha[k] = T(a);
       }
+      reduceAcross(alphas, 3, VLSG_REDUCE_MAX); // findGlobalAlphas over all shards
+      for (int k = 0; k < 3; ++k) A.globalAlpha[k] = T(alphas[k]);
       A.alphaMax = nullptr;
     } else if (lfFamily) {
       A.alphaMax = scal + 1;
@@ -973,17 +1084,17 @@ public:
     lastBand = (int64_t)pinScal[5];
     pointUpdates += (uint64_t)lastActive;
     double tempMax = maxTimeStep;
-    if (hScal[0] != ~0ull) {
-      double m;
-      std::memcpy(&m, &hScal[0], 8);
-      if (m < tempMax) tempMax = m;
-    }
+    double m = DBL_MAX; // no active point: no bound from the points
+    if (hScal[0] != ~0ull) std::memcpy(&m, &hScal[0], 8);
+    reduceAcross(&m, 1, VLSG_REDUCE_MIN); // the time step over all shards
+    if (m < tempMax) tempMax = m;
     if (lfFamily) {
       double fa[3];
       if (globalLF) {
         for (int k = 0; k < 3; ++k) fa[k] = alphas[k];
       } else {
         for (int k = 0; k < 3; ++k) std::memcpy(&fa[k], &hScal[1 + k], 8);
+        if (!stencil) reduceAcross(fa, 3, VLSG_REDUCE_MAX);
       }
       double timeStep = 0;
       for (int i = 0; i < 3; ++i) timeStep += fa[i] / g.delta;
@@ -1196,9 +1307,19 @@ public:
     if (L > 1) {
       VLSG_CUDA(cudaMemcpyAsync(pinCounters, counters, 16 * sizeof(int), cudaMemcpyDeviceToHost, stream));
       VLSG_CUDA(cudaStreamSynchronize(stream));
-      return pinCounters[4] != 0;
+      double moved = pinCounters[4] != 0 ? 1.0 : 0.0;
+      reduceAcross(&moved, 1, VLSG_REDUCE_MAX);
+      return moved != 0.0;
     }
     return false;
+  }
+
+  // The cross-shard reduction (vlsg_set_reduction_callback), or nothing.
+  void reduceAcross(double *v, int n, int op) {
+    if (!reduceCb) return;
+    const int rc = reduceCb(reduceUser, v, n, op);
+    if (rc != 0)
+      throw CudaError("the reduction callback returned " + std::to_string(rc), VLSG_ERR_CALLBACK);
   }
 
   // The RK copy of the top level set is first read by the stage combination,
@@ -1228,7 +1349,8 @@ public:
       {
         Scope sc(this, "copy");
         kCopySlots16<T><<<blocksPass, 256, 0, stream>>>(slotList, nSlotsPtr(), S.vals,
-                                                        S.def[S.cur], D.vals, D.def[D.cur]);
+                                                        S.def[S.cur], D.vals, D.def[D.cur],
+                                                        loOf(L + l), loOf(l));
         checkLaunch();
       }
       VLSG_CUDA(cudaMemcpyAsync(D.farSign, S.farSign, nBricks, cudaMemcpyDeviceToDevice, stream));
@@ -1323,6 +1445,13 @@ public:
     ++generation;
     deferMaintain = false; // an earlier apply may have ended in an error mid-step
     saveTopAt = 0;
+    // point data: every apply ends with a rebuild of the top level set, which
+    // keeps it only with updatePointData (lsAdvect.hpp:418-423)
+    const bool wantPd = P.track_point_data || P.save_advection_velocities;
+    pdTrack = wantPd && P.update_point_data;
+    pdSave = pdTrack && P.save_advection_velocities;
+    pdHas = false;
+    if (pdTrack) initPointData();
     const bool sllf = P.spatial_scheme == VLSG_STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER;
     rebuildCutoff = sllf ? 1.5 : 1.0;
     rebuildWidth = sllf ? 3 : 2;
@@ -1346,6 +1475,8 @@ public:
       advectedTime = currentTime;
     }
     syncErr("advect");
+    pdHas = pdTrack;
+    pdTrack = pdSave = false;
     r.advected_time = advectedTime;
     r.current_time_step = currentTimeStep;
     r.number_of_time_steps = steps;
@@ -1367,7 +1498,8 @@ public:
     VLSG_CUDA(cudaMemcpyAsync(di, idx, n * 3 * sizeof(int), cudaMemcpyHostToDevice, stream));
     {
       Scope sc(this, "query");
-      kQueryValues<T><<<grid1(n), 256, 0, stream>>>(g, mapView(), view(b), (int)n, di, dv);
+      kQueryValues<T><<<grid1(n), 256, 0, stream>>>(g, mapView(), view(b), (int)n, di, dv,
+                                                     loOf(b));
       checkLaunch();
     }
     VLSG_CUDA(cudaMemcpyAsync(out, dv, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
@@ -1488,7 +1620,8 @@ public:
     VLSG_CUDA(cudaMemsetAsync(rowC, 0, rows * sizeof(uint32_t), stream));
     VLSG_CUDA(cudaMemsetAsync(rowG, 0, rows * sizeof(uint32_t), stream));
     kSegScatter<T><<<grid1(nSeg), 256, 0, stream>>>(g, ob, nAlloc, brickMap, nbr, bounds, def,
-                                                    buf[b].vals, P, rb, idx, val, GC, rowC, rowG);
+                                                    buf[b].vals, P, rb, idx, val, GC, rowC, rowG,
+                                                    loOf(b));
     scanExclusive(GC, GE, nSeg, sums);
     scanExclusive(rowC, PB, rows, sums2);
     scanExclusive(rowG, GB, rows, sums2);
@@ -1551,7 +1684,8 @@ public:
     VLSG_CUDA(cudaMemcpyAsync(di, idx, n * 3 * sizeof(int32_t), cudaMemcpyHostToDevice, stream));
     {
       Scope sc(this, "query");
-      kQueryValues<T><<<grid1(n), 256, 0, stream>>>(g, mapView(), view(b), (int)n, di, dv);
+      kQueryValues<T><<<grid1(n), 256, 0, stream>>>(g, mapView(), view(b), (int)n, di, dv,
+                                                     loOf(b));
       checkLaunch();
     }
     VLSG_CUDA(cudaMemcpyAsync(out, dv, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
@@ -1577,9 +1711,32 @@ public:
 
   uint64_t insideCells(int b) override {
     VLSG_CUDA(cudaMemsetAsync(small + 15, 0, sizeof(unsigned long long), stream));
-    kInsideCells<T><<<blocksPass, 256, 0, stream>>>(g, mapView(), view(b), nBricks, small + 15);
+    kInsideCells<T><<<blocksPass, 256, 0, stream>>>(g, mapView(), view(b), nBricks, small + 15,
+                                                    loOf(b));
     checkLaunch();
     return readU64(small + 15);
+  }
+  int64_t pointData(int b, int64_t *src, double *vel, double *diss, int64_t cap) override {
+    if (b != L - 1 || !pdHas) return -1;
+    buildExchange(b);
+    if (!src || !vel || !diss || xPoints > cap) return xPoints;
+    if (!xPoints) return 0;
+    const int nAlloc = readI32(nSlotsPtr());
+    int64_t *ds = scratch<int64_t>(X_PSRC, xPoints);
+    double *dv = scratch<double>(X_PVEL, xPoints);
+    double *dd = scratch<double>(X_PDISS, xPoints);
+    {
+      Scope sc(this, "point_data");
+      kSegPointData<T><<<grid1((size_t)nAlloc * 64), 256, 0, stream>>>(
+          (const int *)xs[X_OB].p, nAlloc, brickMap, (const int4 *)xs[X_BOUNDS].p,
+          buf[b].def[buf[b].cur], (const uint32_t *)xs[X_P].p, pdCells, ds, dv, dd);
+      checkLaunch();
+    }
+    VLSG_CUDA(cudaMemcpyAsync(src, ds, xPoints * sizeof(int64_t), cudaMemcpyDeviceToHost, stream));
+    VLSG_CUDA(cudaMemcpyAsync(vel, dv, xPoints * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    VLSG_CUDA(cudaMemcpyAsync(diss, dd, xPoints * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    VLSG_CUDA(cudaStreamSynchronize(stream));
+    return xPoints;
   }
   int64_t surfaceNodes(int b, double **nodes, uint64_t **keys) override {
     buildExchange(b);
@@ -1591,13 +1748,13 @@ public:
     VLSG_CUDA(cudaMalloc(&off, std::max<int64_t>(n, 1) * sizeof(uint32_t)));
     VLSG_CUDA(cudaMalloc(&sums, (scanScratch(n) + 64) * sizeof(uint32_t)));
     kSurfaceNodes<T><<<grid1(n), 256, 0, stream>>>(g, mapView(), view(b), idx, val, n, cnt, nullptr,
-                                                   nullptr, nullptr);
+                                                   nullptr, nullptr, loOf(b));
     scanExclusive(cnt, off, n, sums);
     const int64_t m = scanTotal(sums, n);
     VLSG_CUDA(cudaMalloc(nodes, std::max<int64_t>(m, 1) * 3 * sizeof(double)));
     VLSG_CUDA(cudaMalloc(keys, std::max<int64_t>(m, 1) * sizeof(uint64_t)));
     kSurfaceNodes<T><<<grid1(n), 256, 0, stream>>>(g, mapView(), view(b), idx, val, n, cnt, off,
-                                                   *nodes, *keys);
+                                                   *nodes, *keys, loOf(b));
     checkLaunch();
     VLSG_CUDA(cudaStreamSynchronize(stream));
     cudaFree(cnt);

@@ -128,7 +128,8 @@ template <class T>
 __global__ void kSegScatter(GridDev g, const int *ob, int nAlloc, const int *brickMap,
                             const int *nbr, const int4 *bounds, const uint64_t *def,
                             const T *vals, const uint32_t *P, RunBox rb, int32_t *idxOut,
-                            double *valOut, uint32_t *GC, uint32_t *rowCount, uint32_t *rowGaps) {
+                            double *valOut, uint32_t *GC, uint32_t *rowCount, uint32_t *rowGaps,
+                            const float *lo) {
   const size_t nSeg = (size_t)nAlloc * 64;
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < nSeg;
        e += (size_t)gridDim.x * blockDim.x) {
@@ -157,7 +158,9 @@ __global__ void kSegScatter(GridDev g, const int *ob, int nAlloc, const int *bri
       idxOut[3 * (size_t)pos + 0] = x0 + lx;
       idxOut[3 * (size_t)pos + 1] = y;
       idxOut[3 * (size_t)pos + 2] = z;
-      valOut[pos] = (double)vals[(size_t)slot * BV + lz * 64 + ly * 8 + lx];
+      const size_t q = (size_t)slot * BV + lz * 64 + ly * 8 + lx;
+      // with a compensation term the value is hi + lo
+      valOut[pos] = lo ? withLo((double)vals[q], lo[q]) : (double)vals[q];
       ++pos;
       const bool adjacent = lx < 7 ? ((byte >> (lx + 1)) & 1u) : nextFirst;
       gaps += adjacent ? 0u : 1u;

@@ -59,11 +59,22 @@ struct Topo {
   int *err;
 };
 
+// Point data carried by the cells of the top level set (null arrays: none):
+// the source id of the data a defined cell carries (the index of a point at
+// the start of the advection, -1: none) and the saved advection velocity and
+// dissipation (lsAdvect.hpp:780-796).  In a change log the same arrays hold
+// the data of each logged cell.
+template <class T> struct Payload {
+  int32_t *src;
+  T *vel, *diss;
+};
+
 template <class T> struct LsView {
   T *vals;               // slots x 512 cells, in place
   const uint64_t *def;   // current masks, slots x 8 words
   uint64_t *defNext;     // masks after the pass
   const int8_t *farSign; // per brick of the map box
+  Payload<T> pd;         // point data per cell, or null arrays
 };
 
 // Change log: segment w (of `per` entries) belongs to warp w of the pass.
@@ -72,7 +83,23 @@ template <class T> struct ChangeLog {
   T *val;
   int *count;     // entries per segment
   size_t per;
+  Payload<T> pd;  // point data per entry (with a view that carries it)
 };
+
+// Point data of the value a rule produced: src -1 keeps the centre's, 0..5
+// takes star neighbour src's (cell loc of slot ref), -2 none.
+template <class T>
+__device__ inline void payloadOf(const Payload<T> &pd, size_t centre, int src, int ref, int loc,
+                                 int32_t &s, T &v, T &d) {
+  if (src == -1) {
+    s = pd.src[centre], v = pd.vel[centre], d = pd.diss[centre];
+  } else if (src >= 0 && ref >= 0) {
+    const size_t q = (size_t)ref * BV + loc;
+    s = pd.src[q], v = pd.vel[q], d = pd.diss[q];
+  } else {
+    s = -1, v = T(0), d = T(0);
+  }
+}
 
 template <class T> __device__ inline T sentinel(bool neg) {
   return neg ? Lim<T>::lowest() : Lim<T>::max();
@@ -240,24 +267,85 @@ __device__ inline void markCell(unsigned long long *words, int c) {
   atomicOr(reinterpret_cast<unsigned *>(words) + (c >> 5), 1u << (c & 31));
 }
 
-// Append the lanes with `has` to the warp's log segment (warp-uniform call).
+// Append the lanes with `has` to the warp's log segment (warp-uniform call),
+// with the point data (ps, pv, pdi) when the log carries it.
 template <class T>
 __device__ inline void logChange(const ChangeLog<T> &lg, size_t base, int &count, bool has,
-                                 uint32_t cell, T val) {
+                                 uint32_t cell, T val, int32_t ps = -1, T pv = T(0),
+                                 T pdi = T(0)) {
   const unsigned m = __ballot_sync(0xffffffffu, has);
   if (has) {
     const size_t p = base + count + __popc(m & ((1u << (threadIdx.x & 31)) - 1));
     lg.cell[p] = cell;
     lg.val[p] = val;
+    if (lg.pd.src) lg.pd.src[p] = ps, lg.pd.vel[p] = pv, lg.pd.diss[p] = pdi;
   }
   count += __popc(m);
 }
 
 enum : int { FP_EXPAND = 0, FP_PRUNE = 1, FP_ALL = 2 };
 
-// One star pass of a rule.  MODE picks the candidates: FP_EXPAND undefined
-// cells next to a defined one, FP_PRUNE the defined cells, FP_ALL the
-// defined cells and their neighbours.
+// One brick of a star pass of a rule (one warp): candidates, evaluation,
+// change log, new masks and visit flags.  MODE picks the candidates:
+// FP_EXPAND undefined cells next to a defined one, FP_PRUNE the defined
+// cells, FP_ALL the defined cells and their neighbours.
+template <class T, int MODE, class Rule>
+__device__ inline void frontierBrick(const Topo &t, const LsView<T> &v, const Rule &rule,
+                                     const ChangeLog<T> &lg, WarpScratch &ws, int slot,
+                                     bool complex, uint64_t own, size_t logBase, int &logged,
+                                     uint8_t *visitOut, bool &zeroHit) {
+  const int lane = threadIdx.x & 31;
+  beginBrick(t, ws, slot, lane);
+  int x0 = 0, y0 = 0, z0 = 0;
+  if (complex) brickOrigin(t, slot, x0, y0, z0);
+  uint64_t cand;
+  if (MODE == FP_PRUNE) {
+    cand = own;
+  } else if (complex) {
+    const uint64_t ex = lane < 8 ? existPlane(t.g, x0, y0, z0, lane) : 0ull;
+    cand = MODE == FP_EXPAND ? ex & ~own : ex;
+  } else {
+    const uint64_t dil = dilatedMask(t, v.def, slot, ws.nb, lane);
+    cand = MODE == FP_EXPAND ? dil & ~own : dil;
+  }
+  const int total = __any_sync(0xffffffffu, cand != 0ull) ? listCells(cand, ws.list) : 0;
+  for (int base = 0; base < total; base += 32) {
+    const int k = base + lane;
+    bool changed = false;
+    T out = T(0);
+    int c = 0;
+    int32_t ps = -1;
+    T pv = T(0), pdi = T(0);
+    if (k < total) {
+      c = ws.list[k];
+      const T center = v.vals[(size_t)slot * BV + c];
+      if (MODE == FP_PRUNE && center == T(0)) zeroHit = true;
+      T nb[6];
+#pragma unroll
+      for (int j = 0; j < 6; ++j) {
+        int loc;
+        const int ref = starRef(t, ws.nb, slot, complex, x0, y0, z0, c, j, loc);
+        nb[j] = refValue<T>(v.vals, v.farSign, ref, loc);
+      }
+      int src = -1;
+      out = rule(center, nb, src);
+      changed = out != center || signbit(out) != signbit(center);
+      if (changed && isDef(out) != isDef(center)) markCell(ws.flip, c);
+      // with point data a value taken from a neighbour is logged even when
+      // it equals the old one: its data changes
+      if (lg.pd.src && isDef(out) && src >= 0) changed = true;
+      if (changed && lg.pd.src && isDef(out)) {
+        int loc = 0, ref = -1;
+        if (src >= 0) ref = starRef(t, ws.nb, slot, complex, x0, y0, z0, c, src, loc);
+        payloadOf<T>(v.pd, (size_t)slot * BV + c, src, ref, loc, ps, pv, pdi);
+      }
+    }
+    logChange<T>(lg, logBase, logged, changed, ((uint32_t)slot << 9) | (uint32_t)c, out, ps, pv,
+                 pdi);
+  }
+  finishBrick(ws, v.defNext, slot, lane, own, visitOut);
+}
+
 template <class T, int MODE, class Rule>
 __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
     kFrontierPass(Topo t, LsView<T> v, Rule rule, ChangeLog<T> lg, const uint8_t *visitIn,
@@ -301,43 +389,8 @@ __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
       if (lane < 8) v.defNext[(size_t)slot * 8 + lane] = 0ull;
       continue;
     }
-    beginBrick(t, ws, slot, lane);
-    int x0 = 0, y0 = 0, z0 = 0;
-    if (complex) brickOrigin(t, slot, x0, y0, z0);
-    uint64_t cand;
-    if (MODE == FP_PRUNE) {
-      cand = own;
-    } else if (complex) {
-      const uint64_t ex = lane < 8 ? existPlane(t.g, x0, y0, z0, lane) : 0ull;
-      cand = MODE == FP_EXPAND ? ex & ~own : ex;
-    } else {
-      const uint64_t dil = dilatedMask(t, v.def, slot, ws.nb, lane);
-      cand = MODE == FP_EXPAND ? dil & ~own : dil;
-    }
-    const int total = __any_sync(0xffffffffu, cand != 0ull) ? listCells(cand, ws.list) : 0;
-    for (int base = 0; base < total; base += 32) {
-      const int k = base + lane;
-      bool changed = false;
-      T out = T(0);
-      int c = 0;
-      if (k < total) {
-        c = ws.list[k];
-        const T center = v.vals[(size_t)slot * BV + c];
-        if (MODE == FP_PRUNE && center == T(0)) zeroHit = true;
-        T nb[6];
-#pragma unroll
-        for (int j = 0; j < 6; ++j) {
-          int loc;
-          const int ref = starRef(t, ws.nb, slot, complex, x0, y0, z0, c, j, loc);
-          nb[j] = refValue<T>(v.vals, v.farSign, ref, loc);
-        }
-        out = rule(center, nb);
-        changed = out != center || signbit(out) != signbit(center);
-        if (changed && isDef(out) != isDef(center)) markCell(ws.flip, c);
-      }
-      logChange<T>(lg, logBase, logged, changed, ((uint32_t)slot << 9) | (uint32_t)c, out);
-    }
-    finishBrick(ws, v.defNext, slot, lane, own, visitOut);
+    frontierBrick<T, MODE, Rule>(t, v, rule, lg, ws, slot, complex, own, logBase, logged, visitOut,
+                                 zeroHit);
   }
   if (lane == 0) lg.count[warp] = logged;
   if (MODE == FP_PRUNE && zeroMode == 1 && __any_sync(0xffffffffu, zeroHit) && lane == 0)
@@ -345,9 +398,12 @@ __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
 }
 
 // Write a change log back: warp w copies segment w.
+// `lo` (FP32 buffers that carry a compensation term, else null): a cell a
+// pass changed holds a value computed from the stored values alone, so its
+// compensation term becomes 0.
 template <class T>
 __global__ void __launch_bounds__(FRONTIER_THREADS)
-    kApplyChanges(T *vals, ChangeLog<T> lg, int segments) {
+    kApplyChanges(T *vals, ChangeLog<T> lg, int segments, float *lo, Payload<T> pd) {
   // block b takes segments b, b + gridDim.x, ...; its 256 threads stride the
   // entries, four loads in flight per thread
   for (int w = blockIdx.x; w < segments; w += gridDim.x) {
@@ -364,11 +420,25 @@ __global__ void __launch_bounds__(FRONTIER_THREADS)
       }
 #pragma unroll
       for (int k = 0; k < 4; ++k) vals[(size_t)(q[k] >> 9) * BV + (q[k] & 511)] = val[k];
+      if (lo) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) lo[(size_t)(q[k] >> 9) * BV + (q[k] & 511)] = 0.f;
+      }
     }
     for (; i < n; i += blockDim.x) {
       const uint32_t q = lg.cell[base + i];
       vals[(size_t)(q >> 9) * BV + (q & 511)] = lg.val[base + i];
+      if (lo) lo[(size_t)(q >> 9) * BV + (q & 511)] = 0.f;
     }
+    // the point data the pass logged with each value
+    if (pd.src && lg.pd.src)
+      for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        const uint32_t q = lg.cell[base + j];
+        const size_t c = (size_t)(q >> 9) * BV + (q & 511);
+        pd.src[c] = lg.pd.src[base + j];
+        pd.vel[c] = lg.pd.vel[base + j];
+        pd.diss[c] = lg.pd.diss[base + j];
+      }
   }
 }
 
@@ -427,6 +497,8 @@ __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
       bool changed = false;
       T out = T(0);
       int c = 0;
+      int32_t ps = -1;
+      T pv = T(0), pdi = T(0);
       if (k < total) {
         c = ws.list[k];
         const T mem = v.vals[(size_t)slot * BV + c];
@@ -438,11 +510,19 @@ __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
           const int ref = starRef(t, ws.nb, slot, complex, x0, y0, z0, c, j, loc);
           nb[j] = reducedValue<T>(v.vals, act, ws.aux, v.farSign, slot, ref, loc);
         }
-        out = rule(center, nb);
+        int src = -1;
+        out = rule(center, nb, src);
         changed = out != mem || signbit(out) != signbit(mem);
         if (changed && isDef(out) != isDef(mem)) markCell(ws.flip, c);
+        if (lg.pd.src && isDef(out) && src >= 0) changed = true;
+        if (changed && lg.pd.src && isDef(out)) {
+          int loc = 0, ref = -1;
+          if (src >= 0) ref = starRef(t, ws.nb, slot, complex, x0, y0, z0, c, src, loc);
+          payloadOf<T>(v.pd, (size_t)slot * BV + c, src, ref, loc, ps, pv, pdi);
+        }
       }
-      logChange<T>(lg, logBase, logged, changed, ((uint32_t)slot << 9) | (uint32_t)c, out);
+      logChange<T>(lg, logBase, logged, changed, ((uint32_t)slot << 9) | (uint32_t)c, out, ps,
+                   pv, pdi);
     }
     // defined cells away from the active ones: undefined with their sign,
     // written in place (32 consecutive cells per step)
@@ -469,7 +549,7 @@ __global__ void __launch_bounds__(FRONTIER_THREADS, VLSG_PASS_MIN_BLOCKS)
 // set when the comparator reports a move (combineLevelSets).
 template <class T, class Comp>
 __global__ void __launch_bounds__(FRONTIER_THREADS)
-    kPointwise(Topo t, T *av, uint64_t *adef, const T *bv, Comp comp, int *flag) {
+    kPointwise(Topo t, T *av, uint64_t *adef, const T *bv, Comp comp, int *flag, float *alo) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nWarps = (gridDim.x * blockDim.x) >> 5;
@@ -494,7 +574,10 @@ __global__ void __launch_bounds__(FRONTIER_THREADS)
           mv = false;
         }
         moved |= mv;
-        if (o != a || signbit(o) != signbit(a)) av[q] = o;
+        if (o != a || signbit(o) != signbit(a)) {
+          av[q] = o;
+          if (alo) alo[q] = 0.f;
+        }
         bits |= (uint64_t)__ballot_sync(0xffffffffu, isDef(o)) << (32 * half);
       }
       if (lane == z) mine = bits;
@@ -507,9 +590,14 @@ __global__ void __launch_bounds__(FRONTIER_THREADS)
 // Pointwise boolean for comparators that keep every undefined cell of A
 // (combineLevelSets, lsAdvect.hpp:218-230): only A's defined cells are read,
 // in place; A's masks lose the cells that became undefined.
+// With compensation terms of both (FP32 buffers: alo for A, blo for B) the
+// comparator sees hi + lo of each value in double and the result is split
+// again into hi and lo (Comp::full); with alo alone a changed value's term
+// becomes 0.
 template <class T, class Comp>
 __global__ void __launch_bounds__(FRONTIER_THREADS)
-    kPointwiseDefined(Topo t, T *av, uint64_t *adef, const T *bv, Comp comp, int *flag) {
+    kPointwiseDefined(Topo t, T *av, uint64_t *adef, const T *bv, Comp comp, int *flag,
+                      float *alo, const float *blo) {
   __shared__ WarpScratch sm[FRONTIER_THREADS / 32];
   WarpScratch &ws = sm[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
@@ -530,10 +618,27 @@ __global__ void __launch_bounds__(FRONTIER_THREADS)
       const size_t q = (size_t)slot * BV + c;
       const T a = av[q];
       bool mv = false;
+      if constexpr (sizeof(T) == 4) {
+        if (alo && blo) {
+          const T b = bv[q];
+          if (isDef(b)) {
+            const double r = comp.full(withLo((double)a, alo[q]), withLo((double)b, blo[q]), mv);
+            const float hi = (float)r;
+            av[q] = hi;
+            alo[q] = (float)(r - (double)hi);
+          } else {
+            av[q] = b;
+            markCell(ws.flip, c);
+          }
+          moved |= mv;
+          continue;
+        }
+      }
       const T o = comp(a, bv[q], mv);
       moved |= mv;
       if (o != a || signbit(o) != signbit(a)) {
         av[q] = o;
+        if (alo) alo[q] = 0.f;
         if (!isDef(o)) markCell(ws.flip, c);
       }
     }
@@ -546,9 +651,12 @@ __global__ void __launch_bounds__(FRONTIER_THREADS)
 
 // Copy the listed slots of one buffer (values and masks) into another, 16
 // bytes per thread.
+// dlo (a compensation array of the destination, or null) receives slo, or
+// zeros when the source has none.
 template <class T>
 __global__ void kCopySlots16(const int *slotList, const int *nSlots, const T *sv,
-                             const uint64_t *sd, T *dv, uint64_t *dd) {
+                             const uint64_t *sd, T *dv, uint64_t *dd, const float *slo,
+                             float *dlo) {
   constexpr int PER = BV * sizeof(T) / 16; // 16-byte words per slot
   const size_t n = (size_t)*nSlots * PER;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
@@ -557,6 +665,11 @@ __global__ void kCopySlots16(const int *slotList, const int *nSlots, const T *sv
     const int k = (int)(i % PER);
     reinterpret_cast<uint4 *>(dv + slot * BV)[k] = reinterpret_cast<const uint4 *>(sv + slot * BV)[k];
     if (k < 4) reinterpret_cast<uint4 *>(dd + slot * 8)[k] = reinterpret_cast<const uint4 *>(sd + slot * 8)[k];
+    if (dlo && k < BV * 4 / 16) {
+      const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+      reinterpret_cast<uint4 *>(dlo + slot * BV)[k] =
+          slo ? reinterpret_cast<const uint4 *>(slo + slot * BV)[k] : z;
+    }
   }
 }
 

@@ -142,6 +142,15 @@ public:
   virtual void finalizeStencilLLF() = 0;
   virtual void prepareLS(int spatialScheme) = 0;
   virtual int64_t surfaceNodes(int b, double **nodes, uint64_t **keys) = 0;
+  // sharding: owned slab (axis -1: all) and the cross-shard reduction
+  int ownAxis = -1;
+  int64_t ownLo = 0, ownHi = 0;
+  vlsg_reduce_cb reduceCb = nullptr;
+  void *reduceUser = nullptr;
+  // Point data of level set b in download order (source id, saved velocity
+  // and dissipation); returns the number of points, or -1 when the level set
+  // carries no point data.  Nothing is written when cap is too small.
+  virtual int64_t pointData(int b, int64_t *src, double *vel, double *diss, int64_t cap) = 0;
 };
 
 EngineBase *makeEngineF32();

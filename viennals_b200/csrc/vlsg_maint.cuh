@@ -355,7 +355,7 @@ __global__ void kInitFreeStack(int *freeStack, int cap) {
 
 template <class T>
 __global__ void kScatterPoints(GridDev g, int n, const int *idx, const double *v,
-                               const int *brickMap, T *vals, int *err) {
+                               const int *brickMap, T *vals, int *err, float *lo) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int rx = idx[3 * i] - g.org[0], ry = idx[3 * i + 1] - g.org[1],
               rz = idx[3 * i + 2] - g.org[2];
@@ -369,7 +369,11 @@ __global__ void kScatterPoints(GridDev g, int n, const int *idx, const double *v
       atomicOr(err, 4);
       continue;
     }
-    vals[(size_t)slot * BV + ((rz & 7) * 64 + (ry & 7) * 8 + (rx & 7))] = T(v[i]);
+    const size_t q = (size_t)slot * BV + ((rz & 7) * 64 + (ry & 7) * 8 + (rx & 7));
+    const T hi = T(v[i]);
+    vals[q] = hi;
+    // the part of the uploaded double that the storage type drops
+    if (lo) lo[q] = (float)(v[i] - (double)hi);
   }
 }
 
@@ -417,12 +421,17 @@ __global__ void kMasksFromValues(GridDev g, const int *slotBrick, const int *slo
   }
 }
 
+// `lo`: compensation terms of the buffer (or null), added to defined values.
 template <class T>
 __global__ void kQueryValues(GridDev g, MapView m, Buf<T> b, int n, const int *idx,
-                             double *out) {
+                             double *out, const float *lo) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const T v = cellValueRaw<T>(g, m, b, idx[3 * i], idx[3 * i + 1], idx[3 * i + 2]);
-    out[i] = isDef(v) ? (double)v : (v < 0 ? -DBL_MAX : DBL_MAX);
+    const int x = mapCoord(g, 0, idx[3 * i]), y = mapCoord(g, 1, idx[3 * i + 1]),
+              z = mapCoord(g, 2, idx[3 * i + 2]);
+    const T v = cellValue<T>(g, m, b, x, y, z);
+    double r = isDef(v) ? (double)v : (v < 0 ? -DBL_MAX : DBL_MAX);
+    if (lo && isDef(v)) r = withLo(r, lo[cellIndex(g, m, x, y, z)]);
+    out[i] = r;
   }
 }
 
@@ -459,12 +468,13 @@ __global__ void kFillSlots(const int *slotList, const int *nSlots, T *vals, uint
 // the listed slots negated (sentinels swap sign), and every far sign.
 template <class T>
 __global__ void kNegateSlots(const int *slotList, const int *nSlots, T *vals, int8_t *farSign,
-                             int nBricks) {
+                             int nBricks, float *lo) {
   const size_t n = (size_t)*nSlots * BV;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
     const size_t slot = slotList[i / BV];
     vals[slot * BV + i % BV] = -vals[slot * BV + i % BV];
+    if (lo) lo[slot * BV + i % BV] = -lo[slot * BV + i % BV];
   }
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nBricks; b += gridDim.x * blockDim.x)
     farSign[b] = (int8_t)-farSign[b];

@@ -27,7 +27,7 @@ namespace { // internal linkage: every compilation unit has its own copy
 // sign is decided at once).
 template <class T>
 __global__ void kInsideCells(GridDev g, MapView m, Buf<T> b, int nBricks,
-                             unsigned long long *count) {
+                             unsigned long long *count, const float *lo) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nWarps = (gridDim.x * blockDim.x) >> 5;
@@ -63,7 +63,7 @@ __global__ void kInsideCells(GridDev g, MapView m, Buf<T> b, int nBricks,
       if (!cellExists(g, x, y, z)) continue;
       double sum = 0;
       for (int k = 0; k < 8; ++k)
-        sum += (double)cellValueRaw<T>(g, m, b, x + (k & 1), y + ((k >> 1) & 1), z + (k >> 2));
+        sum += cellValueFull<T>(g, m, b, lo, x + (k & 1), y + ((k >> 1) & 1), z + (k >> 2));
       inside += (sum / 8.0 <= 0.0) ? 1 : 0;
     }
   }
@@ -76,7 +76,7 @@ __global__ void kInsideCells(GridDev g, MapView m, Buf<T> b, int nBricks,
 template <class T>
 __global__ void kSurfaceNodes(GridDev g, MapView m, Buf<T> b, const int32_t *idx,
                               const double *val, int64_t n, uint32_t *cnt, const uint32_t *off,
-                              double *nodes, uint64_t *nodeKeys) {
+                              double *nodes, uint64_t *nodeKeys, const float *lo) {
   for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n;
        p += (int64_t)gridDim.x * blockDim.x) {
     const int c[3] = {idx[3 * p], idx[3 * p + 1], idx[3 * p + 2]};
@@ -85,7 +85,8 @@ __global__ void kSurfaceNodes(GridDev g, MapView m, Buf<T> b, const int32_t *idx
     for (int dir = 0; dir < 3; ++dir) {
       const T v1 = cellValueRaw<T>(g, m, b, c[0] + (dir == 0), c[1] + (dir == 1), c[2] + (dir == 2));
       if (!isDef(v1)) continue;
-      const double d1 = (double)v1;
+      const double d1 =
+          cellValueFull<T>(g, m, b, lo, c[0] + (dir == 0), c[1] + (dir == 1), c[2] + (dir == 2));
       if ((d0 >= 0.) == (d1 >= 0.)) continue;
       if (nodes) {
         double pos[3] = {(double)c[0], (double)c[1], (double)c[2]};

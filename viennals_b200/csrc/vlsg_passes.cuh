@@ -17,22 +17,25 @@
 namespace vlsg {
 namespace { // internal linkage: every compilation unit has its own copy
 
+// Every rule also names the cell whose point data its result carries (the
+// source ids of the reference's passes): src -1 the centre, 0..5 star
+// neighbour src, -2 none.
 template <class T> struct ExpandRule {
   T totalLimit, limit;
-  __device__ T operator()(T c, const T *nb) const {
+  __device__ T operator()(T c, const T *nb, int &src) const {
     if (fabs(c) <= totalLimit) return c;
     if (c > -Lim<T>::eps()) {
       T distance = Lim<T>::max();
       for (int i = 0; i < 6; ++i) {
         const T nv = nb[i] + T(1);
-        if (distance > nv) distance = nv;
+        if (distance > nv) distance = nv, src = i;
       }
       return distance <= limit ? distance : Lim<T>::max();
     }
     T distance = Lim<T>::lowest();
     for (int i = 0; i < 6; ++i) {
       const T nv = nb[i] - T(1);
-      if (distance < nv) distance = nv;
+      if (distance < nv) distance = nv, src = i;
     }
     return distance >= -limit ? distance : Lim<T>::lowest();
   }
@@ -42,7 +45,7 @@ template <class T> struct PruneRule {
   bool removeStrayZeros;
   __device__ static bool neg(T a) { return a <= -Lim<T>::eps(); }
   __device__ static bool diff(T a, T b) { return neg(a) != neg(b); }
-  __device__ T operator()(T c, const T *nb) const {
+  __device__ T operator()(T c, const T *nb, int &src) const {
     const bool cneg = neg(c);
     if (!isDef(c)) return cneg ? Lim<T>::lowest() : Lim<T>::max();
     bool keep = true;
@@ -61,7 +64,11 @@ template <class T> struct PruneRule {
       for (int i = 0; i < 3; ++i) {
         const T a = nb[i], b = nb[3 + i];
         const bool monotone = a == T(0) || b == T(0) || diff(a, b);
-        if (!monotone) return fabs(a) < fabs(b) ? a : b;
+        // inserted without a data id by the reference (lsPrune.hpp:150-155)
+        if (!monotone) {
+          src = -2;
+          return fabs(a) < fabs(b) ? a : b;
+        }
       }
     }
     if (keep) return c;
@@ -71,7 +78,7 @@ template <class T> struct PruneRule {
 
 template <class T> struct RebuildRule {
   double cutoff;
-  __device__ T operator()(T cT, const T *nb) const {
+  __device__ T operator()(T cT, const T *nb, int &src) const {
     const double c = (double)cT;
     if (fabs(c) <= 1.0) {
       int k = 0;
@@ -82,11 +89,13 @@ template <class T> struct RebuildRule {
           int j = 0;
           for (; j < 6; j++)
             if (fabs((double)nb[j]) <= 1.0 && (double)nb[j] < -0.5) break;
+          if (j != 6) src = j;
           return j == 6 ? cT : T(0.5);
         } else if (c < -0.5) {
           int j = 0;
           for (; j < 6; j++)
             if (fabs((double)nb[j]) <= 1.0 && (double)nb[j] > 0.5) break;
+          if (j != 6) src = j;
           return j == 6 ? cT : T(-0.5);
         }
         return cT;
@@ -98,7 +107,7 @@ template <class T> struct RebuildRule {
       for (int i = 0; i < 6; i++) {
         const double v = (double)nb[i];
         if (fabs(v) <= 1.0 && (v < 0.))
-          if ((double)distance > v + 1.0) distance = T(v + 1.0);
+          if ((double)distance > v + 1.0) distance = T(v + 1.0), src = i;
       }
       return (double)distance <= cutoff ? distance : Lim<T>::max();
     }
@@ -106,7 +115,7 @@ template <class T> struct RebuildRule {
     for (int i = 0; i < 6; i++) {
       const double v = (double)nb[i];
       if (fabs(v) <= 1.0 && (v > 0))
-        if ((double)distance < v - 1.0) distance = T(v - 1.0);
+        if ((double)distance < v - 1.0) distance = T(v - 1.0), src = i;
     }
     return (double)distance >= -cutoff ? distance : Lim<T>::lowest();
   }
@@ -154,6 +163,13 @@ template <class T> struct CombineComp {
     }
     if (!isDef(a)) return a;
     return b;
+  }
+  // both defined, as hi + lo sums in double (FP32 buffers with compensation
+  // terms): the stage combination without rounding to the storage type
+  __device__ double full(double a, double b, bool &moved) const {
+    const double res = wSource * a + wTarget * b;
+    if (res > b) moved = true;
+    return res;
   }
 };
 

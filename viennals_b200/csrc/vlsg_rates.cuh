@@ -134,6 +134,7 @@ template <class T> struct RateArgs {
   // outputs: chain entry j of cell q at j * poolCells + q
   T *rateV;
   T *rateStop;
+  T *rateD; // the dissipation per chain entry (setSaveAdvectionVelocities), or null
   uint8_t *rateLen;
   size_t poolCells;
   unsigned long long *minStep;  // bits of the smallest non-negative step
@@ -155,6 +156,10 @@ template <class T> struct RateArgs {
   double *sllfAlpha;
   // setIgnoreVoids: void bits of the top level set (no rates there), or none
   const uint64_t *voidMask;
+  // sharding: only points with z in [ownLo, ownHi) count towards the time
+  // step, the alphas and the point updates (ownZ false: every point)
+  bool ownZ;
+  int ownLo, ownHi;
 };
 
 // Reader of the top level set around one active point.
@@ -730,6 +735,7 @@ __device__ inline double ratePoint(const RateArgs<T> &A, const Vel &vel,
     }
     A.rateV[(size_t)len * A.poolCells + q] = veff;
     A.rateStop[(size_t)len * A.poolCells + q] = stop;
+    if (A.rateD) A.rateD[(size_t)len * A.poolCells + q] = d;
     ++len;
     if (done) break;
   }
@@ -806,10 +812,19 @@ __global__ void __launch_bounds__(RATE_THREADS, rateMinBlocks<T, FAM>())
     const uint64_t own = lane < 8 ? A.def[(size_t)slot * 8 + lane] : 0ull;
     uint64_t a = 0ull;
     if (__any_sync(0xffffffffu, own != 0ull)) a = activePlanes<T>(top.vals, slot);
+    int z0 = 0;
+    if (A.ownZ) {
+      int bx, by, bz;
+      brickCoords(A.g, A.m.slotBrick[slot], bx, by, bz);
+      z0 = A.g.org[2] + bz * BS;
+    }
     if (lane < 8) {
       if (MODE == 0) A.act[(size_t)slot * 8 + lane] = a;
-      nAct += __popcll(a);
-      nBand += __popcll(own);
+      const bool planeOwned = !A.ownZ || (z0 + lane >= A.ownLo && z0 + lane < A.ownHi);
+      if (planeOwned) {
+        nAct += __popcll(a);
+        nBand += __popcll(own);
+      }
     }
     const int total = listCells(a, list);
     for (int base = 0; base < total; base += 32) {
@@ -824,6 +839,7 @@ __global__ void __launch_bounds__(RATE_THREADS, rateMinBlocks<T, FAM>())
         else
           return FunctorVel{desc};
       }();
+      const bool owned = !A.ownZ || (z0 + (c >> 6) >= A.ownLo && z0 + (c >> 6) < A.ownHi);
       withStencil<T>(A, slot, c, [&](const auto &S, T value) {
         if constexpr (MODE == 0) {
           constexpr bool STENCIL = FAM == FAM_STENCIL;
@@ -831,6 +847,7 @@ __global__ void __launch_bounds__(RATE_THREADS, rateMinBlocks<T, FAM>())
           const double step =
               ratePoint<T, std::decay_t<decltype(S)>, std::decay_t<decltype(vel)>, FAM>(
                   A, vel, S, slot, c, value, alphas);
+          if (!owned) return; // a ghost point: advanced, not counted
           const unsigned long long sb = stepBits(step);
           minBits = sb < minBits ? sb : minBits;
           if constexpr (STENCIL) {
@@ -868,11 +885,12 @@ __global__ void __launch_bounds__(RATE_THREADS, rateMinBlocks<T, FAM>())
             for (int d = 0; d < 3; ++d) normal[d] *= normalModulus;
             T scaVel, vecVel[3];
             vel.get(lower, normal, 0, scaVel, vecVel);
-            for (int d = 0; d < 3; ++d) {
-              const unsigned long long ab =
-                  alphaBits((double)fabs((scaVel + vecVel[d]) * normal[d]));
-              alphaMax[d] = ab > alphaMax[d] ? ab : alphaMax[d];
-            }
+            if (owned)
+              for (int d = 0; d < 3; ++d) {
+                const unsigned long long ab =
+                    alphaBits((double)fabs((scaVel + vecVel[d]) * normal[d]));
+                alphaMax[d] = ab > alphaMax[d] ? ab : alphaMax[d];
+              }
             break;
           }
         }
@@ -937,11 +955,17 @@ __global__ void __launch_bounds__(1024)
 // Value update of updateLevelSet (lsAdvect.hpp:725-777) for every active
 // point, in place on the top level set (the Reduce(1) part is applied by the
 // rebuild pass that follows).
+// `lo` (FP32 top level set with a compensation term, else null): the value is
+// hi + lo, the update and the stop-chain walk run in double and the result is
+// split into hi and lo again.
+// pvel/pdiss (setSaveAdvectionVelocities, else null): each updated point's
+// last leg rate (time x velocity) and the dissipation of the chain entry it
+// ended on (rateD), lsAdvect.hpp:764-767.
 template <class T>
 __global__ void __launch_bounds__(RATE_THREADS)
     kUpdate(const int *slotList, const int *nSlots, const uint64_t *act, T *vals,
             const T *rateV, const T *rateStop, const uint8_t *rateLen, size_t poolCells, int L,
-            double dt, int *err) {
+            double dt, int *err, float *lo, T *pvel, T *pdiss, const T *rateD) {
   __shared__ uint16_t sList[RATE_THREADS / 32][BV];
   uint16_t *list = sList[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
@@ -958,12 +982,42 @@ __global__ void __launch_bounds__(RATE_THREADS)
       if (k >= total) continue;
       const int c = list[k];
       const size_t q = (size_t)slot * BV + c;
-      T value = vals[q];
       int len = rateLen[q];
       if (len < 1 || len > L) {
         atomicOr(err, 2);
         len = 1;
       }
+      if constexpr (sizeof(T) == 4) {
+        if (lo) {
+          double value = withLo((double)vals[q], lo[q]);
+          double time = dt;
+          int j = 0;
+          double velocity = rateV[q];
+          double rate = time * velocity;
+          while (fabs((double)rateStop[(size_t)j * poolCells + q] - value) < fabs(rate)) {
+            const double stop = rateStop[(size_t)j * poolCells + q];
+            time -= fabs((stop - value) / velocity);
+            value = stop;
+            ++j;
+            if (j >= len) {
+              atomicOr(err, 2);
+              break;
+            }
+            velocity = rateV[(size_t)j * poolCells + q];
+            rate = time * velocity;
+          }
+          value -= rate;
+          const float hi = (float)value;
+          vals[q] = hi;
+          lo[q] = (float)(value - (double)hi);
+          if (pvel) {
+            const int jj = j < len ? j : len - 1; // j == len only after a chain overrun
+            pvel[q] = T(rate), pdiss[q] = rateD[(size_t)jj * poolCells + q];
+          }
+          continue;
+        }
+      }
+      T value = vals[q];
       double time = dt;
       int j = 0;
       T velocity = rateV[q];
@@ -982,6 +1036,10 @@ __global__ void __launch_bounds__(RATE_THREADS)
       }
       value -= rate;
       vals[q] = value;
+      if (pvel) {
+        const int jj = j < len ? j : len - 1; // j == len only after a chain overrun
+        pvel[q] = rate, pdiss[q] = rateD[(size_t)jj * poolCells + q];
+      }
     }
   }
 }

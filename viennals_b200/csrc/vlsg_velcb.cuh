@@ -23,6 +23,7 @@
 #pragma once
 
 #include "vlsg_exchange.cuh"
+#include "vlsg_frontier.cuh"
 #include "vlsg_rates.cuh"
 
 namespace vlsg {
@@ -337,6 +338,48 @@ __global__ void __launch_bounds__(RATE_THREADS)
             }
         }
       });
+    }
+  }
+}
+
+// Point data at the start of an advection: every defined cell of the top
+// level set carries its own rank in download order, no saved velocity.
+template <class T>
+__global__ void kInitPointData(const int *slotList, const int *nSlots, const uint64_t *def,
+                               PointRanks R, Payload<T> pd) {
+  const size_t n = (size_t)*nSlots * BV;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const int slot = slotList[i / BV];
+    const int c = (int)(i % BV);
+    if (!((def[(size_t)slot * 8 + (c >> 6)] >> (c & 63)) & 1ull)) continue;
+    const size_t q = (size_t)slot * BV + c;
+    pd.src[q] = (int32_t)R.of(slot, c);
+    pd.vel[q] = T(0);
+    pd.diss[q] = T(0);
+  }
+}
+
+// Point data of the defined cells in download order (the exchange layout of
+// kSegScatter: segment offsets P, x order within a segment).
+template <class T>
+__global__ void kSegPointData(const int *ob, int nAlloc, const int *brickMap, const int4 *bounds,
+                              const uint64_t *def, const uint32_t *P, Payload<T> pd,
+                              int64_t *srcOut, double *velOut, double *dissOut) {
+  const size_t nSeg = (size_t)nAlloc * 64;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < nSeg;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(e >> 6), lz = (int)(e >> 3) & 7, ly = (int)e & 7;
+    const int slot = brickMap[ob[i]];
+    const unsigned byte = segByte(def, slot, lz, ly);
+    if (!byte) continue;
+    uint32_t pos = P[segmentRank(bounds[i], i, lz, ly)];
+    for (unsigned m = byte; m; m &= m - 1) {
+      const size_t q = (size_t)slot * BV + lz * 64 + ly * 8 + (__ffs(m) - 1);
+      srcOut[pos] = pd.src[q];
+      velOut[pos] = (double)pd.vel[q];
+      dissOut[pos] = (double)pd.diss[q];
+      ++pos;
     }
   }
 }

@@ -73,6 +73,8 @@ class Domain:
         self.run_sign = (np.zeros(0, np.int8) if run_sign is None
                          else np.ascontiguousarray(run_sign, np.int8))
         self.width = int(width)
+        # Domain::getPointData(): scalar arrays per defined point, by label
+        self.point_data = {}
 
     @property
     def n_points(self):
