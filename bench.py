@@ -246,6 +246,8 @@ def run_ours(args, rank, world):
     ctx.close()
     if rank == 0 and args.err_steps > 0:
         out["precision_report"] = precision_report(args, grid, dom, vel, p, stream)
+    if rank == 0 and args.batch_domains > 0:
+        out["batching"] = batching_report(args, f"cuda:{args.local_rank}")
     return out
 
 
@@ -262,7 +264,8 @@ def precision_report(args, grid, dom, vel, p, stream):
 
     res = {}
 
-    def run(prec):
+    def run(prec, compensation=0):
+        p.fp32_compensation = compensation
         c = Context(args.local_rank, prec)
         c.set_stream(stream.cuda_stream)
         c.set_grid(grid)
@@ -288,16 +291,36 @@ def precision_report(args, grid, dom, vel, p, stream):
     c32, res["fp32"] = run(Precision.FP32)
     out32 = c32.download_domain(0, grid)
     c32.close()
+    c32c, res["fp32c"] = run(Precision.FP32, 1)
+    out32c = c32c.download_domain(0, grid)
+    c32c.close()
+    p.fp32_compensation = 0
     c64, res["fp64"] = run(Precision.FP64)
-    c32 = Context(args.local_rank, Precision.FP32)
-    c32.set_grid(grid)
-    c32.set_level_set_count(1)
-    c32.upload(0, out32)
-    r = c32.compare(0, c64, 0)
-    c32.close()
+
+    def against64(dom):
+        c = Context(args.local_rank, Precision.FP64)  # the FP32 result, exactly
+        c.set_grid(grid)
+        c.set_level_set_count(1)
+        c.upload(0, dom)
+        r = c.compare(0, c64, 0)
+        c.close()
+        return r
+
+    r = against64(out32)
+    rc = against64(out32c)
     c64.close()
     gd = float(grid.delta)
     vol64, vol32 = r["inside_cells_b"], r["inside_cells_a"]
+    comp = {
+        "fp32_point_updates_per_s": res["fp32c"]["point_updates_per_s"],
+        "fp32_ms_per_step": res["fp32c"]["ms_per_step"],
+        "max_abs_dphi_over_gridDelta": rc["max_abs_diff"],
+        "rms_abs_dphi_over_gridDelta": rc["rms_abs_diff"],
+        "points_with_abs_dphi_above": dict(zip(["1e-6", "1e-5", "1e-4", "1e-3"], rc["diff_above"])),
+        "active_set_differences": rc["active_only_a"] + rc["active_only_b"],
+        "defined_set_differences": rc["defined_only_a"] + rc["defined_only_b"],
+        "chamfer_rms": rc["chamfer_rms"] * gd, "chamfer_max": rc["chamfer_max"] * gd,
+    }
     return {
         "steps": args.err_steps, "against": "FP64 GPU path (bit-identical to the FP64 oracle "
         "in the parity tests)",
@@ -316,7 +339,72 @@ def precision_report(args, grid, dom, vel, p, stream):
         "chamfer_rms": r["chamfer_rms"] * gd, "chamfer_max": r["chamfer_max"] * gd,
         "chamfer_mean": r["chamfer_mean"] * gd, "chamfer_unit": "length (gridDelta x grid units)",
         "surface_nodes_fp32": r["nodes_a"], "surface_nodes_fp64": r["nodes_b"],
+        "compensated": comp,
     }
+
+
+def batching_report(args, device):
+    """The batching form: `args.batch_domains` seeded plane domains with a
+    trench or a hole (bands of 1e4..2e6 points, log-uniform), LLF 1st order,
+    RK2, FP32, per-domain rates in [0.2, 1.5]; one RK2 step of every domain
+    advanced one context after another (loop) and by vlsg_advect_batch (host
+    threads, one stream per context), each set warmed by one step first and
+    timed by the host clock around the step; both sets must end identical."""
+    import torch
+
+    from viennals_b200 import AdvectParams
+    from viennals_b200._abi import Precision
+    from viennals_b200.advect import Context, advect_batch
+    from viennals_b200.synth import batch_domains
+
+    t0 = time.time()
+    doms = batch_domains(args.batch_domains, seed=7, device=device)
+    gen_s = time.time() - t0
+    p = AdvectParams.defaults()
+    p.spatial_scheme = 7  # LOCAL_LAX_FRIEDRICHS_1ST_ORDER
+    p.temporal_scheme = 1  # RUNGE_KUTTA_2ND_ORDER
+    p.advection_time = 0.0
+
+    def contexts():
+        out = []
+        for grid, dom, vel in doms:
+            c = Context(args.local_rank, Precision.FP32)
+            c.set_grid(grid)
+            c.set_level_set_count(1)
+            c.upload(0, dom)
+            c.set_velocity(vel.descriptor())
+            out.append(c)
+        return out
+
+    loop, batch = contexts(), contexts()
+    for c in loop:
+        c.advect(p)
+    advect_batch(batch, p, threads=args.batch_threads)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    upd_loop = sum(c.advect(p).point_updates for c in loop)
+    torch.cuda.synchronize()
+    loop_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    upd_batch = sum(r.point_updates for r in advect_batch(batch, p, threads=args.batch_threads))
+    torch.cuda.synchronize()
+    batch_s = time.perf_counter() - t0
+    same = upd_loop == upd_batch
+    for a, b in zip(loop, batch):
+        ia, va, _ = a.download(0)
+        ib, vb, _ = b.download(0)
+        same = same and ia.shape == ib.shape and bool((ia == ib).all()) and bool((va == vb).all())
+    pts = [d.n_points for _, d, _ in doms]
+    for c in loop + batch:
+        c.close()
+    return {"domains": len(doms), "band_points_total": int(sum(pts)),
+            "band_points_min": int(min(pts)), "band_points_max": int(max(pts)),
+            "scheme": "LLF1 + RK2, FP32, one step per domain", "threads": args.batch_threads,
+            "loop_ms": loop_s * 1e3, "batch_ms": batch_s * 1e3,
+            "loop_point_updates_per_s": upd_loop / loop_s,
+            "batch_point_updates_per_s": upd_batch / batch_s,
+            "batch_over_loop": loop_s / batch_s, "identical": bool(same),
+            "generation_s": gen_s, "timing": "host clock around one step of every domain"}
 
 
 def cpu_baseline(args, sample_radius, steps=1, threads=None):
@@ -429,6 +517,9 @@ def main():
     ap.add_argument("--cpu-runs", type=int, default=5,
                     help="single-step oracle runs behind the cpu_baseline median")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-domains", type=int, default=256,
+                    help="domains of the batching-form report (0: skip)")
+    ap.add_argument("--batch-threads", type=int, default=16)
     ap.add_argument("--err-steps", type=int, default=50,
                     help="RK3 steps of the FP32-vs-FP64 precision report (0: skip)")
     args = ap.parse_args()
@@ -484,6 +575,7 @@ def main():
             "clocks": out["clocks"], "e2e": out.get("e2e"),
             "roofline": roofline(out, peaks, args), "band_points": out["n_points"],
             "precision_report": out.get("precision_report"),
+            "batching": out.get("batching"),
             "kernels": out.get("kernels")}
     if not args.no_cpu_baseline:
         line["cpu_baseline"], _ = cpu_baseline_line(args, args.cpu_runs)

@@ -104,6 +104,14 @@ typedef struct vlsg_advect_params {
                                       of translateFromMultiData); read it with
                                       vlsg_download_point_data.  Implied by
                                       save_advection_velocities. */
+  int32_t fp32_compensation;       /* FP32 contexts: the value update and the
+                                      RK stage combination keep their FP64
+                                      result as an FP32 value plus an FP32
+                                      compensation term (the top level set
+                                      and its RK copy); downloads return the
+                                      sum.  Costs about 18% of an RK3 step;
+                                      0 (default): the FP64 results are
+                                      rounded to FP32 once. */
 } vlsg_advect_params;
 
 /* Getters of viennals::Advect (lsAdvect.hpp:920-932) plus work counters. */

@@ -3,7 +3,8 @@ radius 16 at gridDelta 0.05 (320 cells, about 2.7M band points), radius
 modulated by seeded real spherical harmonics l <= 8 with coefficients
 ~ N(0, 0.02 R), v = 1 + 0.3 n_z, WENO5 + RK3, CFL 0.4, 50 time steps.  The
 FP32 path (phi stored in FP32, stencils in FP32, FP64 time step, advected
-time, value update and compensated stage combination) against the FP64 path,
+time, value update and stage combination, rounded to FP32 or kept with a
+compensation term) against the FP64 path,
 which the parity tests hold bit-identical to the FP64 oracle.
 
 Bound (in grid units, i.e. max |dphi| / gridDelta): <= 1e-3, and the same
@@ -26,7 +27,8 @@ def _context(grid, dom, vel, precision):
     return c
 
 
-def test_precision_form_radius_16_fifty_rk3_steps():
+@pytest.mark.parametrize("compensation", [0, 1], ids=["rounded", "compensated"])
+def test_precision_form_radius_16_fifty_rk3_steps(compensation):
     from viennals_b200 import AdvectParams
     from viennals_b200.synth import perturbed_sphere, precision_velocity
 
@@ -37,6 +39,7 @@ def test_precision_form_radius_16_fifty_rk3_steps():
     p.temporal_scheme = 2  # RUNGE_KUTTA_3RD_ORDER
     p.time_step_ratio = 0.4
     p.advection_time = 0.0  # one step per call
+    p.fp32_compensation = compensation
     c32, c64 = _context(grid, dom, vel, 1), _context(grid, dom, vel, 0)
     t32 = t64 = 0.0
     for _ in range(STEPS):

@@ -103,3 +103,54 @@ def test_batching_form_matches_loop():
         ib, vb, _ = cb.download(0)
         assert np.array_equal(ia, ib) and np.array_equal(va, vb)
     print(f"loop {t_loop * 1e3:.1f} ms, batch {t_batch * 1e3:.1f} ms")
+
+
+def test_batching_form_full_size():
+    """The batching form at its stated size: 256 seeded domains (plane with a
+    trench or a hole, bands of 1e4..2e6 points log-uniform, gridDelta
+    0.05..0.2, rates in [0.2, 1.5]), LLF1 + RK2, FP32: one step of every
+    domain through vlsg_advect_batch equals advancing them one by one."""
+    import time
+
+    import torch
+
+    from viennals_b200._abi import Precision
+    from viennals_b200.advect import Context, advect_batch
+    from viennals_b200.synth import batch_domains
+
+    doms = batch_domains(256, seed=7, device="cuda")
+    pts = [d.n_points for _, d, _ in doms]
+    assert len(doms) == 256 and min(pts) < 3e4 and max(pts) > 1e6
+    p = params(7, 1, 0.0)
+
+    def contexts():
+        out = []
+        for grid, dom, vel in doms:
+            c = Context(0, Precision.FP32)
+            c.set_grid(grid)
+            c.set_level_set_count(1)
+            c.upload(0, dom)
+            c.set_velocity(vel.descriptor())
+            out.append(c)
+        return out
+
+    loop, batch = contexts(), contexts()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res_loop = [c.advect(p) for c in loop]
+    torch.cuda.synchronize()
+    t_loop = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    res_batch = advect_batch(batch, p, threads=16)
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    for a, b, ca, cb in zip(res_loop, res_batch, loop, batch):
+        assert a.current_time_step == b.current_time_step
+        assert a.point_updates == b.point_updates
+        ia, va, _ = ca.download(0)
+        ib, vb, _ = cb.download(0)
+        assert np.array_equal(ia, ib) and np.array_equal(va, vb)
+    print(f"\n256 domains, {sum(pts)} band points ({min(pts)}..{max(pts)}): loop "
+          f"{t_loop * 1e3:.1f} ms, batch {t_batch * 1e3:.1f} ms (first step, buffers sized)")
+    for c in loop + batch:
+        c.close()

@@ -72,6 +72,7 @@ class AdvectParams(ctypes.Structure):
         ("max_steps", ctypes.c_uint32),
         ("max_dissipation", ctypes.c_double),
         ("track_point_data", ctypes.c_int32),
+        ("fp32_compensation", ctypes.c_int32),
     ]
 
     @classmethod
@@ -94,6 +95,7 @@ class AdvectParams(ctypes.Structure):
         p.max_steps = 0
         p.max_dissipation = 0.0  # no limit
         p.track_point_data = 0
+        p.fp32_compensation = 0
         return p
 
 

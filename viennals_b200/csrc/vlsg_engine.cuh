@@ -27,7 +27,6 @@
 #include "vlsg_maint.cuh"
 #include "vlsg_passes.cuh"
 #include "vlsg_rates.cuh"
-#include "vlsg_rows.cuh"
 #include "vlsg_velcb.cuh"
 #include "vlsg_voids.cuh"
 
@@ -363,7 +362,7 @@ public:
       }
     }
   }
-  // The precision form (T = float) keeps, for the top level set and its RK
+  // The precision form (T = float) can keep, for the top level set and its RK
   // copy, a second FP32 array per cell: the compensation term `lo` of the
   // value, whose exact value is hi + lo.  Only the value update and the RK
   // stage combination (both in double) produce a non-zero term; every other
@@ -371,9 +370,16 @@ public:
   // it to zero, so that hi + lo is always the value the FP64 arithmetic of
   // those two steps produced or the stored value itself.  Stencils and pass
   // rules read hi only; downloads and queries return hi + lo.
+  // The terms are kept only by operations run with compensation on (an
+  // upload, an advection with fp32_compensation); loValid tells whether the
+  // arrays are current for downloads and queries.  An advection with
+  // compensation that finds them stale starts from zero terms (value = hi).
   static constexpr bool kComp = sizeof(T) == 4;
+  bool compActive = false;
+  bool loValid = false;
   bool hasLo(int b) const { return kComp && (b == L - 1 || b == 2 * L - 1); }
-  float *loOf(int b) { return hasLo(b) ? buf[b].lo : nullptr; }
+  float *loOf(int b) { return compActive && hasLo(b) ? buf[b].lo : nullptr; }
+  const float *loRead(int b) const { return loValid && hasLo(b) ? buf[b].lo : nullptr; }
 
   // The live buffers (current level sets and the RK copies in use).
   BufSet bufSet() {
@@ -559,6 +565,7 @@ public:
       B.cur = 0, B.width = 1, B.live = false, B.bound = 0, B.nDef = 0;
     }
     allocBuffers(L);
+    compActive = kComp; // the upload keeps the part of the doubles the floats drop
     for (int l = 0; l < L; ++l) {
       Scope sc(this, "upload_farsign");
       kFarSignRows<<<grid1((size_t)g.nb[1] * g.nb[2]), 256, 0, stream>>>(g, runKeys[l], ls[l].runSign,
@@ -599,6 +606,8 @@ public:
         checkLaunch();
       }
     }
+    compActive = false;
+    loValid = kComp;
     VLSG_CUDA(cudaMemcpyAsync(pinScal + 8, small + 6, VLSG_MAX_LEVEL_SETS * sizeof(unsigned long long),
                               cudaMemcpyDeviceToHost, stream));
     syncErr("upload");
@@ -745,27 +754,6 @@ public:
     buf[b].cur ^= 1;
   }
 
-  // One Expand cycle that only defines new cells (every defined |value| is
-  // within the total limit): the row pass.
-  void expandRows(int b, const ExpandRule<T> &rule) {
-    const int64_t nIn = profiling ? defined(b) : 0;
-    {
-      Scope sc(this, "expand", [this, b, nIn] {
-        buf[b].cur ^= 1;
-        buf[b].nDef = defined(b);
-        buf[b].cur ^= 1;
-        return bandPassBytes(nIn, buf[b].nDef);
-      });
-      kExpandRows<T><<<blocksPass, FRONTIER_THREADS, 0, stream>>>(topo(), lsView(b), rule,
-                                                                  changeLog(b), visitIn(b),
-                                                                  visitOut());
-      visitDone(b);
-      checkLaunch();
-    }
-    applyChanges(b);
-    buf[b].cur ^= 1;
-  }
-
   // Expand::apply (lsExpand.hpp:44-172)
   void expand(int b, int width) {
     if (width <= buf[b].width) return;
@@ -776,7 +764,7 @@ public:
     const bool onlyUndefined = buf[b].bound <= (double)totalLimit;
     for (int c = 0; c < cycles; ++c) {
       ExpandRule<T> r{totalLimit, T((startWidth + c + 1) * T(0.5))};
-      if (onlyUndefined) expandRows(b, r);
+      if (onlyUndefined) frontierPass<FP_EXPAND>(b, r, "expand");
       else frontierPass<FP_ALL>(b, r, "expand");
       if (b == L - 1 && startWidth + c + 1 == saveTopAt) {
         // the RK copy of the top level set, taken at this width (saveTop)
@@ -909,6 +897,7 @@ public:
   // element), which is kept.
   void prepareStencil(std::vector<bool> isDepo) {
     ++generation;
+    loValid = false;
     pdTrack = pdSave = pdHas = false; // these operations carry no point data
     isDepo.resize(L, false);
     const int fin = L, above = L + 1;
@@ -946,6 +935,7 @@ public:
   // level set below it.
   void finalizeStencil() {
     ++generation;
+    loValid = false;
     pdTrack = pdSave = pdHas = false;
     dropVisits();
     invertBuffer(L - 1);
@@ -1452,6 +1442,11 @@ public:
     pdSave = pdTrack && P.save_advection_velocities;
     pdHas = false;
     if (pdTrack) initPointData();
+    // FP32 compensation terms for this advection (fp32_compensation)
+    compActive = kComp && P.fp32_compensation != 0;
+    if (compActive && !loValid) // the RK copy takes its terms from the top level set
+      VLSG_CUDA(cudaMemsetAsync(buf[L - 1].lo, 0, buf[L - 1].capLo * BV * sizeof(float), stream));
+    loValid = compActive; // without compensation the passes leave the terms stale
     const bool sllf = P.spatial_scheme == VLSG_STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER;
     rebuildCutoff = sllf ? 1.5 : 1.0;
     rebuildWidth = sllf ? 3 : 2;
@@ -1475,6 +1470,7 @@ public:
       advectedTime = currentTime;
     }
     syncErr("advect");
+    compActive = false;
     pdHas = pdTrack;
     pdTrack = pdSave = false;
     r.advected_time = advectedTime;
@@ -1499,7 +1495,7 @@ public:
     {
       Scope sc(this, "query");
       kQueryValues<T><<<grid1(n), 256, 0, stream>>>(g, mapView(), view(b), (int)n, di, dv,
-                                                     loOf(b));
+                                                     loRead(b));
       checkLaunch();
     }
     VLSG_CUDA(cudaMemcpyAsync(out, dv, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
@@ -1621,7 +1617,7 @@ public:
     VLSG_CUDA(cudaMemsetAsync(rowG, 0, rows * sizeof(uint32_t), stream));
     kSegScatter<T><<<grid1(nSeg), 256, 0, stream>>>(g, ob, nAlloc, brickMap, nbr, bounds, def,
                                                     buf[b].vals, P, rb, idx, val, GC, rowC, rowG,
-                                                    loOf(b));
+                                                    loRead(b));
     scanExclusive(GC, GE, nSeg, sums);
     scanExclusive(rowC, PB, rows, sums2);
     scanExclusive(rowG, GB, rows, sums2);
@@ -1685,7 +1681,7 @@ public:
     {
       Scope sc(this, "query");
       kQueryValues<T><<<grid1(n), 256, 0, stream>>>(g, mapView(), view(b), (int)n, di, dv,
-                                                     loOf(b));
+                                                     loRead(b));
       checkLaunch();
     }
     VLSG_CUDA(cudaMemcpyAsync(out, dv, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
@@ -1705,6 +1701,7 @@ public:
     if (w < 0) throw CudaError("Advect: Discretization scheme not found.", VLSG_ERR_ARGUMENT);
     ++generation; // the exchange format is rebuilt on the next download
     saveTopAt = 0;
+    loValid = false;
     expand(L - 1, w);
     syncErr("prepareLS");
   }
@@ -1712,7 +1709,7 @@ public:
   uint64_t insideCells(int b) override {
     VLSG_CUDA(cudaMemsetAsync(small + 15, 0, sizeof(unsigned long long), stream));
     kInsideCells<T><<<blocksPass, 256, 0, stream>>>(g, mapView(), view(b), nBricks, small + 15,
-                                                    loOf(b));
+                                                    loRead(b));
     checkLaunch();
     return readU64(small + 15);
   }
@@ -1748,13 +1745,13 @@ public:
     VLSG_CUDA(cudaMalloc(&off, std::max<int64_t>(n, 1) * sizeof(uint32_t)));
     VLSG_CUDA(cudaMalloc(&sums, (scanScratch(n) + 64) * sizeof(uint32_t)));
     kSurfaceNodes<T><<<grid1(n), 256, 0, stream>>>(g, mapView(), view(b), idx, val, n, cnt, nullptr,
-                                                   nullptr, nullptr, loOf(b));
+                                                   nullptr, nullptr, loRead(b));
     scanExclusive(cnt, off, n, sums);
     const int64_t m = scanTotal(sums, n);
     VLSG_CUDA(cudaMalloc(nodes, std::max<int64_t>(m, 1) * 3 * sizeof(double)));
     VLSG_CUDA(cudaMalloc(keys, std::max<int64_t>(m, 1) * sizeof(uint64_t)));
     kSurfaceNodes<T><<<grid1(n), 256, 0, stream>>>(g, mapView(), view(b), idx, val, n, cnt, off,
-                                                   *nodes, *keys, loOf(b));
+                                                   *nodes, *keys, loRead(b));
     checkLaunch();
     VLSG_CUDA(cudaStreamSynchronize(stream));
     cudaFree(cnt);

@@ -167,29 +167,83 @@ def batch_domains(n=256, seed=7, points_range=(1e4, 2e6), device=None):
         depth = float(rng.uniform(1.0, 8.0))
         rate = float(rng.uniform(0.2, 1.5))
         target = float(np.exp(rng.uniform(np.log(points_range[0]), np.log(points_range[1]))))
-        lateral = max(2.0 * width, width + 2.0)
-        # band of a plane: ~2.5 layers of (lateral / gd)^2 points, plus walls
-        walls = (4.0 if hole else 2.0) * depth / lateral
-        gd = float(np.clip(np.sqrt(2.5 * lateral * lateral * (1.0 + walls) / target), 0.05, 0.2))
+        gd = float(np.exp(rng.uniform(np.log(0.05), np.log(0.2))))
+        # a width-2 band holds ~2.5 points per cell of surface: the plane
+        # (lateral^2) plus the walls (a trench's two walls along y, a hole's
+        # cylinder); the lateral extent is chosen for the target band and kept
+        # at least twice the feature (then gridDelta is made finer or coarser
+        # within 0.05..0.2 to approach the target)
+        area = target * gd * gd / 2.5
+        if hole:
+            lateral = math.sqrt(max(area - math.pi * width * depth, 0.0))
+        else:
+            lateral = -depth + math.sqrt(depth * depth + area)
+        lmin = max(2.0 * width, width + 2.0)
+        if lateral < lmin:
+            lateral = lmin
+            surf = lateral * lateral + (math.pi * width * depth if hole else 2.0 * lateral * depth)
+            gd = float(np.clip(math.sqrt(2.5 * surf / target), 0.05, 0.2))
         cells = max(16, int(round(lateral / gd)))
         half = cells * gd / 2.0
         zlo, zhi = -depth - 1.5, 1.5
         grid = Grid([-half, half, -half, half, zlo, zhi],
                     [BC.PERIODIC_BOUNDARY, BC.PERIODIC_BOUNDARY, BC.INFINITE_BOUNDARY], gd)
         r = width / 2.0
-
-        def sdf(x, y, z, hole=hole, r=r, depth=depth):
-            if hole:
-                cut = np.maximum(np.sqrt(x * x + y * y) - r, -z - depth)
-            else:
-                cut = sdf_box((x, y, z), (-r, -1e9, -depth), (r, 1e9, 1e9))
-            return np.maximum(z, -cut)
-
         lo = [grid.min[0], grid.min[1], grid.min[2]]
         hi = [grid.max[0] - 1, grid.max[1] - 1, grid.max[2]]
-        dom = sdf_levelset(grid, sdf, lo, hi)
+        if device is None:
+            def sdf(x, y, z, hole=hole, r=r, depth=depth):
+                if hole:
+                    cut = np.maximum(np.sqrt(x * x + y * y) - r, -z - depth)
+                else:
+                    cut = sdf_box((x, y, z), (-r, -1e9, -depth), (r, 1e9, 1e9))
+                return np.maximum(z, -cut)
+
+            dom = sdf_levelset(grid, sdf, lo, hi)
+        else:
+            dom = _torch_domain(grid, _hole_or_trench_torch(hole, r, depth), lo, hi, device)
         out.append((grid, dom, constant_scalar(-rate)))
     return out
+
+
+def _hole_or_trench_torch(hole, r, depth):
+    """The batching form's plane with a cylindrical hole or a trench (along y)
+    as a torch SDF."""
+    import torch
+
+    def sdf(x, y, z):
+        if hole:
+            cut = torch.maximum(torch.sqrt(x * x + y * y) - r, -z - depth)
+        else:
+            # box |x| <= r, z >= -depth (unbounded in y and upwards)
+            qx = torch.abs(x) - r
+            qz = -depth - z
+            outside = torch.sqrt(torch.clamp(qx, min=0.0) ** 2 + torch.clamp(qz, min=0.0) ** 2)
+            cut = outside + torch.clamp(torch.maximum(qx, qz), max=0.0)
+        return torch.maximum(z, -cut)
+
+    return sdf
+
+
+def _torch_domain(grid, sdf, lo, hi, device):
+    """Width-2 band and undefined runs of a torch SDF on `device`."""
+    import torch
+
+    idx, vals = _sdf_band_torch(grid, sdf, lo, hi, device)
+    gd = grid.delta
+
+    def sign_fn(x, y, z):
+        out = np.empty(len(x), np.int64)
+        step = 1 << 22
+        for s in range(0, len(x), step):
+            t = [torch.as_tensor(np.asarray(a[s:s + step], np.float64) * gd, device=device)
+                 for a in (x, y, z)]
+            out[s:s + step] = np.where(sdf(*t).cpu().numpy() < 0, -1, 1)
+        return out
+
+    rs, sg = make_runs(idx, sign_fn, [lo[0] - 1, lo[1] - 1, lo[2] - 1],
+                       [hi[0] + 1, hi[1] + 1, hi[2] + 1])
+    return Domain(grid, idx, vals, rs, sg, width=2)
 
 
 def _sdf_band_torch(grid, sdf, lo, hi, device, chunk_cells=1 << 24):
