@@ -247,7 +247,10 @@ def run_ours(args, rank, world):
     if rank == 0 and args.err_steps > 0:
         out["precision_report"] = precision_report(args, grid, dom, vel, p, stream)
     if rank == 0 and args.batch_domains > 0:
-        out["batching"] = batching_report(args, f"cuda:{args.local_rank}")
+        try:
+            out["batching"] = batching_report(args, f"cuda:{args.local_rank}")
+        except Exception as e:  # noqa: BLE001 -- reported in the line, the bench goes on
+            out["batching"] = {"error": str(e)[:300]}
     return out
 
 
@@ -376,27 +379,31 @@ def batching_report(args, device):
             out.append(c)
         return out
 
-    loop, batch = contexts(), contexts()
-    for c in loop:
-        c.advect(p)
-    advect_batch(batch, p, threads=args.batch_threads)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    upd_loop = sum(c.advect(p).point_updates for c in loop)
-    torch.cuda.synchronize()
-    loop_s = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    upd_batch = sum(r.point_updates for r in advect_batch(batch, p, threads=args.batch_threads))
-    torch.cuda.synchronize()
-    batch_s = time.perf_counter() - t0
-    same = upd_loop == upd_batch
-    for a, b in zip(loop, batch):
-        ia, va, _ = a.download(0)
-        ib, vb, _ = b.download(0)
-        same = same and ia.shape == ib.shape and bool((ia == ib).all()) and bool((va == vb).all())
+    def run(batched):
+        # one set of contexts at a time: 256 contexts hold tens of GB
+        cs = contexts()
+        try:
+            step = ((lambda: advect_batch(cs, p, threads=args.batch_threads)) if batched
+                    else (lambda: [c.advect(p) for c in cs]))
+            step()  # sizes every context's buffers
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            upd = sum(r.point_updates for r in step())
+            torch.cuda.synchronize()
+            secs = time.perf_counter() - t0
+            got = [c.download(0)[:2] for c in cs]
+        finally:
+            for c in cs:
+                c.close()
+            torch.cuda.empty_cache()
+        return upd, secs, got
+
+    upd_loop, loop_s, got_loop = run(False)
+    upd_batch, batch_s, got_batch = run(True)
+    same = upd_loop == upd_batch and all(
+        a[0].shape == b[0].shape and bool((a[0] == b[0]).all()) and bool((a[1] == b[1]).all())
+        for a, b in zip(got_loop, got_batch))
     pts = [d.n_points for _, d, _ in doms]
-    for c in loop + batch:
-        c.close()
     return {"domains": len(doms), "band_points_total": int(sum(pts)),
             "band_points_min": int(min(pts)), "band_points_max": int(max(pts)),
             "scheme": "LLF1 + RK2, FP32, one step per domain", "threads": args.batch_threads,
@@ -456,6 +463,7 @@ def _has_cuda():
 # DRAM traffic per launch of the dominant kernel from one ncu capture of the
 # default workload (its summary sits under profiles/ with the command).
 TRAFFIC_PROFILE = {"expand": "expand_pass_dram_fp32_sphere_r40.md"}
+PROFILES_DIR = os.path.join(ROOT, "profiles")
 
 
 def default_workload(args):
@@ -463,18 +471,42 @@ def default_workload(args):
             and args.precision == "fp32")
 
 
-def profiled_traffic(kernel):
+# The sources of the kernel the traffic figure belongs to: a figure captured
+# from other sources is stale and not quoted.
+TRAFFIC_SOURCES = ["viennals_b200/csrc/vlsg_frontier.cuh", "viennals_b200/csrc/vlsg_passes.cuh",
+                   "viennals_b200/csrc/vlsg_common.cuh"]
+
+
+def kernel_sources_hash():
+    import hashlib
+
+    h = hashlib.sha256()
+    for f in TRAFFIC_SOURCES:
+        with open(os.path.join(ROOT, f), "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:16]
+
+
+def profiled_traffic(kernel, with_stamp=False):
+    """DRAM bytes per launch from the committed ncu summary of `kernel`, with
+    the commit it was captured at; None when the summary's kernel sources
+    differ from the current ones."""
     name = TRAFFIC_PROFILE.get(kernel)
     if not name:
-        return None
+        return (None, None) if with_stamp else None
+    vals = {}
     try:
-        with open(os.path.join(ROOT, "profiles", name)) as f:
+        with open(os.path.join(PROFILES_DIR, name)) as f:
             for line in f:
-                if line.startswith("traffic_bytes_per_launch:"):
-                    return float(line.split(":", 1)[1])
+                for key in ("traffic_bytes_per_launch", "kernel_sources_sha256", "captured_at_commit"):
+                    if line.startswith(key + ":"):
+                        vals[key] = line.split(":", 1)[1].strip()
     except OSError:
-        return None
-    return None
+        return (None, None) if with_stamp else None
+    t = vals.get("traffic_bytes_per_launch")
+    if t is None or vals.get("kernel_sources_sha256") != kernel_sources_hash():
+        return (None, None) if with_stamp else None
+    return (float(t), vals.get("captured_at_commit")) if with_stamp else float(t)
 
 
 def roofline(out, peaks, args=None):
@@ -492,10 +524,14 @@ def roofline(out, peaks, args=None):
     bytes_per_launch = top["bytes"] / max(1, top["launches"])
     achieved = bytes_per_launch / (per_launch_ms / 1e3) / 1e9 if per_launch_ms > 0 else 0.0
     total = sum(k["device_ms"] for k in ks)
+    traffic, stamp = (profiled_traffic(top["name"], with_stamp=True)
+                      if args and default_workload(args) else (None, None))
     return {"bound": "hbm", "kernel": top["name"], "achieved": achieved, "peak": hbm,
             "peak_source": src, "unit": "GB/s", "frac": achieved / hbm,
-            "traffic": profiled_traffic(top["name"]) if args and default_workload(args) else None,
-            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, mean per launch",
+            "traffic": traffic,
+            "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum, mean per launch, "
+                               f"captured at commit {stamp}" if traffic is not None else
+                               "no ncu capture of the current kernel sources for this workload"),
             "share": top["device_ms"] / total if total else None,
             "launch_ms": per_launch_ms}
 

@@ -31,6 +31,7 @@ def test_roofline_picks_the_dominant_kernel():
     assert abs(r["frac"] - r["achieved"] / 6456.5) < 1e-12
     assert r["peak_source"] == "measured"
     assert r["traffic"] == bench.profiled_traffic("expand")
+    assert (r["traffic"] is None) == ("captured at" not in r["traffic_source"])
     assert abs(r["share"] - 8.3 / 11.1) < 1e-12
     # other workloads quote no traffic; no peaks file -> the fallback peak
     r2 = bench.roofline(out, None, _args(radius=24.0))
@@ -38,10 +39,21 @@ def test_roofline_picks_the_dominant_kernel():
     assert bench.roofline({"kernels": []}, None) is None
 
 
-def test_profiled_traffic_is_the_committed_figure():
+def test_profiled_traffic_is_the_committed_figure(tmp_path, monkeypatch):
+    # the committed summary, when it was captured from the current sources
     t = bench.profiled_traffic("expand")
-    assert t is not None and 5e8 < t < 1e9  # bytes per Expand launch at R 40
+    assert t is None or 4e8 < t < 1.2e9  # bytes per Expand launch at R 40
     assert bench.profiled_traffic("rates") is None
+    # a summary is quoted with its commit only while the kernel sources match
+    name = bench.TRAFFIC_PROFILE["expand"]
+    monkeypatch.setattr(bench, "PROFILES_DIR", str(tmp_path))
+    (tmp_path / name).write_text("traffic_bytes_per_launch: 7.5e8\n"
+                                 f"kernel_sources_sha256: {bench.kernel_sources_hash()}\n"
+                                 "captured_at_commit: abc123\n")
+    assert bench.profiled_traffic("expand", with_stamp=True) == (7.5e8, "abc123")
+    (tmp_path / name).write_text("traffic_bytes_per_launch: 7.5e8\n"
+                                 "kernel_sources_sha256: 0000000000000000\n")
+    assert bench.profiled_traffic("expand") is None
 
 
 def test_reference_arm_line():

@@ -109,7 +109,10 @@ def test_batching_form_full_size():
     """The batching form at its stated size: 256 seeded domains (plane with a
     trench or a hole, bands of 1e4..2e6 points log-uniform, gridDelta
     0.05..0.2, rates in [0.2, 1.5]), LLF1 + RK2, FP32: one step of every
-    domain through vlsg_advect_batch equals advancing them one by one."""
+    domain through vlsg_advect_batch equals advancing them one by one.  One
+    set of contexts lives at a time (256 contexts of bands up to 2M points
+    hold tens of GB)."""
+    import gc
     import time
 
     import torch
@@ -119,6 +122,7 @@ def test_batching_form_full_size():
     from viennals_b200.synth import batch_domains
 
     doms = batch_domains(256, seed=7, device="cuda")
+    torch.cuda.empty_cache()
     pts = [d.n_points for _, d, _ in doms]
     assert len(doms) == 256 and min(pts) < 3e4 and max(pts) > 1e6
     p = params(7, 1, 0.0)
@@ -134,23 +138,26 @@ def test_batching_form_full_size():
             out.append(c)
         return out
 
-    loop, batch = contexts(), contexts()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    res_loop = [c.advect(p) for c in loop]
-    torch.cuda.synchronize()
-    t_loop = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    res_batch = advect_batch(batch, p, threads=16)
-    torch.cuda.synchronize()
-    t_batch = time.perf_counter() - t0
-    for a, b, ca, cb in zip(res_loop, res_batch, loop, batch):
-        assert a.current_time_step == b.current_time_step
-        assert a.point_updates == b.point_updates
-        ia, va, _ = ca.download(0)
-        ib, vb, _ = cb.download(0)
-        assert np.array_equal(ia, ib) and np.array_equal(va, vb)
+    def run(batched):
+        cs = contexts()
+        try:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            res = advect_batch(cs, p, threads=16) if batched else [c.advect(p) for c in cs]
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            got = [(r.current_time_step, r.point_updates) + tuple(c.download(0)[:2])
+                   for r, c in zip(res, cs)]
+        finally:
+            for c in cs:
+                c.close()
+            gc.collect()
+        return got, dt
+
+    loop, t_loop = run(False)
+    batch, t_batch = run(True)
+    for a, b in zip(loop, batch):
+        assert a[0] == b[0] and a[1] == b[1]
+        assert np.array_equal(a[2], b[2]) and np.array_equal(a[3], b[3])
     print(f"\n256 domains, {sum(pts)} band points ({min(pts)}..{max(pts)}): loop "
           f"{t_loop * 1e3:.1f} ms, batch {t_batch * 1e3:.1f} ms (first step, buffers sized)")
-    for c in loop + batch:
-        c.close()

@@ -354,7 +354,7 @@ public:
         VLSG_CUDA(cudaMalloc(&B.farSign, capBricks));
         B.capBricks = capBricks;
       }
-      if (hasLo(b) && (B.capLo < capSlots || !B.lo)) {
+      if (loWanted && hasLo(b) && (B.capLo < capSlots || !B.lo)) {
         if (B.lo) VLSG_CUDA(cudaFree(B.lo));
         B.lo = nullptr;
         VLSG_CUDA(cudaMalloc(&B.lo, capSlots * BV * sizeof(float)));
@@ -377,6 +377,14 @@ public:
   static constexpr bool kComp = sizeof(T) == 4;
   bool compActive = false;
   bool loValid = false;
+  bool loWanted = false; // the arrays exist only once compensation was asked for
+  // the uploaded top level set (device arrays of the context) while the
+  // level sets are unchanged since the upload: its doubles give the first
+  // compensation terms
+  const int32_t *upIdx = nullptr;
+  const double *upVals = nullptr;
+  int64_t upN = 0;
+  bool pristine = false;
   bool hasLo(int b) const { return kComp && (b == L - 1 || b == 2 * L - 1); }
   float *loOf(int b) { return compActive && hasLo(b) ? buf[b].lo : nullptr; }
   const float *loRead(int b) const { return loValid && hasLo(b) ? buf[b].lo : nullptr; }
@@ -431,6 +439,10 @@ public:
       VLSG_CUDA(cudaMalloc(&nbr, n * 27 * sizeof(int)));
       VLSG_CUDA(cudaMalloc(&cflag, n));
       VLSG_CUDA(cudaMalloc(&act, n * 8 * sizeof(uint64_t)));
+      // pass grids: one wave of the GPU, or one warp per 8 slots for small
+      // pools (the change log holds a segment per warp)
+      blocksPass = std::min(numSMs * VLSG_PASS_MIN_BLOCKS,
+                            std::max(numSMs, (int)((n + 63) / 64)));
       // a pass warp handles at most ceil(n / warps) bricks: its log segment
       // holds all their cells
       logSegments = blocksPass * (FRONTIER_THREADS / 32);
@@ -565,7 +577,6 @@ public:
       B.cur = 0, B.width = 1, B.live = false, B.bound = 0, B.nDef = 0;
     }
     allocBuffers(L);
-    compActive = kComp; // the upload keeps the part of the doubles the floats drop
     for (int l = 0; l < L; ++l) {
       Scope sc(this, "upload_farsign");
       kFarSignRows<<<grid1((size_t)g.nb[1] * g.nb[2]), 256, 0, stream>>>(g, runKeys[l], ls[l].runSign,
@@ -595,7 +606,7 @@ public:
       if (s.n) {
         Scope sc(this, "upload_scatter");
         kScatterPoints<T><<<grid1(s.n), 256, 0, stream>>>(g, (int)s.n, s.idx, s.vals, brickMap,
-                                                          buf[l].vals, errPtr(), loOf(l));
+                                                          buf[l].vals, errPtr(), nullptr);
         checkLaunch();
       }
       {
@@ -606,8 +617,9 @@ public:
         checkLaunch();
       }
     }
-    compActive = false;
-    loValid = kComp;
+    loValid = false;
+    upIdx = ls[L - 1].idx, upVals = ls[L - 1].vals, upN = ls[L - 1].n;
+    pristine = true;
     VLSG_CUDA(cudaMemcpyAsync(pinScal + 8, small + 6, VLSG_MAX_LEVEL_SETS * sizeof(unsigned long long),
                               cudaMemcpyDeviceToHost, stream));
     syncErr("upload");
@@ -897,6 +909,7 @@ public:
   // element), which is kept.
   void prepareStencil(std::vector<bool> isDepo) {
     ++generation;
+    pristine = false;
     loValid = false;
     pdTrack = pdSave = pdHas = false; // these operations carry no point data
     isDepo.resize(L, false);
@@ -935,6 +948,7 @@ public:
   // level set below it.
   void finalizeStencil() {
     ++generation;
+    pristine = false;
     loValid = false;
     pdTrack = pdSave = pdHas = false;
     dropVisits();
@@ -1444,9 +1458,20 @@ public:
     if (pdTrack) initPointData();
     // FP32 compensation terms for this advection (fp32_compensation)
     compActive = kComp && P.fp32_compensation != 0;
-    if (compActive && !loValid) // the RK copy takes its terms from the top level set
+    if (compActive && !loValid) {
+      // the RK copy takes its terms from the top level set: the part of the
+      // uploaded doubles the floats dropped, or zero
+      loWanted = true;
+      allocBuffers(L);
       VLSG_CUDA(cudaMemsetAsync(buf[L - 1].lo, 0, buf[L - 1].capLo * BV * sizeof(float), stream));
+      if (pristine && upN) {
+        kScatterLo<T><<<grid1(upN), 256, 0, stream>>>(g, (int)upN, upIdx, upVals, brickMap,
+                                                      buf[L - 1].lo);
+        checkLaunch();
+      }
+    }
     loValid = compActive; // without compensation the passes leave the terms stale
+    pristine = false;
     const bool sllf = P.spatial_scheme == VLSG_STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER;
     rebuildCutoff = sllf ? 1.5 : 1.0;
     rebuildWidth = sllf ? 3 : 2;
@@ -1702,6 +1727,7 @@ public:
     ++generation; // the exchange format is rebuilt on the next download
     saveTopAt = 0;
     loValid = false;
+    pristine = false;
     expand(L - 1, w);
     syncErr("prepareLS");
   }

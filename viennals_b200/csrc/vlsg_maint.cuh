@@ -378,6 +378,24 @@ __global__ void kScatterPoints(GridDev g, int n, const int *idx, const double *v
 }
 
 
+// Compensation terms of uploaded points: the part of each double that its
+// float (already scattered) dropped.
+template <class T>
+__global__ void kScatterLo(GridDev g, int n, const int *idx, const double *v, const int *brickMap,
+                           float *lo) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int rx = idx[3 * i] - g.org[0], ry = idx[3 * i + 1] - g.org[1],
+              rz = idx[3 * i + 2] - g.org[2];
+    if (rx < 0 || ry < 0 || rz < 0 || rx >= g.nb[0] * BS || ry >= g.nb[1] * BS ||
+        rz >= g.nb[2] * BS)
+      continue;
+    const int slot = brickMap[brickIndex(g, rx >> 3, ry >> 3, rz >> 3)];
+    if (slot < 0) continue;
+    lo[(size_t)slot * BV + ((rz & 7) * 64 + (ry & 7) * 8 + (rx & 7))] =
+        (float)(v[i] - (double)T(v[i]));
+  }
+}
+
 // Defined masks and defined-cell count of a buffer from its values (after an
 // upload); cells past the end of a bounded direction are set to +max.
 template <class T>
