@@ -267,13 +267,13 @@ def precision_report(args, grid, dom, vel, p, stream):
 
     res = {}
 
-    def run(prec, compensation=0):
+    def run(prec, compensation=0, dom_in=None):
         p.fp32_compensation = compensation
         c = Context(args.local_rank, prec)
         c.set_stream(stream.cuda_stream)
         c.set_grid(grid)
         c.set_level_set_count(1)
-        c.upload(0, dom)
+        c.upload(0, dom if dom_in is None else dom_in)
         c.set_velocity(vel.descriptor())
         c.count(0)
         torch.cuda.synchronize()
@@ -311,6 +311,18 @@ def precision_report(args, grid, dom, vel, p, stream):
 
     r = against64(out32)
     rc = against64(out32c)
+    # the reference algorithm's own sensitivity: the FP64 path started from
+    # the input rounded to FP32 (one rounding of each value, no FP32
+    # arithmetic), against the FP64 path from the exact input
+    import numpy as np
+
+    from viennals_b200.domain import Domain
+
+    rounded = Domain(grid, dom.idx, dom.values.astype(np.float32).astype(np.float64),
+                     dom.run_start, dom.run_sign, width=dom.width)
+    c64r, _ = run(Precision.FP64, dom_in=rounded)
+    rr = c64r.compare(0, c64, 0)
+    c64r.close()
     c64.close()
     gd = float(grid.delta)
     vol64, vol32 = r["inside_cells_b"], r["inside_cells_a"]
@@ -343,6 +355,16 @@ def precision_report(args, grid, dom, vel, p, stream):
         "chamfer_mean": r["chamfer_mean"] * gd, "chamfer_unit": "length (gridDelta x grid units)",
         "surface_nodes_fp32": r["nodes_a"], "surface_nodes_fp64": r["nodes_b"],
         "compensated": comp,
+        "fp64_from_fp32_rounded_input": {
+            "what": "FP64 path from the input values rounded to FP32 once, against the FP64 "
+                    "path from the exact input (no FP32 arithmetic anywhere)",
+            "max_abs_dphi_over_gridDelta": rr["max_abs_diff"],
+            "rms_abs_dphi_over_gridDelta": rr["rms_abs_diff"],
+            "points_with_abs_dphi_above": dict(zip(["1e-6", "1e-5", "1e-4", "1e-3"], rr["diff_above"])),
+            "active_set_differences": rr["active_only_a"] + rr["active_only_b"],
+            "defined_set_differences": rr["defined_only_a"] + rr["defined_only_b"],
+            "chamfer_rms": rr["chamfer_rms"] * gd, "chamfer_max": rr["chamfer_max"] * gd,
+        },
     }
 
 
@@ -350,14 +372,17 @@ def batching_report(args, device):
     """The batching form: `args.batch_domains` seeded plane domains with a
     trench or a hole (bands of 1e4..2e6 points, log-uniform), LLF 1st order,
     RK2, FP32, per-domain rates in [0.2, 1.5]; one RK2 step of every domain
-    advanced one context after another (loop) and by vlsg_advect_batch (host
-    threads, one stream per context), each set warmed by one step first and
-    timed by the host clock around the step; both sets must end identical."""
+    advanced three ways: one context after another (loop), vlsg_advect_batch
+    (host threads, one stream per context) and the batch context (every pass
+    one launch over all domains, per-domain time steps on the device).  Each
+    way is warmed by one step first and timed by the host clock around the
+    step; all three must end identical."""
+    import numpy as np
     import torch
 
     from viennals_b200 import AdvectParams
     from viennals_b200._abi import Precision
-    from viennals_b200.advect import Context, advect_batch
+    from viennals_b200.advect import BatchContext, Context, advect_batch
     from viennals_b200.synth import batch_domains
 
     t0 = time.time()
@@ -379,38 +404,59 @@ def batching_report(args, device):
             out.append(c)
         return out
 
-    def run(batched):
+    def run(mode):
         # one set of contexts at a time: 256 contexts hold tens of GB
-        cs = contexts()
-        try:
-            step = ((lambda: advect_batch(cs, p, threads=args.batch_threads)) if batched
+        if mode == "batch":
+            b = BatchContext(args.local_rank, Precision.FP32)
+            b.set_domains(doms)
+            cs = None
+            step = lambda: b.advect(p)  # noqa: E731
+        else:
+            cs = contexts()
+            step = ((lambda: advect_batch(cs, p, threads=args.batch_threads)) if mode == "threads"
                     else (lambda: [c.advect(p) for c in cs]))
-            step()  # sizes every context's buffers
+        try:
+            step()  # sizes the buffers
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            upd = sum(r.point_updates for r in step())
+            res = step()
             torch.cuda.synchronize()
             secs = time.perf_counter() - t0
-            got = [c.download(0)[:2] for c in cs]
+            upd = sum(r.point_updates for r in res)
+            launches = (res[0].kernel_launches if mode == "batch"
+                        else sum(r.kernel_launches for r in res))
+            got = ([b.download(d)[:2] for d in range(len(doms))] if mode == "batch"
+                   else [c.download(0)[:2] for c in cs])
         finally:
-            for c in cs:
-                c.close()
+            if cs:
+                for c in cs:
+                    c.close()
+            else:
+                b.close()
             torch.cuda.empty_cache()
-        return upd, secs, got
+        return upd, secs, got, launches
 
-    upd_loop, loop_s, got_loop = run(False)
-    upd_batch, batch_s, got_batch = run(True)
-    same = upd_loop == upd_batch and all(
-        a[0].shape == b[0].shape and bool((a[0] == b[0]).all()) and bool((a[1] == b[1]).all())
-        for a, b in zip(got_loop, got_batch))
+    upd_loop, loop_s, got_loop, l_loop = run("loop")
+    upd_thr, thr_s, got_thr, l_thr = run("threads")
+    upd_b, b_s, got_b, l_b = run("batch")
+
+    def same(a, b):
+        return all(x[0].shape == y[0].shape and bool((x[0] == y[0]).all()) and
+                   bool((x[1].view(np.int64) == y[1].view(np.int64)).all()) for x, y in zip(a, b))
+
     pts = [d.n_points for _, d, _ in doms]
     return {"domains": len(doms), "band_points_total": int(sum(pts)),
             "band_points_min": int(min(pts)), "band_points_max": int(max(pts)),
-            "scheme": "LLF1 + RK2, FP32, one step per domain", "threads": args.batch_threads,
-            "loop_ms": loop_s * 1e3, "batch_ms": batch_s * 1e3,
+            "scheme": "LLF1 + RK2, FP32, one step per domain",
+            "loop_ms": loop_s * 1e3, "threads_ms": thr_s * 1e3, "batch_ms": b_s * 1e3,
+            "threads": args.batch_threads,
             "loop_point_updates_per_s": upd_loop / loop_s,
-            "batch_point_updates_per_s": upd_batch / batch_s,
-            "batch_over_loop": loop_s / batch_s, "identical": bool(same),
+            "threads_point_updates_per_s": upd_thr / thr_s,
+            "batch_point_updates_per_s": upd_b / b_s,
+            "batch_over_loop": loop_s / b_s, "threads_over_loop": loop_s / thr_s,
+            "kernel_launches": {"loop": l_loop, "threads": l_thr, "batch": l_b},
+            "identical": bool(upd_loop == upd_thr == upd_b and same(got_loop, got_thr)
+                              and same(got_loop, got_b)),
             "generation_s": gen_s, "timing": "host clock around one step of every domain"}
 
 

@@ -399,6 +399,49 @@ int vlsg_advect(vlsg_context *ctx, const vlsg_advect_params *params,
 int vlsg_advect_batch(vlsg_context **ctxs, int32_t n, const vlsg_advect_params *params,
                       vlsg_advect_result *results, int32_t threads);
 
+/* Batching form, in one context: many independent domains (each with its own
+ * grid, one level set and a velocity functor) share one brick pool, and every
+ * band pass, rate pass and value update of a time step is ONE kernel launch
+ * over the bricks of all domains.  Each domain keeps its own gridDelta,
+ * velocity and time step; the time steps are reduced per domain on the
+ * device, so a step needs no host synchronisation until its end.  No
+ * counterpart in Advect: it replaces a loop over many Advect objects
+ * (examples/SquareEtch/SquareEtch.cpp:189-229 advances one domain per
+ * Advect), with results bit-identical to advancing each domain by itself
+ * (vlsg_advect on one context per domain).
+ * Limits: every domain periodic in x and y with extents that are multiples
+ * of 8 points and infinite in z; one level set per domain; one time step per
+ * vlsg_batch_advect (advection_time 0); device velocity functors; not with
+ * global LAX_FRIEDRICHS, STENCIL_LOCAL_LAX_FRIEDRICHS, voids, point data or
+ * FP32 compensation (VLSG_ERR_ARGUMENT); a domain whose first stage gets no
+ * positive time step (no active point, zero velocity) ends the step with
+ * VLSG_ERR_DEVICE_CHECK.  vlsg_set_grid returns the context to one domain. */
+typedef struct vlsg_batch_domain {
+  const int64_t *grid_min, *grid_max; /* index bounds, 3 each (vlsg_set_grid) */
+  const int32_t *boundary;            /* 3: PERIODIC, PERIODIC, INFINITE */
+  double grid_delta;
+  int64_t n_points;                   /* as vlsg_upload_levelset */
+  const int32_t *indices;
+  const double *values;
+  int64_t n_runs;
+  const int32_t *run_start;
+  const int8_t *run_sign;
+  int32_t width;
+  const vlsg_velocity_desc *velocity;
+} vlsg_batch_domain;
+int vlsg_batch_set_domains(vlsg_context *ctx, int32_t n, const vlsg_batch_domain *domains);
+/* One time step of every domain; results[d] receives domain d's getters. */
+int vlsg_batch_advect(vlsg_context *ctx, const vlsg_advect_params *params,
+                      vlsg_advect_result *results);
+/* Domain d's defined points in HRLE order, in its own indices. */
+int vlsg_batch_count_points(vlsg_context *ctx, int32_t domain, int64_t *n_points);
+int vlsg_batch_download(vlsg_context *ctx, int32_t domain, int64_t capacity,
+                        int32_t *indices, double *values, int32_t *width);
+/* vlsg_get_values for domain d (its indices, mapped through its periodic
+ * boundaries): what a caller rebuilds the undefined runs from. */
+int vlsg_batch_get_values(vlsg_context *ctx, int32_t domain, int64_t n,
+                          const int32_t *indices, double *values);
+
 /* Timing of the last vlsg_advect: per kernel family, device milliseconds and
  * algorithmic bytes, as measured with CUDA events on the context stream
  * (filled only when profiling is switched on with vlsg_set_profiling). */

@@ -159,5 +159,22 @@ def test_batching_form_full_size():
     for a, b in zip(loop, batch):
         assert a[0] == b[0] and a[1] == b[1]
         assert np.array_equal(a[2], b[2]) and np.array_equal(a[3], b[3])
+    # the batch context: one launch per pass over all 256 domains
+    from viennals_b200.advect import BatchContext
+
+    bc = BatchContext(0, Precision.FP32)
+    bc.set_domains(doms)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = bc.advect(p)
+    torch.cuda.synchronize()
+    t_one = time.perf_counter() - t0
+    one = [(r.current_time_step, r.point_updates) + tuple(bc.download(d)[:2])
+           for d, r in enumerate(res)]
+    bc.close()
+    for a, b in zip(loop, one):
+        assert a[0] == b[0] and a[1] == b[1]
+        assert np.array_equal(a[2], b[2]) and np.array_equal(a[3].view(np.int64), b[3].view(np.int64))
     print(f"\n256 domains, {sum(pts)} band points ({min(pts)}..{max(pts)}): loop "
-          f"{t_loop * 1e3:.1f} ms, batch {t_batch * 1e3:.1f} ms (first step, buffers sized)")
+          f"{t_loop * 1e3:.1f} ms, threads {t_batch * 1e3:.1f} ms, batch context "
+          f"{t_one * 1e3:.1f} ms (first step, buffers sized)")

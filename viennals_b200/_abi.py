@@ -202,3 +202,21 @@ VELOCITY_CALLBACK = ctypes.CFUNCTYPE(
     ctypes.POINTER(ctypes.c_double),
     ctypes.POINTER(ctypes.c_double),
 )
+
+
+class BatchDomain(ctypes.Structure):
+    """vlsg_batch_domain: one domain of the batching form."""
+    _fields_ = [
+        ("grid_min", ctypes.POINTER(ctypes.c_int64)),
+        ("grid_max", ctypes.POINTER(ctypes.c_int64)),
+        ("boundary", ctypes.POINTER(ctypes.c_int32)),
+        ("grid_delta", ctypes.c_double),
+        ("n_points", ctypes.c_int64),
+        ("indices", ctypes.POINTER(ctypes.c_int32)),
+        ("values", ctypes.POINTER(ctypes.c_double)),
+        ("n_runs", ctypes.c_int64),
+        ("run_start", ctypes.POINTER(ctypes.c_int32)),
+        ("run_sign", ctypes.POINTER(ctypes.c_int8)),
+        ("width", ctypes.c_int32),
+        ("velocity", ctypes.POINTER(VelocityDesc)),
+    ]

@@ -2,8 +2,8 @@
 import ctypes
 import os
 
-from ._abi import (ALPHA_CALLBACK, REDUCE_CALLBACK, UPDATE_CALLBACK, VELOCITY_CALLBACK, AdvectParams, AdvectResult, CompareResult, KernelStat,
-                   VelocityDesc)
+from ._abi import (ALPHA_CALLBACK, REDUCE_CALLBACK, UPDATE_CALLBACK, VELOCITY_CALLBACK, AdvectParams,
+                   AdvectResult, BatchDomain, CompareResult, KernelStat, VelocityDesc)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libvlsgpu.so")
@@ -48,6 +48,11 @@ def load(build_if_missing=True):
     L.vlsg_download_runs.argtypes = [vp, i32, i64, P(i32), P(ctypes.c_int8), P(i64)]
     L.vlsg_compare.argtypes = [vp, i32, vp, i32, P(CompareResult)]
     L.vlsg_advect_batch.argtypes = [P(vp), i32, P(AdvectParams), P(AdvectResult), i32]
+    L.vlsg_batch_set_domains.argtypes = [vp, i32, P(BatchDomain)]
+    L.vlsg_batch_advect.argtypes = [vp, P(AdvectParams), P(AdvectResult)]
+    L.vlsg_batch_count_points.argtypes = [vp, i32, P(i64)]
+    L.vlsg_batch_download.argtypes = [vp, i32, i64, P(i32), P(ctypes.c_double), P(i32)]
+    L.vlsg_batch_get_values.argtypes = [vp, i32, i64, P(i32), P(ctypes.c_double)]
     L.vlsg_get_values_noalloc.argtypes = [vp, i32, i64, P(i32), P(ctypes.c_double)]
     L.vlsg_set_velocity_functor.argtypes = [vp, P(VelocityDesc)]
     L.vlsg_set_velocity_callback.argtypes = [vp, VELOCITY_CALLBACK, vp]
@@ -75,4 +80,6 @@ EXPORTED = [
     "vlsg_set_velocity_update_callback", "vlsg_advect", "vlsg_advect_batch",
     "vlsg_set_profiling", "vlsg_get_kernel_stats", "vlsg_compare",
     "vlsg_set_owned_region", "vlsg_set_reduction_callback",
+    "vlsg_batch_set_domains", "vlsg_batch_advect", "vlsg_batch_count_points",
+    "vlsg_batch_download", "vlsg_batch_get_values",
 ]

@@ -270,6 +270,76 @@ def advect_batch(contexts, params, threads=0):
     return list(results)
 
 
+class BatchContext(Context):
+    """The batching form: many independent domains advanced together in one
+    context (vlsg_batch_set_domains / vlsg_batch_advect): every pass of a
+    time step is one kernel launch over all domains, each domain with its own
+    gridDelta, velocity functor and time step."""
+
+    def set_domains(self, items):
+        """items: (grid, domain, velocity) triples -- a Grid periodic in x and y
+        (extents multiples of 8 points) and infinite in z, its Domain, and a
+        FunctorVelocity."""
+        from ._abi import BatchDomain, VelocityDesc
+
+        self._grids = []
+        keep = []
+        arr = (BatchDomain * len(items))()
+        for k, (grid, dom, vel) in enumerate(items):
+            gmin = np.array(grid.min[:3], np.int64)
+            gmax = np.array(grid.max[:3], np.int64)
+            bc = np.array(grid.bc[:3], np.int32)
+            idx = np.ascontiguousarray(dom.idx, np.int32)
+            val = np.ascontiguousarray(dom.values, np.float64)
+            rs = np.ascontiguousarray(dom.run_start, np.int32)
+            sg = np.ascontiguousarray(dom.run_sign, np.int8)
+            desc = vel.descriptor()
+            if not isinstance(desc, VelocityDesc):
+                raise RuntimeError("batching form: device velocity functors only")
+            keep += [gmin, gmax, bc, idx, val, rs, sg, desc]
+            arr[k] = BatchDomain(_p(gmin, ctypes.c_int64), _p(gmax, ctypes.c_int64),
+                                 _p(bc, ctypes.c_int32), float(grid.delta), len(val),
+                                 _p(idx, ctypes.c_int32), _p(val, ctypes.c_double), len(sg),
+                                 _p(rs, ctypes.c_int32), _p(sg, ctypes.c_int8), int(dom.width),
+                                 ctypes.pointer(desc))
+            self._grids.append(grid)
+        self._check(self.lib.vlsg_batch_set_domains(self.h, len(items), arr))
+        del keep
+
+    def advect(self, params):
+        n = len(self._grids)
+        results = (AdvectResult * n)()
+        self._check(self.lib.vlsg_batch_advect(self.h, ctypes.byref(params), results))
+        return list(results)
+
+    def count(self, domain):
+        n = ctypes.c_int64()
+        self._check(self.lib.vlsg_batch_count_points(self.h, int(domain), ctypes.byref(n)))
+        return n.value
+
+    def download(self, domain, idx_out=None, val_out=None):
+        """(idx, values, width) of domain `domain`'s defined points in HRLE
+        order, in its own indices."""
+        n = self.count(domain)
+        idx = np.empty((n, 3), np.int32)
+        val = np.empty(n)
+        w = ctypes.c_int32()
+        self._check(self.lib.vlsg_batch_download(self.h, int(domain), n, _p(idx, ctypes.c_int32),
+                                                 _p(val, ctypes.c_double), ctypes.byref(w)))
+        return idx, val, w.value
+
+    def values_at(self, domain, idx):
+        idx = np.ascontiguousarray(idx, np.int32)
+        out = np.zeros(len(idx))
+        self._check(self.lib.vlsg_batch_get_values(self.h, int(domain), len(idx),
+                                                   _p(idx, ctypes.c_int32), _p(out, ctypes.c_double)))
+        return out
+
+    def download_domain(self, domain, grid=None, out=None):
+        """Domain `domain` with its undefined runs rebuilt from point queries."""
+        return self.download_domain_host_runs(domain, grid or self._grids[domain])
+
+
 class Advect:
     """Mirror of viennals::Advect<T,3> running on the GPU."""
 

@@ -27,7 +27,7 @@ UNITS = {
 SOURCES = list(UNITS)
 HEADERS = ["vlsg_common.cuh", "vlsg_iface.h", "vlsg_passes.cuh", "vlsg_frontier.cuh",
            "vlsg_rates.cuh", "vlsg_maint.cuh", "vlsg_scan.cuh", "vlsg_exchange.cuh",
-           "vlsg_metrics.cuh", "vlsg_compare.cuh", "vlsg_velcb.cuh", "vlsg_voids.cuh", "vlsg_engine.cuh"]
+           "vlsg_metrics.cuh", "vlsg_compare.cuh", "vlsg_velcb.cuh", "vlsg_voids.cuh", "vlsg_batch.cuh", "vlsg_engine.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -39,6 +39,20 @@ struct vlsg_context {
   int64_t ownLo = 0, ownHi = 0;
   bool profiling = false;
   std::unique_ptr<EngineBase> eng; // Engine<double> or Engine<float>
+  // batching form (vlsg_batch_set_domains): where each domain lies in the
+  // shared brick box, and the box's points downloaded once per state
+  struct Batch {
+    int n = 0;
+    std::vector<int64_t> gmin, gmax;        // 3 per domain
+    std::vector<int64_t> shift;             // 3 per domain: box index = domain index + shift
+    std::vector<int64_t> z0, z1;            // box cell planes [z0, z1) of each domain
+    bool cached = false;
+    std::vector<int32_t> idx;               // the box's points in HRLE order
+    std::vector<double> val;
+    std::vector<int64_t> first;             // per domain: first point; [n]: total
+    int width = 2;
+  };
+  std::unique_ptr<Batch> batch;
 };
 
 namespace {
@@ -279,6 +293,7 @@ int vlsg_set_grid(vlsg_context *ctx, int32_t dim, const int64_t *gmin, const int
   if (dim != 3) return fail(ctx, VLSG_ERR_ARGUMENT, "only D = 3 is supported on the GPU");
   if (!gmin || !gmax || !bc || !(delta > 0))
     return fail(ctx, VLSG_ERR_ARGUMENT, "vlsg_set_grid: bad argument");
+  ctx->batch.reset(); // back to one domain
   GridDev g{};
   for (int d = 0; d < 3; ++d) {
     if (bc[d] < 0 || bc[d] > 4) return fail(ctx, VLSG_ERR_ARGUMENT, "unknown boundary condition");
@@ -342,6 +357,226 @@ int vlsg_upload_levelset(vlsg_context *ctx, int32_t slot, int64_t n, const int32
     s.nRuns = nRuns;
     s.width = width;
     ctx->dirty = true;
+    return VLSG_OK;
+  });
+}
+
+// ---------------------------------------------------------- batching form
+namespace {
+constexpr int32_t kInfIndex = (1 << 20) - 2; // run starts below the box: -kInfIndex
+
+// The box's points, downloaded once per state, split by domain.
+void batchCache(vlsg_context *ctx) {
+  auto &B = *ctx->batch;
+  if (B.cached) return;
+  const int64_t n = ctx->eng->compact(0, nullptr, nullptr, 0);
+  B.idx.resize(3 * (size_t)n);
+  B.val.resize((size_t)n);
+  ctx->eng->compact(0, B.idx.data(), B.val.data(), n);
+  B.width = ctx->eng->width(0);
+  // HRLE order is z-major and every domain owns a range of z planes
+  B.first.assign(B.n + 1, n);
+  int64_t p = 0;
+  for (int d = 0; d < B.n; ++d) {
+    while (p < n && B.idx[3 * p + 2] < B.z0[d]) ++p;
+    B.first[d] = p;
+  }
+  B.first[B.n] = n;
+  B.cached = true;
+}
+
+int batchDomain(vlsg_context *ctx, int32_t d) {
+  if (!ctx->batch || !ctx->eng) return fail(ctx, VLSG_ERR_STATE, "no batch of domains set");
+  if (d < 0 || d >= ctx->batch->n) return fail(ctx, VLSG_ERR_ARGUMENT, "domain out of range");
+  return VLSG_OK;
+}
+} // namespace
+
+int vlsg_batch_set_domains(vlsg_context *ctx, int32_t n, const vlsg_batch_domain *doms) {
+  if (!ctx) return fail(nullptr, VLSG_ERR_ARGUMENT, "NULL context");
+  if (n <= 0 || !doms) return fail(ctx, VLSG_ERR_ARGUMENT, "vlsg_batch_set_domains: no domains");
+  return guarded(ctx, [&] {
+    auto B = std::make_unique<vlsg_context::Batch>();
+    B->n = n;
+    B->gmin.resize(3 * (size_t)n), B->gmax.resize(3 * (size_t)n), B->shift.resize(3 * (size_t)n);
+    B->z0.resize(n), B->z1.resize(n);
+    std::vector<DomainDev> dd(n);
+    std::vector<double> delta(n);
+    std::vector<vlsg_velocity_desc> vels(n);
+    int64_t nPoints = 0, nRuns = 0, planes = 0, maxBx = 1, maxBy = 1;
+    constexpr int margin = 4; // brick planes above and below each band
+    for (int32_t d = 0; d < n; ++d) {
+      const vlsg_batch_domain &D = doms[d];
+      if (!D.grid_min || !D.grid_max || !D.boundary || !D.velocity || D.n_points <= 0 ||
+          !D.indices || !D.values || D.n_runs < 0 || (D.n_runs > 0 && (!D.run_start || !D.run_sign)))
+        return fail(ctx, VLSG_ERR_ARGUMENT, "vlsg_batch_set_domains: domain " + std::to_string(d) +
+                                                ": bad arrays");
+      if (D.boundary[0] != VLSG_PERIODIC_BOUNDARY || D.boundary[1] != VLSG_PERIODIC_BOUNDARY ||
+          D.boundary[2] != VLSG_INFINITE_BOUNDARY)
+        return fail(ctx, VLSG_ERR_ARGUMENT, "batching form: domains must be periodic in x and y "
+                                            "and infinite in z");
+      for (int k = 0; k < 2; ++k)
+        if ((D.grid_max[k] - D.grid_min[k]) % 8 != 0 || D.grid_max[k] <= D.grid_min[k])
+          return fail(ctx, VLSG_ERR_ARGUMENT, "batching form: periodic extents must be positive "
+                                              "multiples of 8 points");
+      int64_t zmin = INT64_MAX, zmax = INT64_MIN;
+      for (int64_t i = 0; i < D.n_points; ++i) {
+        zmin = std::min<int64_t>(zmin, D.indices[3 * i + 2]);
+        zmax = std::max<int64_t>(zmax, D.indices[3 * i + 2]);
+      }
+      const int64_t zo = (int64_t)std::floor((zmin - 8.0 * margin) / 8.0) * 8;
+      const int64_t nbz = (zmax + 8 * margin - zo) / 8 + 1;
+      for (int k = 0; k < 3; ++k) B->gmin[3 * d + k] = D.grid_min[k], B->gmax[3 * d + k] = D.grid_max[k];
+      B->shift[3 * d + 0] = -D.grid_min[0];
+      B->shift[3 * d + 1] = -D.grid_min[1];
+      B->shift[3 * d + 2] = 8 * planes - zo;
+      B->z0[d] = 8 * planes, B->z1[d] = 8 * (planes + nbz);
+      dd[d] = DomainDev{(int)((D.grid_max[0] - D.grid_min[0]) / 8), (int)((D.grid_max[1] - D.grid_min[1]) / 8),
+                        (int)planes, (int)(planes + nbz)};
+      maxBx = std::max<int64_t>(maxBx, dd[d].nbx), maxBy = std::max<int64_t>(maxBy, dd[d].nby);
+      planes += nbz;
+      delta[d] = D.grid_delta;
+      vels[d] = *D.velocity;
+      nPoints += D.n_points, nRuns += D.n_runs;
+    }
+    if (8 * planes >= (1 << 19) || 8 * maxBx >= (1 << 19) || 8 * maxBy >= (1 << 19) ||
+        nPoints > INT_MAX / 4 || nRuns > INT_MAX / 4)
+      return fail(ctx, VLSG_ERR_CAPACITY, "batching form: the domains do not fit one brick box");
+    // one level set holding every domain, translated into the box
+    std::vector<int32_t> idx(3 * (size_t)nPoints), rs(3 * (size_t)nRuns);
+    std::vector<double> val((size_t)nPoints);
+    std::vector<int8_t> sg((size_t)nRuns);
+    std::vector<int> domOfBz((size_t)planes);
+    int64_t p = 0, r = 0;
+    int width = doms[0].width;
+    for (int32_t d = 0; d < n; ++d) {
+      const vlsg_batch_domain &D = doms[d];
+      const int64_t *sh = &B->shift[3 * (size_t)d];
+      width = std::min(width, D.width);
+      for (int64_t i = 0; i < D.n_points; ++i, ++p) {
+        for (int k = 0; k < 3; ++k) idx[3 * p + k] = (int32_t)(D.indices[3 * i + k] + sh[k]);
+        val[p] = D.values[i];
+      }
+      for (int64_t i = 0; i < D.n_runs; ++i, ++r) {
+        const int32_t *q = &D.run_start[3 * i];
+        if (q[2] <= -kInfIndex) {
+          // before the domain's first point: from the start of its planes
+          rs[3 * r] = -kInfIndex, rs[3 * r + 1] = -kInfIndex, rs[3 * r + 2] = (int32_t)B->z0[d];
+        } else {
+          for (int k = 0; k < 3; ++k)
+            rs[3 * r + k] = q[k] <= -kInfIndex ? -kInfIndex : (int32_t)(q[k] + sh[k]);
+        }
+        sg[r] = D.run_sign[i];
+      }
+      for (int64_t z = dd[d].bz0; z < dd[d].bz1; ++z) domOfBz[z] = d;
+    }
+    std::vector<StagedLS> staged(1);
+    StagedLS &S = staged[0];
+    growDevice(S.idx, S.capIdx, idx.size());
+    growDevice(S.vals, S.capVals, val.size());
+    growDevice(S.runStart, S.capRunStart, rs.size());
+    growDevice(S.runSign, S.capRunSign, sg.size());
+    VLSG_CUDA(cudaMemcpyAsync(S.idx, idx.data(), idx.size() * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream));
+    VLSG_CUDA(cudaMemcpyAsync(S.vals, val.data(), val.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    if (nRuns) {
+      VLSG_CUDA(cudaMemcpyAsync(S.runStart, rs.data(), rs.size() * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream));
+      VLSG_CUDA(cudaMemcpyAsync(S.runSign, sg.data(), sg.size(), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    VLSG_CUDA(cudaStreamSynchronize(ctx->stream));
+    S.n = nPoints, S.nRuns = nRuns, S.width = width;
+    // the box: every domain from brick (0, 0), its planes stacked in z
+    GridDev g{};
+    for (int k = 0; k < 3; ++k) g.bc[k] = VLSG_INFINITE_BOUNDARY, g.org[k] = 0;
+    g.gmax[0] = (int)(8 * maxBx), g.gmax[1] = (int)(8 * maxBy), g.gmax[2] = (int)(8 * planes);
+    g.nb[0] = (int)maxBx, g.nb[1] = (int)maxBy, g.nb[2] = (int)planes;
+    g.delta = 1.0; // per domain in the batching form
+    if (!ctx->eng) {
+      unsigned char *scratch = nullptr;
+      const int rc = noallocScratch(ctx, ctx->device, &scratch);
+      if (rc != VLSG_OK) throw CudaError(ctx->err, rc);
+      ctx->eng.reset(ctx->precision == VLSG_FP64 ? makeEngineF64() : makeEngineF32());
+    }
+    ctx->eng->stream = ctx->stream;
+    ctx->eng->velCb = nullptr, ctx->eng->alphaCb = nullptr, ctx->eng->updCb = nullptr;
+    ctx->eng->profiling = ctx->profiling;
+    ctx->eng->buildBatch(g, dd, domOfBz, delta, vels, staged);
+    ctx->batch = std::move(B);
+    ctx->hasGrid = false; // the single-domain entry points need their own grid again
+    ctx->staged.clear();
+    ctx->dirty = true;
+    return VLSG_OK;
+  });
+}
+
+int vlsg_batch_advect(vlsg_context *ctx, const vlsg_advect_params *params,
+                      vlsg_advect_result *results) {
+  if (!ctx || !params || !results) return fail(ctx, VLSG_ERR_ARGUMENT, "bad argument");
+  return guarded(ctx, [&] {
+    if (!ctx->batch || !ctx->eng) return fail(ctx, VLSG_ERR_STATE, "no batch of domains set");
+    ctx->eng->stream = ctx->stream;
+    ctx->eng->profiling = ctx->profiling;
+    ctx->batch->cached = false;
+    ctx->eng->applyBatch(*params, results);
+    return VLSG_OK;
+  });
+}
+
+int vlsg_batch_count_points(vlsg_context *ctx, int32_t domain, int64_t *n) {
+  if (!ctx || !n) return fail(ctx, VLSG_ERR_ARGUMENT, "bad argument");
+  return guarded(ctx, [&] {
+    const int rc = batchDomain(ctx, domain);
+    if (rc != VLSG_OK) return rc;
+    batchCache(ctx);
+    *n = ctx->batch->first[domain + 1] - ctx->batch->first[domain];
+    return VLSG_OK;
+  });
+}
+
+int vlsg_batch_download(vlsg_context *ctx, int32_t domain, int64_t capacity, int32_t *idx,
+                        double *values, int32_t *width) {
+  if (!ctx || capacity < 0) return fail(ctx, VLSG_ERR_ARGUMENT, "bad argument");
+  return guarded(ctx, [&] {
+    const int rc = batchDomain(ctx, domain);
+    if (rc != VLSG_OK) return rc;
+    batchCache(ctx);
+    auto &B = *ctx->batch;
+    const int64_t a = B.first[domain], m = B.first[domain + 1] - a;
+    if (width) *width = B.width;
+    if (m > capacity) return fail(ctx, VLSG_ERR_CAPACITY, "download capacity too small");
+    if (m > 0 && (!idx || !values)) return fail(ctx, VLSG_ERR_ARGUMENT, "bad arrays");
+    const int64_t *sh = &B.shift[3 * (size_t)domain];
+    for (int64_t i = 0; i < m; ++i) {
+      for (int k = 0; k < 3; ++k) idx[3 * i + k] = (int32_t)(B.idx[3 * (a + i) + k] - sh[k]);
+      values[i] = B.val[a + i];
+    }
+    return VLSG_OK;
+  });
+}
+
+int vlsg_batch_get_values(vlsg_context *ctx, int32_t domain, int64_t n, const int32_t *idx,
+                          double *values) {
+  if (!ctx || n < 0 || (n > 0 && (!idx || !values)))
+    return fail(ctx, VLSG_ERR_ARGUMENT, "bad argument");
+  return guarded(ctx, [&] {
+    const int rc = batchDomain(ctx, domain);
+    if (rc != VLSG_OK) return rc;
+    if (n > INT_MAX / 4) return fail(ctx, VLSG_ERR_ARGUMENT, "too many queries");
+    auto &B = *ctx->batch;
+    const int64_t *sh = &B.shift[3 * (size_t)domain];
+    const int64_t *lo = &B.gmin[3 * (size_t)domain], *hi = &B.gmax[3 * (size_t)domain];
+    std::vector<int32_t> q(3 * (size_t)n);
+    for (int64_t i = 0; i < n; ++i) {
+      for (int k = 0; k < 2; ++k) { // periodic in x and y
+        const int64_t e = hi[k] - lo[k];
+        int64_t c = (idx[3 * i + k] - lo[k]) % e;
+        if (c < 0) c += e;
+        q[3 * i + k] = (int32_t)(lo[k] + c + sh[k]);
+      }
+      // z beyond the domain's planes: its first / last plane (no band there)
+      const int64_t z = std::min(std::max<int64_t>(idx[3 * i + 2] + sh[2], B.z0[domain]), B.z1[domain] - 1);
+      q[3 * i + 2] = (int32_t)z;
+    }
+    ctx->eng->queryValues(0, n, q.data(), values);
     return VLSG_OK;
   });
 }

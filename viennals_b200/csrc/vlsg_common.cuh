@@ -44,6 +44,19 @@ template <class T> __host__ __device__ inline bool isDef(T v) {
   return v != Lim<T>::max() && v != Lim<T>::lowest();
 }
 
+// Batching form: several independent domains share one brick box, stacked
+// in z (each in its own range of brick planes, so that every domain's HRLE
+// order is one contiguous stretch of the box's).  Per domain: its brick
+// extent in x and y (the periodic extent / 8; it starts at the box's first
+// brick) and its brick planes [bz0, bz1).  Every domain is periodic in x and
+// y with extents that are multiples of the brick edge and unbounded in z, so
+// no cell of the box is remapped: the 27-neighbour table wraps whole bricks
+// within each domain.
+struct DomainDev {
+  int nbx, nby;
+  int bz0, bz1;
+};
+
 // Grid and brick-map geometry, passed by value to kernels.
 struct GridDev {
   int gmin[3], gmax[3]; // index bounds of the grid
@@ -51,6 +64,10 @@ struct GridDev {
   int org[3];           // global cell index of brick (0,0,0), cell (0,0,0)
   int nb[3];            // bricks per direction in the map box
   double delta;
+  // batching form (nDom > 0): the domains and the domain of every brick plane
+  int nDom;
+  const DomainDev *dom;
+  const int *domOfBz;
 };
 
 __host__ __device__ inline int mapCoord(const GridDev &g, int d, int c) {
@@ -92,6 +109,16 @@ struct MapView {
 
 __device__ inline int brickIndex(const GridDev &g, int bx, int by, int bz) {
   return (bz * g.nb[1] + by) * g.nb[0] + bx;
+}
+
+// Batching form: brick (x, y, z) next to a brick of domain d (x, y at most
+// one brick outside d's extent), wrapped in x and y within d; false when z
+// lies outside d's brick planes.
+__device__ inline bool domainNeighbour(const GridDev &g, int d, int &x, int &y, int &z) {
+  const DomainDev D = g.dom[d];
+  x = (x + D.nbx) % D.nbx;
+  y = (y + D.nby) % D.nby;
+  return z >= D.bz0 && z < D.bz1;
 }
 
 // Value of global cell (x,y,z) (already mapped through the boundary

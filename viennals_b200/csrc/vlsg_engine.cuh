@@ -27,6 +27,7 @@
 #include "vlsg_maint.cuh"
 #include "vlsg_passes.cuh"
 #include "vlsg_rates.cuh"
+#include "vlsg_batch.cuh"
 #include "vlsg_velcb.cuh"
 #include "vlsg_voids.cuh"
 
@@ -55,6 +56,7 @@ public:
   unsigned long long *defCnt = nullptr; // defined cells per buffer (counted on demand)
   unsigned long long *rateCounts = nullptr; // active cells, band cells of the last rates
   int *nbr = nullptr;                   // 27 per slot
+  int *slotDom = nullptr;               // batching form: the domain of each slot
   uint8_t *cflag = nullptr;             // CF_* per slot
   uint8_t *core = nullptr;              // per brick: holds an uploaded point
   unsigned long long *small = nullptr;  // 0..5 point box, 6.. |value| bounds per level set
@@ -137,7 +139,7 @@ public:
          X_ROWC, X_ROWG, X_PB, X_GB, X_RSTART, X_RSIGN, X_RPB, X_KEEP, X_KPOS, X_OSTART,
          X_OSIGN, X_VCNT, X_VOFF, X_VSUMS, X_QC, X_QM, X_QN, X_QP, X_VS, X_VV, X_AD, X_AM,
          X_AC, X_AV, X_SKEY, X_SALPHA, X_QC2, X_QN2, X_QM2, X_QP2, X_VS2, X_VPARENT, X_VMASK,
-         X_VTOP, X_PSRC, X_PVEL, X_PDISS, X_COUNT };
+         X_VTOP, X_PSRC, X_PVEL, X_PDISS, X_SCAN2, X_COUNT };
   // pinned host staging of the velocity callback's queries and answers
   struct PinScratch {
     void *p = nullptr;
@@ -160,11 +162,16 @@ public:
   }
 
   void release() {
+    dropGraphs();
     auto f = [](void *p) { if (p) cudaFree(p); };
     for (auto &b : buf) f(b.lo);
     f(brickMap); f(slotBrick); f(slotList); f(freeStack); f(newList); f(counters); f(needed);
     f(scal); f(defCnt); f(rateCounts); f(nbr); f(cflag); f(core); f(small); f(rateV);
     f(rateStop); f(rateLen); f(act); f(logCell); f(logVal); f(logCount); f(visitSpare);
+    f(slotDom); slotDom = nullptr;
+    f(domDev); f(domOfBzDev); f(domDelta); f(domVelDev); f(domRed); f(domUpdates); f(domDt);
+    domDev = nullptr, domOfBzDev = nullptr, domDelta = nullptr, domVelDev = nullptr;
+    domRed = nullptr, domUpdates = nullptr, domDt = nullptr, nDom = 0;
     freePayload(pdCells);
     freePayload(pdLog);
     f(rateD);
@@ -421,14 +428,14 @@ public:
       for (void *p : {(void *)slotBrick, (void *)slotList, (void *)freeStack, (void *)newList,
                       (void *)nbr, (void *)cflag, (void *)act, (void *)logCell, (void *)logVal,
                       (void *)logCount, (void *)rateV, (void *)rateStop, (void *)rateLen,
-                      (void *)visitSpare})
+                      (void *)visitSpare, (void *)slotDom})
         if (p) VLSG_CUDA(cudaFree(p));
       for (auto &v : visit) {
         if (v) VLSG_CUDA(cudaFree(v));
         v = nullptr;
       }
       slotBrick = slotList = freeStack = newList = nbr = logCount = nullptr;
-      cflag = rateLen = nullptr, act = nullptr, logCell = nullptr;
+      cflag = rateLen = nullptr, act = nullptr, logCell = nullptr, slotDom = nullptr;
       logVal = rateV = rateStop = nullptr;
       const size_t n = std::max(c, capSlots);
       const int l = std::max(L, capL);
@@ -438,6 +445,7 @@ public:
       VLSG_CUDA(cudaMalloc(&newList, n * sizeof(int)));
       VLSG_CUDA(cudaMalloc(&nbr, n * 27 * sizeof(int)));
       VLSG_CUDA(cudaMalloc(&cflag, n));
+      VLSG_CUDA(cudaMalloc(&slotDom, n * sizeof(int)));
       VLSG_CUDA(cudaMalloc(&act, n * 8 * sizeof(uint64_t)));
       // pass grids: one wave of the GPU, or one warp per 8 slots for small
       // pools (the change log holds a segment per warp)
@@ -487,6 +495,8 @@ public:
   // are large enough.
   void build(const GridDev &grid, std::vector<StagedLS> &ls, int margin) override {
     ++generation;
+    dropGraphs(); // captured steps hold the old layout's pointers
+    batchSteps = 0;
     dropVisits();
     pdTrack = pdSave = pdHas = false;
     ensureSmall();
@@ -519,7 +529,8 @@ public:
     std::memcpy(hb, pinCounters + 16, sizeof(hb));
     if (hCounters[12]) sortRuns(ls);
     // box: bounded directions cover the grid, infinite ones the points + margin
-    for (int d = 0; d < 3; ++d) {
+    // (the batching form brings its box with the domain table)
+    for (int d = 0; d < 3 && !g.nDom; ++d) {
       const bool bounded = g.bc[d] == VLSG_PERIODIC_BOUNDARY || g.bc[d] == VLSG_REFLECTIVE_BOUNDARY;
       if (bounded) {
         g.org[d] = g.gmin[d];
@@ -690,7 +701,7 @@ public:
     {
       Scope sc(this, "neighbours");
       kBuildNeighbours<<<grid1(cap), 256, 0, stream>>>(g, brickMap, slotBrick, slotList,
-                                                       nSlotsPtr(), nbr, cflag);
+                                                       nSlotsPtr(), nbr, cflag, slotDom);
       checkLaunch();
     }
   }
@@ -815,7 +826,8 @@ public:
     buf[b].bound = 1.0;
   }
   // updateLevelSet (value update + Reduce(1)) followed by rebuildLS
-  void updateRebuild(double dt) {
+  // domDts (batching form): the time step per domain instead of dt
+  void updateRebuild(double dt, const double *domDts = nullptr) {
     const int top = L - 1;
     {
       // active values read and written, their rates read
@@ -825,7 +837,8 @@ public:
                                                           dt, errPtr(), loOf(top),
                                                           pdSave ? pdCells.vel : nullptr,
                                                           pdSave ? pdCells.diss : nullptr,
-                                                          pdSave ? rateD : nullptr);
+                                                          pdSave ? rateD : nullptr,
+                                                          domDts ? slotDom : nullptr, domDts);
       checkLaunch();
     }
     {
@@ -1506,6 +1519,275 @@ public:
     r.kernel_launches = launches - l0;
   }
 
+  // ------------------------------------------------------- batching form
+  // Many independent domains in one brick box (GridDev's domain table): one
+  // launch per pass and per rate / update step over the bricks of all
+  // domains, the time step of every domain on the device (kDomainSteps), no
+  // host synchronisation inside the step.
+  int nDom = 0;
+  DomainDev *domDev = nullptr;
+  int *domOfBzDev = nullptr;
+  double *domDelta = nullptr;
+  vlsg_velocity_desc *domVelDev = nullptr;
+  unsigned long long *domRed = nullptr;     // RED_WORDS per domain (vlsg_rates.cuh)
+  unsigned long long *domUpdates = nullptr; // point updates of the step per domain
+  double *domDt = nullptr;                  // stage steps a, b, c and advected time
+
+  void buildBatch(const GridDev &grid, const std::vector<DomainDev> &doms,
+                  const std::vector<int> &domOfBz, const std::vector<double> &delta,
+                  const std::vector<vlsg_velocity_desc> &vels, std::vector<StagedLS> &ls) override {
+    ensureSmall();
+    auto f = [](void *p) { if (p) cudaFree(p); };
+    f(domDev); f(domOfBzDev); f(domDelta); f(domVelDev); f(domRed); f(domUpdates); f(domDt);
+    nDom = (int)doms.size();
+    VLSG_CUDA(cudaMalloc(&domDev, nDom * sizeof(DomainDev)));
+    VLSG_CUDA(cudaMalloc(&domOfBzDev, domOfBz.size() * sizeof(int)));
+    VLSG_CUDA(cudaMalloc(&domDelta, nDom * sizeof(double)));
+    VLSG_CUDA(cudaMalloc(&domVelDev, nDom * sizeof(vlsg_velocity_desc)));
+    VLSG_CUDA(cudaMalloc(&domRed, (size_t)RED_WORDS * nDom * sizeof(unsigned long long)));
+    VLSG_CUDA(cudaMalloc(&domUpdates, nDom * sizeof(unsigned long long)));
+    VLSG_CUDA(cudaMalloc(&domDt, 4 * (size_t)nDom * sizeof(double)));
+    VLSG_CUDA(cudaMemcpyAsync(domDev, doms.data(), nDom * sizeof(DomainDev), cudaMemcpyHostToDevice, stream));
+    VLSG_CUDA(cudaMemcpyAsync(domOfBzDev, domOfBz.data(), domOfBz.size() * sizeof(int),
+                              cudaMemcpyHostToDevice, stream));
+    VLSG_CUDA(cudaMemcpyAsync(domDelta, delta.data(), nDom * sizeof(double), cudaMemcpyHostToDevice, stream));
+    VLSG_CUDA(cudaMemcpyAsync(domVelDev, vels.data(), nDom * sizeof(vlsg_velocity_desc),
+                              cudaMemcpyHostToDevice, stream));
+    std::vector<unsigned long long> red((size_t)RED_WORDS * nDom, 0ull);
+    for (int d = 0; d < nDom; ++d) red[(size_t)RED_WORDS * d + RED_MIN] = ~0ull;
+    VLSG_CUDA(cudaMemcpyAsync(domRed, red.data(), red.size() * sizeof(unsigned long long),
+                              cudaMemcpyHostToDevice, stream));
+    VLSG_CUDA(cudaStreamSynchronize(stream)); // the host vectors go out of scope
+    GridDev g2 = grid;
+    g2.nDom = nDom;
+    g2.dom = domDev;
+    g2.domOfBz = domOfBzDev;
+    build(g2, ls, 0);
+  }
+
+  // One forward-Euler stage of every domain: Expand, rates with per-domain
+  // reductions, the per-domain step (capped by cap, null: none) into out,
+  // value update, Reduce + rebuild.
+  void stageBatch(const vlsg_advect_params &P, const double *cap, double *out, bool first) {
+    const int top = L - 1;
+    expand(top, schemeWidth(P.spatial_scheme));
+    const int s = P.spatial_scheme;
+    const bool lfFamily = !(s == VLSG_ENGQUIST_OSHER_1ST_ORDER || s == VLSG_ENGQUIST_OSHER_2ND_ORDER ||
+                            s == VLSG_WENO_3RD_ORDER || s == VLSG_WENO_5TH_ORDER);
+    RateArgs<T> A{};
+    A.g = g;
+    A.m = mapView();
+    for (int l = 0; l < L; ++l) A.ls[l] = view(l);
+    A.L = L;
+    A.slotList = slotList;
+    A.nSlots = nSlotsPtr();
+    A.nbr = nbr;
+    A.cflag = cflag;
+    A.def = buf[top].def[buf[top].cur];
+    A.act = act;
+    A.scheme = s;
+    A.cfl = P.time_step_ratio;
+    A.dissipationAlpha = P.dissipation_alpha;
+    A.calcNormals = P.calculate_normal_vectors;
+    A.adaptive = P.adaptive_time_stepping;
+    A.adaptiveFactor = 1.0 / (P.adaptive_subdivisions < 1 ? 1u : P.adaptive_subdivisions);
+    A.checkDiss = P.check_dissipation;
+    A.rateV = rateV;
+    A.rateStop = rateStop;
+    A.rateLen = rateLen;
+    A.poolCells = poolCells;
+    A.err = errPtr();
+    A.slotDom = slotDom;
+    A.domDelta = domDelta;
+    A.domVel = domVelDev;
+    A.domRed = domRed;
+    {
+      Scope sc(this, "rates");
+      if (s == VLSG_WENO_3RD_ORDER || s == VLSG_WENO_5TH_ORDER)
+        kRates<T, 0, false, FAM_WENO, true><<<blocksRateWeno, RATE_THREADS, 0, stream>>>(A, vel);
+      else
+        kRates<T, 0, false, FAM_ANY, true><<<blocksRate, RATE_THREADS, 0, stream>>>(A, vel);
+      checkLaunch();
+    }
+    {
+      Scope sc(this, "domain_steps");
+      kDomainSteps<<<grid1(nDom), 256, 0, stream>>>(nDom, domRed, domDelta, lfFamily ? 1 : 0, cap,
+                                                    out, domUpdates, first ? 1 : 0, errPtr());
+      checkLaunch();
+    }
+    updateRebuild(0.0, out);
+    if (!deferMaintain) maintain();
+  }
+
+  // CUDA graphs of the batching form's time step.  A batch step reads
+  // nothing back until it ends, so its launches can be captured once and
+  // replayed.  The host tracks, between steps, which of two mask arrays is
+  // current per buffer and which array holds which buffer's visit flags; a
+  // captured step is only valid from the host state it was captured in, so
+  // graphs are kept per (state, parameters), and a replay leaves the host in
+  // the state the captured step ended in.
+  struct HostState {
+    int cur[MAXB], width[MAXB];
+    double bound[MAXB];
+    uint8_t live[MAXB], visitOk[MAXB];
+    uint8_t *visit[MAXB];
+    uint8_t *visitSpare;
+  };
+  HostState hostState() const {
+    HostState h;
+    std::memset(&h, 0, sizeof(h));
+    for (int b = 0; b < MAXB; ++b) {
+      h.cur[b] = buf[b].cur, h.width[b] = buf[b].width, h.bound[b] = buf[b].bound;
+      h.live[b] = buf[b].live, h.visitOk[b] = visitOk[b], h.visit[b] = visit[b];
+    }
+    h.visitSpare = visitSpare;
+    return h;
+  }
+  void setHostState(const HostState &h) {
+    for (int b = 0; b < MAXB; ++b) {
+      buf[b].cur = h.cur[b], buf[b].width = h.width[b], buf[b].bound = h.bound[b];
+      buf[b].live = h.live[b], visitOk[b] = h.visitOk[b], visit[b] = h.visit[b];
+    }
+    visitSpare = h.visitSpare;
+  }
+  struct StepGraph {
+    HostState pre, post;
+    vlsg_advect_params P;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t launches = 0;
+    uint32_t stages = 0;
+  };
+  std::vector<StepGraph> stepGraphs;
+  uint64_t batchSteps = 0;
+  void dropGraphs() {
+    for (auto &g2 : stepGraphs)
+      if (g2.exec) cudaGraphExecDestroy(g2.exec);
+    stepGraphs.clear();
+  }
+
+  // The device work of one batch step (no host reads).
+  void batchStepDevice(const vlsg_advect_params &P) {
+    double *dA = domDt, *dB = domDt + nDom, *dC = domDt + 2 * nDom, *tm = domDt + 3 * nDom;
+    VLSG_CUDA(cudaMemsetAsync(domUpdates, 0, nDom * sizeof(unsigned long long), stream));
+    switch (P.temporal_scheme) {
+    case VLSG_RUNGE_KUTTA_2ND_ORDER:
+      deferMaintain = P.time_step_ratio <= 0.5;
+      saveTop(P, 2);
+      stageBatch(P, nullptr, dA, true);
+      stageBatch(P, dA, dB, false);
+      combineLevelSets(P, 0.5, 0.5);
+      endStep();
+      break;
+    case VLSG_RUNGE_KUTTA_3RD_ORDER:
+      deferMaintain = P.time_step_ratio <= 0.5;
+      saveTop(P, 3);
+      stageBatch(P, nullptr, dA, true);
+      stageBatch(P, dA, dB, false);
+      combineLevelSets(P, 0.75, 0.25);
+      stageBatch(P, dA, dC, false);
+      combineLevelSets(P, 1.0 / 3.0, 2.0 / 3.0);
+      endStep();
+      break;
+    default:
+      stageBatch(P, nullptr, dA, true);
+      break;
+    }
+    {
+      Scope sc(this, "domain_time");
+      kDomainTime<<<grid1(nDom), 256, 0, stream>>>(nDom, P.temporal_scheme, dA, dB, dC, tm);
+      checkLaunch();
+    }
+  }
+
+  void applyBatch(const vlsg_advect_params &P, vlsg_advect_result *res) override {
+    if (!nDom) throw CudaError("no batch of domains set", VLSG_ERR_STATE);
+    const int s = P.spatial_scheme;
+    if (schemeWidth(s) < 0) throw CudaError("Advect: Discretization scheme not found.", VLSG_ERR_ARGUMENT);
+    if (s == VLSG_LAX_FRIEDRICHS_1ST_ORDER || s == VLSG_LAX_FRIEDRICHS_2ND_ORDER ||
+        s == VLSG_STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER)
+      throw CudaError("batching form: global Lax-Friedrichs and Stencil-LLF schemes are not "
+                      "supported", VLSG_ERR_ARGUMENT);
+    if (P.advection_time != 0.)
+      throw CudaError("batching form: one time step per call (advection_time 0)", VLSG_ERR_ARGUMENT);
+    if (P.ignore_voids || P.track_point_data || P.save_advection_velocities || P.fp32_compensation)
+      throw CudaError("batching form: voids, point data and FP32 compensation are not supported",
+                      VLSG_ERR_ARGUMENT);
+    if (velCb || updCb) throw CudaError("batching form: device velocity functors only", VLSG_ERR_STATE);
+    ++generation;
+    deferMaintain = false;
+    saveTopAt = 0;
+    pdTrack = pdSave = pdHas = false;
+    compActive = false;
+    loValid = false;
+    pristine = false;
+    rebuildCutoff = 1.0;
+    rebuildWidth = 2;
+    pointUpdates = 0;
+    stages = 0;
+    const uint64_t l0 = launches;
+    double *dA = domDt, *dB = domDt + nDom, *dC = domDt + 2 * nDom, *tm = domDt + 3 * nDom;
+    const double *last = P.temporal_scheme == VLSG_RUNGE_KUTTA_2ND_ORDER   ? dB
+                         : P.temporal_scheme == VLSG_RUNGE_KUTTA_3RD_ORDER ? dC
+                                                                            : dA;
+    // the first step runs as it is (it sizes what the step allocates); later
+    // steps replay the graph captured from the same host state and
+    // parameters, capturing it the first time (not while profiling, whose
+    // per-launch events read the device back)
+    const HostState pre = hostState();
+    StepGraph *hit = nullptr;
+    for (auto &sg : stepGraphs)
+      if (!std::memcmp(&sg.pre, &pre, sizeof(pre)) && !std::memcmp(&sg.P, &P, sizeof(P))) hit = &sg;
+    if (hit) {
+      VLSG_CUDA(cudaGraphLaunch(hit->exec, stream));
+      setHostState(hit->post);
+      launches += hit->launches;
+      stages = hit->stages;
+    } else if (batchSteps > 0 && !profiling) {
+      StepGraph sg;
+      sg.pre = pre;
+      sg.P = P;
+      VLSG_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed));
+      try {
+        batchStepDevice(P);
+      } catch (...) {
+        cudaGraph_t gr = nullptr;
+        cudaStreamEndCapture(stream, &gr);
+        if (gr) cudaGraphDestroy(gr);
+        throw;
+      }
+      cudaGraph_t gr = nullptr;
+      VLSG_CUDA(cudaStreamEndCapture(stream, &gr));
+      const cudaError_t e = cudaGraphInstantiate(&sg.exec, gr, 0);
+      cudaGraphDestroy(gr);
+      VLSG_CUDA(e);
+      sg.post = hostState();
+      sg.launches = launches - l0;
+      sg.stages = stages;
+      VLSG_CUDA(cudaGraphLaunch(sg.exec, stream));
+      stepGraphs.push_back(sg);
+    } else {
+      batchStepDevice(P);
+    }
+    ++batchSteps;
+    std::vector<double> hTime(nDom), hLast(nDom);
+    std::vector<unsigned long long> hUpd(nDom);
+    VLSG_CUDA(cudaMemcpyAsync(hTime.data(), tm, nDom * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    VLSG_CUDA(cudaMemcpyAsync(hLast.data(), last, nDom * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    VLSG_CUDA(cudaMemcpyAsync(hUpd.data(), domUpdates, nDom * sizeof(unsigned long long),
+                              cudaMemcpyDeviceToHost, stream));
+    syncErr("batch advect");
+    const uint64_t nl = launches - l0;
+    for (int d = 0; d < nDom; ++d) {
+      res[d].advected_time = hTime[d];
+      res[d].current_time_step = hLast[d];
+      res[d].number_of_time_steps = 1;
+      res[d].number_of_stages = stages;
+      res[d].point_updates = hUpd[d];
+      res[d].kernel_launches = nl;
+      pointUpdates += hUpd[d];
+    }
+  }
+
   // ------------------------------------------------------------ download
   int64_t countDefined(int b) override { return defined(b); }
   int width(int b) const override { return buf[b].width; }
@@ -1555,16 +1837,25 @@ public:
     return (V *)xs[k].p;
   }
   // Exclusive scan of n counts; the total lands in sums[(n + tile - 1) / tile].
-  void scanExclusive(const uint32_t *in, uint32_t *out, size_t n, uint32_t *sums) {
+  // Up to SCAN_TOP_THREADS * SCAN_TOP_ITEMS tiles the tile sums are scanned
+  // by one block; beyond that (a batch of many domains has a large brick
+  // box) they are scanned by this same three-kernel scan, one level deeper.
+  void scanExclusive(const uint32_t *in, uint32_t *out, size_t n, uint32_t *sums, int depth = 0) {
     const size_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
-    if (nb > (size_t)SCAN_TOP_THREADS * SCAN_TOP_ITEMS)
-      throw CudaError("exchange: too many elements for the scan", VLSG_ERR_CAPACITY);
     if (nb == 0) {
       VLSG_CUDA(cudaMemsetAsync(sums, 0, sizeof(uint32_t), stream));
       return;
     }
     kScanReduce<<<(unsigned)nb, SCAN_THREADS, 0, stream>>>(in, n, sums);
-    kScanTop<<<1, SCAN_TOP_THREADS, 0, stream>>>(sums, (int)nb);
+    if (nb <= (size_t)SCAN_TOP_THREADS * SCAN_TOP_ITEMS) {
+      kScanTop<<<1, SCAN_TOP_THREADS, 0, stream>>>(sums, (int)nb);
+    } else {
+      if (depth >= 1) throw CudaError("exchange: too many elements for the scan", VLSG_ERR_CAPACITY);
+      uint32_t *sums2 = scratch<uint32_t>(X_SCAN2, scanScratch(nb) + 64);
+      scanExclusive(sums, sums, nb, sums2, depth + 1); // in place: each tile is read before written
+      VLSG_CUDA(cudaMemcpyAsync(sums + nb, sums2 + (nb + SCAN_TILE - 1) / SCAN_TILE, sizeof(uint32_t),
+                                cudaMemcpyDeviceToDevice, stream));
+    }
     kScanApply<<<(unsigned)nb, SCAN_THREADS, 0, stream>>>(in, n, sums, out);
     checkLaunch();
   }

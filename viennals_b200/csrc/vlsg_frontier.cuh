@@ -695,12 +695,28 @@ __device__ inline bool remapNear(const GridDev &g, int d, int lo, int hi) {
 
 __global__ void kBuildNeighbours(GridDev g, const int *brickMap, const int *slotBrick,
                                  const int *slotList, const int *nSlots, int *nbr,
-                                 uint8_t *cflag) {
+                                 uint8_t *cflag, int *slotDom) {
   const int n = *nSlots;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int slot = slotList[i];
     int bx, by, bz;
     brickCoords(g, slotBrick[slot], bx, by, bz);
+    if (g.nDom) {
+      // batching form: wrap within the brick's domain; a neighbour past the
+      // domain's brick planes is the nearest plane's (unallocated) brick
+      const int d = g.domOfBz[bz];
+      slotDom[slot] = d;
+      cflag[slot] = 0;
+      for (int k = 0; k < 27; ++k) {
+        int x = bx + k % 3 - 1, y = by + (k / 3) % 3 - 1, z = bz + k / 9 - 1;
+        const bool inside = domainNeighbour(g, d, x, y, z);
+        if (!inside) z = z < g.dom[d].bz0 ? g.dom[d].bz0 : g.dom[d].bz1 - 1;
+        const int bi = brickIndex(g, x, y, z);
+        const int s = brickMap[bi];
+        nbr[(size_t)slot * 27 + k] = (s >= 0 && inside) ? s : -1 - bi;
+      }
+      continue;
+    }
     const int bc[3] = {bx, by, bz};
     uint8_t f = 0;
     for (int d = 0; d < 3; ++d) {

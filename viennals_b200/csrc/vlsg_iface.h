@@ -151,6 +151,14 @@ public:
   // and dissipation); returns the number of points, or -1 when the level set
   // carries no point data.  Nothing is written when cap is too small.
   virtual int64_t pointData(int b, int64_t *src, double *vel, double *diss, int64_t cap) = 0;
+  // batching form: the domain table and one level set holding every domain
+  // (stacked in z, in the box `grid` gives), then one time step of all
+  // domains with results per domain
+  virtual void buildBatch(const GridDev &grid, const std::vector<DomainDev> &doms,
+                          const std::vector<int> &domOfBz, const std::vector<double> &delta,
+                          const std::vector<vlsg_velocity_desc> &vels,
+                          std::vector<StagedLS> &ls) = 0;
+  virtual void applyBatch(const vlsg_advect_params &P, vlsg_advect_result *res) = 0;
 };
 
 EngineBase *makeEngineF32();

@@ -41,6 +41,18 @@ __device__ inline bool neighbourBrick(const GridDev &g, int &x, int &y, int &z) 
 __device__ inline void markDilated(const GridDev &g, int bi, uint8_t *needed, int *err) {
   int bx, by, bz;
   brickCoords(g, bi, bx, by, bz);
+  if (g.nDom) {
+    // the band must stay off the domain's first and last brick planes
+    const int d = g.domOfBz[bz];
+    if (bz <= g.dom[d].bz0 || bz >= g.dom[d].bz1 - 1) atomicOr(err, 1);
+    for (int dz = -1; dz <= 1; ++dz)
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx) {
+          int x = bx + dx, y = by + dy, z = bz + dz;
+          if (domainNeighbour(g, d, x, y, z)) needed[brickIndex(g, x, y, z)] = 1;
+        }
+    return;
+  }
   const int c[3] = {bx, by, bz};
   for (int d = 0; d < 3; ++d)
     if (g.bc[d] != VLSG_PERIODIC_BOUNDARY && g.bc[d] != VLSG_REFLECTIVE_BOUNDARY &&

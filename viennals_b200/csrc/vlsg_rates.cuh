@@ -160,7 +160,16 @@ template <class T> struct RateArgs {
   // step, the alphas and the point updates (ownZ false: every point)
   bool ownZ;
   int ownLo, ownHi;
+  // batching form (slotDom non-null): per slot its domain; per domain its
+  // gridDelta and velocity functor, and this pass's reductions (RED_* words
+  // per domain: smallest step bits, alpha bits x3, active cells) in place of
+  // minStep / alphaMax / counts
+  const int *slotDom;
+  const double *domDelta;
+  const vlsg_velocity_desc *domVel;
+  unsigned long long *domRed;
 };
+constexpr int RED_MIN = 0, RED_ALPHA = 1, RED_ACTIVE = 4, RED_WORDS = 5;
 
 // Reader of the top level set around one active point.
 template <class T> struct Stencil {
@@ -441,13 +450,13 @@ enum : int { FAM_ANY = 0, FAM_WENO = 1, FAM_STENCIL = 2 };
 template <class T, class St, class Vel, int FAM = FAM_ANY>
 __device__ void evalScheme(const RateArgs<T> &A, const Vel &vel,
                            const St &S, T C, int material, T *alphas,
-                           T &outG, T &outD) {
+                           T &outG, T &outD, double delta) {
   if constexpr (FAM == FAM_STENCIL) {
     (void)C;
     evalStencilLLF<T>(A, vel, S, material, alphas, outG, outD);
     return;
   }
-  const T gridDelta = T(A.g.delta);
+  const T gridDelta = T(delta);
   const int sch = A.scheme;
   if (FAM == FAM_WENO || sch == VLSG_WENO_3RD_ORDER || sch == VLSG_WENO_5TH_ORDER) {
     const int r = sch == VLSG_WENO_3RD_ORDER ? 2 : 3;
@@ -688,7 +697,8 @@ __device__ inline unsigned long long warpMaxU64(unsigned long long b) {
 // lsAdvect.hpp:738-744, and the stop value) and the point's time budget.
 template <class T, class St, class Vel, int FAM = FAM_ANY>
 __device__ inline double ratePoint(const RateArgs<T> &A, const Vel &vel,
-                                   const St &S, int slot, int c, T C, T *alphas) {
+                                   const St &S, int slot, int c, T C, T *alphas,
+                                   double delta) {
   const int L = A.L;
   const size_t q = (size_t)slot * BV + c;
   T value = C;
@@ -701,7 +711,7 @@ __device__ inline double ratePoint(const RateArgs<T> &A, const Vel &vel,
     for (int lower = 0; lower < L && !isVoid; ++lower) {
       const T lv = lower == L - 1 ? C : lsValueAt<T>(A.ls[lower], slot, c);
       if ((double)lv <= (double)value + 1e-4) {
-        evalScheme<T, St, Vel, FAM>(A, vel, S, C, lower, alphas, g, d);
+        evalScheme<T, St, Vel, FAM>(A, vel, S, C, lower, alphas, g, d, delta);
         break;
       }
     }
@@ -792,7 +802,9 @@ template <class T, int FAM = FAM_ANY> constexpr int rateMinBlocks() {
 // MODE 0: rates (integrateTime); MODE 1: the global alphas of the
 // Lax-Friedrichs schemes (findGlobalAlphas).  TABLE: velocities from the
 // host callback's table instead of the device functor.
-template <class T, int MODE, bool TABLE = false, int FAM = FAM_ANY>
+// BATCH: the batching form (per-domain spacing, velocity and reductions,
+// A.slotDom set).
+template <class T, int MODE, bool TABLE = false, int FAM = FAM_ANY, bool BATCH = false>
 __global__ void __launch_bounds__(RATE_THREADS, rateMinBlocks<T, FAM>())
     kRates(RateArgs<T> A, const vlsg_velocity_desc desc) {
   __shared__ uint16_t sList[RATE_THREADS / 32][BV];
@@ -807,8 +819,33 @@ __global__ void __launch_bounds__(RATE_THREADS, rateMinBlocks<T, FAM>())
   // StencilLLF: HRLE key and finalAlphas of this thread's last passing call
   unsigned long long lastKey = 0;
   T lastAlpha[3] = {0, 0, 0};
+  // batching form: the domain whose partial reductions the registers hold;
+  // they go to its RED_* words when the warp moves to another domain's brick
+  int dom = -1;
+  double delta = A.g.delta;
+  const auto flushDomain = [&] {
+    minBits = warpMinU64(minBits);
+    for (int d = 0; d < 3; ++d) alphaMax[d] = warpMaxU64(alphaMax[d]);
+    for (int o = 16; o > 0; o >>= 1) nAct += __shfl_xor_sync(0xffffffffu, nAct, o);
+    if (lane == 0) {
+      unsigned long long *red = A.domRed + (size_t)RED_WORDS * dom;
+      if (MODE == 0 && minBits != ~0ull) atomicMin(red + RED_MIN, minBits);
+      for (int d = 0; d < 3; ++d)
+        if (alphaMax[d]) atomicMax(red + RED_ALPHA + d, alphaMax[d]);
+      if (MODE == 0 && nAct) atomicAdd(red + RED_ACTIVE, nAct);
+    }
+    minBits = ~0ull, alphaMax[0] = alphaMax[1] = alphaMax[2] = 0, nAct = nBand = 0;
+  };
   for (int w = warp; w < n; w += nWarps) {
     const int slot = A.slotList[w];
+    if constexpr (BATCH) {
+      const int d = A.slotDom[slot];
+      if (d != dom) {
+        if (dom >= 0) flushDomain();
+        dom = d;
+        delta = A.domDelta[d];
+      }
+    }
     const uint64_t own = lane < 8 ? A.def[(size_t)slot * 8 + lane] : 0ull;
     uint64_t a = 0ull;
     if (__any_sync(0xffffffffu, own != 0ull)) a = activePlanes<T>(top.vals, slot);
@@ -836,6 +873,8 @@ __global__ void __launch_bounds__(RATE_THREADS, rateMinBlocks<T, FAM>())
           return TableVel{A.velS, A.velV, ((size_t)A.actOff[w] + k) * L * A.velSites,
                           A.velSites, A.alphaTab, ((size_t)A.actOff[w] + k) * L * 81,
                           A.velS2, ((size_t)A.actOff[w] + k) * L * 162};
+        else if constexpr (BATCH)
+          return FunctorVel{A.domVel[dom]};
         else
           return FunctorVel{desc};
       }();
@@ -846,7 +885,7 @@ __global__ void __launch_bounds__(RATE_THREADS, rateMinBlocks<T, FAM>())
           T alphas[STENCIL ? 4 : 3] = {};
           const double step =
               ratePoint<T, std::decay_t<decltype(S)>, std::decay_t<decltype(vel)>, FAM>(
-                  A, vel, S, slot, c, value, alphas);
+                  A, vel, S, slot, c, value, alphas, delta);
           if (!owned) return; // a ghost point: advanced, not counted
           const unsigned long long sb = stepBits(step);
           minBits = sb < minBits ? sb : minBits;
@@ -905,6 +944,10 @@ __global__ void __launch_bounds__(RATE_THREADS, rateMinBlocks<T, FAM>())
       A.sllfKey[warp] = best;
       for (int d = 0; d < 3; ++d) A.sllfAlpha[3 * warp + d] = (double)lastAlpha[d];
     }
+  }
+  if constexpr (BATCH) {
+    if (dom >= 0) flushDomain();
+    return;
   }
   minBits = warpMinU64(minBits);
   for (int d = 0; d < 3; ++d) alphaMax[d] = warpMaxU64(alphaMax[d]);
@@ -965,7 +1008,8 @@ template <class T>
 __global__ void __launch_bounds__(RATE_THREADS)
     kUpdate(const int *slotList, const int *nSlots, const uint64_t *act, T *vals,
             const T *rateV, const T *rateStop, const uint8_t *rateLen, size_t poolCells, int L,
-            double dt, int *err, float *lo, T *pvel, T *pdiss, const T *rateD) {
+            double dt, int *err, float *lo, T *pvel, T *pdiss, const T *rateD,
+            const int *slotDom = nullptr, const double *domDt = nullptr) {
   __shared__ uint16_t sList[RATE_THREADS / 32][BV];
   uint16_t *list = sList[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
@@ -976,6 +1020,8 @@ __global__ void __launch_bounds__(RATE_THREADS)
     const int slot = slotList[w];
     const uint64_t a = lane < 8 ? act[(size_t)slot * 8 + lane] : 0ull;
     if (!__any_sync(0xffffffffu, a != 0ull)) continue;
+    // batching form: the time step of the slot's domain
+    const double dtS = domDt ? domDt[slotDom[slot]] : dt;
     const int total = listCells(a, list);
     for (int base = 0; base < total; base += 32) {
       const int k = base + lane;
@@ -990,7 +1036,7 @@ __global__ void __launch_bounds__(RATE_THREADS)
       if constexpr (sizeof(T) == 4) {
         if (lo) {
           double value = withLo((double)vals[q], lo[q]);
-          double time = dt;
+          double time = dtS;
           int j = 0;
           double velocity = rateV[q];
           double rate = time * velocity;
@@ -1018,7 +1064,7 @@ __global__ void __launch_bounds__(RATE_THREADS)
         }
       }
       T value = vals[q];
-      double time = dt;
+      double time = dtS;
       int j = 0;
       T velocity = rateV[q];
       T rate = T(time * velocity);
