@@ -20,11 +20,14 @@ namespace { // internal linkage: every compilation unit has its own copy
 // Every rule also names the cell whose point data its result carries (the
 // source ids of the reference's passes): src -1 the centre, 0..5 star
 // neighbour src, -2 none.
+// Sign classes are decided with the FP64 epsilon in both precisions: the FP32
+// precision form follows the decisions of Advect<double>, the path it is held
+// to (Advect<float> would compare with FLT_EPSILON).
 template <class T> struct ExpandRule {
   T totalLimit, limit;
   __device__ T operator()(T c, const T *nb, int &src) const {
     if (fabs(c) <= totalLimit) return c;
-    if (c > -Lim<T>::eps()) {
+    if ((double)c > -Lim<double>::eps()) {
       T distance = Lim<T>::max();
       for (int i = 0; i < 6; ++i) {
         const T nv = nb[i] + T(1);
@@ -43,7 +46,7 @@ template <class T> struct ExpandRule {
 
 template <class T> struct PruneRule {
   bool removeStrayZeros;
-  __device__ static bool neg(T a) { return a <= -Lim<T>::eps(); }
+  __device__ static bool neg(T a) { return (double)a <= -Lim<double>::eps(); }
   __device__ static bool diff(T a, T b) { return neg(a) != neg(b); }
   __device__ T operator()(T c, const T *nb, int &src) const {
     const bool cneg = neg(c);

@@ -183,11 +183,14 @@ def batch_domains(n=256, seed=7, points_range=(1e4, 2e6), device=None):
             lateral = lmin
             surf = lateral * lateral + (math.pi * width * depth if hole else 2.0 * lateral * depth)
             gd = float(np.clip(math.sqrt(2.5 * surf / target), 0.05, 0.2))
-        cells = max(16, int(round(lateral / gd)))
-        half = cells * gd / 2.0
+        # periodic extents in whole bricks (multiples of 8 points), which the
+        # batching form's shared brick box needs
+        cells = max(16, 8 * int(round(lateral / gd / 8.0)))
+        c2 = cells // 2
         zlo, zhi = -depth - 1.5, 1.5
-        grid = Grid([-half, half, -half, half, zlo, zhi],
-                    [BC.PERIODIC_BOUNDARY, BC.PERIODIC_BOUNDARY, BC.INFINITE_BOUNDARY], gd)
+        grid = Grid(None, [BC.PERIODIC_BOUNDARY, BC.PERIODIC_BOUNDARY, BC.INFINITE_BOUNDARY], gd,
+                    index_min=[-c2, -c2, math.floor(zlo / gd)],
+                    index_max=[c2, c2, math.ceil(zhi / gd)])
         r = width / 2.0
         lo = [grid.min[0], grid.min[1], grid.min[2]]
         hi = [grid.max[0] - 1, grid.max[1] - 1, grid.max[2]]
@@ -293,16 +296,15 @@ def _sdf_band_torch(grid, sdf, lo, hi, device, chunk_cells=1 << 24):
 
 
 def hole_stack(lateral_cells=4096, grid_delta=0.02, pitch=1.28, radius=0.5, depth=2.0,
-               layers=(0.1, 0.3), shift=(0.31, 0.17), device="cpu"):
+               layers=(0.1, 0.3), shift=(0.0, 0.0), device="cpu"):
     """The stacked-layer hole array: a substrate (material 0) with a square
     array of cylindrical holes (radius, depth, pitch; periodic in x/y) under
     two slabs on the flat top between the holes, of thickness layers[0]
     (material 1) and layers[1] (material 2, the top level set); every level
     set wraps the ones below.  Velocity per material 1.0 / 0.6 / 0.0 plus
-    0.2 |n_z|.  The hole axes sit `shift` cells off the grid points: with
-    axes on grid points, cells at exactly the radius carry values of order
-    1e-9 whose sign FP32 and FP64 Prune decide differently (it compares with
-    the precision's epsilon), which moves the lower bands by a cell.
+    0.2 |n_z|.  The hole axes lie on grid points, `shift` cells away when
+    given: cells at exactly the radius then carry values of order 1e-9, whose
+    sign classes both precisions decide with the FP64 epsilon.
     Returns (grid, [three Domains], velocity)."""
     import torch
 
