@@ -374,9 +374,10 @@ def batching_report(args, device):
     RK2, FP32, per-domain rates in [0.2, 1.5]; one RK2 step of every domain
     advanced three ways: one context after another (loop), vlsg_advect_batch
     (host threads, one stream per context) and the batch context (every pass
-    one launch over all domains, per-domain time steps on the device).  Each
-    way is warmed by one step first and timed by the host clock around the
-    step; all three must end identical."""
+    one launch over all domains, per-domain time steps on the device, the
+    step replayed from a CUDA graph).  Each way is warmed by two steps and
+    the third is timed by the host clock around it; all three must end
+    identical."""
     import numpy as np
     import torch
 
@@ -417,6 +418,7 @@ def batching_report(args, device):
                     else (lambda: [c.advect(p) for c in cs]))
         try:
             step()  # sizes the buffers
+            step()  # the batch context captures its step into a CUDA graph here
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             res = step()
@@ -458,6 +460,93 @@ def batching_report(args, device):
             "identical": bool(upd_loop == upd_thr == upd_b and same(got_loop, got_thr)
                               and same(got_loop, got_b)),
             "generation_s": gen_s, "timing": "host clock around one step of every domain"}
+
+
+def deposition_report(args):
+    """Config 5, the stacked deposition over a periodic hole array: (1024 x
+    tiles)^2 lateral cells at gridDelta 0.02 (tiles 4: the stated 4096^2,
+    64 x 64 holes of radius 0.5 and depth 2.0), three level sets, rates
+    1.0 / 0.6 / 0.0 + 0.2 |n_z|, WENO5 + RK3, CFL 0.4, 20 steps, FP32.  The
+    input is the 1024^2 workload tiled (synth.tiled_hole_stack), so every
+    1024^2 tile of the result must equal the FP32 1024^2 run bit for bit
+    (checked on the four corner tiles).  The 20 steps are timed with CUDA
+    events on the context's stream."""
+    import numpy as np
+    import torch
+
+    from viennals_b200 import AdvectParams
+    from viennals_b200._abi import Precision
+    from viennals_b200.advect import Context
+    from viennals_b200.domain import lex_order
+    from viennals_b200.synth import tiled_hole_stack
+
+    dev = f"cuda:{args.local_rank}"
+    t0 = time.time()
+    grid, doms, vel, grid_s, doms_s = tiled_hole_stack(args.deposition_tiles, 1024, device=dev)
+    gen_s = time.time() - t0
+    p = AdvectParams.defaults()
+    p.spatial_scheme = 11  # WENO_5TH_ORDER
+    p.temporal_scheme = 2  # RUNGE_KUTTA_3RD_ORDER
+    p.time_step_ratio = 0.4
+    p.advection_time = 1.0
+    p.single_step = 1
+    steps = 20
+
+    def run(g, ds, timed):
+        stream = torch.cuda.Stream(device=dev)
+        c = Context(args.local_rank, Precision.FP32)
+        c.set_stream(stream.cuda_stream)
+        c.set_grid(g)
+        c.set_level_set_count(len(ds))
+        for i, d in enumerate(ds):
+            c.upload(i, d)
+        c.set_velocity(vel.descriptor())
+        c.count(len(ds) - 1)  # builds the layout before the timed region
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        upd = 0
+        t = 0.0
+        e0.record(stream)
+        for _ in range(steps):
+            r = c.advect(p)
+            upd += r.point_updates
+            t += r.advected_time
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        used = torch.cuda.mem_get_info()[1] - min(free0, torch.cuda.mem_get_info()[0])
+        out = [c.download(i)[:2] for i in range(len(ds))]
+        c.close()
+        return out, {"ms": ms, "updates": upd, "time": t, "device_bytes_used": int(used)}
+
+    big, rb = run(grid, doms, True)
+    small, rs = run(grid_s, doms_s, False)
+    n, tiles = 1024, args.deposition_tiles
+    half_big = tiles * n // 2
+    same = rb["time"] == rs["time"]
+    for (bi, bv), (si, sv) in zip(big, small):
+        same &= len(bi) == tiles * tiles * len(si)
+        for a, b in ((0, 0), (0, tiles - 1), (tiles - 1, 0), (tiles - 1, tiles - 1)):
+            x0, y0 = -half_big + n * a, -half_big + n * b
+            m = (bi[:, 0] >= x0) & (bi[:, 0] < x0 + n) & (bi[:, 1] >= y0) & (bi[:, 1] < y0 + n)
+            ti = bi[m].astype(np.int64)
+            ti[:, 0] -= x0 + n // 2
+            ti[:, 1] -= y0 + n // 2
+            o = lex_order(ti)
+            same &= bool(np.array_equal(ti[o], si)) and bool(
+                np.array_equal(bv[m][o].view(np.int64), sv.view(np.int64)))
+    return {"workload": f"stacked deposition over a periodic hole array, {tiles * n}^2 lateral "
+                        f"cells at gridDelta 0.02 ({tiles * 16} x {tiles * 16} holes, r 0.5, depth "
+                        f"2.0), 3 level sets, rates 1.0/0.6/0.0 + 0.2|n_z|, WENO5 + RK3, CFL 0.4, "
+                        f"FP32, {steps} steps",
+            "band_points_per_level_set": [int(d.n_points) for d in doms],
+            "point_updates": int(rb["updates"]), "ms": rb["ms"],
+            "point_updates_per_s": rb["updates"] / (rb["ms"] / 1e3),
+            "advected_time": rb["time"], "device_bytes_used": rb["device_bytes_used"],
+            "tiles_equal_the_1024_run": bool(same), "generation_s": gen_s,
+            "timing": "CUDA events around the 20 vlsg_advect calls on the context stream"}
 
 
 def cpu_baseline(args, sample_radius, steps=1, threads=None):
@@ -602,6 +691,8 @@ def main():
     ap.add_argument("--batch-domains", type=int, default=256,
                     help="domains of the batching-form report (0: skip)")
     ap.add_argument("--batch-threads", type=int, default=16)
+    ap.add_argument("--deposition-tiles", type=int, default=0,
+                    help="run only the deposition workload at (1024 x tiles)^2 lateral cells")
     ap.add_argument("--err-steps", type=int, default=50,
                     help="RK3 steps of the FP32-vs-FP64 precision report (0: skip)")
     args = ap.parse_args()
@@ -613,6 +704,11 @@ def main():
                        f"(seed {args.seed}), WENO5+RK3, CFL 0.4, v=1+0.3 n_z",
            "precision": args.precision, "step": "one RK3 time step (3 FE stages + 2 combines)",
            "l2": "inputs larger than L2 (band ~17M points, ~1.3 GB of values per buffer at R 40)", "parallelism": f"replicas x{world}"}
+
+    if args.deposition_tiles > 0:
+        print(json.dumps({"metric": "deposition point-updates/s (FP32)",
+                          "deposition": deposition_report(args)}))
+        return
 
     if args.impl == "reference":
         if rank != 0:

@@ -437,8 +437,12 @@ int vlsg_batch_advect(vlsg_context *ctx, const vlsg_advect_params *params,
 int vlsg_batch_count_points(vlsg_context *ctx, int32_t domain, int64_t *n_points);
 int vlsg_batch_download(vlsg_context *ctx, int32_t domain, int64_t capacity,
                         int32_t *indices, double *values, int32_t *width);
+/* Domain d's undefined runs, in the layout and with the capacity protocol
+ * of vlsg_download_runs (built on the host from point queries). */
+int vlsg_batch_download_runs(vlsg_context *ctx, int32_t domain, int64_t capacity,
+                             int32_t *run_start, int8_t *run_sign, int64_t *n_runs);
 /* vlsg_get_values for domain d (its indices, mapped through its periodic
- * boundaries): what a caller rebuilds the undefined runs from. */
+ * boundaries). */
 int vlsg_batch_get_values(vlsg_context *ctx, int32_t domain, int64_t n,
                           const int32_t *indices, double *values);
 

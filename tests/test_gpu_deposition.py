@@ -62,57 +62,23 @@ def test_deposition_hole_stack_fp32_vs_fp64():
 @pytest.mark.gpu
 def test_deposition_hole_stack_2048_fp32_tiles():
     """FP32 at 2048^2 lateral cells (32 x 32 holes, four times the area of
-    the FP64 comparison above; the full 4096^2 extent does not fit one GPU,
-    see the memory arithmetic in the design notes).  The input is the 1024^2
-    workload tiled 2 x 2 (the hole array's period divides 1024 cells), so
-    after 20 steps every 1024^2 tile of the 2048^2 run must equal the 1024^2
-    run bit for bit: nothing in a step depends on where a point lies."""
+    the FP64 comparison above; the full 4096^2 extent is bench.py's
+    --deposition-tiles 4 run).  The input is the 1024^2 workload tiled 2 x 2
+    (the hole period divides 1024 cells), so after 20 steps every 1024^2
+    tile of the 2048^2 run must equal the 1024^2 run bit for bit: nothing in
+    a step depends on where a point lies."""
     import time
 
     import numpy as np
 
     from parity_cases import params
     from viennals_b200 import SpatialSchemeEnum as S, TemporalSchemeEnum as TS
-    from viennals_b200.advect import Context
-    from viennals_b200.domain import Domain, Grid, lex_order, make_runs
-    from viennals_b200.synth import hole_stack
+    from viennals_b200.domain import lex_order
+    from viennals_b200.synth import tiled_hole_stack
 
     p = params(S.WENO_5TH_ORDER, TS.RUNGE_KUTTA_3RD_ORDER, 1.0, cfl=0.4, single_step=1)
-    grid_s, doms_s, vel = hole_stack(lateral_cells=1024, device="cuda")
+    grid_l, doms_l, vel, grid_s, doms_s = tiled_hole_stack(2, 1024, device="cuda")
     n = 1024
-    grid_l = Grid(None, grid_s.bc, grid_s.delta, index_min=[-n, -n, grid_s.min[2]],
-                  index_max=[n, n, grid_s.max[2]])
-    # the tiled input: points shifted into the four tiles, runs rebuilt from
-    # the small level set's signs
-    q = Context(0, 1)
-    q.set_grid(grid_s)
-    q.set_level_set_count(3)
-    for i, d in enumerate(doms_s):
-        q.upload(i, d)
-    doms_l = []
-    for i, d in enumerate(doms_s):
-        parts = []
-        for a in range(2):
-            for b in range(2):
-                t = d.idx.astype(np.int64).copy()
-                t[:, 0] += n * a - n // 2
-                t[:, 1] += n * b - n // 2
-                parts.append(t)
-        idx = np.concatenate(parts)
-        val = np.tile(d.values, 4)
-        o = lex_order(idx)
-        idx, val = idx[o], val[o]
-
-        def sign_fn(x, y, z, i=i):
-            w = np.stack([(np.asarray(x) + n // 2) % n - n // 2, (np.asarray(y) + n // 2) % n - n // 2,
-                          np.asarray(z)], 1).astype(np.int32)
-            return np.where(q.values_at(i, w) < 0, -1, 1)
-
-        lo = idx.min(0) - 1
-        hi = idx.max(0) + 1
-        rs, sg = make_runs(idx, sign_fn, lo, hi)
-        doms_l.append(Domain(grid_l, idx.astype(np.int32), val, rs, sg, width=d.width))
-    q.close()
     small, t_s, _ = advect_steps(grid_s, doms_s, vel, p, 1, 20)
     small_pts = [small.download(i)[:2] for i in range(3)]
     small.close()

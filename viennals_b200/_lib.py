@@ -53,6 +53,7 @@ def load(build_if_missing=True):
     L.vlsg_batch_count_points.argtypes = [vp, i32, P(i64)]
     L.vlsg_batch_download.argtypes = [vp, i32, i64, P(i32), P(ctypes.c_double), P(i32)]
     L.vlsg_batch_get_values.argtypes = [vp, i32, i64, P(i32), P(ctypes.c_double)]
+    L.vlsg_batch_download_runs.argtypes = [vp, i32, i64, P(i32), P(ctypes.c_int8), P(i64)]
     L.vlsg_get_values_noalloc.argtypes = [vp, i32, i64, P(i32), P(ctypes.c_double)]
     L.vlsg_set_velocity_functor.argtypes = [vp, P(VelocityDesc)]
     L.vlsg_set_velocity_callback.argtypes = [vp, VELOCITY_CALLBACK, vp]
@@ -81,5 +82,5 @@ EXPORTED = [
     "vlsg_set_profiling", "vlsg_get_kernel_stats", "vlsg_compare",
     "vlsg_set_owned_region", "vlsg_set_reduction_callback",
     "vlsg_batch_set_domains", "vlsg_batch_advect", "vlsg_batch_count_points",
-    "vlsg_batch_download", "vlsg_batch_get_values",
+    "vlsg_batch_download", "vlsg_batch_get_values", "vlsg_batch_download_runs",
 ]

@@ -335,9 +335,23 @@ class BatchContext(Context):
                                                    _p(idx, ctypes.c_int32), _p(out, ctypes.c_double)))
         return out
 
+    def download_runs(self, domain):
+        n = ctypes.c_int64()
+        rc = self.lib.vlsg_batch_download_runs(self.h, int(domain), 0, None, None, ctypes.byref(n))
+        if rc not in (0, -3):  # -3: the count, with capacity 0
+            self._check(rc)
+        rs = np.empty((n.value, 3), np.int32)
+        sg = np.empty(n.value, np.int8)
+        self._check(self.lib.vlsg_batch_download_runs(self.h, int(domain), n.value,
+                                                      _p(rs, ctypes.c_int32), _p(sg, ctypes.c_int8),
+                                                      ctypes.byref(n)))
+        return rs, sg
+
     def download_domain(self, domain, grid=None, out=None):
-        """Domain `domain` with its undefined runs rebuilt from point queries."""
-        return self.download_domain_host_runs(domain, grid or self._grids[domain])
+        """Domain `domain`: its points and its undefined runs."""
+        idx, val, w = self.download(domain)
+        rs, sg = self.download_runs(domain)
+        return Domain(grid or self._grids[domain], idx, val, rs, sg, width=w)
 
 
 class Advect:

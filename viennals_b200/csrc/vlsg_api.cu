@@ -553,6 +553,105 @@ int vlsg_batch_download(vlsg_context *ctx, int32_t domain, int64_t capacity, int
   });
 }
 
+int vlsg_batch_download_runs(vlsg_context *ctx, int32_t domain, int64_t capacity,
+                             int32_t *runStart, int8_t *runSign, int64_t *nRuns) {
+  if (!ctx || !nRuns || capacity < 0 || (capacity > 0 && (!runStart || !runSign)))
+    return fail(ctx, VLSG_ERR_ARGUMENT, "bad argument");
+  return guarded(ctx, [&] {
+    const int rc = batchDomain(ctx, domain);
+    if (rc != VLSG_OK) return rc;
+    batchCache(ctx);
+    auto &B = *ctx->batch;
+    const int64_t a = B.first[domain], m = B.first[domain + 1] - a;
+    const int64_t *sh = &B.shift[3 * (size_t)domain];
+    // the layout of vlsg_download_runs over the box [min - 1, max + 1] of the
+    // domain's points (indices in the domain's own grid)
+    int64_t lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    if (m) {
+      for (int k = 0; k < 3; ++k) lo[k] = INT64_MAX, hi[k] = INT64_MIN;
+      for (int64_t i = 0; i < m; ++i)
+        for (int k = 0; k < 3; ++k) {
+          const int64_t v = B.idx[3 * (a + i) + k] - sh[k];
+          lo[k] = std::min(lo[k], v), hi[k] = std::max(hi[k], v);
+        }
+      for (int k = 0; k < 3; ++k) --lo[k], ++hi[k];
+    }
+    const int64_t NI = -kInfIndex;
+    auto floorDiv2 = [](int64_t v) { return v >= 0 ? v / 2 : -((-v + 1) / 2); };
+    const int64_t cxf = floorDiv2(lo[0] + hi[0]), cyf = floorDiv2(lo[1] + hi[1]);
+    struct Ev { int64_t s[3], at[3]; };
+    std::vector<Ev> ev;
+    auto add = [&](int64_t sx, int64_t sy, int64_t sz, int64_t ax, int64_t ay, int64_t az) {
+      ev.push_back(Ev{{sx, sy, sz}, {ax, ay, az}});
+    };
+    add(NI, NI, NI, cxf, cyf, lo[2] - 1);
+    add(NI, NI, hi[2] + 1, cxf, cyf, hi[2] + 1);
+    for (int64_t z = lo[2]; z <= hi[2]; ++z) {
+      add(NI, NI, z, cxf, lo[1] - 1, z);
+      add(NI, hi[1] + 1, z, cxf, hi[1] + 1, z);
+    }
+    // rows of the box: a run at the head of every row (at its first point, or
+    // the whole row), one after every point not followed by its +x neighbour
+    const int64_t ny = hi[1] - lo[1] + 1, nz = hi[2] - lo[2] + 1;
+    if (ny * nz > ((int64_t)1 << 34)) return fail(ctx, VLSG_ERR_CAPACITY, "runs: box too large");
+    std::vector<uint8_t> has((size_t)(ny * nz), 0);
+    auto P = [&](int64_t i, int k) { return B.idx[3 * (a + i) + k] - sh[k]; };
+    for (int64_t i = 0; i < m; ++i) {
+      const int64_t x = P(i, 0), y = P(i, 1), z = P(i, 2);
+      const bool first = i == 0 || P(i - 1, 1) != y || P(i - 1, 2) != z;
+      const bool last = i + 1 == m || P(i + 1, 1) != y || P(i + 1, 2) != z;
+      if (first) {
+        has[(size_t)((z - lo[2]) * ny + (y - lo[1]))] = 1;
+        add(NI, y, z, x - 1, y, z);
+      }
+      if (last || P(i + 1, 0) > x + 1) add(x + 1, y, z, x + 1, y, z);
+    }
+    for (int64_t z = lo[2]; z <= hi[2]; ++z)
+      for (int64_t y = lo[1]; y <= hi[1]; ++y)
+        if (!has[(size_t)((z - lo[2]) * ny + (y - lo[1]))]) add(NI, y, z, lo[0], y, z);
+    // signs of the cells the runs start at, through the domain's query
+    const int64_t ne = (int64_t)ev.size();
+    std::vector<int32_t> q(3 * (size_t)ne);
+    for (int64_t i = 0; i < ne; ++i)
+      for (int k = 0; k < 3; ++k) q[3 * i + k] = (int32_t)ev[i].at[k];
+    std::vector<double> vals((size_t)ne);
+    const int qrc = vlsg_batch_get_values(ctx, domain, ne, q.data(), vals.data());
+    if (qrc != VLSG_OK) return qrc;
+    auto key = [](const int64_t *c) {
+      return ((uint64_t)(c[2] + (1 << 20)) << 42) | ((uint64_t)(c[1] + (1 << 20)) << 21) |
+             (uint64_t)(c[0] + (1 << 20));
+    };
+    std::vector<int64_t> o((size_t)ne);
+    for (int64_t i = 0; i < ne; ++i) o[i] = i;
+    std::stable_sort(o.begin(), o.end(),
+                     [&](int64_t x, int64_t y) { return key(ev[x].s) < key(ev[y].s); });
+    std::vector<uint64_t> pk((size_t)m);
+    for (int64_t i = 0; i < m; ++i) {
+      const int64_t c[3] = {P(i, 0), P(i, 1), P(i, 2)};
+      pk[i] = key(c);
+    }
+    // drop a run that repeats the previous run's sign with no point between
+    std::vector<int64_t> keepIdx;
+    int8_t prevSign = 0;
+    int64_t prevBefore = -1;
+    for (int64_t j = 0; j < ne; ++j) {
+      const Ev &e = ev[o[j]];
+      const int8_t sg = vals[o[j]] < 0 ? -1 : 1;
+      const int64_t before = std::lower_bound(pk.begin(), pk.end(), key(e.s)) - pk.begin();
+      if (j == 0 || sg != prevSign || before != prevBefore) keepIdx.push_back(o[j]);
+      prevSign = sg, prevBefore = before;
+      vals[o[j]] = sg;
+    }
+    *nRuns = (int64_t)keepIdx.size();
+    if (capacity < *nRuns) return fail(ctx, VLSG_ERR_CAPACITY, "run capacity too small");
+    for (size_t i = 0; i < keepIdx.size(); ++i) {
+      for (int k = 0; k < 3; ++k) runStart[3 * i + k] = (int32_t)ev[keepIdx[i]].s[k];
+      runSign[i] = (int8_t)vals[keepIdx[i]];
+    }
+    return VLSG_OK;
+  });
+}
+
 int vlsg_batch_get_values(vlsg_context *ctx, int32_t domain, int64_t n, const int32_t *idx,
                           double *values) {
   if (!ctx || n < 0 || (n > 0 && (!idx || !values)))

@@ -79,8 +79,13 @@ public:
     size_t capLo = 0;
   };
   DBuf buf[MAXB];
-  T *rateV = nullptr, *rateStop = nullptr; // pool shaped, L chain entries
+  // rates of the active points, compact: rateCap entries per chain entry
+  // (L of them), found per slot through rateBase (vlsg_rates.cuh)
+  T *rateV = nullptr, *rateStop = nullptr;
   uint8_t *rateLen = nullptr;
+  unsigned long long *rateBase = nullptr; // per slot
+  size_t rateCap = 0;
+  int rateL = 0;
   uint64_t *act = nullptr;  // active masks of the top level set
   // change log of a pass: one segment of logPer entries per warp of the pass
   uint32_t *logCell = nullptr;
@@ -169,9 +174,11 @@ public:
     f(scal); f(defCnt); f(rateCounts); f(nbr); f(cflag); f(core); f(small); f(rateV);
     f(rateStop); f(rateLen); f(act); f(logCell); f(logVal); f(logCount); f(visitSpare);
     f(slotDom); slotDom = nullptr;
+    f(rateBase); rateBase = nullptr; rateCap = 0; rateL = 0;
     f(domDev); f(domOfBzDev); f(domDelta); f(domVelDev); f(domRed); f(domUpdates); f(domDt);
+    f(domRedInit);
     domDev = nullptr, domOfBzDev = nullptr, domDelta = nullptr, domVelDev = nullptr;
-    domRed = nullptr, domUpdates = nullptr, domDt = nullptr, nDom = 0;
+    domRed = nullptr, domUpdates = nullptr, domDt = nullptr, domRedInit = nullptr, nDom = 0;
     freePayload(pdCells);
     freePayload(pdLog);
     f(rateD);
@@ -257,7 +264,7 @@ public:
     const int top = L - 1;
     allocPayload(pdCells, capPdCells, poolCells);
     allocPayload(pdLog, capPdLog, logPer * (size_t)logSegments);
-    if (pdSave) growDevice(rateD, capRateD, poolCells * (size_t)L);
+    if (pdSave) growDevice(rateD, capRateD, std::max<size_t>(rateCap, 1) * (size_t)L);
     const int nList = readI32(nSlotsPtr());
     xBuf = -1; // the point layout below reuses the exchange's scratch
     pointLayout(top, nList);
@@ -427,16 +434,15 @@ public:
     if (c > 0 && (c > capSlots || L > capL)) {
       for (void *p : {(void *)slotBrick, (void *)slotList, (void *)freeStack, (void *)newList,
                       (void *)nbr, (void *)cflag, (void *)act, (void *)logCell, (void *)logVal,
-                      (void *)logCount, (void *)rateV, (void *)rateStop, (void *)rateLen,
-                      (void *)visitSpare, (void *)slotDom})
+                      (void *)logCount, (void *)visitSpare, (void *)slotDom, (void *)rateBase})
         if (p) VLSG_CUDA(cudaFree(p));
       for (auto &v : visit) {
         if (v) VLSG_CUDA(cudaFree(v));
         v = nullptr;
       }
       slotBrick = slotList = freeStack = newList = nbr = logCount = nullptr;
-      cflag = rateLen = nullptr, act = nullptr, logCell = nullptr, slotDom = nullptr;
-      logVal = rateV = rateStop = nullptr;
+      cflag = nullptr, act = nullptr, logCell = nullptr, slotDom = nullptr, rateBase = nullptr;
+      logVal = nullptr;
       const size_t n = std::max(c, capSlots);
       const int l = std::max(L, capL);
       VLSG_CUDA(cudaMalloc(&slotBrick, n * sizeof(int)));
@@ -461,14 +467,30 @@ public:
       for (auto &v : visit) VLSG_CUDA(cudaMalloc(&v, n));
       VLSG_CUDA(cudaMalloc(&visitSpare, n));
       dropVisits();
-      VLSG_CUDA(cudaMalloc(&rateV, n * BV * sizeof(T) * l));
-      VLSG_CUDA(cudaMalloc(&rateStop, n * BV * sizeof(T) * l));
-      VLSG_CUDA(cudaMalloc(&rateLen, n * BV));
+      VLSG_CUDA(cudaMalloc(&rateBase, n * sizeof(unsigned long long)));
       capSlots = n;
       capL = l;
     }
     cap = (int)capSlots;
     poolCells = (size_t)cap * BV;
+  }
+
+  // Compact rate arrays for at least n active points and L chain entries
+  // (the saved dissipation too with setSaveAdvectionVelocities).
+  void ensureRateCap(size_t n) {
+    if (n <= rateCap && L <= rateL && rateV && (!pdSave || (rateD && capRateD >= rateCap * L)))
+      return;
+    const size_t c = std::max(n, rateCap);
+    const int l = std::max(L, rateL);
+    for (void *p : {(void *)rateV, (void *)rateStop, (void *)rateLen})
+      if (p) VLSG_CUDA(cudaFree(p));
+    rateV = rateStop = nullptr, rateLen = nullptr;
+    VLSG_CUDA(cudaMalloc(&rateV, c * l * sizeof(T)));
+    VLSG_CUDA(cudaMalloc(&rateStop, c * l * sizeof(T)));
+    VLSG_CUDA(cudaMalloc(&rateLen, c));
+    rateCap = c, rateL = l;
+    if (pdSave) growDevice(rateD, capRateD, c * l);
+    dropGraphs(); // captured steps hold the old arrays
   }
 
   void ensureSmall() {
@@ -484,7 +506,7 @@ public:
     VLSG_CUDA(cudaMalloc(&counters, 16 * sizeof(int)));
     VLSG_CUDA(cudaMalloc(&scal, 4 * sizeof(unsigned long long)));
     VLSG_CUDA(cudaMalloc(&defCnt, MAXB * sizeof(unsigned long long)));
-    VLSG_CUDA(cudaMalloc(&rateCounts, 2 * sizeof(unsigned long long)));
+    VLSG_CUDA(cudaMalloc(&rateCounts, 4 * sizeof(unsigned long long))); // active, band, rate entries
     VLSG_CUDA(cudaMalloc(&small, 16 * sizeof(unsigned long long)));
   }
 
@@ -570,10 +592,20 @@ public:
     const long long nNeeded = hCounters[13];
     // the pool keeps room for the band to grow: reallocate only when the
     // allocated slots fall below 1.25x the needed ones, then to 2x
+    // (2x, or less where 2x would take more than about half of the free
+    // device memory: every level set and its RK copy hold values and masks
+    // for every slot, and the change log a share of 512 cells per slot)
     {
       const size_t minSlots = (size_t)std::max<long long>(1024, nNeeded + nNeeded / 4 + 256);
-      ensureLayout(nBricks, capSlots >= minSlots ? capSlots
-                                                 : (size_t)std::max<long long>(1024, nNeeded * 2 + 256));
+      size_t want = (size_t)std::max<long long>(1024, nNeeded * 2 + 256);
+      size_t freeB = 0, totalB = 0;
+      if (cudaMemGetInfo(&freeB, &totalB) == cudaSuccess) {
+        const size_t perSlot = (size_t)(2 * L) * (BV * sizeof(T) + 2 * 8 * sizeof(uint64_t) + 1) +
+                               (size_t)BV * (sizeof(uint32_t) + sizeof(T)) + 27 * sizeof(int) + 128;
+        const size_t budget = freeB / 100 * 55 / perSlot;
+        if (want > budget) want = std::max(minSlots, budget);
+      }
+      ensureLayout(nBricks, capSlots >= minSlots ? capSlots : want);
     }
     {
       Scope sc(this, "upload_pool");
@@ -685,6 +717,8 @@ public:
       if (e & 64) m += " band reached an unallocated brick;";
       if (e & 128) m += " a point index lies outside the supported range (+-2^19);";
       if (e & 256) m += " the void search did not settle within its bound;";
+      if (e & 512) m += " batching form: a domain's first stage found no positive time step;";
+      if (e & 1024) m += " the rate storage was too small for the active points;";
       int z = 0;
       cudaMemcpy(errPtr(), &z, sizeof(int), cudaMemcpyHostToDevice);
       throw CudaError(m, (e & 4) ? VLSG_ERR_CAPACITY : VLSG_ERR_DEVICE_CHECK);
@@ -833,7 +867,7 @@ public:
       // active values read and written, their rates read
       Scope sc(this, "update", [this] { return 3.0 * double(sizeof(T)) * double(lastActive); });
       kUpdate<T><<<blocksPass, RATE_THREADS, 0, stream>>>(slotList, nSlotsPtr(), act, buf[top].vals,
-                                                          rateV, rateStop, rateLen, poolCells, L,
+                                                          rateV, rateStop, rateLen, rateBase, rateCap, L,
                                                           dt, errPtr(), loOf(top),
                                                           pdSave ? pdCells.vel : nullptr,
                                                           pdSave ? pdCells.diss : nullptr,
@@ -1019,11 +1053,6 @@ public:
     A.adaptive = P.adaptive_time_stepping;
     A.adaptiveFactor = 1.0 / (P.adaptive_subdivisions < 1 ? 1u : P.adaptive_subdivisions);
     A.checkDiss = P.check_dissipation;
-    A.rateV = rateV;
-    A.rateStop = rateStop;
-    A.rateD = pdSave ? rateD : nullptr;
-    A.rateLen = rateLen;
-    A.poolCells = poolCells;
     A.minStep = scal;
     A.counts = rateCounts;
     A.err = errPtr();
@@ -1069,6 +1098,18 @@ public:
     }
     A.voidMask = P.ignore_voids ? markVoids() : nullptr;
     if (velCb) gatherVelocities<0>(A);
+    if (!rateCap) ensureRateCap(65536);
+    for (;;) {
+    // the compact rate arrays; a pass that finds them too small is run again
+    // with larger ones (the bricks left out wrote nothing)
+    A.rateV = rateV;
+    A.rateStop = rateStop;
+    A.rateD = pdSave ? rateD : nullptr;
+    A.rateLen = rateLen;
+    A.rateCap = rateCap;
+    A.rateNext = rateCounts + 2;
+    A.rateBase = rateBase;
+    VLSG_CUDA(cudaMemsetAsync(rateCounts + 2, 0, sizeof(unsigned long long), stream));
     {
       // stencil input (each band value once) + output per active point
       Scope sc(this, "rates", [this] {
@@ -1093,9 +1134,15 @@ public:
       checkLaunch();
     }
     VLSG_CUDA(cudaMemcpyAsync(pinScal, scal, sizeof(init), cudaMemcpyDeviceToHost, stream));
-    VLSG_CUDA(cudaMemcpyAsync(pinScal + 4, rateCounts, 2 * sizeof(unsigned long long),
+    VLSG_CUDA(cudaMemcpyAsync(pinScal + 4, rateCounts, 3 * sizeof(unsigned long long),
                               cudaMemcpyDeviceToHost, stream));
     syncErr("rates");
+    const unsigned long long need = pinScal[6];
+    if (need <= rateCap) break;
+    ensureRateCap(need + need / 4 + 4096);
+    VLSG_CUDA(cudaMemcpyAsync(scal, init, sizeof(init), cudaMemcpyHostToDevice, stream));
+    VLSG_CUDA(cudaMemsetAsync(rateCounts, 0, 2 * sizeof(unsigned long long), stream));
+    }
     std::memcpy(hScal, pinScal, sizeof(hScal));
     lastActive = (int64_t)pinScal[4];
     lastBand = (int64_t)pinScal[5];
@@ -1530,6 +1577,7 @@ public:
   double *domDelta = nullptr;
   vlsg_velocity_desc *domVelDev = nullptr;
   unsigned long long *domRed = nullptr;     // RED_WORDS per domain (vlsg_rates.cuh)
+  unsigned long long *domRedInit = nullptr; // their reset values
   unsigned long long *domUpdates = nullptr; // point updates of the step per domain
   double *domDt = nullptr;                  // stage steps a, b, c and advected time
 
@@ -1539,12 +1587,15 @@ public:
     ensureSmall();
     auto f = [](void *p) { if (p) cudaFree(p); };
     f(domDev); f(domOfBzDev); f(domDelta); f(domVelDev); f(domRed); f(domUpdates); f(domDt);
+    f(domRedInit);
     nDom = (int)doms.size();
+    rateShape[0] = rateShape[1] = 0; // tune again for the new batch
     VLSG_CUDA(cudaMalloc(&domDev, nDom * sizeof(DomainDev)));
     VLSG_CUDA(cudaMalloc(&domOfBzDev, domOfBz.size() * sizeof(int)));
     VLSG_CUDA(cudaMalloc(&domDelta, nDom * sizeof(double)));
     VLSG_CUDA(cudaMalloc(&domVelDev, nDom * sizeof(vlsg_velocity_desc)));
     VLSG_CUDA(cudaMalloc(&domRed, (size_t)RED_WORDS * nDom * sizeof(unsigned long long)));
+    VLSG_CUDA(cudaMalloc(&domRedInit, (size_t)RED_WORDS * nDom * sizeof(unsigned long long)));
     VLSG_CUDA(cudaMalloc(&domUpdates, nDom * sizeof(unsigned long long)));
     VLSG_CUDA(cudaMalloc(&domDt, 4 * (size_t)nDom * sizeof(double)));
     VLSG_CUDA(cudaMemcpyAsync(domDev, doms.data(), nDom * sizeof(DomainDev), cudaMemcpyHostToDevice, stream));
@@ -1557,12 +1608,79 @@ public:
     for (int d = 0; d < nDom; ++d) red[(size_t)RED_WORDS * d + RED_MIN] = ~0ull;
     VLSG_CUDA(cudaMemcpyAsync(domRed, red.data(), red.size() * sizeof(unsigned long long),
                               cudaMemcpyHostToDevice, stream));
+    VLSG_CUDA(cudaMemcpyAsync(domRedInit, red.data(), red.size() * sizeof(unsigned long long),
+                              cudaMemcpyHostToDevice, stream));
     VLSG_CUDA(cudaStreamSynchronize(stream)); // the host vectors go out of scope
     GridDev g2 = grid;
     g2.nDom = nDom;
     g2.dom = domDev;
     g2.domOfBz = domOfBzDev;
     build(g2, ls, 0);
+  }
+
+  // Launch-shape autotuner of the batching form.  The rate kernel is
+  // compiled for several resident-block counts per SM (FP32: 2, 3 or 4, i.e.
+  // up to 128, 80 or 64 registers per thread; FP64: 1 or 2): more blocks hide
+  // more latency, fewer spill less.  The first stage of the first batch step
+  // runs every shape once (the pass only reads the level sets, so it can run
+  // again; its reductions are reset in between) and keeps the fastest per
+  // scheme family (WENO or not) until the batch changes.
+  int rateShape[2] = {0, 0};
+  bool capturing = false;
+  static const char *rateShapeName(int k) {
+    switch (k) {
+    case 1: return "rates_b1";
+    case 2: return "rates_b2";
+    case 3: return "rates_b3";
+    default: return "rates_b4";
+    }
+  }
+  void launchBatchRates(const RateArgs<T> &A, bool weno, int k) {
+    const dim3 grid(numSMs * k);
+    if constexpr (sizeof(T) == 4) {
+      if (weno) {
+        if (k == 2) kRates<T, 0, false, FAM_WENO, true, 2><<<grid, RATE_THREADS, 0, stream>>>(A, vel);
+        else if (k == 3) kRates<T, 0, false, FAM_WENO, true, 3><<<grid, RATE_THREADS, 0, stream>>>(A, vel);
+        else kRates<T, 0, false, FAM_WENO, true, 4><<<grid, RATE_THREADS, 0, stream>>>(A, vel);
+      } else {
+        if (k == 2) kRates<T, 0, false, FAM_ANY, true, 2><<<grid, RATE_THREADS, 0, stream>>>(A, vel);
+        else if (k == 3) kRates<T, 0, false, FAM_ANY, true, 3><<<grid, RATE_THREADS, 0, stream>>>(A, vel);
+        else kRates<T, 0, false, FAM_ANY, true, 4><<<grid, RATE_THREADS, 0, stream>>>(A, vel);
+      }
+    } else {
+      if (weno) {
+        if (k == 1) kRates<T, 0, false, FAM_WENO, true, 1><<<grid, RATE_THREADS, 0, stream>>>(A, vel);
+        else kRates<T, 0, false, FAM_WENO, true, 2><<<grid, RATE_THREADS, 0, stream>>>(A, vel);
+      } else {
+        if (k == 1) kRates<T, 0, false, FAM_ANY, true, 1><<<grid, RATE_THREADS, 0, stream>>>(A, vel);
+        else kRates<T, 0, false, FAM_ANY, true, 2><<<grid, RATE_THREADS, 0, stream>>>(A, vel);
+      }
+    }
+  }
+  void tuneRates(const RateArgs<T> &A, bool weno) {
+    const std::vector<int> shapes = sizeof(T) == 4 ? std::vector<int>{2, 3, 4} : std::vector<int>{1, 2};
+    cudaEvent_t e0, e1;
+    VLSG_CUDA(cudaEventCreate(&e0));
+    VLSG_CUDA(cudaEventCreate(&e1));
+    float best = 0.f;
+    int pick = shapes.back();
+    for (int k : shapes) {
+      VLSG_CUDA(cudaMemsetAsync(rateCounts + 2, 0, sizeof(unsigned long long), stream));
+      VLSG_CUDA(cudaEventRecord(e0, stream));
+      launchBatchRates(A, weno, k);
+      checkLaunch();
+      VLSG_CUDA(cudaEventRecord(e1, stream));
+      VLSG_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      VLSG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if (k == shapes.front() || ms < best) best = ms, pick = k;
+      // the next run (and the real one) starts from fresh reductions
+      VLSG_CUDA(cudaMemcpyAsync(domRed, domRedInit, (size_t)RED_WORDS * nDom * sizeof(unsigned long long),
+                                cudaMemcpyDeviceToDevice, stream));
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    rateShape[weno ? 1 : 0] = pick;
   }
 
   // One forward-Euler stage of every domain: Expand, rates with per-domain
@@ -1595,18 +1713,25 @@ public:
     A.rateV = rateV;
     A.rateStop = rateStop;
     A.rateLen = rateLen;
-    A.poolCells = poolCells;
+    A.rateCap = rateCap;
+    A.rateNext = rateCounts + 2;
+    A.rateBase = rateBase;
+    A.rateOverflowErr = 1024; // capacity is set before the step (applyBatch)
     A.err = errPtr();
     A.slotDom = slotDom;
     A.domDelta = domDelta;
     A.domVel = domVelDev;
     A.domRed = domRed;
+    const bool weno = s == VLSG_WENO_3RD_ORDER || s == VLSG_WENO_5TH_ORDER;
+    const int fi = weno ? 1 : 0;
+    if (!rateShape[fi] && !capturing) tuneRates(A, weno);
+    // untuned (a family first met while capturing): the single-domain shape
+    const int shape = rateShape[fi] ? rateShape[fi]
+                                    : (sizeof(T) == 4 ? (weno ? 4 : 3) : 2);
+    VLSG_CUDA(cudaMemsetAsync(rateCounts + 2, 0, sizeof(unsigned long long), stream));
     {
-      Scope sc(this, "rates");
-      if (s == VLSG_WENO_3RD_ORDER || s == VLSG_WENO_5TH_ORDER)
-        kRates<T, 0, false, FAM_WENO, true><<<blocksRateWeno, RATE_THREADS, 0, stream>>>(A, vel);
-      else
-        kRates<T, 0, false, FAM_ANY, true><<<blocksRate, RATE_THREADS, 0, stream>>>(A, vel);
+      Scope sc(this, rateShapeName(shape));
+      launchBatchRates(A, weno, shape);
       checkLaunch();
     }
     {
@@ -1725,6 +1850,9 @@ public:
     pointUpdates = 0;
     stages = 0;
     const uint64_t l0 = launches;
+    // rate storage for every active point of the step: at most twice the
+    // band the step starts from (sized here, before any capture)
+    ensureRateCap((size_t)(2 * defined(L - 1) + 65536));
     double *dA = domDt, *dB = domDt + nDom, *dC = domDt + 2 * nDom, *tm = domDt + 3 * nDom;
     const double *last = P.temporal_scheme == VLSG_RUNGE_KUTTA_2ND_ORDER   ? dB
                          : P.temporal_scheme == VLSG_RUNGE_KUTTA_3RD_ORDER ? dC
@@ -1747,14 +1875,17 @@ public:
       sg.pre = pre;
       sg.P = P;
       VLSG_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed));
+      capturing = true;
       try {
         batchStepDevice(P);
       } catch (...) {
+        capturing = false;
         cudaGraph_t gr = nullptr;
         cudaStreamEndCapture(stream, &gr);
         if (gr) cudaGraphDestroy(gr);
         throw;
       }
+      capturing = false;
       cudaGraph_t gr = nullptr;
       VLSG_CUDA(cudaStreamEndCapture(stream, &gr));
       const cudaError_t e = cudaGraphInstantiate(&sg.exec, gr, 0);

@@ -16,8 +16,9 @@
 // mask and taken 32 at a time, one thread per active point.  Stencil values
 // come through the slot's 27-neighbour table, or through the brick map and
 // the boundary mapping for bricks within 8 cells of a boundary that remaps
-// cells.  Outputs are pool shaped (cell q of chain entry j at
-// j * poolCells + q).
+// cells.  Outputs are compact over the active points: each brick reserves
+// one entry per active cell, in the order of its cell list, and the value
+// update walks the same list (entry r of chain entry j at j * rateCap + r).
 #pragma once
 
 #include <type_traits>
@@ -131,12 +132,18 @@ template <class T> struct RateArgs {
   double adaptiveFactor;
   int checkDiss;
   T globalAlpha[3];
-  // outputs: chain entry j of cell q at j * poolCells + q
+  // outputs, compact over the active points: a brick reserves one entry per
+  // active cell (rateNext) and records where they start (rateBase[slot]);
+  // chain entry j of entry r is at j * rateCap + r, in the order of the
+  // brick's active cells
   T *rateV;
   T *rateStop;
   T *rateD; // the dissipation per chain entry (setSaveAdvectionVelocities), or null
   uint8_t *rateLen;
-  size_t poolCells;
+  size_t rateCap;
+  unsigned long long *rateNext;
+  unsigned long long *rateBase;
+  int rateOverflowErr; // err bit for a brick left out (0: the host checks rateNext)
   unsigned long long *minStep;  // bits of the smallest non-negative step
   unsigned long long *alphaMax; // bits of the LLF/LLLF alphas
   unsigned long long *counts;   // out: active cells, band cells
@@ -698,9 +705,8 @@ __device__ inline unsigned long long warpMaxU64(unsigned long long b) {
 template <class T, class St, class Vel, int FAM = FAM_ANY>
 __device__ inline double ratePoint(const RateArgs<T> &A, const Vel &vel,
                                    const St &S, int slot, int c, T C, T *alphas,
-                                   double delta) {
+                                   double delta, size_t q) {
   const int L = A.L;
-  const size_t q = (size_t)slot * BV + c;
   T value = C;
   double maxStepTime = 0;
   double cfl = A.cfl;
@@ -743,9 +749,9 @@ __device__ inline double ratePoint(const RateArgs<T> &A, const Vel &vel,
         done = false;
       }
     }
-    A.rateV[(size_t)len * A.poolCells + q] = veff;
-    A.rateStop[(size_t)len * A.poolCells + q] = stop;
-    if (A.rateD) A.rateD[(size_t)len * A.poolCells + q] = d;
+    A.rateV[(size_t)len * A.rateCap + q] = veff;
+    A.rateStop[(size_t)len * A.rateCap + q] = stop;
+    if (A.rateD) A.rateD[(size_t)len * A.rateCap + q] = d;
     ++len;
     if (done) break;
   }
@@ -804,8 +810,10 @@ template <class T, int FAM = FAM_ANY> constexpr int rateMinBlocks() {
 // host callback's table instead of the device functor.
 // BATCH: the batching form (per-domain spacing, velocity and reductions,
 // A.slotDom set).
-template <class T, int MODE, bool TABLE = false, int FAM = FAM_ANY, bool BATCH = false>
-__global__ void __launch_bounds__(RATE_THREADS, rateMinBlocks<T, FAM>())
+// MINB: resident blocks per SM to compile for (0: rateMinBlocks), the launch
+// shapes the batching form's autotuner chooses from.
+template <class T, int MODE, bool TABLE = false, int FAM = FAM_ANY, bool BATCH = false, int MINB = 0>
+__global__ void __launch_bounds__(RATE_THREADS, MINB ? MINB : rateMinBlocks<T, FAM>())
     kRates(RateArgs<T> A, const vlsg_velocity_desc desc) {
   __shared__ uint16_t sList[RATE_THREADS / 32][BV];
   uint16_t *list = sList[threadIdx.x >> 5];
@@ -864,6 +872,19 @@ __global__ void __launch_bounds__(RATE_THREADS, rateMinBlocks<T, FAM>())
       }
     }
     const int total = listCells(a, list);
+    // MODE 0: the brick's entries in the compact rate arrays; a pool that is
+    // too small leaves the brick out (the host sees rateNext > rateCap, grows
+    // the arrays and runs the pass again)
+    unsigned long long rbase = 0;
+    if (MODE == 0 && total) {
+      if (lane == 0) rbase = atomicAdd(A.rateNext, (unsigned long long)total);
+      rbase = __shfl_sync(0xffffffffu, rbase, 0);
+      if (rbase + (unsigned long long)total > A.rateCap) {
+        if (lane == 0 && A.rateOverflowErr) atomicOr(A.err, A.rateOverflowErr);
+        continue;
+      }
+      if (lane == 0) A.rateBase[slot] = rbase;
+    }
     for (int base = 0; base < total; base += 32) {
       const int k = base + lane;
       if (k >= total) continue;
@@ -885,7 +906,7 @@ __global__ void __launch_bounds__(RATE_THREADS, rateMinBlocks<T, FAM>())
           T alphas[STENCIL ? 4 : 3] = {};
           const double step =
               ratePoint<T, std::decay_t<decltype(S)>, std::decay_t<decltype(vel)>, FAM>(
-                  A, vel, S, slot, c, value, alphas, delta);
+                  A, vel, S, slot, c, value, alphas, delta, (size_t)(rbase + k));
           if (!owned) return; // a ghost point: advanced, not counted
           const unsigned long long sb = stepBits(step);
           minBits = sb < minBits ? sb : minBits;
@@ -1007,7 +1028,8 @@ __global__ void __launch_bounds__(1024)
 template <class T>
 __global__ void __launch_bounds__(RATE_THREADS)
     kUpdate(const int *slotList, const int *nSlots, const uint64_t *act, T *vals,
-            const T *rateV, const T *rateStop, const uint8_t *rateLen, size_t poolCells, int L,
+            const T *rateV, const T *rateStop, const uint8_t *rateLen,
+            const unsigned long long *rateBase, size_t rateCap, int L,
             double dt, int *err, float *lo, T *pvel, T *pdiss, const T *rateD,
             const int *slotDom = nullptr, const double *domDt = nullptr) {
   __shared__ uint16_t sList[RATE_THREADS / 32][BV];
@@ -1023,12 +1045,18 @@ __global__ void __launch_bounds__(RATE_THREADS)
     // batching form: the time step of the slot's domain
     const double dtS = domDt ? domDt[slotDom[slot]] : dt;
     const int total = listCells(a, list);
+    const unsigned long long rbase = rateBase[slot];
     for (int base = 0; base < total; base += 32) {
       const int k = base + lane;
       if (k >= total) continue;
       const int c = list[k];
       const size_t q = (size_t)slot * BV + c;
-      int len = rateLen[q];
+      const size_t r = (size_t)(rbase + k); // this point's rate entries
+      if (r >= rateCap) { // the rate pass left this brick out (storage too small)
+        atomicOr(err, 1024);
+        continue;
+      }
+      int len = rateLen[r];
       if (len < 1 || len > L) {
         atomicOr(err, 2);
         len = 1;
@@ -1038,10 +1066,10 @@ __global__ void __launch_bounds__(RATE_THREADS)
           double value = withLo((double)vals[q], lo[q]);
           double time = dtS;
           int j = 0;
-          double velocity = rateV[q];
+          double velocity = rateV[r];
           double rate = time * velocity;
-          while (fabs((double)rateStop[(size_t)j * poolCells + q] - value) < fabs(rate)) {
-            const double stop = rateStop[(size_t)j * poolCells + q];
+          while (fabs((double)rateStop[(size_t)j * rateCap + r] - value) < fabs(rate)) {
+            const double stop = rateStop[(size_t)j * rateCap + r];
             time -= fabs((stop - value) / velocity);
             value = stop;
             ++j;
@@ -1049,7 +1077,7 @@ __global__ void __launch_bounds__(RATE_THREADS)
               atomicOr(err, 2);
               break;
             }
-            velocity = rateV[(size_t)j * poolCells + q];
+            velocity = rateV[(size_t)j * rateCap + r];
             rate = time * velocity;
           }
           value -= rate;
@@ -1058,7 +1086,7 @@ __global__ void __launch_bounds__(RATE_THREADS)
           lo[q] = (float)(value - (double)hi);
           if (pvel) {
             const int jj = j < len ? j : len - 1; // j == len only after a chain overrun
-            pvel[q] = T(rate), pdiss[q] = rateD[(size_t)jj * poolCells + q];
+            pvel[q] = T(rate), pdiss[q] = rateD[(size_t)jj * rateCap + r];
           }
           continue;
         }
@@ -1066,10 +1094,10 @@ __global__ void __launch_bounds__(RATE_THREADS)
       T value = vals[q];
       double time = dtS;
       int j = 0;
-      T velocity = rateV[q];
+      T velocity = rateV[r];
       T rate = T(time * velocity);
-      while (fabs(rateStop[(size_t)j * poolCells + q] - value) < fabs(rate)) {
-        const T stop = rateStop[(size_t)j * poolCells + q];
+      while (fabs(rateStop[(size_t)j * rateCap + r] - value) < fabs(rate)) {
+        const T stop = rateStop[(size_t)j * rateCap + r];
         time -= fabs((stop - value) / velocity);
         value = stop;
         ++j;
@@ -1077,14 +1105,14 @@ __global__ void __launch_bounds__(RATE_THREADS)
           atomicOr(err, 2);
           break;
         }
-        velocity = rateV[(size_t)j * poolCells + q];
+        velocity = rateV[(size_t)j * rateCap + r];
         rate = T(time * velocity);
       }
       value -= rate;
       vals[q] = value;
       if (pvel) {
         const int jj = j < len ? j : len - 1; // j == len only after a chain overrun
-        pvel[q] = rate, pdiss[q] = rateD[(size_t)jj * poolCells + q];
+        pvel[q] = rate, pdiss[q] = rateD[(size_t)jj * rateCap + r];
       }
     }
   }

@@ -12,7 +12,7 @@ import math
 import numpy as np
 
 from ._abi import BoundaryConditionEnum as BC
-from .domain import Domain, Grid, make_runs
+from .domain import Domain, Grid, lex_order, make_runs
 
 
 def sh_coefficients(lmax, sigma, seed):
@@ -355,3 +355,53 @@ def hole_stack(lateral_cells=4096, grid_delta=0.02, pitch=1.28, radius=0.5, dept
         vel.set_rate(m, rate)
         vel.set_abs(m, 2, 0.2)
     return grid, doms, vel
+
+
+def tiled_hole_stack(tiles, base_cells=1024, device="cuda", precision=1):
+    """hole_stack at (tiles * base_cells)^2 lateral cells, built by tiling
+    the base_cells^2 workload tiles x tiles times (the hole period divides
+    base_cells): the points are shifted into every tile and the undefined
+    runs rebuilt from the base level sets' signs (point queries on a context
+    holding them).  Returns (grid, [three Domains], velocity, base grid,
+    [three base Domains])."""
+    from .advect import Context
+
+    grid_s, doms_s, vel = hole_stack(lateral_cells=base_cells, device=device)
+    n, half = base_cells, base_cells // 2
+    big = tiles * n
+    grid = Grid(None, grid_s.bc, grid_s.delta, index_min=[-big // 2, -big // 2, grid_s.min[2]],
+                index_max=[big // 2, big // 2, grid_s.max[2]])
+    q = Context(0, precision)
+    q.set_grid(grid_s)
+    q.set_level_set_count(len(doms_s))
+    for i, d in enumerate(doms_s):
+        q.upload(i, d)
+    doms = []
+    for i, d in enumerate(doms_s):
+        parts = []
+        for a in range(tiles):
+            for b in range(tiles):
+                t = d.idx.astype(np.int64)
+                t = t + np.array([n * a - big // 2 + half, n * b - big // 2 + half, 0], np.int64)
+                parts.append(t)
+        idx = np.concatenate(parts)
+        val = np.tile(d.values, tiles * tiles)
+        o = lex_order(idx)
+        idx, val = idx[o], val[o]
+        del parts, o
+
+        def sign_fn(x, y, z, i=i):
+            out = np.empty(len(x), np.int64)
+            step = 1 << 24
+            for s0 in range(0, len(x), step):
+                # big-grid x = -big/2 + n a + (x_base + half) in tile a
+                w = np.stack([(np.asarray(x[s0:s0 + step]) + big // 2) % n - half,
+                              (np.asarray(y[s0:s0 + step]) + big // 2) % n - half,
+                              np.asarray(z[s0:s0 + step])], 1).astype(np.int32)
+                out[s0:s0 + step] = np.where(q.values_at(i, w) < 0, -1, 1)
+            return out
+
+        rs, sg = make_runs(idx, sign_fn, idx.min(0) - 1, idx.max(0) + 1)
+        doms.append(Domain(grid, idx.astype(np.int32), val, rs, sg, width=d.width))
+    q.close()
+    return grid, doms, vel, grid_s, doms_s
