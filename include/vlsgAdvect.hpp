@@ -14,6 +14,7 @@
 #include <atomic>
 #include <cstdint>
 #include <cstdio>
+#include <cstring>
 #include <functional>
 #include <map>
 #include <memory>
@@ -74,6 +75,12 @@ struct LevelSet {
   std::map<std::string, std::vector<double>> pointData;
   int64_t numberOfPoints() const { return (int64_t)values.size(); }
 };
+
+// Stamps for LevelSet::version (one counter for every front).
+inline uint64_t freshLevelSetStamp() {
+  static std::atomic<uint64_t> next{1};
+  return next.fetch_add(1);
+}
 
 // Device velocity field: per-material polynomial in the normal (vlsg.h).
 struct VelocityFunctor {
@@ -307,10 +314,7 @@ private:
     size_t points, runs;
   };
   std::vector<Resident> resident;
-  static uint64_t freshStamp() {
-    static std::atomic<uint64_t> next{1};
-    return next.fetch_add(1);
-  }
+  static uint64_t freshStamp() { return freshLevelSetStamp(); }
   bool residentUnchanged() const {
     if (!ctx || resident.size() != levelSets.size()) return false;
     for (size_t i = 0; i < levelSets.size(); ++i) {
@@ -404,6 +408,130 @@ private:
     ls.runSign.resize(m);
     return check(vlsg_download_runs(ctx, (int32_t)i, m, ls.runStart.data(), ls.runSign.data(), &m));
   }
+};
+
+// The batching form for C++ callers: many independent domains, one level set
+// and one device velocity functor each, advanced together in one context
+// (vlsg_batch_*: every pass of a time step one kernel launch over all of
+// them).  It replaces a loop over one Advect per domain (the style of
+// examples/SquareEtch/SquareEtch.cpp:189-229); each apply() is one time step
+// of every domain and writes the results back into the same LevelSet
+// objects, with the getters per domain.  The domains stay on the device
+// between applies while the objects are unchanged (version stamps, as
+// Advect; a changed velocity functor sets the domains up again).  Limits as
+// vlsg_batch_set_domains: periodic in x and y with
+// extents in whole bricks of 8 points, infinite in z.
+template <class T> class AdvectBatch {
+  std::vector<std::shared_ptr<LevelSet>> domains;
+  std::vector<std::shared_ptr<VelocityFunctor>> velocities;
+  vlsg_advect_params params{};
+  std::vector<vlsg_advect_result> results;
+  vlsg_context *ctx = nullptr;
+  int device = 0;
+  struct Resident {
+    const LevelSet *ls;
+    uint64_t version;
+    vlsg_velocity_desc vel; // the velocity the device copy was set up with
+  };
+  std::vector<Resident> resident;
+  uint64_t skippedUploads = 0;
+
+  static void logError(const std::string &m) { std::fprintf(stderr, "[vlsg] %s\n", m.c_str()); }
+  bool check(int rc) {
+    if (rc == VLSG_OK) return true;
+    logError(vlsg_last_error(ctx));
+    return false;
+  }
+  bool residentUnchanged() const {
+    if (!ctx || resident.size() != domains.size()) return false;
+    for (size_t d = 0; d < domains.size(); ++d)
+      if (resident[d].ls != domains[d].get() || domains[d]->version == 0 ||
+          resident[d].version != domains[d]->version ||
+          std::memcmp(&resident[d].vel, &velocities[d]->desc, sizeof(vlsg_velocity_desc)) != 0)
+        return false;
+    return true;
+  }
+  bool upload() {
+    if (!ctx && !check(vlsg_create(&ctx, device, sizeof(T) == 4 ? VLSG_FP32 : VLSG_FP64)))
+      return false;
+    if (residentUnchanged()) {
+      ++skippedUploads;
+      return true;
+    }
+    std::vector<vlsg_batch_domain> b(domains.size());
+    for (size_t d = 0; d < domains.size(); ++d) {
+      const LevelSet &ls = *domains[d];
+      b[d] = vlsg_batch_domain{ls.grid.min.data(),   ls.grid.max.data(),  ls.grid.boundary.data(),
+                               ls.grid.gridDelta,    ls.numberOfPoints(), ls.indices.data(),
+                               ls.values.data(),     (int64_t)ls.runSign.size(),
+                               ls.runStart.data(),   ls.runSign.data(),   ls.width,
+                               &velocities[d]->desc};
+    }
+    return check(vlsg_batch_set_domains(ctx, (int32_t)b.size(), b.data()));
+  }
+  bool download(size_t d) {
+    LevelSet &ls = *domains[d];
+    int64_t n = 0;
+    if (!check(vlsg_batch_count_points(ctx, (int32_t)d, &n))) return false;
+    ls.indices.resize(3 * n);
+    ls.values.resize(n);
+    int32_t w = 0;
+    if (!check(vlsg_batch_download(ctx, (int32_t)d, n, ls.indices.data(), ls.values.data(), &w)))
+      return false;
+    ls.width = w;
+    int64_t m = 0;
+    const int rc = vlsg_batch_download_runs(ctx, (int32_t)d, 0, nullptr, nullptr, &m);
+    if (rc != VLSG_OK && rc != VLSG_ERR_CAPACITY && !check(rc)) return false;
+    ls.runStart.resize(3 * m);
+    ls.runSign.resize(m);
+    return check(vlsg_batch_download_runs(ctx, (int32_t)d, m, ls.runStart.data(), ls.runSign.data(), &m));
+  }
+
+public:
+  AdvectBatch() { vlsg_default_params(&params); }
+  AdvectBatch(const AdvectBatch &) = delete;
+  AdvectBatch &operator=(const AdvectBatch &) = delete;
+  ~AdvectBatch() {
+    if (ctx) vlsg_destroy(ctx);
+  }
+  void setDevice(int d) { device = d; }
+  void insertNextDomain(std::shared_ptr<LevelSet> ls, std::shared_ptr<VelocityFunctor> v) {
+    domains.push_back(std::move(ls));
+    velocities.push_back(std::move(v));
+  }
+  void clearDomains() { domains.clear(), velocities.clear(), resident.clear(); }
+  void setTimeStepRatio(const double &cfl) { params.time_step_ratio = cfl; }
+  void setCalculateNormalVectors(bool b) { params.calculate_normal_vectors = b; }
+  void setAdaptiveTimeStepping(bool b = true, unsigned subdivisions = 20) {
+    params.adaptive_time_stepping = b;
+    params.adaptive_subdivisions = subdivisions < 1 ? 1 : subdivisions;
+  }
+  void setSpatialScheme(SpatialSchemeEnum s) { params.spatial_scheme = (int32_t)s; }
+  void setTemporalScheme(TemporalSchemeEnum s) { params.temporal_scheme = (int32_t)s; }
+  void setDissipationAlpha(const double &a) { params.dissipation_alpha = a; }
+  void setCheckDissipation(bool b) { params.check_dissipation = b; }
+
+  // one time step of every domain, results written back
+  void apply() {
+    if (domains.empty()) return logError("No domains passed to AdvectBatch.");
+    for (auto &v : velocities)
+      if (!v) return logError("No velocity field passed to AdvectBatch.");
+    if (!upload()) return;
+    results.assign(domains.size(), vlsg_advect_result{});
+    params.advection_time = 0.;
+    if (!check(vlsg_batch_advect(ctx, &params, results.data()))) return;
+    resident.clear();
+    for (size_t d = 0; d < domains.size(); ++d) {
+      if (!download(d)) return;
+      domains[d]->version = freshLevelSetStamp();
+      resident.push_back(Resident{domains[d].get(), domains[d]->version, velocities[d]->desc});
+    }
+  }
+  double getAdvectedTime(size_t d) const { return results.at(d).advected_time; }
+  double getCurrentTimeStep(size_t d) const { return results.at(d).current_time_step; }
+  uint64_t getPointUpdates(size_t d) const { return results.at(d).point_updates; }
+  // applies that found every domain's device copy current
+  uint64_t getSkippedUploads() const { return skippedUploads; }
 };
 
 } // namespace vlsg
