@@ -212,7 +212,15 @@ int vlsg_get_stream(vlsg_context *ctx, void **stream);
 /* Grid: Domain(bounds, boundaryConditions, gridDelta), lsDomain.hpp:68-78.
  * grid_min/grid_max are INDEX bounds (floor(min/dx), ceil(max/dx)); for a
  * periodic direction the points are grid_min..grid_max-1, for a reflective
- * one grid_min..grid_max, an infinite direction is unbounded. */
+ * one grid_min..grid_max, an infinite direction is unbounded.
+ * dim = 2 (Advect<T,2>): grid_min, grid_max and boundary hold 2 entries; the
+ * level set is held as the plane z = 0 of a grid periodic in z with period
+ * 1, so every z neighbour of a point is the point itself and every z
+ * difference is 0.  Every index array of the other entry points keeps 3
+ * int32 per point or run start, the third 0 (downloads return 0 there); the
+ * velocity field sees coordinates and normals with a zero z component.
+ * STENCIL_LOCAL_LAX_FRIEDRICHS and LOCAL_LAX_FRIEDRICHS_ANALYTICAL are
+ * rejected for dim = 2 (VLSG_ERR_ARGUMENT). */
 int vlsg_set_grid(vlsg_context *ctx, int32_t dim, const int64_t *grid_min,
                   const int64_t *grid_max, const int32_t *boundary,
                   double grid_delta);

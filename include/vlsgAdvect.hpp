@@ -51,6 +51,9 @@ struct Grid {
   std::array<int32_t, 3> boundary{VLSG_INFINITE_BOUNDARY, VLSG_INFINITE_BOUNDARY,
                                    VLSG_INFINITE_BOUNDARY};
   double gridDelta = 1.0;
+  // 2 for Advect<T,2>: min, max and boundary use their first two entries, and
+  // the indices of the level sets keep 3 per point with the third 0
+  int dim = 3;
 };
 
 struct LevelSet {
@@ -347,7 +350,7 @@ private:
       if (!check(vlsg_create(&ctx, device, precision))) return false;
     }
     const Grid &g = levelSets.back()->grid;
-    if (!check(vlsg_set_grid(ctx, 3, g.min.data(), g.max.data(), g.boundary.data(), g.gridDelta)))
+    if (!check(vlsg_set_grid(ctx, g.dim, g.min.data(), g.max.data(), g.boundary.data(), g.gridDelta)))
       return false;
     if (!check(vlsg_set_level_set_count(ctx, (int32_t)levelSets.size()))) return false;
     for (size_t i = 0; i < levelSets.size(); ++i) {
@@ -516,6 +519,8 @@ public:
     if (domains.empty()) return logError("No domains passed to AdvectBatch.");
     for (auto &v : velocities)
       if (!v) return logError("No velocity field passed to AdvectBatch.");
+    for (auto &d : domains)
+      if (d->grid.dim != 3) return logError("AdvectBatch: three-dimensional domains only.");
     if (!upload()) return;
     results.assign(domains.size(), vlsg_advect_result{});
     params.advection_time = 0.;

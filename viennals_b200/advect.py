@@ -13,11 +13,20 @@ import numpy as np
 from . import _lib
 from ._abi import (AdvectParams, AdvectResult, KernelStat, Precision,
                    SpatialSchemeEnum, TemporalSchemeEnum)
-from .domain import Domain, make_runs
+from .domain import Domain, make_runs, make_runs_2d
 
 
 def _p(a, t):
     return a.ctypes.data_as(ctypes.POINTER(t))
+
+
+def _as3(a):
+    """Index rows of a D = 2 domain with a zero third component (the library's
+    layout for D = 2); 3-column rows as they are."""
+    a = np.asarray(a)
+    if a.ndim == 2 and a.shape[1] == 2:
+        return np.concatenate([a, np.zeros((len(a), 1), a.dtype)], 1)
+    return a
 
 
 class Context:
@@ -56,7 +65,11 @@ class Context:
         return s.value
 
     def set_grid(self, grid):
+        """vlsg_set_grid; a D = 2 grid (grid.dim 2) takes 2D domains, whose
+        indices go to the library with a zero third component and come back
+        without it."""
         self._grid = grid
+        self._dim = grid.dim
         gmin = np.array(grid.min[:3], np.int64)
         gmax = np.array(grid.max[:3], np.int64)
         bc = np.array(grid.bc[:3], np.int32)
@@ -68,9 +81,9 @@ class Context:
         self._check(self.lib.vlsg_set_level_set_count(self.h, int(n)))
 
     def upload(self, slot, dom):
-        idx = np.ascontiguousarray(dom.idx, np.int32)
+        idx = np.ascontiguousarray(_as3(dom.idx), np.int32)
         val = np.ascontiguousarray(dom.values, np.float64)
-        rs = np.ascontiguousarray(dom.run_start, np.int32)
+        rs = np.ascontiguousarray(_as3(dom.run_start), np.int32)
         sg = np.ascontiguousarray(dom.run_sign, np.int8)
         self._check(self.lib.vlsg_upload_levelset(
             self.h, int(slot), len(val), _p(idx, ctypes.c_int32), _p(val, ctypes.c_double),
@@ -87,7 +100,9 @@ class Context:
         (e.g. pinned host memory), the points land there and views of their
         first n rows are returned."""
         n = self.count(slot)
-        if idx_out is not None and val_out is not None and len(idx_out) >= n and len(val_out) >= n:
+        planar = getattr(self, "_dim", 3) == 2
+        if (not planar and idx_out is not None and val_out is not None and len(idx_out) >= n
+                and len(val_out) >= n):
             idx, val = idx_out[:n], val_out[:n]
         else:
             idx = np.empty((n, 3), np.int32)
@@ -95,6 +110,8 @@ class Context:
         w = ctypes.c_int32()
         self._check(self.lib.vlsg_download_levelset(self.h, int(slot), n, _p(idx, ctypes.c_int32),
                                                     _p(val, ctypes.c_double), ctypes.byref(w)))
+        if planar:
+            idx = np.ascontiguousarray(idx[:, :2])
         return idx, val, w.value
 
     def set_owned_region(self, axis, lo=0, hi=0):
@@ -137,7 +154,7 @@ class Context:
         return (src, vel, diss) if has.value else None
 
     def values_at(self, slot, idx):
-        idx = np.ascontiguousarray(idx, np.int32)
+        idx = np.ascontiguousarray(_as3(idx), np.int32)
         out = np.zeros(len(idx))
         self._check(self.lib.vlsg_get_values(self.h, int(slot), len(idx), _p(idx, ctypes.c_int32),
                                              _p(out, ctypes.c_double)))
@@ -201,7 +218,13 @@ class Context:
     def download_runs(self, slot, start_out=None, sign_out=None):
         """(run_start (K,3) int32, run_sign (K,) int8) of the undefined runs in
         HRLE order, built on the device (vlsg_download_runs); optional output
-        buffers as for download()."""
+        buffers as for download().  A D = 2 context returns (K,2) starts."""
+        if getattr(self, "_dim", 3) == 2:
+            starts, signs = self._runs(slot, None, None)
+            return np.ascontiguousarray(starts[:, :2]), signs
+        return self._runs(slot, start_out, sign_out)
+
+    def _runs(self, slot, start_out, sign_out):
         n = ctypes.c_int64()
         cap = 0
         if start_out is not None and sign_out is not None:
@@ -238,6 +261,16 @@ class Context:
         """Same as download_domain with the runs rebuilt on the host from
         point queries (the reference layout the device builder follows)."""
         idx, val, w = self.download(slot)
+        if getattr(self, "_dim", 3) == 2:
+            lo = idx.min(0) - 1 if len(idx) else np.zeros(2, np.int64)
+            hi = idx.max(0) + 1 if len(idx) else np.zeros(2, np.int64)
+
+            def sign2(x, y):
+                q = np.stack([np.asarray(x), np.asarray(y)], 1).astype(np.int32)
+                return np.where(self.values_at(slot, q) < 0, -1, 1)
+
+            rs, sg = make_runs_2d(idx, sign2, lo, hi)
+            return Domain(grid, idx, val, rs, sg, width=w)
         if len(idx):
             lo = idx.min(0) - 1
             hi = idx.max(0) + 1
@@ -355,7 +388,8 @@ class BatchContext(Context):
 
 
 class Advect:
-    """Mirror of viennals::Advect<T,3> running on the GPU."""
+    """Mirror of viennals::Advect<T,D> running on the GPU (D from the level
+    sets' grid: 3, or 2 held as one plane)."""
 
     velocityLabel = "AdvectionVelocities"
     dissipationLabel = "Dissipation"

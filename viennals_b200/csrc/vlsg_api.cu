@@ -22,6 +22,7 @@ struct vlsg_context {
   cudaStream_t ownStream = nullptr; // stream created with the context
   std::string err;
   bool hasGrid = false;
+  int dim = 3;
   GridDev grid{};
   std::vector<StagedLS> staged;
   bool dirty = true;
@@ -290,12 +291,15 @@ int vlsg_get_stream(vlsg_context *ctx, void **stream) {
 int vlsg_set_grid(vlsg_context *ctx, int32_t dim, const int64_t *gmin, const int64_t *gmax,
                   const int32_t *bc, double delta) {
   if (!ctx) return fail(nullptr, VLSG_ERR_ARGUMENT, "NULL context");
-  if (dim != 3) return fail(ctx, VLSG_ERR_ARGUMENT, "only D = 3 is supported on the GPU");
+  if (dim != 2 && dim != 3) return fail(ctx, VLSG_ERR_ARGUMENT, "D must be 2 or 3");
   if (!gmin || !gmax || !bc || !(delta > 0))
     return fail(ctx, VLSG_ERR_ARGUMENT, "vlsg_set_grid: bad argument");
   ctx->batch.reset(); // back to one domain
   GridDev g{};
-  for (int d = 0; d < 3; ++d) {
+  // D = 2: the plane z = 0 of a grid periodic in z with period 1 (every z
+  // neighbour is the cell itself, every z difference 0)
+  if (dim == 2) g.gmin[2] = 0, g.gmax[2] = 1, g.bc[2] = VLSG_PERIODIC_BOUNDARY, g.planar = 1;
+  for (int d = 0; d < dim; ++d) {
     if (bc[d] < 0 || bc[d] > 4) return fail(ctx, VLSG_ERR_ARGUMENT, "unknown boundary condition");
     if (gmin[d] < -(1 << 19) || gmax[d] > (1 << 19))
       return fail(ctx, VLSG_ERR_ARGUMENT, "grid index bounds exceed +-2^19");
@@ -308,6 +312,7 @@ int vlsg_set_grid(vlsg_context *ctx, int32_t dim, const int64_t *gmin, const int
   }
   g.delta = delta;
   ctx->grid = g;
+  ctx->dim = dim;
   ctx->hasGrid = true;
   ctx->dirty = true;
   return VLSG_OK;
@@ -877,6 +882,15 @@ int vlsg_advect(vlsg_context *ctx, const vlsg_advect_params *p, vlsg_advect_resu
   if (ctx->ownAxis >= 0 && p->spatial_scheme == VLSG_STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER)
     return fail(ctx, VLSG_ERR_ARGUMENT,
                 "an owned region (sharding) is not supported with STENCIL_LOCAL_LAX_FRIEDRICHS");
+  // D = 2 runs as the plane of a z-periodic grid: the schemes whose
+  // dissipation asks the velocity field per direction (the z direction
+  // included) are not held to the 2D reference there
+  if (ctx->hasGrid && ctx->dim == 2 &&
+      (p->spatial_scheme == VLSG_STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER ||
+       p->spatial_scheme == VLSG_LOCAL_LAX_FRIEDRICHS_ANALYTICAL_1ST_ORDER))
+    return fail(ctx, VLSG_ERR_ARGUMENT,
+                "D = 2: STENCIL_LOCAL_LAX_FRIEDRICHS and LOCAL_LAX_FRIEDRICHS_ANALYTICAL are "
+                "not supported on the GPU");
   return guarded(ctx, [&] {
     ensureBuilt(ctx);
     EngineBase &e = *ctx->eng;

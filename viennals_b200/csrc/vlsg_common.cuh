@@ -68,6 +68,9 @@ struct GridDev {
   int nDom;
   const DomainDev *dom;
   const int *domOfBz;
+  // D = 2: the plane z = 0 of a grid periodic in z with period 1, so every
+  // z neighbour of a cell is the cell itself and every z difference is 0
+  int planar;
 };
 
 __host__ __device__ inline int mapCoord(const GridDev &g, int d, int c) {

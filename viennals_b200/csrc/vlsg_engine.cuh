@@ -821,8 +821,14 @@ public:
     const bool onlyUndefined = buf[b].bound <= (double)totalLimit;
     for (int c = 0; c < cycles; ++c) {
       ExpandRule<T> r{totalLimit, T((startWidth + c + 1) * T(0.5))};
-      if (onlyUndefined) frontierPass<FP_EXPAND>(b, r, "expand");
-      else frontierPass<FP_ALL>(b, r, "expand");
+      if (g.planar) {
+        if (onlyUndefined) frontierPass<FP_EXPAND>(b, PlanarExpandRule<T>{r}, "expand");
+        else frontierPass<FP_ALL>(b, PlanarExpandRule<T>{r}, "expand");
+      } else if (onlyUndefined) {
+        frontierPass<FP_EXPAND>(b, r, "expand");
+      } else {
+        frontierPass<FP_ALL>(b, r, "expand");
+      }
       if (b == L - 1 && startWidth + c + 1 == saveTopAt) {
         // the RK copy of the top level set, taken at this width (saveTop)
         saveTopAt = 0;
@@ -2048,6 +2054,9 @@ public:
       rb.lo[d] = nPts ? hbox[d] - 1 : 0;
       rb.hi[d] = nPts ? hbox[3 + d] + 1 : 0;
     }
+    // D = 2: the plane z = 0 alone, without the runs before and after it
+    // (the first and last of the list, left out of the merge below)
+    if (g.planar) rb.lo[2] = rb.hi[2] = 0;
     rb.ny = rb.hi[1] - rb.lo[1] + 1;
     rb.nz = rb.hi[2] - rb.lo[2] + 1;
     const size_t rows = (size_t)rb.ny * rb.nz;
@@ -2081,12 +2090,15 @@ public:
     uint32_t *keep = scratch<uint32_t>(X_KEEP, nRuns);
     uint32_t *kpos = scratch<uint32_t>(X_POS, std::max<size_t>(nRuns, nBricks));
     uint32_t *sums3 = scratch<uint32_t>(X_SUMS, scanScratch(std::max<size_t>(nRuns, std::max(nBricks, nAlloc * 64))) + 64);
-    kRunKeep<<<grid1(nRuns), 256, 0, stream>>>(sink.sign, sink.pb, (uint32_t)nRuns, keep);
-    scanExclusive(keep, kpos, nRuns, sums3);
-    const uint32_t kept = scanTotal(sums3, nRuns);
-    kRunCompact<<<grid1(nRuns), 256, 0, stream>>>(sink.start, sink.sign, keep, kpos,
-                                                  (uint32_t)nRuns, scratch<int32_t>(X_OSTART, 3 * (size_t)kept),
-                                                  scratch<int8_t>(X_OSIGN, kept));
+    const size_t r0 = g.planar ? 1 : 0, nMerge = nRuns - 2 * r0;
+    kRunKeep<<<grid1(nMerge), 256, 0, stream>>>(sink.sign + r0, sink.pb + r0, (uint32_t)nMerge,
+                                                keep);
+    scanExclusive(keep, kpos, nMerge, sums3);
+    const uint32_t kept = scanTotal(sums3, nMerge);
+    kRunCompact<<<grid1(nMerge), 256, 0, stream>>>(sink.start + 3 * r0, sink.sign + r0, keep, kpos,
+                                                   (uint32_t)nMerge,
+                                                   scratch<int32_t>(X_OSTART, 3 * (size_t)kept),
+                                                   scratch<int8_t>(X_OSIGN, kept));
     checkLaunch();
     syncErr("exchange");
     xBuf = b;

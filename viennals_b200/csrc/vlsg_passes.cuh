@@ -44,6 +44,22 @@ template <class T> struct ExpandRule {
   }
 };
 
+// Expand of a D = 2 level set held as the plane of a z-periodic grid of
+// period 1 (GridDev::planar): the z neighbours (2, 5) are the cell itself,
+// which the 2D star does not have; they read as undefined on the side the
+// rule takes for the cell, which never decides the result (a defined cell
+// recomputed from its neighbours would otherwise see its own value +-1).
+// Prune and rebuild need no such rule: a cell's own sign class and value
+// never decide them.
+template <class T> struct PlanarExpandRule {
+  ExpandRule<T> r;
+  __device__ T operator()(T c, const T *nb, int &src) const {
+    const T self = (double)c > -Lim<double>::eps() ? Lim<T>::max() : Lim<T>::lowest();
+    const T nb4[6] = {nb[0], nb[1], self, nb[3], nb[4], self};
+    return r(c, nb4, src);
+  }
+};
+
 template <class T> struct PruneRule {
   bool removeStrayZeros;
   __device__ static bool neg(T a) { return (double)a <= -Lim<double>::eps(); }

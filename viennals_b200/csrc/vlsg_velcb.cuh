@@ -215,6 +215,9 @@ __global__ void __launch_bounds__(RATE_THREADS)
           if (s > 0) {
             const int off[3] = {(s - 1) % 3 - 1, ((s - 1) / 3) % 3 - 1, (s - 1) / 9 - 1};
             for (int d = 0; d < 3; ++d) crd[d] = T(coordinate[d] + off[d] * delta);
+            // D = 2: the sites above and below the plane are the plane's own
+            // (the same normal and, here, the same coordinate)
+            if (A.g.planar) crd[2] = coordinate[2];
           }
           for (int m = 0; m < L; ++m) {
             const size_t q = (p * L + m) * sites + s;

@@ -97,7 +97,22 @@ def lex_order(idx):
     return np.lexsort(tuple(idx[:, d] for d in range(idx.shape[1])))
 
 
-def make_runs(idx, sign_fn, lo, hi):
+def make_runs_2d(idx, sign_fn, lo, hi):
+    """HRLE-style undefined runs of a D = 2 point set (idx (N,2), sign_fn(x,
+    y), lo/hi inclusive (x, y) box holding every defined point): the runs of
+    make_runs for the one plane of the box, as (x, y) starts -- the region
+    before the box, the rows of the box (heads, gaps, tails, empty rows) and
+    the region after it."""
+    idx = np.asarray(idx, np.int64).reshape(-1, 2)
+    idx3 = np.concatenate([idx, np.zeros((len(idx), 1), np.int64)], 1)
+    lo, hi = [int(lo[0]), int(lo[1])], [int(hi[0]), int(hi[1])]
+    # make_runs over the plane z = 0 with no z levels outside it
+    rs, sg = make_runs(idx3, lambda x, y, z: sign_fn(x, y), [lo[0], lo[1], 0], [hi[0], hi[1], 0],
+                       planar=True)
+    return np.ascontiguousarray(rs[:, :2]), sg
+
+
+def make_runs(idx, sign_fn, lo, hi, planar=False):
     """HRLE-style undefined runs for a point set.
 
     idx: (N,3) defined points; sign_fn(x, y, z) -> array of +1/-1 for the
@@ -123,9 +138,11 @@ def make_runs(idx, sign_fn, lo, hi):
     cx = (lo[0] + hi[0]) // 2
     cy = (lo[1] + hi[1]) // 2
     NI = -INF_INDEX
-    # region before the box (z < lo.z) and after it (z > hi.z)
-    add([NI], [NI], [NI], [cx], [cy], [lo[2] - 1])
-    add([NI], [NI], [hi[2] + 1], [cx], [cy], [hi[2] + 1])
+    # region before the box (z < lo.z) and after it (z > hi.z); a planar
+    # (D = 2) box has no z levels outside its plane
+    if not planar:
+        add([NI], [NI], [NI], [cx], [cy], [lo[2] - 1])
+        add([NI], [NI], [hi[2] + 1], [cx], [cy], [hi[2] + 1])
     zs = np.arange(lo[2], hi[2] + 1)
     # rows before / after the box inside each plane
     add(np.full(nz, NI), np.full(nz, NI), zs, np.full(nz, cx), np.full(nz, lo[1] - 1), zs)

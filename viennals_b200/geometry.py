@@ -10,7 +10,7 @@ band.
 """
 import numpy as np
 
-from .domain import Domain, make_runs
+from .domain import Domain, make_runs, make_runs_2d
 
 
 def _box_points(lo, hi):
@@ -36,6 +36,72 @@ def sphere_distance(X, Y, Z, origin, radius, gd):
         upd = ok & (np.abs(dir_radius) < np.abs(distance))
         distance = np.where(upd, dir_radius, distance)
     return distance
+
+
+def make_circle(grid, origin, radius):
+    """makeSphere for D = 2 (lsMakeGeometry.hpp:177-241 with D = 2): the
+    distance along the two grid lines through each index of the box around
+    the circle, kept when |d| <= gridDelta + 1e-5, width 2."""
+    gd = grid.delta
+    ox, oy = float(origin[0]), float(origin[1])
+    lo = [int((ox - radius) / gd - 1), int((oy - radius) / gd - 1)]
+    hi = [int((ox + radius) / gd + 1), int((oy + radius) / gd + 1)]
+    ys, xs = np.meshgrid(np.arange(lo[1], hi[1] + 1), np.arange(lo[0], hi[0] + 1), indexing="ij")
+    X, Y = xs.ravel(), ys.ravel()
+    last = (X == hi[0]) & (Y == hi[1])
+    r2 = radius * radius
+    idx = (X, Y)
+    org = (ox, oy)
+    distance = np.full(X.shape, np.finfo(np.float64).max)
+    for i in range(2):
+        y = idx[(i + 1) % 2] * gd - org[(i + 1) % 2]
+        x = r2 - y * y
+        ok = ~(x < 0.0)
+        with np.errstate(invalid="ignore"):
+            dir_radius = np.abs(idx[i] * gd - org[i]) - np.sqrt(np.where(ok, x, 0.0))
+        upd = ok & (np.abs(dir_radius) < np.abs(distance))
+        distance = np.where(upd, dir_radius, distance)
+    keep = (np.abs(distance) <= 2.0 * 0.5 * gd + 1e-5) & ~last
+    pts = np.stack([X[keep], Y[keep]], axis=1)
+    vals = distance[keep] / gd
+    for d in range(2):
+        if grid.is_periodic(d):
+            pts[:, d] = grid.map_index(d, pts[:, d])
+    o = np.lexsort((pts[:, 0], pts[:, 1]))
+    pts, vals = pts[o], vals[o]
+
+    def sign_fn(x, y):
+        dx = np.asarray(x) * gd - ox
+        dy = np.asarray(y) * gd - oy
+        return np.where(dx * dx + dy * dy < r2, -1, 1)
+
+    rs, sg = make_runs_2d(pts, sign_fn, [lo[0] - 1, lo[1] - 1], [hi[0] + 1, hi[1] + 1])
+    return Domain(grid, pts.astype(np.int32), vals, rs, sg, width=2)
+
+
+def sdf_levelset_2d(grid, sdf, lo, hi, half_width=1.0):
+    """Band of a 2D signed distance function (physical units) over the index
+    box [lo, hi]: every index with |sdf| <= half_width * gridDelta, value
+    sdf / gridDelta, undefined runs with the sign of sdf."""
+    gd = grid.delta
+    ys, xs = np.meshgrid(np.arange(lo[1], hi[1] + 1), np.arange(lo[0], hi[0] + 1), indexing="ij")
+    X, Y = xs.ravel(), ys.ravel()
+    v = sdf(X * gd, Y * gd) / gd
+    keep = np.abs(v) <= half_width
+    pts = np.stack([X[keep], Y[keep]], axis=1)
+    vals = v[keep]
+    for d in range(2):
+        if grid.is_periodic(d):
+            pts[:, d] = grid.map_index(d, pts[:, d])
+    key = pts[:, 1].astype(np.int64) * (1 << 21) + pts[:, 0]
+    _, first = np.unique(key, return_index=True)
+    pts, vals = pts[first], vals[first]
+
+    def sign_fn(x, y):
+        return np.where(sdf(np.asarray(x) * gd, np.asarray(y) * gd) < 0, -1, 1)
+
+    rs, sg = make_runs_2d(pts, sign_fn, [lo[0] - 1, lo[1] - 1], [hi[0] + 1, hi[1] + 1])
+    return Domain(grid, pts.astype(np.int32), vals, rs, sg, width=int(round(2 * half_width)))
 
 
 def make_sphere(grid, origin, radius):
