@@ -134,3 +134,27 @@ def test_mark_void_points_known_answer():
     marks = ls.void_markers()
     assert len(marks) == len(pi) and marks.any() and not marks.all()
     assert np.array_equal(marks, pi[:, 1] < -2)
+
+
+def test_two_dimensional_generators_are_valid_level_sets():
+    # the 2D inputs of tests/test_gpu_2d.py: makeSphere's rule in 2D (the
+    # Advection2D.cpp circle) and a signed-distance band with periodic x; the
+    # oracle's Check accepts both, and the circle grows under the
+    # LAX_FRIEDRICHS_1ST_ORDER advection of Advection2D.cpp
+    from viennals_b200.geometry import make_circle, sdf_levelset_2d
+    from viennals_b200.velocity import constant_scalar
+
+    g = Grid([-20, 20, -20, 20], [BC.REFLECTIVE_BOUNDARY, BC.REFLECTIVE_BOUNDARY], 0.5, dim=2)
+    c = make_circle(g, [5.0, 0.0], 7.3)
+    assert c.idx.shape[1] == 2 and c.run_start.shape[1] == 2
+    ls = O.OracleLS(g, c)
+    assert ls.check() == 0
+    p = AdvectParams.defaults()
+    p.spatial_scheme = 2  # LAX_FRIEDRICHS_1ST_ORDER
+    p.advection_time = 1.0
+    O.advect([ls], p, constant_scalar(1.0))
+    assert ls.check() == 0
+    assert len(ls.points(0)[1]) > len(c.values)
+    g2 = Grid([-20, 20, -20, 20], [BC.PERIODIC_BOUNDARY, BC.INFINITE_BOUNDARY], 1.0, dim=2)
+    band = sdf_levelset_2d(g2, lambda x, y: y - 0.3 * x / 20.0, [g2.min[0], -6], [g2.max[0] - 1, 6])
+    assert O.OracleLS(g2, band).check() == 0
