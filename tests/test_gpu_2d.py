@@ -156,8 +156,39 @@ def test_fp32_matches_fp64_points():
     c32.close()
 
 
-@pytest.mark.parametrize("spatial", [4, 9])  # LLF-analytical, StencilLLF
-def test_per_direction_dissipation_schemes_are_rejected(spatial):
+class _AlphaCallback(FunctorVelocity):
+    """The functor's velocity and alphas through the host callbacks; records
+    the directions the alpha callback is asked for."""
+
+    def __init__(self, n):
+        super().__init__(n)
+        self.directions = set()
+
+    def descriptor(self):
+        return None
+
+    def alpha_batch(self, directions, materials, central_differences, alpha_out):
+        self.directions.update(int(d) for d in np.unique(directions))
+        super().alpha_batch(directions, materials, central_differences, alpha_out)
+
+
+@pytest.mark.parametrize("host", [False, True], ids=["functor", "callback"])
+def test_llf_analytical(host):
+    # LOCAL_LAX_FRIEDRICHS_ANALYTICAL_1ST_ORDER: the user's alphas of the 3x3
+    # box in x and y (the z direction is never asked)
+    g, c = _circle_case()
+    v = _AlphaCallback(1) if host else FunctorVelocity(1)
+    v.set_rate(0, 1.0)
+    v.set_square(0, 0, 1.6, 0.4)
+    v.set_dissipation_alpha(0, 0, 1.6)
+    v.set_dissipation_alpha(0, 1, 1.0)
+    v.set_dissipation_alpha(0, 2, 7.0)  # never asked in 2D: must not bound the step
+    _same(g, [c], v, params(4, 2, 0.8, cfl=0.4))
+    if host:
+        assert v.directions == {0, 1}
+
+
+def test_stencil_llf_is_rejected():
     g, c = _circle_case()
     ctx = Context(0, 0)
     ctx.set_grid(g)
@@ -165,5 +196,5 @@ def test_per_direction_dissipation_schemes_are_rejected(spatial):
     ctx.upload(0, c)
     ctx.set_velocity(constant_scalar(1.0).descriptor())
     with pytest.raises(RuntimeError, match="D = 2"):
-        ctx.advect(params(spatial, 0, 0.5))
+        ctx.advect(params(9, 0, 0.5))
     ctx.close()

@@ -1308,9 +1308,32 @@ public:
     VLSG_CUDA(cudaMemcpyAsync(hm, am, nA * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
     VLSG_CUDA(cudaMemcpyAsync(hc, ac, 3 * nA * sizeof(double), cudaMemcpyDeviceToHost, stream));
     syncErr("alpha queries");
-    hostPool(nA, [&](size_t i, int64_t n) {
-      return alphaCb(alphaUser, n, hd + i, hm + i, hc + 3 * i, hv + i);
-    }, "the dissipation alpha callback returned ");
+    if (g.planar) {
+      // D = 2: only the plane's 9 box neighbours (q 9..17) and the directions
+      // x and y are asked, as the 2D reference asks them; the rate kernel
+      // reads no other entry
+      const size_t nq = nA / 81 * 18;
+      std::vector<size_t> at(nq);
+      std::vector<int32_t> qd(nq), qm(nq);
+      std::vector<double> qc(3 * nq), qv(nq);
+      size_t k = 0;
+      for (size_t e = 0; e < nA; ++e) {
+        const size_t q = (e / 3) % 27;
+        if (q < 9 || q >= 18 || e % 3 == 2) continue;
+        at[k] = e, qd[k] = hd[e], qm[k] = hm[e];
+        for (int c = 0; c < 3; ++c) qc[3 * k + c] = hc[3 * e + c];
+        ++k;
+      }
+      hostPool(nq, [&](size_t i, int64_t n) {
+        return alphaCb(alphaUser, n, qd.data() + i, qm.data() + i, qc.data() + 3 * i, qv.data() + i);
+      }, "the dissipation alpha callback returned ");
+      std::fill(hv, hv + nA, 0.0);
+      for (size_t i = 0; i < nq; ++i) hv[at[i]] = qv[i];
+    } else {
+      hostPool(nA, [&](size_t i, int64_t n) {
+        return alphaCb(alphaUser, n, hd + i, hm + i, hc + 3 * i, hv + i);
+      }, "the dissipation alpha callback returned ");
+    }
     VLSG_CUDA(cudaMemcpyAsync(av, hv, nA * sizeof(double), cudaMemcpyHostToDevice, stream));
     A.alphaTab = av;
   }

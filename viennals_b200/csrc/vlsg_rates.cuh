@@ -613,11 +613,14 @@ __device__ void evalScheme(const RateArgs<T> &A, const Vel &vel,
   if (sch == VLSG_LOCAL_LAX_FRIEDRICHS_ANALYTICAL_1ST_ORDER) {
     // the user's alphas over the 3x3x3 box at the central differences
     // (calculateNormalComponent, not normalised), no alphaFactor
+    // (D = 2, the plane of a z-periodic grid: the plane's 3x3 box and the
+    // directions x and y, as the 2D reference asks them)
     T alpha[3] = {0, 0, 0};
-    for (int q = 0; q < 27; ++q) {
+    const int q0 = A.g.planar ? 9 : 0, q1 = A.g.planar ? 18 : 27, nDir = A.g.planar ? 2 : 3;
+    for (int q = q0; q < q1; ++q) {
       T cd[3];
       boxDifferences<T>(S, gridDelta, q, cd);
-      for (int dir = 0; dir < 3; ++dir) {
+      for (int dir = 0; dir < nDir; ++dir) {
         const T tempAlpha = vel.alpha(dir, material, cd, q);
         alpha[dir] = stdMax(alpha[dir], tempAlpha);
         alphas[dir] = stdMax(alphas[dir], tempAlpha);
