@@ -219,9 +219,9 @@ int vlsg_get_stream(vlsg_context *ctx, void **stream);
  * difference is 0.  Every index array of the other entry points keeps 3
  * int32 per point or run start, the third 0 (downloads return 0 there); the
  * velocity field sees coordinates and normals with a zero z component.
- * LOCAL_LAX_FRIEDRICHS_ANALYTICAL asks the alphas of the plane's 3x3 box in
- * the directions x and y; STENCIL_LOCAL_LAX_FRIEDRICHS is rejected for
- * dim = 2 (VLSG_ERR_ARGUMENT). */
+ * The schemes that ask the velocity field around a point (LocalLaxFriedrichs,
+ * LLF-analytical, Stencil-LLF) ask it at the plane's 3x3 box only, in the
+ * directions x and y, as the 2D reference does. */
 int vlsg_set_grid(vlsg_context *ctx, int32_t dim, const int64_t *grid_min,
                   const int64_t *grid_max, const int32_t *boundary,
                   double grid_delta);

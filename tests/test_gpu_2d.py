@@ -6,8 +6,8 @@ follow the reference's 2D tests: a circle grown with reflective boundaries
 (tests/Advection2D/Advection2D.cpp: LAX_FRIEDRICHS_1ST_ORDER, v = 1) and a
 plane with a pillar moved by a vector velocity across a periodic boundary
 (tests/PeriodicBoundary2D/PeriodicBoundary2D.cpp: v = (1, 0), single steps);
-every scheme the 2D path supports, the integration schemes, a host velocity
-field, two materials and the FP32 form."""
+every scheme, the integration schemes, host velocity and alpha fields (asked
+at the plane only), two materials and the FP32 form."""
 import numpy as np
 import pytest
 
@@ -188,13 +188,40 @@ def test_llf_analytical(host):
         assert v.directions == {0, 1}
 
 
-def test_stencil_llf_is_rejected():
+class _CountingField(VelocityField):
+    """A host velocity field of the normal; records the largest |z| of the
+    coordinates and normals it is asked at."""
+
+    def __init__(self):
+        self.max_abs_z = 0.0
+
+    def batch(self, coords, materials, normals, point_ids, scalar_out, vector_out):
+        self.max_abs_z = max(self.max_abs_z, float(np.max(np.abs(coords[:, 2]), initial=0.0)),
+                             float(np.max(np.abs(normals[:, 2]), initial=0.0)))
+        scalar_out[:] = 1.0 + 0.4 * normals[:, 0] * normals[:, 0]
+        vector_out[:] = 0.0
+
+
+@pytest.mark.parametrize("host", [False, True], ids=["functor", "callback"])
+def test_stencil_llf(host):
+    # StencilLocalLaxFriedrichsScalar in 2D: the plane's 3x3 stencil and the
+    # normal nudged in x and y; a host field is asked at the plane only
     g, c = _circle_case()
-    ctx = Context(0, 0)
-    ctx.set_grid(g)
-    ctx.set_level_set_count(1)
-    ctx.upload(0, c)
-    ctx.set_velocity(constant_scalar(1.0).descriptor())
-    with pytest.raises(RuntimeError, match="D = 2"):
-        ctx.advect(params(9, 0, 0.5))
-    ctx.close()
+    if host:
+        v = _CountingField()
+    else:
+        v = FunctorVelocity(1)
+        v.set_rate(0, 1.0)
+        v.set_square(0, 0, 0.4, 0.4)
+    _same(g, [c], v, params(9, 0, 0.6, cfl=0.4))
+    if host:
+        assert v.max_abs_z == 0.0
+
+
+@pytest.mark.parametrize("spatial", [7, 8])
+def test_llf_box_sites_on_the_plane(spatial):
+    # LocalLaxFriedrichs asks its box sites: in 2D the plane's 9, at z = 0
+    g, c = _circle_case()
+    f = _CountingField()
+    _same(g, [c], f, params(spatial, 1, 0.5, cfl=0.4))
+    assert f.max_abs_z == 0.0

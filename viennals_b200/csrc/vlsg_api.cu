@@ -882,13 +882,6 @@ int vlsg_advect(vlsg_context *ctx, const vlsg_advect_params *p, vlsg_advect_resu
   if (ctx->ownAxis >= 0 && p->spatial_scheme == VLSG_STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER)
     return fail(ctx, VLSG_ERR_ARGUMENT,
                 "an owned region (sharding) is not supported with STENCIL_LOCAL_LAX_FRIEDRICHS");
-  // D = 2 runs as the plane of a z-periodic grid: Stencil-LLF's
-  // finite differences of the velocity in normal space would perturb the
-  // normal in z too, which the 2D reference never does
-  if (ctx->hasGrid && ctx->dim == 2 &&
-      p->spatial_scheme == VLSG_STENCIL_LOCAL_LAX_FRIEDRICHS_1ST_ORDER)
-    return fail(ctx, VLSG_ERR_ARGUMENT,
-                "D = 2: STENCIL_LOCAL_LAX_FRIEDRICHS is not supported on the GPU");
   return guarded(ctx, [&] {
     ensureBuilt(ctx);
     EngineBase &e = *ctx->eng;

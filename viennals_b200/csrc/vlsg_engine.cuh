@@ -1279,9 +1279,37 @@ public:
     VLSG_CUDA(cudaMemcpyAsync(hn, qn, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, stream));
     VLSG_CUDA(cudaMemcpyAsync(hp, qp, n * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream));
     syncErr("velocity queries");
-    hostPool(n, [&](size_t i, int64_t m) {
-      return velCb(velUser, m, hc + 3 * i, hm + i, hn + 3 * i, hp + i, hsv + i, hvv + 3 * i);
-    }, "the velocity callback returned ");
+    if (g.planar) {
+      // D = 2: the queries the gathers marked with material -1 (sites off
+      // the plane) are not asked; their answers are 0 and nothing reads them
+      std::vector<size_t> at;
+      at.reserve(n);
+      for (size_t i = 0; i < n; ++i)
+        if (hm[i] >= 0) at.push_back(i);
+      const size_t k = at.size();
+      std::vector<double> qc(3 * k), qn(3 * k), qs(k), qv(3 * k);
+      std::vector<int32_t> qm(k);
+      std::vector<uint64_t> qp(k);
+      for (size_t j = 0; j < k; ++j) {
+        const size_t i = at[j];
+        for (int d = 0; d < 3; ++d) qc[3 * j + d] = hc[3 * i + d], qn[3 * j + d] = hn[3 * i + d];
+        qm[j] = hm[i], qp[j] = hp[i];
+      }
+      hostPool(k, [&](size_t i, int64_t m) {
+        return velCb(velUser, m, qc.data() + 3 * i, qm.data() + i, qn.data() + 3 * i,
+                     qp.data() + i, qs.data() + i, qv.data() + 3 * i);
+      }, "the velocity callback returned ");
+      std::fill(hsv, hsv + n, 0.0);
+      std::fill(hvv, hvv + 3 * n, 0.0);
+      for (size_t j = 0; j < k; ++j) {
+        hsv[at[j]] = qs[j];
+        for (int d = 0; d < 3; ++d) hvv[3 * at[j] + d] = qv[3 * j + d];
+      }
+    } else {
+      hostPool(n, [&](size_t i, int64_t m) {
+        return velCb(velUser, m, hc + 3 * i, hm + i, hn + 3 * i, hp + i, hsv + i, hvv + 3 * i);
+      }, "the velocity callback returned ");
+    }
     VLSG_CUDA(cudaMemcpyAsync(sOut, hsv, n * sizeof(double), cudaMemcpyHostToDevice, stream));
     if (vOut)
       VLSG_CUDA(cudaMemcpyAsync(vOut, hvv, 3 * n * sizeof(double), cudaMemcpyHostToDevice, stream));

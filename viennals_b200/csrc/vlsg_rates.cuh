@@ -382,8 +382,13 @@ __device__ void evalStencilLLF(const RateArgs<T> &A, const Vel &vel, const St &S
   }
   const T hamiltonian = T((double)sqrt(gradSq) * scalarVelocity);
   T maxAlpha[3] = {0, 0, 0};
-  int cx = -1, cy = -1, cz = -1;
-  for (int st = 0; st < 27; ++st) {
+  // D = 2 (the plane of a z-periodic grid): the 3x3 stencil of the plane and
+  // the normal nudged in x and y only, as the 2D reference does; the z terms
+  // below then add exact zeros
+  const bool planar = A.g.planar != 0;
+  const int nSt = planar ? 9 : 27, nDir = planar ? 2 : 3;
+  int cx = -1, cy = -1, cz = planar ? 0 : -1;
+  for (int st = 0; st < nSt; ++st) {
     T ln[3];
     sllfNormal<T>(S, delta, cx, cy, cz, ln);
     // a corrupted normal leaves the stencil index where it is (:288-293)
@@ -393,8 +398,8 @@ __device__ void evalStencilLLF(const RateArgs<T> &A, const Vel &vel, const St &S
     vel.get(material, ln, 1 + q, lsv, lvv);
     for (int dir = 0; dir < 3; ++dir) lsv += lvv[dir] * ln[dir];
     const T DN = sllfEpsilon<T>(lsv, A.sllfEps, delta);
-    T np[3] = {ln[0], ln[1], ln[2]}, nn[3] = {ln[0], ln[1], ln[2]}, vd[3];
-    for (int k = 0; k < 3; ++k) {
+    T np[3] = {ln[0], ln[1], ln[2]}, nn[3] = {ln[0], ln[1], ln[2]}, vd[3] = {0, 0, 0};
+    for (int k = 0; k < nDir; ++k) {
       np[k] -= DN;
       nn[k] += DN;
       T vp, vn, unused[3];
@@ -642,9 +647,11 @@ __device__ void evalScheme(const RateArgs<T> &A, const Vel &vel,
     outD = dissipation;
     return;
   }
-  // LocalLaxFriedrichs: alphas over the 3x3x3 box, x fastest
+  // LocalLaxFriedrichs: alphas over the 3x3x3 box, x fastest (D = 2: the
+  // plane's 3x3 box, q 9..17)
   T alpha[3] = {0, 0, 0};
-  for (int q = 0; q < 27; ++q) {
+  const int q1 = A.g.planar ? 18 : 27;
+  for (int q = A.g.planar ? 9 : 0; q < q1; ++q) {
     const int ox = q % 3 - 1, oy = (q / 3) % 3 - 1, oz = q / 9 - 1;
     T normal[3];
     T nm = 0.;

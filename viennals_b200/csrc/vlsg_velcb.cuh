@@ -215,17 +215,17 @@ __global__ void __launch_bounds__(RATE_THREADS)
           if (s > 0) {
             const int off[3] = {(s - 1) % 3 - 1, ((s - 1) / 3) % 3 - 1, (s - 1) / 9 - 1};
             for (int d = 0; d < 3; ++d) crd[d] = T(coordinate[d] + off[d] * delta);
-            // D = 2: the sites above and below the plane are the plane's own
-            // (the same normal and, here, the same coordinate)
-            if (A.g.planar) crd[2] = coordinate[2];
           }
+          // D = 2: the box sites above and below the plane are not asked
+          // (material -1; the rate kernels read only the plane's)
+          const bool unasked = A.g.planar && s > 0 && (s - 1) / 9 != 1;
           for (int m = 0; m < L; ++m) {
             const size_t q = (p * L + m) * sites + s;
             for (int d = 0; d < 3; ++d) {
               coord[3 * q + d] = (double)crd[d];
               normal[3 * q + d] = (double)nrm[d];
             }
-            material[q] = m;
+            material[q] = unasked ? -1 : m;
             pid[q] = id;
           }
         }
@@ -291,7 +291,8 @@ __global__ void __launch_bounds__(RATE_THREADS)
                   coord[3 * e + d] = (double)crd[d];
                   normal[3 * e + d] = (double)nv[d];
                 }
-                material[e] = m;
+                // D = 2: only the plane's stencil, nudged in x and y, is asked
+                material[e] = (A.g.planar && (q / 9 != 1 || kk == 2)) ? -1 : m;
                 pid[e] = id;
               }
               np[kk] += DN;
