@@ -1,4 +1,4 @@
-"""`Advect` -- the drop-in front of viennals::Advect<T,3> over libvlsgpu.
+"""`Advect` -- the drop-in front of viennals::Advect<T,D> (D = 3, or 2) over libvlsgpu.
 
 Same setters, getters and semantics as the reference (lsAdvect.hpp:836-1043,
 bound to Python at python/pyWrap.hpp:324-401): level sets are inserted bottom
@@ -319,6 +319,8 @@ class BatchContext(Context):
         keep = []
         arr = (BatchDomain * len(items))()
         for k, (grid, dom, vel) in enumerate(items):
+            if grid.dim != 3:
+                raise RuntimeError("batching form: three-dimensional domains only")
             gmin = np.array(grid.min[:3], np.int64)
             gmax = np.array(grid.max[:3], np.int64)
             bc = np.array(grid.bc[:3], np.int32)

@@ -909,6 +909,8 @@ int vlsg_set_owned_region(vlsg_context *ctx, int32_t axis, int64_t lo, int64_t h
   if (axis != -1 && axis != 2)
     return fail(ctx, VLSG_ERR_ARGUMENT, "vlsg_set_owned_region: axis must be 2 (or -1: all)");
   if (axis == 2 && !(lo < hi)) return fail(ctx, VLSG_ERR_ARGUMENT, "vlsg_set_owned_region: empty");
+  if (axis == 2 && ctx->hasGrid && ctx->dim == 2)
+    return fail(ctx, VLSG_ERR_ARGUMENT, "vlsg_set_owned_region: D = 2 has no z slabs to own");
   ctx->ownAxis = axis;
   ctx->ownLo = lo;
   ctx->ownHi = hi;
