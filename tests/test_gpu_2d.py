@@ -225,3 +225,19 @@ def test_llf_box_sites_on_the_plane(spatial):
     f = _CountingField()
     _same(g, [c], f, params(spatial, 1, 0.5, cfl=0.4))
     assert f.max_abs_z == 0.0
+
+
+def test_three_dimensional_only_forms_reject_2d_grids():
+    # the batching form and owned z slabs (sharding) are three-dimensional
+    from viennals_b200.advect import BatchContext
+
+    g, c = _circle_case()
+    b = BatchContext(0, 1)
+    with pytest.raises(RuntimeError, match="three-dimensional"):
+        b.set_domains([(g, c, constant_scalar(1.0))])
+    b.close()
+    ctx = Context(0, 0)
+    ctx.set_grid(g)
+    with pytest.raises(RuntimeError, match="D = 2"):
+        ctx.set_owned_region(2, 0, 4)
+    ctx.close()
