@@ -883,6 +883,12 @@ int vlsg_advect(vlsg_context *ctx, const vlsg_advect_params *p, vlsg_advect_resu
     return fail(ctx, VLSG_ERR_ARGUMENT,
                 "an owned region (sharding) is not supported with STENCIL_LOCAL_LAX_FRIEDRICHS");
   return guarded(ctx, [&] {
+    // profiling: the timers of this call include the build of a fresh upload
+    const bool hadEngine = ctx->eng != nullptr;
+    if (hadEngine) {
+      ctx->eng->profiling = ctx->profiling;
+      if (ctx->profiling) ctx->eng->timers.clear();
+    }
     ensureBuilt(ctx);
     EngineBase &e = *ctx->eng;
     e.vel = ctx->vel;
@@ -898,7 +904,7 @@ int vlsg_advect(vlsg_context *ctx, const vlsg_advect_params *p, vlsg_advect_resu
     e.ownLo = ctx->ownLo;
     e.ownHi = ctx->ownHi;
     e.profiling = ctx->profiling;
-    if (ctx->profiling) e.timers.clear();
+    if (ctx->profiling && !hadEngine) e.timers.clear();
     e.apply(*p, *r);
     return VLSG_OK;
   });
