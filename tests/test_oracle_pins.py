@@ -158,3 +158,39 @@ def test_two_dimensional_generators_are_valid_level_sets():
     g2 = Grid([-20, 20, -20, 20], [BC.PERIODIC_BOUNDARY, BC.INFINITE_BOUNDARY], 1.0, dim=2)
     band = sdf_levelset_2d(g2, lambda x, y: y - 0.3 * x / 20.0, [g2.min[0], -6], [g2.max[0] - 1, 6])
     assert O.OracleLS(g2, band).check() == 0
+
+
+def test_two_dimensional_runs_cover_every_undefined_cell():
+    # make_runs_2d: every undefined cell of the box reads the sign of the last
+    # run start at or before it in HRLE order (y slowest, x fastest), and no
+    # run repeats its predecessor's sign with no defined point between them
+    from viennals_b200.domain import INF_INDEX, make_runs_2d
+
+    # a valid band: two circles' signed distance, defined where |d| <= 1 cell
+    # (every sign change along a grid line then passes a defined point)
+    lo, hi = [-9, -7], [11, 8]
+    cells = [(x, y) for y in range(lo[1], hi[1] + 1) for x in range(lo[0], hi[0] + 1)]
+
+    def sdf(x, y):
+        x, y = np.asarray(x, float), np.asarray(y, float)
+        return np.minimum(np.hypot(x - 3.2, y + 0.4) - 4.6, np.hypot(x + 5.1, y - 3.3) - 2.2)
+
+    pts = np.array([c for c in cells if abs(sdf(*c)) <= 1.0], np.int64)
+
+    def sign_fn(x, y):
+        return np.where(sdf(x, y) < 0, -1, 1)
+
+    rs, sg = make_runs_2d(pts, sign_fn, lo, hi)
+    key = lambda x, y: (int(y) + INF_INDEX) * (1 << 22) + (int(x) + INF_INDEX)
+    rk = [key(x, y) for x, y in rs]
+    assert rk == sorted(rk)
+    defined = {tuple(p) for p in pts.tolist()}
+    for x, y in cells:
+        if (x, y) in defined:
+            continue
+        j = np.searchsorted(rk, key(x, y), side="right") - 1
+        assert j >= 0 and sg[j] == sign_fn(x, y), (x, y)
+    pk = sorted(key(x, y) for x, y in defined)
+    before = np.searchsorted(pk, rk)
+    for i in range(1, len(sg)):
+        assert sg[i] != sg[i - 1] or before[i] != before[i - 1]
