@@ -241,3 +241,49 @@ def test_three_dimensional_only_forms_reject_2d_grids():
     with pytest.raises(RuntimeError, match="D = 2"):
         ctx.set_owned_region(2, 0, 4)
     ctx.close()
+
+
+class _Stateful(VelocityField):
+    """A velocity that depends on what the velocity update callback saw."""
+
+    def __init__(self):
+        self.k = 0
+        self.seen = []
+        self.columns = set()
+
+    def update(self, dom):
+        self.columns.add(dom.idx.shape[1])
+        self.seen.append((len(dom.values), float(np.sum(dom.values))))
+        self.k = len(dom.values)
+        return True
+
+    def batch(self, coords, materials, normals, point_ids, scalar_out, vector_out):
+        scalar_out[:] = 0.6 + 0.2 * normals[:, 1] + 1e-5 * self.k
+        vector_out[:] = 0.0
+
+
+def test_velocity_update_callback():
+    # setVelocityUpdateCallback between the RK3 stages: the callback gets the
+    # 2D top level set (two indices per point) and the result matches the
+    # oracle's 2D path
+    from oracle import oracle as O
+
+    g, c = _circle_case()
+    p = params(7, 2, 0.5, cfl=0.4)
+    vo, vg = _Stateful(), _Stateful()
+    ols = [O.OracleLS(g, c)]
+    O.advect(ols, p, vo, update=vo.update)
+    ctx = Context(0, 0)
+    ctx.set_grid(g)
+    ctx.set_level_set_count(1)
+    ctx.upload(0, c)
+    ctx.set_velocity_callback(vg)
+    ctx.set_velocity_update_callback(vg.update)
+    ctx.advect(p)
+    oi, ov = ols[0].points(0)
+    gi, gv, _ = ctx.download(0)
+    ctx.close()
+    assert np.array_equal(oi, gi)
+    assert np.array_equal(ov.view(np.int64), gv.view(np.int64))
+    assert vo.seen == vg.seen and len(vg.seen) > 0
+    assert vg.columns == {2}

@@ -587,6 +587,9 @@ def update_callback(fn, grid=None):
             d.run_start = a(v.run_start, (m, 3)).copy() if m else np.zeros((0, 3), np.int32)
             d.run_sign = a(v.run_sign, (m,)).copy() if m else np.zeros(0, np.int8)
             d.width = int(v.width)
+            if grid is not None and grid.dim == 2:  # the library's third index is 0
+                d.idx = np.ascontiguousarray(d.idx[:, :2])
+                d.run_start = np.ascontiguousarray(d.run_start[:, :2])
             fn(d)
             return 0
         except Exception:  # reported through the library's status
