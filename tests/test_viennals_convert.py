@@ -117,3 +117,28 @@ def test_advect_through_domain_conversions(tmp_path, case):
     assert np.array_equal(val.view(np.int64), gv.view(np.int64))
     assert w == gw
     assert np.array_equal(ids, np.where(src_ids >= 0, src_ids, 0).astype(np.float64))
+
+
+def test_header_instantiates_for_float_and_both_dimensions(tmp_path):
+    # toVlsg / fromVlsg for Domain<float, 2>, Domain<float, 3> and Domain<double, 2>
+    # (Advect<float, D> callers) compile against the stand-ins too
+    src = tmp_path / "inst.cpp"
+    src.write_text(
+        '#include "vlsgViennaLS.hpp"\n'
+        "template <class T, int D> int roundTrip() {\n"
+        "  viennals::Domain<T, D> a, b;\n"
+        "  typename viennals::Domain<T, D>::DomainType::Entry e;\n"
+        "  for (int k = 0; k < D; ++k) e.start[k] = k;\n"
+        "  e.value = T(0.25);\n"
+        "  e.defined = true;\n"
+        "  a.domain.entries.push_back(e);\n"
+        "  vlsg::LevelSet ls = vlsg::toVlsg(a);\n"
+        "  vlsg::fromVlsg(ls, b);\n"
+        "  return ls.grid.dim == D && b.getDomain().getNumberOfPoints() == 1 ? 0 : 1;\n"
+        "}\n"
+        "int main() { return roundTrip<float, 2>() + roundTrip<float, 3>() + roundTrip<double, 2>(); }\n")
+    exe = str(tmp_path / "inst")
+    subprocess.check_call(["g++", "-std=c++17", "-O1", "-Wall", "-Werror", "-I",
+                           os.path.join(ROOT, "include"), "-I", STUB, str(src), "-L", LIBDIR,
+                           "-lvlsgpu", f"-Wl,-rpath,{LIBDIR}", "-o", exe])
+    assert subprocess.call([exe]) == 0
